@@ -1,0 +1,187 @@
+/*
+ * bmadgpu.h -- C-ABI of the B200 (sm_100a, FP64) multi-particle tracker.
+ *
+ * This is the drop-in boundary for Bmad's multi-particle bmad_standard tracking path
+ * (track_bunch -> track1_bunch -> track1_bunch_hom -> track1 -> track1_bmad -> track_a_*).
+ * Every entry point is plain C: pointers, sizes and status codes, no C++ or torch types.
+ *
+ * Reference interfaces replaced (paths inside bmad-sim/bmad-ecosystem):
+ *   - track1_bunch_hook_ptr / track1_bunch_hook          bmad/custom/track1_bunch_hook.f90:25-43,
+ *                                                         called at bmad/multiparticle/beam_mod.f90:263-266
+ *   - track_bunch (element loop over a branch)           bmad/multiparticle/beam_mod.f90:103-170
+ *   - ltt_run_beam_mode turn loop + ltt_track_bmad_bunch bsim/modules/lt_tracking_mod.f90:1631-1713, 3189-3224
+ *   - track1_bunch_hom OpenMP particle loop               bmad/multiparticle/beam_utils.f90:81-86
+ *   - coord_struct / bunch_struct marshalling             bmad/modules/bmad_struct.f90:551-579, 1117-1135
+ *     (component-wise, as cpp_bmad_interface/code/bmad_cpp_convert_mod.f90:1767-1844 does)
+ *
+ * Units and conventions are Bmad's: vec = (x, px, y, py, z, pz) canonical, px/py normalised by
+ * p0c, pz = (p - p0)/p0, z = -beta*c*(t - t_ref). Integer enums below carry Bmad's own values so a
+ * Fortran caller can pass ele%key, ele%value(fringe_type$), coord%state, ... unchanged.
+ *
+ * Status: every function returns 0 on success or a negative BMADGPU_E* code; the message of the
+ * last failure on the calling host thread is available from bmadgpu_last_error().
+ */
+#ifndef BMADGPU_H
+#define BMADGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BMADGPU_ABI_VERSION 1
+#define BMADGPU_N_POLE 22          /* multipole arrays 0:n_pole_maxx, n_pole_maxx = 21 (bmad_struct.f90:48) */
+#define BMADGPU_N_MOMENTS 28       /* per reported turn: n_live, sum vec_i (6), sum vec_i vec_j i<=j (21) */
+
+/* ---- status codes ------------------------------------------------------------------------ */
+enum {
+  BMADGPU_OK = 0,
+  BMADGPU_EINVAL = -1,        /* bad argument (null pointer, n < 0, inconsistent sizes) */
+  BMADGPU_ENOMEM = -2,        /* device or pinned-host allocation failed, or admission refused */
+  BMADGPU_ECUDA = -3,         /* a CUDA runtime call failed */
+  BMADGPU_ETIMEDOUT = -4,     /* a bounded device/host wait ran out */
+  BMADGPU_EUNSUPPORTED = -5,  /* element type, flag or method outside the bmad_standard hot path */
+  BMADGPU_EBUSY = -6,         /* serving queue full */
+  BMADGPU_ENOTFOUND = -7      /* unknown job id */
+};
+
+/* ---- Bmad enum values (bmad/modules/bmad_struct.f90) ---------------------------------------- */
+/* element keys, bmad_struct.f90:1696-1710 */
+enum {
+  BMADGPU_DRIFT = 1, BMADGPU_SBEND = 2, BMADGPU_QUADRUPOLE = 3, BMADGPU_SEXTUPOLE = 5,
+  BMADGPU_RFCAVITY = 9, BMADGPU_MARKER = 14, BMADGPU_OCTUPOLE = 17, BMADGPU_MULTIPOLE = 19,
+  BMADGPU_AB_MULTIPOLE = 22, BMADGPU_MONITOR = 31, BMADGPU_INSTRUMENT = 32, BMADGPU_PIPE = 44,
+  BMADGPU_THICK_MULTIPOLE = 67
+};
+/* particle states, bmad_struct.f90:525-532 */
+enum {
+  BMADGPU_ALIVE = 1, BMADGPU_LOST = 2, BMADGPU_LOST_NEG_X = 3, BMADGPU_LOST_POS_X = 4,
+  BMADGPU_LOST_NEG_Y = 5, BMADGPU_LOST_POS_Y = 6, BMADGPU_LOST_Z = 7, BMADGPU_LOST_PZ = 8
+};
+/* coord%location, bmad_struct.f90:376-377 */
+enum { BMADGPU_UPSTREAM_END = 1, BMADGPU_DOWNSTREAM_END = 2, BMADGPU_INSIDE = 3 };
+/* fringe_at / aperture_at, bmad_struct.f90:373-374 */
+enum {
+  BMADGPU_ENTRANCE_END = 1, BMADGPU_EXIT_END = 2, BMADGPU_BOTH_ENDS = 3, BMADGPU_NO_END = 4,
+  BMADGPU_CONTINUOUS = 5
+};
+/* fringe_type, bmad_struct.f90:27, 168-169 */
+enum {
+  BMADGPU_FRINGE_NONE = 1, BMADGPU_FRINGE_SOFT_EDGE_ONLY = 2, BMADGPU_FRINGE_HARD_EDGE_ONLY = 3,
+  BMADGPU_FRINGE_FULL = 4, BMADGPU_FRINGE_SAD_FULL = 5, BMADGPU_FRINGE_LINEAR_EDGE = 6,
+  BMADGPU_FRINGE_BASIC_BEND = 7
+};
+/* aperture_type, bmad_struct.f90:158 */
+enum { BMADGPU_APERTURE_AUTO = 1, BMADGPU_APERTURE_RECTANGULAR = 2, BMADGPU_APERTURE_ELLIPTICAL = 3 };
+
+/* ---- lattice element -------------------------------------------------------------------------
+ * One record per tracked element, in tracking order (branch%ele(1:n_ele_track)). Field names are
+ * the ele%value(...) attribute names. Defaults a caller must set explicitly (there is no parser):
+ * sbend fringe_type = basic_bend, every other element none; fringe_at = both_ends;
+ * aperture_at = exit_end; aperture_type = rectangular; scale_multipoles = 1; is_on = 1;
+ * fintx/hgapx = fint/hgap when unset (set_ele_defaults.f90:36-37, 295-300;
+ * bmad_parser_mod.f90:5238-5239).
+ * For key = multipole, a_pole holds knl(0:21) and b_pole holds tn(0:21) as in Bmad.
+ */
+typedef struct bmadgpu_element {
+  int32_t key;
+  int32_t is_on;
+  int32_t fringe_type;
+  int32_t fringe_at;
+  int32_t aperture_at;
+  int32_t aperture_type;
+  int32_t num_steps;          /* 0 => computed as attribute_bookkeeper.f90:292-400 does */
+  int32_t scale_multipoles;
+  int32_t field_master;       /* must be 0 (normalised strengths) */
+  int32_t exact_multipoles;   /* must be off$ (= 1) or 0 */
+  int32_t orientation;        /* must be +1 */
+  int32_t reserved;
+  double l, k1, k2, k3, g, dg, e1, e2, fint, fintx, hgap, hgapx;
+  double tilt, ref_tilt, roll, x_offset, y_offset, z_offset, x_pitch, y_pitch;
+  double hkick, vkick;
+  double x1_limit, x2_limit, y1_limit, y2_limit;
+  double voltage, rf_frequency, phi0, phi0_multipass;
+  double ds_step, r0_mag, r0_elec;
+  double delta_ref_time;      /* ele%value(delta_ref_time$); used only for the time coordinate */
+  double a_pole[BMADGPU_N_POLE], b_pole[BMADGPU_N_POLE];
+  double a_pole_elec[BMADGPU_N_POLE], b_pole_elec[BMADGPU_N_POLE];
+} bmadgpu_element;
+
+/* Branch/global parameters: lat_param_struct + the bmad_common_struct switches on the path. */
+typedef struct bmadgpu_param {
+  double p0c;                 /* reference momentum [eV], ele%value(p0c$) (constant along the ring) */
+  double e_tot;               /* reference total energy [eV], ele%value(e_tot$) */
+  double mass;                /* mass_of(species) [eV] */
+  double charge;              /* charge_of(species) [e] */
+  double max_aperture_limit;  /* bmad_com%max_aperture_limit, default 1e3 */
+  double default_ds_step;     /* bmad_com%default_ds_step, default 0.2 */
+  int32_t aperture_limit_on;  /* bmad_com%aperture_limit_on, default 1 */
+  int32_t absolute_time_tracking; /* must be 0 (relative time, bmad_struct.f90:2350) */
+  int32_t radiation_on;       /* must be 0: radiation, spin, wakes, space charge are off the path */
+  int32_t reserved;
+} bmadgpu_param;
+
+/* Particles in structure-of-arrays form; the Fortran shim gathers coord_struct fields into it. */
+typedef struct bmadgpu_bunch {
+  int64_t n;                  /* number of particles */
+  double* vec;                /* [6*n]: vec[i*n + j] = coordinate i (0..5) of particle j */
+  double* beta;               /* [n]: coord%beta */
+  double* t;                  /* [n] or NULL: coord%t (FP64; the reference keeps it in real(qp)) */
+  int32_t* state;             /* [n]: coord%state */
+  int32_t* ix_ele;            /* [n] or NULL: element index (0-based) of the loss; untouched if alive */
+  int32_t* ix_turn;           /* [n] or NULL: turn index of the loss; untouched if alive */
+  int32_t* location;          /* [n] or NULL: coord%location at the loss */
+} bmadgpu_bunch;
+
+typedef struct bmadgpu_ctx bmadgpu_ctx;
+typedef struct bmadgpu_lattice bmadgpu_lattice;
+
+/* ---- library, context, lattice -------------------------------------------------------------- */
+int bmadgpu_abi_version(void);
+const char* bmadgpu_last_error(void);
+
+/* One context per host thread and device; it owns a CUDA stream and device scratch. */
+int bmadgpu_ctx_create(int32_t device, bmadgpu_ctx** out);
+int bmadgpu_ctx_destroy(bmadgpu_ctx* ctx);
+
+/* Packs the element records into the device element table (per-element invariants hoisted,
+ * n_step bookkeeping as attribute_bookkeeper.f90:292-400, multipoles as
+ * multipole_ele_to_ab.f90:31-678). Replaces what branch%ele(:) provides to track1. */
+int bmadgpu_lattice_create(bmadgpu_ctx* ctx, const bmadgpu_element* eles, int32_t n_ele,
+                           const bmadgpu_param* param, bmadgpu_lattice** out);
+int bmadgpu_lattice_destroy(bmadgpu_lattice* lat);
+/* Resolved integration steps of element i (ds_step/num_steps bookkeeping); -1 on bad index. */
+int32_t bmadgpu_lattice_n_step(const bmadgpu_lattice* lat, int32_t i);
+/* Bytes of the packed element table (what is staged into shared memory). */
+int64_t bmadgpu_lattice_table_bytes(const bmadgpu_lattice* lat);
+
+/* ---- tracking ------------------------------------------------------------------------------- */
+/* Track the bunch through elements [ix_start, ix_end) of the lattice, repeated over n_turns
+ * turns, starting at turn index turn0. With ix_start = 0, ix_end = n_ele this is
+ * n_turns passes of track_bunch(lat, bunch, ele0, ele0) as ltt_run_beam_mode does
+ * (lt_tracking_mod.f90:1631-1713). Lost particles are skipped afterwards, as
+ * track1_bunch_hom does (beam_utils.f90:83). Host buffers; copies in and out on ctx's stream.
+ * moments: NULL, or [n_turns * BMADGPU_N_MOMENTS] sums over live particles after each turn. */
+int bmadgpu_track_bunch(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* bunch,
+                        int32_t ix_start, int32_t ix_end, int32_t turn0, int32_t n_turns,
+                        double* moments);
+
+/* Same, with every pointer in the bunch (and moments) already in device memory; no copies. */
+int bmadgpu_track_bunch_device(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* bunch,
+                               int32_t ix_start, int32_t ix_end, int32_t turn0, int32_t n_turns,
+                               double* moments);
+
+/* The per-element hook: one element for the whole bunch, the work of track1_bunch_hom
+ * (beam_utils.f90:32-172) for bmad_standard elements. ix_ele is 0-based. */
+int bmadgpu_track1_bunch(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* bunch,
+                         int32_t ix_ele, int32_t turn);
+
+/* Waits for all work queued on the context's stream. */
+int bmadgpu_ctx_synchronize(bmadgpu_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BMADGPU_H */

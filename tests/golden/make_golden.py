@@ -1,0 +1,95 @@
+"""Generates the golden-vector fixtures in this folder from the reference's own regression tests.
+
+Run in a checkout that has the reference at REF (default /root/reference); the outputs are small
+JSON files committed next to this script, so nothing at test time reads the reference.
+
+Sources (paths inside bmad-sim/bmad-ecosystem):
+  regression_tests/tracking_method_test/tracking_method_test.bmad   element definitions, start orbit
+  regression_tests/tracking_method_test/output.correct              "NAME: Bmad_Standard" lines
+  regression_tests/fringe_test/fringe_test.bmad, output.correct     hwang_bend_edge_kick goldens
+
+Element attributes are transcribed below from the .bmad lines cited beside each entry; Bmad's
+parser defaults are applied explicitly (tilt flag -> pi/4 quad, pi/6 sextupole, pi/8 octupole,
+parser_set_attribute_mod.f90:1813-1823; multipole tN flag -> pi/(2N+2), :1809).
+"""
+import json
+import math
+import os
+import re
+import sys
+
+REF = os.environ.get("BMAD_REFERENCE", "/root/reference")
+HERE = os.path.dirname(os.path.abspath(__file__))
+PI = 3.141592653589793238462643383279
+
+# particle_start, tracking_method_test.bmad:9-14; l1[e_tot] = 1e6, :141. The file sets no
+# parameter[particle], so the species is Bmad's default positron (bmad_parser.f90:966): charge +1.
+TM_START = [0.001, 0.002, 0.003, 0.004, 0.005, 0.006]
+TM_E_TOT = 1e6
+TM_CHARGE = 1.0
+
+_q0 = dict(a_pole={0: 0.01, 1: 0.1}, vkick=-0.0001, b_pole_elec={0: -2e3}, a_pole_elec={1: 2e4})  # :62
+
+TM_ELEMENTS = {
+    # name: (key, attributes, source line in tracking_method_test.bmad)
+    "DRIFT1": ("DRIFT", dict(l=4.5, num_steps=10, x_offset=0.05, y_pitch=0.001, tilt=0.1), 27),
+    "INSTRUMENT1": ("INSTRUMENT", dict(l=4.5, num_steps=10), 41),
+    "MONITOR1": ("MONITOR", dict(l=4.5, num_steps=10), 55),
+    "MULTIPOLE1": ("MULTIPOLE", dict(a_pole={1: 1.0, 3: 4.5}, b_pole={1: PI / (2 * 1 + 2), 3: 0.31 * PI},
+                                     x_offset=0.05), 56),
+    "AB_MULTIPOLE1": ("AB_MULTIPOLE", dict(a_pole={2: 1e2}, b_pole={2: 1e2}, x_offset=0.02, tilt=0.1), 20),
+    "OCTUPOLE1": ("OCTUPOLE", dict(l=4.5, k3=1e3, tilt=PI / 8.0, num_steps=10, x_offset=0.01,
+                                   y_pitch=0.001), 58),
+    "SEXTUPOLE1": ("SEXTUPOLE", dict(l=0.6, k2=1.0, tilt=PI / 6.0, num_steps=10, x_offset=0.05,
+                                     y_pitch=0.001), 93),
+    "RFCAVITY1": ("RFCAVITY", dict(l=4.5, rf_frequency=500e6, voltage=1e5, phi0=0.1, num_steps=10,
+                                   x_offset=0.05, y_pitch=0.001, tilt=0.1), 69),
+    "RFCAVITY3": ("RFCAVITY", dict(rf_frequency=500e6, voltage=1e5, phi0=0.1, num_steps=10, x_offset=0.05,
+                                   y_pitch=0.001, tilt=0.1, a_pole={2: 0.02}), 73),
+    "QUADRUPOLE1": ("QUADRUPOLE", dict(_q0, l=0.6, k1=1.0, tilt=PI / 4.0, num_steps=10, x_offset=0.05,
+                                       y_pitch=0.001), 63),
+    "QUADRUPOLE2": ("QUADRUPOLE", dict(_q0, l=0.6, k1=-1.0, tilt=PI / 4.0, num_steps=10, x_offset=0.05,
+                                       y_pitch=0.001), 64),
+    "QUADRUPOLE3": ("QUADRUPOLE", dict(_q0, l=0.6, k1=1e-20, tilt=PI / 4.0, num_steps=10, x_offset=0.05,
+                                       y_pitch=0.001), 65),
+}
+
+# fringe_test.bmad: e_tot 1e6 electrons, particle_start, b: sbend ...
+FR_START = [0.01, 0.02, 0.03, 0.04, 0.00, 0.5]
+FR_ELEMENT = dict(e1=0.1, e2=-0.2, k1=0.1, g=0.1, fint=0.5, hgap=0.4)
+
+
+def parse_output_correct(path):
+    out = {}
+    for ln, line in enumerate(open(path), start=1):
+        m = re.match(r'\s*"([^"]+)"\s+(ABS|REL|VEC_REL)\s+(\S+)\s+(.*)$', line)
+        if not m:
+            continue
+        vals = [float(v) for v in m.group(4).split()]
+        out[m.group(1)] = dict(tol_type=m.group(2), tol=float(m.group(3)), values=vals, line=ln)
+    return out
+
+
+def main():
+    tm = parse_output_correct(os.path.join(REF, "regression_tests/tracking_method_test/output.correct"))
+    cases = []
+    for name, (key, attrs, src_line) in TM_ELEMENTS.items():
+        g = tm[name + ": Bmad_Standard"]
+        cases.append(dict(name=name, key=key, attrs=attrs, bmad_line=src_line, output_line=g["line"],
+                          tol=g["tol"], expected_vec=g["values"][:6]))
+    json.dump(dict(source="regression_tests/tracking_method_test", e_tot=TM_E_TOT, charge=TM_CHARGE, start=TM_START,
+                   cases=cases), open(os.path.join(HERE, "tracking_method_bmad_standard.json"), "w"), indent=1)
+
+    fr = parse_output_correct(os.path.join(REF, "regression_tests/fringe_test/output.correct"))
+    fcases = []
+    for edge, tag in (("first_track_edge", "Up"), ("second_track_edge", "Dn")):
+        rows = [fr["%s-Mat%d" % (tag, i)]["values"] for i in range(1, 7)]
+        fcases.append(dict(edge=edge, tol=fr[tag + "-Orb"]["tol"], expected_dorb=fr[tag + "-Orb"]["values"],
+                           expected_dmat=rows))
+    json.dump(dict(source="regression_tests/fringe_test", e_tot=1e6, charge=-1.0, start=FR_START, element=FR_ELEMENT,
+                   cases=fcases), open(os.path.join(HERE, "fringe_test_hwang.json"), "w"), indent=1)
+    print("wrote", len(cases), "tracking_method cases and", len(fcases), "fringe cases")
+
+
+if __name__ == "__main__":
+    sys.exit(main())
