@@ -1,0 +1,578 @@
+// lattice.cpp -- host-side element-table packer.
+//
+// Turns bmadgpu_element records (Bmad ele%value attributes) into the packed device table of
+// table.h. This is the work Bmad's lattice bookkeeping does before tracking:
+//   - tilt_tot / has_misalign:          bmad/code/attribute_bookkeeper.f90:146-170
+//   - ds_step / num_steps (check_bend):  bmad/code/attribute_bookkeeper.f90:292-400,
+//                                        forest/code/So_fitting.f90:3516-3548
+//   - element a/b multipoles, b1 pull:   bmad/code/multipole_ele_to_ab.f90:31-678
+//   - multipole kt <-> ab:               bmad/low_level/multipole1_{kt_to_ab,ab_to_kt}.f90
+// and the per-element invariants the maps would otherwise recompute for every particle:
+// bend-angle trig (track_a_bend.f90:134-160), Hwang edge coefficients (fringe_mod.f90:275-290),
+// scaled kick coefficients (multipole_mod.f90:336-360), tilt cos/sin (tilt_coords.f90:40-41).
+
+#include "lattice.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace bmadgpu {
+namespace {
+
+const double kPi = 3.141592653589793238462643383279;
+const int kNPole = BMADGPU_N_POLE;
+
+int nint(double x) { return (int)std::lround(x); }
+
+int max_nonzero(const double* a, const double* b, int ub) {
+  for (int i = ub; i >= 0; i--)
+    if (a[i] != 0 || (b && b[i] != 0)) return i;
+  return -1;
+}
+
+bool any_nonzero(const double* a, int n) {
+  for (int i = 0; i < n; i++)
+    if (a[i] != 0) return true;
+  return false;
+}
+
+double factorial(int n) {
+  double f = 1;
+  for (int i = 2; i <= n; i++) f *= i;
+  return f;
+}
+
+double sinc0(double x) { return std::fabs(x) < 1e-8 ? 1.0 : std::sin(x) / x; }
+double cosc0(double x) {
+  if (std::fabs(x) < 1e-8) return 0.5;
+  double s = sinc0(x / 2);
+  return 0.5 * (s * s);
+}
+double sincc0(double x) {
+  double x2 = x * x;
+  if (std::fabs(x) < 0.1)
+    return 1.0 / 6.0 + x2 * (-1.0 / 120.0 + x2 * (1.0 / 5040.0 + x2 * (-1.0 / 362880.0)));
+  return (x - std::sin(x)) / (x * x2);
+}
+
+struct Fail {
+  int code;
+  std::string msg;
+};
+
+bool key_supported(int key) {
+  switch (key) {
+    case BMADGPU_DRIFT: case BMADGPU_SBEND: case BMADGPU_QUADRUPOLE: case BMADGPU_SEXTUPOLE:
+    case BMADGPU_RFCAVITY: case BMADGPU_MARKER: case BMADGPU_OCTUPOLE: case BMADGPU_MULTIPOLE:
+    case BMADGPU_AB_MULTIPOLE: case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE:
+    case BMADGPU_THICK_MULTIPOLE:
+      return true;
+  }
+  return false;
+}
+
+bool key_has_hkick(int key) {
+  switch (key) {
+    case BMADGPU_QUADRUPOLE: case BMADGPU_SBEND: case BMADGPU_SEXTUPOLE: case BMADGPU_OCTUPOLE:
+    case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RFCAVITY:
+      return true;
+  }
+  return false;
+}
+
+// Element magnetic a/b multipoles in the body frame with the non-multipole kick terms included
+// (multipole_ele_to_ab with use_ele_tilt = F, include_kicks = include_kicks$).
+void mag_ab(const bmadgpu_element& e, double tilt_tot, double ref_tilt_tot, double* a, double* b,
+            int* ix_pole_max) {
+  for (int i = 0; i < kNPole; i++) { a[i] = 0; b[i] = 0; }
+  *ix_pole_max = -1;
+  if (!e.is_on || e.key == BMADGPU_PIPE) return;
+  if (e.key == BMADGPU_MULTIPOLE) {
+    for (int n = 0; n < kNPole; n++) {
+      double knl = e.a_pole[n], tn = e.b_pole[n];
+      if (knl == 0) continue;
+      double angle = -tn * (n + 1);
+      b[n] = (knl * std::cos(angle) - 0.0 * std::sin(angle)) / factorial(n);
+      a[n] = (knl * std::sin(angle) + 0.0 * std::cos(angle)) / factorial(n);
+    }
+    *ix_pole_max = max_nonzero(a, b, kNPole - 1);
+    return;
+  }
+  // convert_this_ab (multipole_ele_to_ab.f90:472-600), scale_multipoles with r0_mag
+  if (any_nonzero(e.a_pole, kNPole) || any_nonzero(e.b_pole, kNPole)) {
+    for (int i = 0; i < kNPole; i++) { a[i] = e.a_pole[i]; b[i] = e.b_pole[i]; }
+    if (e.scale_multipoles) {
+      double cnst = 1;
+      int ref_exp = 0;
+      bool scale = true;
+      switch (e.key) {
+        case BMADGPU_SBEND: cnst = e.l * (e.g + e.dg); ref_exp = 0; break;
+        case BMADGPU_QUADRUPOLE: cnst = e.k1 * e.l; ref_exp = 1; break;
+        case BMADGPU_SEXTUPOLE: cnst = e.k2 * e.l; ref_exp = 2; break;
+        case BMADGPU_OCTUPOLE: cnst = e.k3 * e.l; ref_exp = 3; break;
+        default: scale = false;
+      }
+      if (scale) {
+        if (e.r0_mag == 0) {
+          for (int i = 0; i < kNPole; i++) { a[i] = cnst * a[i]; b[i] = cnst * b[i]; }
+        } else {
+          double factor = cnst * std::pow(e.r0_mag, ref_exp + 1);
+          for (int i = 0; i < kNPole; i++) {
+            factor = factor / e.r0_mag;
+            a[i] = factor * a[i];
+            b[i] = factor * b[i];
+          }
+        }
+      }
+    }
+  }
+  // this_ele_non_multipoles (multipole_ele_to_ab.f90:326-405)
+  double ak[4] = {0, 0, 0, 0}, bk[4] = {0, 0, 0, 0};
+  if (key_has_hkick(e.key) && (e.hkick != 0 || e.vkick != 0)) {
+    double tilt = (e.key == BMADGPU_SBEND) ? ref_tilt_tot : tilt_tot;
+    if (tilt != 0) {
+      double c = std::cos(tilt), s = std::sin(tilt);
+      bk[0] = -e.hkick * c - e.vkick * s;
+      ak[0] = -e.hkick * s + e.vkick * c;
+    } else {
+      bk[0] = -e.hkick;
+      ak[0] = e.vkick;
+    }
+  }
+  switch (e.key) {
+    case BMADGPU_QUADRUPOLE: bk[1] = e.k1 * e.l; break;
+    case BMADGPU_SBEND:
+      bk[0] = bk[0] + e.dg * e.l;
+      bk[1] = e.k1 * e.l;
+      bk[2] = e.k2 * e.l / 2.0;
+      break;
+    case BMADGPU_SEXTUPOLE: bk[2] = e.k2 * e.l / 2.0; break;
+    case BMADGPU_OCTUPOLE: bk[3] = e.k3 * e.l / 6.0; break;
+  }
+  for (int i = 0; i < 4; i++) { a[i] = a[i] + ak[i]; b[i] = b[i] + bk[i]; }
+  *ix_pole_max = max_nonzero(a, b, kNPole - 1);
+}
+
+// tilt_this_multipole(+1) for ab_multipole elements (use_ele_tilt = T)
+void tilt_ab(double tilt, double* a, double* b, int ix_pole_max) {
+  if (tilt == 0) return;
+  for (int n = 0; n <= ix_pole_max; n++) {
+    if (a[n] == 0 && b[n] == 0) continue;
+    double an = a[n], bn = b[n];
+    double c = std::cos((n + 1) * tilt), s = std::sin((n + 1) * tilt);
+    b[n] = bn * c + an * s;
+    a[n] = -bn * s + an * c;
+  }
+}
+
+// pull_this_b1 (multipole_ele_to_ab.f90:664-676)
+double pull_b1(double* a, double* b, int* ix_pole_max) {
+  double b1 = b[1];
+  b[1] = 0;
+  if (*ix_pole_max > 1) return b1;
+  *ix_pole_max = max_nonzero(a, b, 1);
+  return b1;
+}
+
+// check_bend (forest/code/So_fitting.f90:3516-3548): integration steps for a given error budget.
+void check_bend(double xl, double ggi, double rhoi, double xbend1, double gf[8], int* met) {
+  double gg = (double)(long long)ggi;
+  if (gg == 0.0) gg = 1.0;
+  const double co[8] = {0, 0, 1.0 / 12.0, 0, 0.17, 0, 0.17e-1, 0};
+  for (int i = 0; i < 8; i++) gf[i] = 0;
+  for (int i = 3; i <= 7; i += 2) {
+    double ar = i - 1;
+    gf[i] = std::pow(co[i - 1] / xbend1, 1.0 / ar) * std::fabs(rhoi) * xl;
+    if (gf[i] < gg) gf[i] = gg;
+  }
+  gf[2] = gf[3];
+  gf[4] = gf[5] * 3;
+  gf[6] = gf[7] * 7;
+  *met = 2;
+  if (gf[4] < gf[2]) *met = 4;
+  if (gf[6] < gf[4] && gf[6] < gf[2]) *met = 6;
+}
+
+// ds_step and num_steps as attribute_bookkeeper.f90:292-400 resolves them.
+void resolve_steps(const bmadgpu_element& e, const bmadgpu_param& p, double tilt_tot, double* ds_out,
+                   int* n_out) {
+  double ds_step = e.ds_step;
+  double num_steps = e.num_steps;
+  if (num_steps == 0 && e.key == BMADGPU_RFCAVITY) num_steps = 10;  // set_ele_defaults.f90:319
+  double L = e.l;
+  if (ds_step == 0 && num_steps == 0) {
+    switch (e.key) {
+      case BMADGPU_DRIFT: case BMADGPU_PIPE: case BMADGPU_INSTRUMENT: case BMADGPU_MONITOR:
+        num_steps = 1;
+        ds_step = L;
+        break;
+      case BMADGPU_SBEND: case BMADGPU_QUADRUPOLE: case BMADGPU_SEXTUPOLE:
+        if (L != 0) {
+          double a[kNPole], b[kNPole], knl[kNPole];
+          int ix;
+          mag_ab(e, tilt_tot, e.ref_tilt, a, b, &ix);
+          for (int n = 0; n < kNPole; n++)
+            knl[n] = (a[n] == 0 && b[n] == 0) ? 0.0 : factorial(n) * std::sqrt(a[n] * a[n] + b[n] * b[n]);
+          double bend_factor = knl[0] / L;
+          double radius0 = e.r0_mag == 0 ? 0.01 : e.r0_mag;
+          double quad_factor;
+          if (e.key == BMADGPU_SBEND) {
+            bend_factor = bend_factor + std::max(std::fabs(e.g), std::fabs(e.g + e.dg));
+            quad_factor = knl[1] + knl[2] * radius0 + L * (bend_factor * bend_factor);
+          } else if (e.key == BMADGPU_QUADRUPOLE) {
+            quad_factor = 50 * (knl[1] + L * (bend_factor * bend_factor));
+          } else {
+            quad_factor = knl[2] * radius0 + L * (bend_factor * bend_factor);
+          }
+          double gf[8];
+          int met;
+          check_bend(L, quad_factor, bend_factor, 1e-8, gf, &met);
+          int ixm = std::min(met, 4);
+          num_steps = std::max(nint(gf[ixm + 1]), 1);
+          ds_step = std::fabs(L) / num_steps;
+        }
+        break;
+      default:
+        break;
+    }
+  }
+  if (ds_step <= 0) {
+    if (num_steps <= 0 || std::fabs(L) == 0) ds_step = p.default_ds_step;
+    else ds_step = std::fabs(L) / num_steps;
+  }
+  *ds_out = ds_step;
+  *n_out = std::max(1, nint(std::fabs(L / ds_step)));
+}
+
+struct Packer {
+  std::vector<EleHdr> hdr;
+  std::vector<ApRec> ap;
+  std::vector<double> pool;
+  std::map<std::vector<double>, uint32_t> dedupe;
+  std::map<std::vector<double>, uint16_t> ap_dedupe;
+
+  uint32_t add_block(const std::vector<double>& blk) {
+    if (blk.empty()) return 0;
+    auto it = dedupe.find(blk);
+    if (it != dedupe.end()) return it->second;
+    // keep blocks 16-byte aligned so a block can be fetched with 16-byte loads
+    if (pool.size() % 2) pool.push_back(0.0);
+    uint32_t off = (uint32_t)pool.size();
+    pool.insert(pool.end(), blk.begin(), blk.end());
+    dedupe[blk] = off;
+    return off;
+  }
+  uint16_t add_ap(const ApRec& r) {
+    std::vector<double> k = {r.x1_lim, r.x2_lim, r.y1_lim, r.y2_lim};
+    auto it = ap_dedupe.find(k);
+    if (it != ap_dedupe.end()) return it->second;
+    uint16_t ix = (uint16_t)ap.size();
+    ap.push_back(r);
+    ap_dedupe[k] = ix;
+    return ix;
+  }
+};
+
+void push_kicks(std::vector<double>& blk, const double* a, const double* b, int n_pole, double scale) {
+  for (int n = 0; n < n_pole; n++) {
+    blk.push_back(scale * b[n]);
+    blk.push_back(scale * a[n]);
+  }
+}
+
+}  // namespace
+
+int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p, PackedLattice& out,
+                 std::string& err) {
+  try {
+    if (n_ele <= 0 || n_ele > 0xFFFFFF) throw Fail{BMADGPU_EINVAL, "n_ele out of range"};
+    if (p.absolute_time_tracking) throw Fail{BMADGPU_EUNSUPPORTED, "absolute_time_tracking is not on the path"};
+    if (p.radiation_on) throw Fail{BMADGPU_EUNSUPPORTED, "radiation/spin/wakes are not on the path"};
+    if (!(p.p0c > 0) || !(p.e_tot > p.mass) || !(p.mass > 0))
+      throw Fail{BMADGPU_EINVAL, "param: need p0c > 0, e_tot > mass > 0"};
+    Packer pk;
+    out.n_step.assign(n_ele, 1);
+    out.ds_step.assign(n_ele, 0.0);
+    double turn_ref = 0;
+    for (int i = 0; i < n_ele; i++) {
+      const bmadgpu_element& e = eles[i];
+      auto fail = [&](int code, const std::string& m) {
+        throw Fail{code, "element " + std::to_string(i) + " (key " + std::to_string(e.key) + "): " + m};
+      };
+      if (!key_supported(e.key)) fail(BMADGPU_EUNSUPPORTED, "element type not on the bmad_standard path");
+      if (e.orientation != 1 && e.orientation != 0) fail(BMADGPU_EUNSUPPORTED, "orientation -1");
+      if (e.field_master) fail(BMADGPU_EUNSUPPORTED, "field_master = T");
+      if (e.exact_multipoles != 0 && e.exact_multipoles != 1) fail(BMADGPU_EUNSUPPORTED, "exact_multipoles");
+      if (e.key != BMADGPU_MULTIPOLE &&
+          (any_nonzero(e.a_pole_elec, kNPole) || any_nonzero(e.b_pole_elec, kNPole)))
+        fail(BMADGPU_EUNSUPPORTED, "electric multipoles");
+      if (e.key == BMADGPU_MULTIPOLE && any_nonzero(e.a_pole_elec, kNPole))
+        fail(BMADGPU_EUNSUPPORTED, "multipole ksl");
+      if (e.x_pitch != 0 || e.y_pitch != 0 || e.z_offset != 0)
+        if (e.key != BMADGPU_DRIFT && e.key != BMADGPU_MARKER)
+          fail(BMADGPU_EUNSUPPORTED, "pitch / z_offset misalignment");
+      if (e.key == BMADGPU_SBEND && (e.tilt != 0 || e.roll != 0 || e.x_offset != 0 || e.y_offset != 0))
+        fail(BMADGPU_EUNSUPPORTED, "misaligned sbend (bend_shift geometry)");
+      if (e.key != BMADGPU_SBEND && e.ref_tilt != 0) fail(BMADGPU_EUNSUPPORTED, "ref_tilt on a non-bend");
+      if (e.key == BMADGPU_RFCAVITY && (e.hkick != 0 || e.vkick != 0))
+        fail(BMADGPU_EUNSUPPORTED, "rfcavity hkick/vkick");
+      if (!key_has_hkick(e.key) && (e.hkick != 0 || e.vkick != 0) && e.key != BMADGPU_DRIFT)
+        fail(BMADGPU_EUNSUPPORTED, "hkick/vkick on this element type");
+      if (e.aperture_type != BMADGPU_APERTURE_RECTANGULAR && e.aperture_type != BMADGPU_APERTURE_AUTO &&
+          e.aperture_type != BMADGPU_APERTURE_ELLIPTICAL)
+        fail(BMADGPU_EUNSUPPORTED, "aperture_type");
+      if (e.aperture_at < 1 || e.aperture_at > 4) fail(BMADGPU_EUNSUPPORTED, "aperture_at");
+
+      double tilt_tot = (e.key == BMADGPU_SBEND) ? 0.0 : e.tilt;
+      bool has_misalign = (e.key == BMADGPU_SBEND)
+                              ? (e.ref_tilt != 0 || e.roll != 0)
+                              : (e.tilt != 0 || e.x_offset != 0 || e.y_offset != 0);
+      double ds_step;
+      int num_steps;
+      resolve_steps(e, p, tilt_tot, &ds_step, &num_steps);
+      out.ds_step[i] = ds_step;
+      turn_ref += e.delta_ref_time;
+
+      EleHdr h;
+      std::memset(&h, 0, sizeof(h));
+      h.n_step = 1;
+      uint16_t flags = 0;
+      std::vector<double> blk;
+      int key = e.key;
+      if (!e.is_on && key != BMADGPU_SBEND && key != BMADGPU_MULTIPOLE && key != BMADGPU_AB_MULTIPOLE)
+        key = BMADGPU_DRIFT;  // track1_bmad.f90:51-60
+      if (e.l == 0) flags |= F_ZERO_LEN;
+
+      // aperture (check_aperture_limit.f90), offset_moves_aperture = F
+      if (p.aperture_limit_on && e.aperture_at != BMADGPU_NO_END) {
+        ApRec r{-e.x1_limit, e.x2_limit, -e.y1_limit, e.y2_limit};
+        bool any = (r.x1_lim != 0 || r.x2_lim != 0 || r.y1_lim != 0 || r.y2_lim != 0);
+        if (e.aperture_type == BMADGPU_APERTURE_ELLIPTICAL) {
+          if (e.x1_limit != e.x2_limit || e.y1_limit != e.y2_limit || e.x1_limit == 0 || e.y1_limit == 0)
+            fail(BMADGPU_EUNSUPPORTED, "elliptical aperture with asymmetric or zero limits");
+          flags |= F_AP_ELLIPTICAL;
+        }
+        if (any) {
+          h.ap_index = pk.add_ap(r);
+          if (e.aperture_at == BMADGPU_ENTRANCE_END || e.aperture_at == BMADGPU_BOTH_ENDS) flags |= F_AP_ENTRANCE;
+          if (e.aperture_at == BMADGPU_EXIT_END || e.aperture_at == BMADGPU_BOTH_ENDS) flags |= F_AP_EXIT;
+        }
+      }
+
+      double a[kNPole], b[kNPole];
+      int ix_mag_max;
+      std::vector<double> mis;
+      auto misalign_block = [&](double tilt) {
+        mis = {e.x_offset, e.y_offset, std::cos(tilt), std::sin(tilt)};
+        flags |= F_MISALIGN;
+      };
+
+      switch (key) {
+        case BMADGPU_MARKER:
+          h.kind = K_MARKER;
+          break;
+        case BMADGPU_DRIFT:
+          h.kind = K_DRIFT;
+          blk = {e.l};
+          break;
+        case BMADGPU_QUADRUPOLE: {  // track_a_quadrupole.f90
+          h.kind = K_QUAD;
+          mag_ab(e, tilt_tot, 0, a, b, &ix_mag_max);
+          double b1 = pull_b1(a, b, &ix_mag_max);
+          int n_step = 1;
+          if (ix_mag_max > -1) n_step = std::max(nint(std::fabs(e.l) / ds_step), 1);
+          double r_step = 1.0 / n_step;
+          double step_len = e.l * r_step;
+          double b1_l = (e.l != 0) ? b1 / e.l : 0.0;
+          blk = {b1_l, std::sqrt(std::fabs(b1_l)), step_len};
+          if (ix_mag_max > -1) {
+            flags |= F_KICKS;
+            h.n_pole = (uint8_t)(ix_mag_max + 1);
+            push_kicks(blk, a, b, ix_mag_max + 1, r_step / 2);
+            push_kicks(blk, a, b, ix_mag_max + 1, r_step);
+          }
+          h.n_step = (uint16_t)(e.l == 0 ? 0 : n_step);
+          if (has_misalign) misalign_block(tilt_tot);
+          break;
+        }
+        case BMADGPU_SEXTUPOLE: case BMADGPU_OCTUPOLE: case BMADGPU_THICK_MULTIPOLE:
+        case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE: {  // track_a_thick_multipole.f90
+          h.kind = K_THICK;
+          mag_ab(e, tilt_tot, 0, a, b, &ix_mag_max);
+          int n_step = (ix_mag_max == -1) ? 1 : std::max(nint(std::fabs(e.l / ds_step)), 1);
+          double r_step = 1.0 / n_step;
+          double step_len = e.l / n_step;
+          blk = {step_len};
+          if (ix_mag_max > -1) {
+            flags |= F_KICKS;
+            h.n_pole = (uint8_t)(ix_mag_max + 1);
+            push_kicks(blk, a, b, ix_mag_max + 1, r_step / 2);
+            push_kicks(blk, a, b, ix_mag_max + 1, r_step);
+          }
+          h.n_step = (uint16_t)n_step;
+          if (has_misalign) misalign_block(tilt_tot);
+          break;
+        }
+        case BMADGPU_SBEND: {  // track_a_bend.f90
+          h.kind = K_SBEND;
+          mag_ab(e, 0, e.ref_tilt, a, b, &ix_mag_max);
+          double b1 = pull_b1(a, b, &ix_mag_max);
+          if (std::fabs(b1) < 1e-10) {
+            b[1] = b1;
+            b1 = 0;
+          }
+          double g = e.g, dg;
+          if (e.l == 0) {
+            dg = 0;
+          } else {
+            dg = b[0] / e.l;
+            b[0] = 0;
+          }
+          double g_tot = g + dg;
+          if (!e.is_on) {
+            dg = -g;
+            g_tot = 0;
+            b1 = 0;
+          }
+          int n_step = 1;
+          if (ix_mag_max > -1) n_step = std::max(nint(std::fabs(e.l) / ds_step), 1);
+          double r_step = 1.0 / n_step;
+          double step_len = e.l / n_step;
+          double angle = g * step_len;
+          double gl = g * step_len;
+          blk = {step_len, g, g_tot, dg, angle, std::cos(angle), std::sin(angle), sinc0(angle), cosc0(angle),
+                 (gl * gl) * sincc0(angle), (b1 != 0 && e.l != 0) ? b1 / e.l : 0.0, r_step};
+          if (b1 != 0) flags |= F_BEND_K1;
+          else if ((g == 0 && dg == 0) || step_len == 0) flags |= F_BEND_DRIFT;
+          // Hwang edge coefficients (fringe_mod.f90:262-290); bend_edge_kick acts for
+          // fringe_type basic_bend / hard_edge_only when at_this_ele_end(fringe_at).
+          double ge = e.is_on ? (e.g + e.dg) : 0.0;
+          double k1e = e.is_on ? e.k1 : 0.0;
+          for (int end = 0; end < 2; end++) {
+            double ee = end == 0 ? e.e1 : e.e2;
+            double fint_gap = end == 0 ? e.fint * e.hgap : e.fintx * e.hgapx;
+            if (e.fringe_type == BMADGPU_FRINGE_HARD_EDGE_ONLY || e.fringe_type == BMADGPU_FRINGE_SAD_FULL) fint_gap = 0;
+            double cos_e = std::cos(ee), sin_e = std::sin(ee);
+            double tan_e = sin_e / cos_e, sec_e = 1 / cos_e;
+            double gt = ge * tan_e;
+            double gt2 = ge * (tan_e * tan_e);
+            double gs2 = ge * (sec_e * sec_e);
+            double k1_tane = k1e * tan_e * 1.0;
+            double fg_factor = 2 * fint_gap * gs2 * ge * sec_e * (1 + sin_e * sin_e);
+            double cdpx = gt * ge * (1 + 2 * (tan_e * tan_e));
+            blk.insert(blk.end(), {gt, gt2, gs2, k1_tane, fg_factor, ge, cdpx});
+          }
+          if (e.fringe_type == BMADGPU_FRINGE_BASIC_BEND || e.fringe_type == BMADGPU_FRINGE_HARD_EDGE_ONLY) {
+            if (e.fringe_at == BMADGPU_ENTRANCE_END || e.fringe_at == BMADGPU_BOTH_ENDS) flags |= F_EDGE_IN;
+            if (e.fringe_at == BMADGPU_EXIT_END || e.fringe_at == BMADGPU_BOTH_ENDS) flags |= F_EDGE_OUT;
+          } else if (e.fringe_type != BMADGPU_FRINGE_NONE) {
+            fail(BMADGPU_EUNSUPPORTED, "sbend fringe_type other than none/basic_bend/hard_edge_only");
+          }
+          if (ix_mag_max > -1) {
+            flags |= F_KICKS;
+            h.n_pole = (uint8_t)(ix_mag_max + 1);
+            push_kicks(blk, a, b, ix_mag_max + 1, 1.0);
+          }
+          h.n_step = (uint16_t)n_step;
+          if (has_misalign) {  // ref_tilt only (offsets/roll rejected above)
+            mis = {0.0, 0.0, std::cos(e.ref_tilt), std::sin(e.ref_tilt)};
+            flags |= F_MISALIGN;
+          }
+          break;
+        }
+        case BMADGPU_MULTIPOLE: case BMADGPU_AB_MULTIPOLE: {  // track1_bmad.f90:142-166
+          h.kind = K_THIN;
+          double knl0 = 0, c0 = 1, s0 = 0;
+          mag_ab(e, tilt_tot, 0, a, b, &ix_mag_max);
+          if (key == BMADGPU_AB_MULTIPOLE) {
+            tilt_ab(tilt_tot, a, b, ix_mag_max);
+          } else {
+            // multipole_ele_to_kt: tilt(n) = tn + tilt_tot; redo the kt -> ab conversion with it
+            for (int n = 0; n < kNPole; n++) {
+              a[n] = 0;
+              b[n] = 0;
+              double knl = e.a_pole[n], tn = e.b_pole[n] + tilt_tot;
+              if (knl == 0) continue;
+              if (n == 0) {
+                knl0 = knl;
+                if (tn != 0) { c0 = std::cos(tn); s0 = std::sin(tn); }
+                flags |= F_REF_ORB_N0;
+                continue;
+              }
+              double angle = -tn * (n + 1);
+              b[n] = knl * std::cos(angle) / factorial(n);
+              a[n] = knl * std::sin(angle) / factorial(n);
+            }
+            ix_mag_max = max_nonzero(a, b, kNPole - 1);
+          }
+          blk = {knl0, c0, s0};
+          if (ix_mag_max > -1) {
+            flags |= F_KICKS;
+            h.n_pole = (uint8_t)(ix_mag_max + 1);
+            push_kicks(blk, a, b, ix_mag_max + 1, 1.0);
+          }
+          if (e.tilt != 0 || e.x_offset != 0 || e.y_offset != 0) {
+            if (e.x_offset != 0 || e.y_offset != 0) {
+              mis = {e.x_offset, e.y_offset, 1.0, 0.0};  // set_tilt = .false.
+              flags |= F_MISALIGN;
+            }
+          }
+          break;
+        }
+        case BMADGPU_RFCAVITY: {  // track_a_rfcavity.f90
+          h.kind = K_RFCAV;
+          if (e.rf_frequency == 0 && e.voltage != 0) fail(BMADGPU_EINVAL, "rfcavity with zero rf_frequency");
+          mag_ab(e, tilt_tot, 0, a, b, &ix_mag_max);
+          int n_slice = std::max(1, nint(std::fabs(e.l) / ds_step));
+          double voltage = (e.is_on ? e.voltage : 0.0) * 1.0;
+          blk = {voltage, e.rf_frequency, e.phi0, 2 * kPi * e.phi0_multipass, e.l / n_slice, (double)n_slice};
+          if (ix_mag_max > -1) {
+            flags |= F_KICKS;
+            h.n_pole = (uint8_t)(ix_mag_max + 1);
+            push_kicks(blk, a, b, ix_mag_max + 1, 0.5 * 1.0);
+          }
+          h.n_step = (uint16_t)std::min(n_slice, 65535);
+          if (n_slice > 65535) fail(BMADGPU_EUNSUPPORTED, "too many rf slices");
+          if (e.tilt != 0 || e.x_offset != 0 || e.y_offset != 0) misalign_block(tilt_tot);
+          break;
+        }
+        default:
+          fail(BMADGPU_EUNSUPPORTED, "element type");
+      }
+      if ((flags & F_MISALIGN) && mis.size() == 4 && mis[3] != 0) flags |= F_TILT;
+      blk.insert(blk.end(), mis.begin(), mis.end());
+      h.flags = flags;
+      h.param = pk.add_block(blk);
+      out.n_step[i] = h.n_step;
+      pk.hdr.push_back(h);
+    }
+    if (pk.ap.size() > 0xFFFF) throw Fail{BMADGPU_EUNSUPPORTED, "too many distinct apertures"};
+    if (pk.pool.empty()) pk.pool.push_back(0.0);
+    TableInfo& ti = out.info;
+    ti.n_ele = (uint32_t)n_ele;
+    ti.n_ap = (uint32_t)pk.ap.size();
+    ti.hdr_bytes = (uint32_t)(n_ele * sizeof(EleHdr));
+    ti.ap_bytes = (uint32_t)(pk.ap.size() * sizeof(ApRec));
+    ti.pool_doubles = (uint32_t)pk.pool.size();
+    size_t total = ti.hdr_bytes + ti.ap_bytes + pk.pool.size() * sizeof(double);
+    total = (total + 15) & ~size_t(15);
+    ti.total_bytes = (uint32_t)total;
+    ti.turn_ref_time = turn_ref;
+    out.image.assign(total, 0);
+    std::memcpy(out.image.data(), pk.hdr.data(), ti.hdr_bytes);
+    if (ti.ap_bytes) std::memcpy(out.image.data() + ti.hdr_bytes, pk.ap.data(), ti.ap_bytes);
+    std::memcpy(out.image.data() + ti.hdr_bytes + ti.ap_bytes, pk.pool.data(), pk.pool.size() * sizeof(double));
+    out.ref_time_prefix.assign(n_ele + 1, 0.0);
+    for (int i = 0; i < n_ele; i++) out.ref_time_prefix[i + 1] = out.ref_time_prefix[i] + eles[i].delta_ref_time;
+    return BMADGPU_OK;
+  } catch (const Fail& f) {
+    err = f.msg;
+    return f.code;
+  }
+}
+
+}  // namespace bmadgpu

@@ -1,0 +1,82 @@
+// table.h -- packed device element table, shared by the host packer (lattice.cpp) and the
+// sm_100a kernels (track.cu).
+//
+// A lattice becomes one contiguous, 16-byte aligned byte image:
+//   [EleHdr x n_ele][ApRec x n_ap][double pool]
+// Each element header names its map kind, flags and the offset of its parameter block in the
+// pool. Identical parameter blocks are stored once (a ring of identical FODO cells packs into a
+// few hundred bytes). All per-element invariants (step lengths, bend-angle trig, edge-kick
+// coefficients, scaled multipole coefficients, tilt cos/sin) are computed on the host, once.
+#pragma once
+#include <stdint.h>
+
+namespace bmadgpu {
+
+enum Kind : uint8_t {
+  K_MARKER = 0,  // no map (reference time only)
+  K_DRIFT = 1,   // track_a_drift
+  K_QUAD = 2,    // track_a_quadrupole
+  K_THICK = 3,   // track_a_thick_multipole (sextupole, octupole, thick_multipole, monitor, ...)
+  K_SBEND = 4,   // track_a_bend
+  K_THIN = 5,    // multipole / ab_multipole thin kicks (track1_bmad.f90:142-166)
+  K_RFCAV = 6    // track_a_rfcavity
+};
+
+enum Flag : uint16_t {
+  F_MISALIGN = 1 << 0,     // straight offset + tilt transform around the body
+  F_AP_ENTRANCE = 1 << 1,  // aperture checked at the entrance
+  F_AP_EXIT = 1 << 2,      // aperture checked at the exit
+  F_AP_ELLIPTICAL = 1 << 3,
+  F_EDGE_IN = 1 << 4,      // sbend entrance edge kick (Hwang)
+  F_EDGE_OUT = 1 << 5,     // sbend exit edge kick (Hwang)
+  F_KICKS = 1 << 6,        // multipole kicks present
+  F_BEND_K1 = 1 << 7,      // sbend body with k1 (sbend_body_with_k1_map)
+  F_REF_ORB_N0 = 1 << 8,   // thin multipole: n = 0 as a zero-length bend (MAD convention)
+  F_BEND_DRIFT = 1 << 9,   // sbend with g == 0 and dg == 0 or zero step: drift body
+  F_ZERO_LEN = 1 << 10,    // element length is zero
+  F_TILT = 1 << 11         // misalign block carries a non-zero tilt rotation
+};
+
+struct EleHdr {            // 16 bytes
+  uint8_t kind;
+  uint8_t n_pole;          // number of multipole orders kicked (ix_mag_max + 1), 0 = none
+  uint16_t flags;
+  uint16_t n_step;
+  uint16_t ap_index;       // index into the aperture records
+  uint32_t param;          // offset (in doubles) of the parameter block in the pool
+  uint32_t reserved;
+};
+
+struct ApRec {             // 32 bytes: rectangular/elliptical limits (x1_lim = -x1_limit, ...)
+  double x1_lim, x2_lim, y1_lim, y2_lim;
+};
+
+// Parameter block layouts (indices in doubles from EleHdr::param).
+// K_DRIFT:  [0] L
+// K_QUAD:   [0] b1/L  [1] sqrt(|b1/L|)  [2] step_len  then kicks, then misalign
+// K_THICK:  [0] step_len  then kicks, then misalign
+// K_SBEND:  [0] step_len [1] g [2] g_tot [3] dg [4] angle [5] cos_a [6] sin_a [7] sinc_a
+//           [8] cosc_a [9] (g step_len)^2 sincc_a [10] k1 = b1/L [11] r_step
+//           [12..18] entrance edge: gt gt2 gs2 k1_tane fg_factor g_tot gt*g_tot*(1+2tan^2)
+//           [19..25] exit edge:     (same)
+//           then kicks (bend form: plain b_n, a_n), then misalign (ref_tilt only: cos, sin)
+// K_THIN:   [0] knl0 [1] cos0 [2] sin0 then kicks (plain b_n, a_n)
+// K_RFCAV:  [0] voltage [1] rf_frequency [2] phi0 [3] twopi*phi0_multipass [4] slice_len
+//           [5] n_slice  then kicks (half kicks 0.5*r_step), then misalign
+// kicks: n_pole pairs for the end (half) kick followed, for K_QUAD/K_THICK, by n_pole pairs for
+//        the interior (full) kick: (b_n*scale, a_n*scale), n = 0 .. n_pole-1.
+// misalign: [x_off, y_off, cos_t, sin_t]
+constexpr int SB_EDGE_IN = 12, SB_EDGE_OUT = 19, SB_FIXED = 26;
+constexpr int RF_FIXED = 6;
+
+struct TableInfo {
+  uint32_t n_ele;
+  uint32_t n_ap;
+  uint32_t hdr_bytes;      // n_ele * sizeof(EleHdr), 16-aligned
+  uint32_t ap_bytes;       // n_ap * sizeof(ApRec)
+  uint32_t pool_doubles;
+  uint32_t total_bytes;    // whole image, 16-aligned
+  double turn_ref_time;    // sum of delta_ref_time over the elements
+};
+
+}  // namespace bmadgpu

@@ -1,0 +1,403 @@
+// track.cu -- sm_100a kernels for multi-turn bunch tracking.
+//
+// k_track: one thread per particle; the particle lives in registers for all n_turns turns of
+// the launch, running the element loop of track_bunch (bmad/multiparticle/beam_mod.f90:159-166)
+// with the per-element wrapper of track1 (bmad/code/track1.f90:179-329) around each map. The
+// packed element table is staged once per CTA into shared memory by a TMA bulk copy
+// (cp.async.bulk, mbarrier completion, bounded wait), so the element loop reads invariants with
+// broadcast shared-memory loads. Lost particles leave the loop at once and record where they
+// were lost (state, element, turn, location) as track1_bunch_hom leaves them
+// (bmad/multiparticle/beam_utils.f90:81-86). Optional per-turn sums over live particles
+// (n_live, <x_i>, <x_i x_j>; bsim/modules/lt_tracking_mod.f90:2393-2421) are reduced with warp
+// shuffles and one atomic per warp and value.
+//
+// k_compact: warp ballot / popc stream compaction of the live-particle index list.
+
+#include <cuda_runtime.h>
+
+#include "track.cuh"
+
+namespace bmadgpu {
+
+namespace {
+
+constexpr uint32_t kBulkChunk = 32768;
+constexpr int kSpinLimit = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// 1-D bulk copy global -> this CTA's shared memory (no multicast), completion on an mbarrier.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void load_hdr(const EleHdr* hdr, int i, EleHdr& h) {
+  uint4 raw = *reinterpret_cast<const uint4*>(hdr + i);
+  h = *reinterpret_cast<const EleHdr*>(&raw);
+}
+
+// ---- element bodies (track1_bmad dispatch, bmad/low_level/track1_bmad.f90:64-272) ----------
+
+__device__ __forceinline__ void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b) {
+  // track_a_quadrupole, bmad/low_level/track_a_quadrupole.f90
+  const int np = h.n_pole;
+  const double* kh = b + 3;
+  const double* kf = kh + 2 * np;
+  const double* mis = b + 3 + 4 * np;
+  const bool has_t = h.flags & F_TILT;
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
+  if (np) kicks(p, kh, np);
+  const double b1_l = b[0], sqrt_bl = b[1], step_len = b[2];
+  for (int i = 1; i <= h.n_step; i++) {
+    quad_step(p, b1_l, sqrt_bl, step_len);
+    if (np) kicks(p, i == h.n_step ? kh : kf, np);
+  }
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
+}
+
+__device__ __forceinline__ void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b) {
+  // track_a_thick_multipole, bmad/low_level/track_a_thick_multipole.f90:18-133
+  const int np = h.n_pole;
+  const double* kh = b + 1;
+  const double* kf = kh + 2 * np;
+  const double* mis = b + 1 + 4 * np;
+  const bool has_t = h.flags & F_TILT;
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
+  if (np) kicks(p, kh, np);
+  const double step_len = b[0];
+  for (int i = 1; i <= h.n_step; i++) {
+    drift(p, step_len);
+    if (np) kicks(p, i == h.n_step ? kh : kf, np);
+  }
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
+}
+
+__device__ __forceinline__ void bend_kick(Particle& p, const double* __restrict__ b, int np, double coef) {
+  // apply_multipole_kicks (magnetic, exact_multipoles = off), track_a_bend.f90:338-411:
+  // the field form reduces to coef * r_step * (1 + g x) * (kx, ky).
+  double kx, ky;
+  multipole_kick_sum(b + SB_FIXED, np, p.x, p.y, kx, ky);
+  double f = coef * b[11] * (1 + b[1] * p.x);
+  p.px = p.px + f * kx;
+  p.py = p.py + f * ky;
+}
+
+__device__ __forceinline__ void body_bend(Particle& p, const EleHdr& h, const double* __restrict__ b,
+                                          const Globals& G) {
+  // track_a_bend, bmad/low_level/track_a_bend.f90:18-333
+  const int np = h.n_pole;
+  const double* mis = b + SB_FIXED + 2 * np;
+  if (h.flags & F_MISALIGN) offset_set(p, mis, true);  // ref_tilt rotation
+  if (h.flags & F_EDGE_IN) hwang_edge(p, b + SB_EDGE_IN, true);
+  if (orbit_too_large(p, G)) return;
+  if (np) bend_kick(p, b, np, 0.5);
+  for (int n = 1; n <= h.n_step; n++) {
+    if (h.flags & F_BEND_K1) {
+      bend_k1_step(p, b);
+      p.z = p.z + b[0] * p.lez;
+    } else if (h.flags & F_BEND_DRIFT) {
+      drift(p, b[0]);
+    } else {
+      if (!bend_exact_step(p, b, G)) return;
+    }
+    if (np) bend_kick(p, b, np, n == h.n_step ? 0.5 : 1.0);
+  }
+  if (orbit_too_large(p, G)) return;
+  if (h.flags & F_EDGE_OUT) hwang_edge(p, b + SB_EDGE_OUT, false);
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, true);
+}
+
+__device__ __forceinline__ void body_thin(Particle& p, const EleHdr& h, const double* __restrict__ b) {
+  // multipole / ab_multipole, track1_bmad.f90:142-166 with multipole_kicks (multipole_mod.f90:32-51)
+  const int np = h.n_pole;
+  const double* mis = b + 3 + 2 * np;
+  if (h.flags & F_MISALIGN) offset_set(p, mis, false);
+  if (h.flags & F_REF_ORB_N0) {  // multipole_mod.f90:250-255
+    double knl = b[0], c0 = b[1], s0 = b[2];
+    double x = p.x, y = p.y;
+    p.px = p.px + knl * c0 * p.pz;
+    p.py = p.py + knl * s0 * p.pz;
+    p.z = p.z - knl * (c0 * x + s0 * y);
+  }
+  if (np) kicks(p, b + 3, np);
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, false);
+}
+
+__device__ __forceinline__ void body_rf(Particle& p, const EleHdr& h, const double* __restrict__ b,
+                                        const Globals& G) {
+  // track_a_rfcavity, bmad/low_level/track_a_rfcavity.f90:17-146 (relative time tracking)
+  const int np = h.n_pole;
+  const double* kh = b + RF_FIXED;
+  const double* mis = kh + 2 * np;
+  const bool has_t = h.flags & F_TILT;
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
+  if (np) kicks(p, kh, np);
+  const double voltage = b[0], f = b[1], slice_len = b[4];
+  const int n_slice = h.n_step;
+  double phase = rf_phase(p, b[2], f, b[3]);
+  double sin_ph = sin(phase);
+  for (int i = 0; i <= n_slice; i++) {
+    double dE = voltage * sin_ph / n_slice;
+    if (i == 0 || i == n_slice) dE = dE / 2;
+    energy_kick(p, dE, G);
+    if (p.pz == -1) {
+      p.state = S_LOST_PZ;
+      return;
+    }
+    if (i != n_slice) {
+      refresh(p, G);
+      double z0 = p.z;
+      drift(p, slice_len);
+      phase = phase + kTwoPi * f * (p.z - z0) / (kCLight * p.beta);
+      sin_ph = sin(phase);
+    }
+  }
+  refresh(p, G);
+  if (np) kicks(p, kh, np);
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
+}
+
+// track1 around one element: entrance orbit/aperture checks, body, exit checks
+// (track1.f90:179-196, 221-236, 289-329). Returns 0 if the particle survived, else its
+// coord%location at the loss. The entrance orbit_too_large test repeats the previous element's
+// exit test on unchanged coordinates, so it runs only for the first element of a launch.
+__device__ __forceinline__ int track1(Particle& p, const EleHdr& h, const double* __restrict__ pool,
+                                      const ApRec* __restrict__ ap, const Globals& G, bool entry_check) {
+  if (entry_check && orbit_too_large(p, G)) return L_UPSTREAM;
+  if (h.flags & F_AP_ENTRANCE) {
+    aperture(p, ap[h.ap_index], h.flags & F_AP_ELLIPTICAL);
+    if (p.state != S_ALIVE) return L_UPSTREAM;
+  }
+  const double* b = pool + h.param;
+  switch (h.kind) {
+    case K_DRIFT: drift(p, b[0]); break;
+    case K_QUAD: body_quad(p, h, b); break;
+    case K_THICK: body_thick(p, h, b); break;
+    case K_SBEND: body_bend(p, h, b, G); break;
+    case K_THIN: body_thin(p, h, b); break;
+    case K_RFCAV: body_rf(p, h, b, G); break;
+    default: break;  // K_MARKER
+  }
+  if (orbit_too_large(p, G)) return L_UPSTREAM;
+  if (p.state != S_ALIVE) return L_INSIDE;
+  if (h.flags & F_AP_EXIT) {
+    aperture(p, ap[h.ap_index], h.flags & F_AP_ELLIPTICAL);
+    if (p.state != S_ALIVE) return L_DOWNSTREAM;
+  }
+  return 0;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ void add_moments(const Particle& p, bool alive, double* __restrict__ m) {
+  const double v[6] = {p.x, p.px, p.y, p.py, p.z, p.pz};
+  const int lane = threadIdx.x & 31;
+  double s = warp_sum(alive ? 1.0 : 0.0);
+  if (lane == 0 && s != 0) atomicAdd(m, s);
+  if (__any_sync(0xffffffffu, alive) == 0) return;
+  int k = 7;
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    double si = warp_sum(alive ? v[i] : 0.0);
+    if (lane == 0) atomicAdd(m + 1 + i, si);
+#pragma unroll
+    for (int j = i; j < 6; j++) {
+      double sij = warp_sum(alive ? v[i] * v[j] : 0.0);
+      if (lane == 0) atomicAdd(m + k, sij);
+      k++;
+    }
+  }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_track(const TrackArgs a, int stage_smem) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(8) uint64_t bar;
+  const uint8_t* tbl = a.table;
+  bool staged = false;
+  if (stage_smem) {
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      mbar_arrive_expect_tx(&bar, a.table_bytes);
+      for (uint32_t off = 0; off < a.table_bytes; off += kBulkChunk) {
+        uint32_t n = a.table_bytes - off < kBulkChunk ? a.table_bytes - off : kBulkChunk;
+        bulk_g2s(smem + off, a.table + off, n, &bar);
+      }
+    }
+    bool ok = false;
+    for (int it = 0; it < kSpinLimit; ++it) {
+      if (mbar_try_wait(&bar, 0)) { ok = true; break; }
+    }
+    // Every thread must agree; a timed-out copy falls back to reading the table from global
+    // memory and raises the error flag for the host.
+    staged = __syncthreads_and(ok);
+    if (!staged && threadIdx.x == 0) atomicOr(a.err_flag, 1);
+    if (staged) tbl = smem;
+  }
+  const EleHdr* hdr = reinterpret_cast<const EleHdr*>(tbl);
+  const ApRec* ap = reinterpret_cast<const ApRec*>(tbl + a.hdr_bytes);
+  const double* pool = reinterpret_cast<const double*>(tbl + a.hdr_bytes + a.ap_bytes);
+  const Globals G = a.G;
+  const int64_t n_work = *a.n_work;
+  const int64_t ld = a.ld;
+  const double seg_ref = a.ref_prefix[a.ix_end] - a.ref_prefix[a.ix_start];
+
+  for (int64_t base = (int64_t)blockIdx.x * BLOCK; base < n_work; base += (int64_t)gridDim.x * BLOCK) {
+    const int64_t w = base + threadIdx.x;
+    const bool valid = w < n_work;
+    const int64_t j = valid ? (a.live ? (int64_t)a.live[w] : w) : 0;
+    Particle p;
+    p.state = 0;
+    if (valid) {
+      p.x = a.vec[j];
+      p.px = a.vec[ld + j];
+      p.y = a.vec[2 * ld + j];
+      p.py = a.vec[3 * ld + j];
+      p.z = a.vec[4 * ld + j];
+      p.pz = a.vec[5 * ld + j];
+      p.beta = a.beta[j];
+      p.state = a.state[j];
+    }
+    bool alive = valid && p.state == S_ALIVE;
+    const double z_in = p.z, beta_in = p.beta;
+    int lost_loc = 0, lost_ele = -1, lost_turn = -1;
+    if (alive) refresh(p, G);
+    for (int turn = 0; turn < a.n_turns; ++turn) {
+      if (alive) {
+        for (int ie = a.ix_start; ie < a.ix_end; ++ie) {
+          EleHdr h;
+          load_hdr(hdr, ie, h);
+          int loc = track1(p, h, pool, ap, G, turn == 0 && ie == a.ix_start);
+          if (loc) {
+            alive = false;
+            lost_loc = loc;
+            lost_ele = ie;
+            lost_turn = a.turn0 + turn;
+            break;
+          }
+        }
+      }
+      if (a.moments) add_moments(p, alive, a.moments + (int64_t)turn * 28);
+    }
+    if (valid && (alive || lost_loc)) {
+      a.vec[j] = p.x;
+      a.vec[ld + j] = p.px;
+      a.vec[2 * ld + j] = p.y;
+      a.vec[3 * ld + j] = p.py;
+      a.vec[4 * ld + j] = p.z;
+      a.vec[5 * ld + j] = p.pz;
+      a.beta[j] = p.beta;
+      a.state[j] = p.state;
+      if (a.t && beta_in > 0) {
+        // t + z/(beta c) advances by delta_ref_time in every element (track_a_*: orbit%t update),
+        // so the time follows from the reference time elapsed.
+        double elapsed = alive ? a.n_turns * seg_ref
+                               : (lost_turn - a.turn0) * seg_ref + (a.ref_prefix[lost_ele] - a.ref_prefix[a.ix_start]);
+        double tb = (p.beta > 0) ? p.z / (p.beta * kCLight) : 0.0;
+        a.t[j] = a.t[j] + (z_in / (beta_in * kCLight) + elapsed - tb);
+      }
+      if (!alive) {
+        if (a.ix_ele) a.ix_ele[j] = lost_ele;
+        if (a.ix_turn) a.ix_turn[j] = lost_turn;
+        if (a.location) a.location[j] = lost_loc;
+      }
+    }
+  }
+  if (stage_smem && !staged) {
+    // Let our own bulk copy drain (bounded) before the CTA's shared memory is released.
+    for (int it = 0; it < kSpinLimit; ++it)
+      if (mbar_try_wait(&bar, 0)) break;
+  }
+}
+
+__global__ void k_compact(const int32_t* __restrict__ state, const int32_t* __restrict__ live_in,
+                          const int64_t* __restrict__ n_in, int32_t* __restrict__ live_out,
+                          unsigned long long* __restrict__ n_out) {
+  const int64_t n = *n_in;
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+    int64_t w = base + threadIdx.x;
+    int32_t j = (w < n) ? (live_in ? live_in[w] : (int32_t)w) : 0;
+    bool keep = (w < n) && state[j] == S_ALIVE;
+    unsigned mask = __ballot_sync(0xffffffffu, keep);
+    unsigned long long off = 0;
+    if (lane == 0 && mask) off = atomicAdd(n_out, (unsigned long long)__popc(mask));
+    off = __shfl_sync(0xffffffffu, off, 0);
+    if (keep) live_out[off + __popc(mask & ((1u << lane) - 1))] = j;
+  }
+}
+
+}  // namespace
+
+int table_fits_smem(uint32_t table_bytes) { return table_bytes <= 200 * 1024; }
+
+cudaError_t launch_track(const TrackArgs& a, const LaunchCfg& cfg, int sm_count, cudaStream_t stream) {
+  int stage = (cfg.stage_smem && table_fits_smem(a.table_bytes)) ? 1 : 0;
+  size_t smem = stage ? a.table_bytes : 0;
+  const void* fn;
+  switch (cfg.block) {
+    case 64: fn = (const void*)k_track<64>; break;
+    case 128: fn = (const void*)k_track<128>; break;
+    case 256: fn = (const void*)k_track<256>; break;
+    case 512: fn = (const void*)k_track<512>; break;
+    default: return cudaErrorInvalidValue;
+  }
+  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  int per_sm = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, cfg.block, smem);
+  if (err != cudaSuccess) return err;
+  if (per_sm < 1) per_sm = 1;
+  if (cfg.ctas_per_sm > 0 && cfg.ctas_per_sm < per_sm) per_sm = cfg.ctas_per_sm;
+  // Persistent grid: at most one full wave; every CTA strides over the particle range.
+  int64_t grid = (int64_t)sm_count * per_sm;
+  void* args[] = {(void*)&a, (void*)&stage};
+  return cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(cfg.block), args, smem, stream);
+}
+
+cudaError_t launch_compact(const int32_t* state, const int32_t* live_in, const int64_t* n_in, int64_t n_max,
+                           int32_t* live_out, int64_t* n_out, cudaStream_t stream) {
+  cudaError_t err = cudaMemsetAsync(n_out, 0, sizeof(int64_t), stream);
+  if (err != cudaSuccess) return err;
+  int64_t blocks = (n_max + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  k_compact<<<(unsigned)blocks, 256, 0, stream>>>(state, live_in, n_in, live_out,
+                                                   reinterpret_cast<unsigned long long*>(n_out));
+  return cudaGetLastError();
+}
+
+}  // namespace bmadgpu

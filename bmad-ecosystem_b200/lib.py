@@ -1,0 +1,235 @@
+"""ctypes binding of libbmadgpu.so (include/bmadgpu.h) and a thin object layer over it.
+
+Names follow the reference: ``track_bunch`` is track_bunch (bmad/multiparticle/beam_mod.f90:103)
+over turns, ``track1_bunch`` the per-element hook (beam_mod.f90:238). Errors raise
+``BmadGpuError`` with the library's last-error message; nothing here falls back to a CPU path.
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libbmadgpu.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "bmadgpu.h")
+
+
+class BmadGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (abi.STATUS_NAMES.get(code, "?"), code, msg))
+        self.code = code
+
+
+class Tuning(C.Structure):
+    _fields_ = [("block", C.c_int32), ("ctas_per_sm", C.c_int32), ("stage_smem", C.c_int32),
+                ("turns_per_launch", C.c_int32), ("compact", C.c_int32), ("reserved", C.c_int32 * 3)]
+
+
+_lib = None
+
+
+def load(path=LIB_PATH):
+    """Load the shared library (built by csrc/Makefile). Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise BmadGpuError(abi.EINVAL, "libbmadgpu.so not built: run make -C bmad-ecosystem_b200/csrc")
+    lib = C.CDLL(path)
+    P, V = C.POINTER, C.c_void_p
+    sig = {
+        "bmadgpu_abi_version": ([], C.c_int),
+        "bmadgpu_last_error": ([], C.c_char_p),
+        "bmadgpu_sizeof": ([C.c_int32], C.c_int64),
+        "bmadgpu_ctx_create": ([C.c_int32, P(V)], C.c_int),
+        "bmadgpu_ctx_destroy": ([V], C.c_int),
+        "bmadgpu_ctx_synchronize": ([V], C.c_int),
+        "bmadgpu_ctx_set_tuning": ([V, P(Tuning)], C.c_int),
+        "bmadgpu_ctx_get_tuning": ([V, P(Tuning)], C.c_int),
+        "bmadgpu_ctx_info": ([V, P(C.c_int32), P(C.c_int32), P(V)], C.c_int),
+        "bmadgpu_lattice_create": ([V, P(abi.Element), C.c_int32, P(abi.Param), P(V)], C.c_int),
+        "bmadgpu_lattice_destroy": ([V], C.c_int),
+        "bmadgpu_lattice_n_step": ([V, C.c_int32], C.c_int32),
+        "bmadgpu_lattice_table_bytes": ([V], C.c_int64),
+        "bmadgpu_lattice_check": ([P(abi.Element), C.c_int32, P(abi.Param), P(C.c_int32), P(C.c_int64)], C.c_int),
+        "bmadgpu_track_bunch": ([V, V, P(abi.Bunch), C.c_int32, C.c_int32, C.c_int32, C.c_int32, V], C.c_int),
+        "bmadgpu_track_bunch_device": ([V, V, P(abi.Bunch), C.c_int32, C.c_int32, C.c_int32, C.c_int32, V],
+                                       C.c_int),
+        "bmadgpu_track1_bunch": ([V, V, P(abi.Bunch), C.c_int32, C.c_int32], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name, None)
+        if f is None:
+            continue
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def declared_symbols(header=HEADER_PATH):
+    """Function names declared in include/bmadgpu.h."""
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(bmadgpu_[a-z0-9_]+)\s*\(", text)))
+
+
+def check(code):
+    if code != 0:
+        raise BmadGpuError(code, load().bmadgpu_last_error().decode())
+    return code
+
+
+def check_layout():
+    """Compare ctypes struct sizes with the compiled library's sizeof()."""
+    lib = load()
+    for i, st in enumerate((abi.Element, abi.Param, abi.Bunch, Tuning)):
+        if lib.bmadgpu_sizeof(i) != C.sizeof(st):
+            raise BmadGpuError(abi.EINVAL, "ABI size mismatch for %s" % st.__name__)
+
+
+def lattice_check(elements, param):
+    """Host-only validation and bookkeeping: returns (n_step per element, packed table bytes)."""
+    lib = load()
+    arr = abi.element_array(elements) if not isinstance(elements, C.Array) else elements
+    n = len(arr)
+    steps = (C.c_int32 * n)()
+    nbytes = C.c_int64(0)
+    check(lib.bmadgpu_lattice_check(arr, n, C.byref(param), steps, C.byref(nbytes)))
+    return list(steps), nbytes.value
+
+
+class Context:
+    """A device context (bmadgpu_ctx): one CUDA stream plus staging buffers."""
+
+    def __init__(self, device=0):
+        lib = load()
+        check_layout()
+        self._h = C.c_void_p()
+        check(lib.bmadgpu_ctx_create(device, C.byref(self._h)))
+        d, sm, st = C.c_int32(), C.c_int32(), C.c_void_p()
+        check(lib.bmadgpu_ctx_info(self._h, C.byref(d), C.byref(sm), C.byref(st)))
+        self.device, self.sm_count, self.stream = d.value, sm.value, st.value
+
+    @property
+    def handle(self):
+        return self._h
+
+    def synchronize(self):
+        check(load().bmadgpu_ctx_synchronize(self._h))
+
+    def get_tuning(self):
+        t = Tuning()
+        check(load().bmadgpu_ctx_get_tuning(self._h, C.byref(t)))
+        return dict(block=t.block, ctas_per_sm=t.ctas_per_sm, stage_smem=t.stage_smem,
+                    turns_per_launch=t.turns_per_launch, compact=t.compact)
+
+    def set_tuning(self, **kw):
+        cur = self.get_tuning()
+        cur.update(kw)
+        t = Tuning(cur["block"], cur["ctas_per_sm"], cur["stage_smem"], cur["turns_per_launch"], cur["compact"])
+        check(load().bmadgpu_ctx_set_tuning(self._h, C.byref(t)))
+
+    def close(self):
+        if self._h:
+            load().bmadgpu_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Lattice:
+    """Packed, device-resident element table (bmadgpu_lattice)."""
+
+    def __init__(self, ctx, elements, param):
+        lib = load()
+        self.ctx = ctx
+        self.elements = abi.element_array(elements) if not isinstance(elements, C.Array) else elements
+        self.param = param
+        self.n_ele = len(self.elements)
+        self._h = C.c_void_p()
+        check(lib.bmadgpu_lattice_create(ctx.handle, self.elements, self.n_ele, C.byref(param), C.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def n_step(self, i):
+        return load().bmadgpu_lattice_n_step(self._h, i)
+
+    @property
+    def table_bytes(self):
+        return load().bmadgpu_lattice_table_bytes(self._h)
+
+    def close(self):
+        if self._h:
+            load().bmadgpu_lattice_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HostBunch:
+    """Structure-of-arrays particle arrays in host memory (numpy), the bmadgpu_bunch view of a
+    bunch_struct. vec is [6, n] C-contiguous so vec[i] is coordinate i of every particle."""
+
+    def __init__(self, vec, beta, state=None, t=None, track_losses=True):
+        self.vec = np.ascontiguousarray(vec, dtype=np.float64)
+        n = self.vec.shape[1]
+        self.beta = np.ascontiguousarray(beta, dtype=np.float64)
+        self.state = (np.full(n, abi.ALIVE, dtype=np.int32) if state is None
+                      else np.ascontiguousarray(state, dtype=np.int32))
+        self.t = None if t is None else np.ascontiguousarray(t, dtype=np.float64)
+        if track_losses:
+            self.ix_ele = np.full(n, -1, dtype=np.int32)
+            self.ix_turn = np.full(n, -1, dtype=np.int32)
+            self.location = np.zeros(n, dtype=np.int32)
+        else:
+            self.ix_ele = self.ix_turn = self.location = None
+
+    @classmethod
+    def from_vec(cls, vec, param, **kw):
+        """Particles at the upstream end with beta from pz as init_coord computes it."""
+        vec = np.asarray(vec, dtype=np.float64)
+        pc = param.p0c * (1 + vec[5])
+        beta = np.where(vec[5] == 0, param.p0c / param.e_tot, pc / np.sqrt(pc * pc + param.mass * param.mass))
+        return cls(vec, beta, **kw)
+
+    @property
+    def n(self):
+        return self.vec.shape[1]
+
+    def view(self):
+        def ptr(a):
+            return None if a is None else a.ctypes.data
+        return abi.Bunch(self.n, ptr(self.vec), ptr(self.beta), ptr(self.t), ptr(self.state), ptr(self.ix_ele),
+                         ptr(self.ix_turn), ptr(self.location))
+
+
+def track_bunch(ctx, lat, bunch, n_turns=1, ix_start=0, ix_end=None, turn0=0, moments=False):
+    """Track a HostBunch for n_turns over elements [ix_start, ix_end) (host buffers, copies
+    included). Returns the per-turn moment sums [n_turns, 28] if moments is True."""
+    lib = load()
+    ix_end = lat.n_ele if ix_end is None else ix_end
+    mom = np.zeros((max(n_turns, 1), abi.N_MOMENTS)) if moments else None
+    v = bunch.view()
+    check(lib.bmadgpu_track_bunch(ctx.handle, lat.handle, C.byref(v), ix_start, ix_end, turn0, n_turns,
+                                  mom.ctypes.data if mom is not None else None))
+    return mom
+
+
+def track1_bunch(ctx, lat, bunch, ix_ele, turn=0):
+    """One element for the whole bunch: the work of track1_bunch / track1_bunch_hom."""
+    v = bunch.view()
+    check(load().bmadgpu_track1_bunch(ctx.handle, lat.handle, C.byref(v), ix_ele, turn))

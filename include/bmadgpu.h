@@ -151,6 +151,11 @@ int bmadgpu_ctx_destroy(bmadgpu_ctx* ctx);
 int bmadgpu_lattice_create(bmadgpu_ctx* ctx, const bmadgpu_element* eles, int32_t n_ele,
                            const bmadgpu_param* param, bmadgpu_lattice** out);
 int bmadgpu_lattice_destroy(bmadgpu_lattice* lat);
+/* Host-only validation and bookkeeping of an element list (no device needed): fills
+ * n_step_out[n_ele] (nullable) with the resolved integration steps and *table_bytes (nullable)
+ * with the packed table size. Returns BMADGPU_EUNSUPPORTED for elements off the device path. */
+int bmadgpu_lattice_check(const bmadgpu_element* eles, int32_t n_ele, const bmadgpu_param* param,
+                          int32_t* n_step_out, int64_t* table_bytes);
 /* Resolved integration steps of element i (ds_step/num_steps bookkeeping); -1 on bad index. */
 int32_t bmadgpu_lattice_n_step(const bmadgpu_lattice* lat, int32_t i);
 /* Bytes of the packed element table (what is staged into shared memory). */
@@ -179,6 +184,25 @@ int bmadgpu_track1_bunch(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_b
 
 /* Waits for all work queued on the context's stream. */
 int bmadgpu_ctx_synchronize(bmadgpu_ctx* ctx);
+
+/* Launch shape of the tracking kernel, chosen by the autotuner or set by the caller. */
+typedef struct bmadgpu_tuning {
+  int32_t block;              /* threads per CTA: 64, 128, 256 or 512 */
+  int32_t ctas_per_sm;        /* resident CTAs per SM; 0 = as many as fit */
+  int32_t stage_smem;         /* stage the element table in shared memory (TMA bulk copy) */
+  int32_t turns_per_launch;   /* turns per kernel launch; 0 = all turns in one launch */
+  int32_t compact;            /* compact the live-particle list between launches */
+  int32_t reserved[3];
+} bmadgpu_tuning;
+int bmadgpu_ctx_set_tuning(bmadgpu_ctx* ctx, const bmadgpu_tuning* tuning);
+int bmadgpu_ctx_get_tuning(const bmadgpu_ctx* ctx, bmadgpu_tuning* tuning);
+
+/* Device the context runs on, its SM count, and the CUDA stream it enqueues work on
+ * (cudaStream_t, returned as void*). */
+int bmadgpu_ctx_info(const bmadgpu_ctx* ctx, int32_t* device, int32_t* sm_count, void** stream);
+
+/* sizeof() of the ABI structs as this library was compiled, for binding checks. */
+int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning */
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,40 @@
+"""Test helpers: run the same bunch through the CPU oracle (checker) and compare results."""
+import ctypes
+
+import numpy as np
+
+from conftest import load_abi, load_oracle
+
+
+def oracle_track(elements, param, vec, n_turns, n_threads=0, moments=False, t=None):
+    """Track vec[6, n] through the element list with the oracle. Returns a dict of arrays."""
+    abi, lib = load_abi(), load_oracle()
+    arr = abi.element_array(elements) if not isinstance(elements, ctypes.Array) else elements
+    vec = np.ascontiguousarray(vec, dtype=np.float64).copy()
+    n = vec.shape[1]
+    pc = param.p0c * (1 + vec[5])
+    beta = np.where(vec[5] == 0, param.p0c / param.e_tot, pc / np.sqrt(pc * pc + param.mass * param.mass))
+    beta = np.ascontiguousarray(beta)
+    state = np.full(n, abi.ALIVE, dtype=np.int32)
+    ix_ele = np.full(n, -1, dtype=np.int32)
+    ix_turn = np.full(n, -1, dtype=np.int32)
+    loc = np.zeros(n, dtype=np.int32)
+    tt = np.zeros(n) if t is None else np.ascontiguousarray(t, dtype=np.float64).copy()
+    b = abi.Bunch(n, vec.ctypes.data, beta.ctypes.data, tt.ctypes.data, state.ctypes.data, ix_ele.ctypes.data,
+                  ix_turn.ctypes.data, loc.ctypes.data)
+    mom = np.zeros((max(n_turns, 1), abi.N_MOMENTS)) if moments else None
+    err = lib.oracle_track_ring(arr, len(arr), ctypes.byref(param), ctypes.byref(b), 0, n_turns, n_threads,
+                                mom.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if moments else None)
+    assert err == 0, err
+    return dict(vec=vec, beta=beta, state=state, ix_ele=ix_ele, ix_turn=ix_turn, location=loc, t=tt, moments=mom)
+
+
+def rel_err(got, want, floor):
+    """Per-coordinate error relative to max(|want|, floor)."""
+    return np.abs(got - want) / np.maximum(np.abs(want), floor)
+
+
+def coord_floor(vec, frac=1e-3):
+    """A per-coordinate floor for relative errors: frac * RMS of the coordinate over the bunch."""
+    rms = np.sqrt(np.mean(vec * vec, axis=1))
+    return np.maximum(frac * rms, 1e-30)[:, None]

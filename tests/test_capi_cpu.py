@@ -1,0 +1,74 @@
+"""C-ABI library checks that need no GPU: symbols, struct layout, host-side bookkeeping."""
+import ctypes
+import importlib
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_abi, load_oracle
+
+lib = importlib.import_module("bmad-ecosystem_b200.lib")
+rings = importlib.import_module("bmad-ecosystem_b200.rings")
+
+
+def test_library_exports_every_declared_symbol():
+    so = lib.load()
+    declared = lib.declared_symbols()
+    assert len(declared) >= 15
+    missing = [s for s in declared if not hasattr(so, s)]
+    assert not missing, missing
+    out = subprocess.check_output(["nm", "-D", "--defined-only", lib.LIB_PATH]).decode()
+    for s in declared:
+        assert (" T " + s) in out, s
+
+
+def test_struct_layout_matches():
+    lib.check_layout()
+    assert lib.load().bmadgpu_abi_version() == 1
+
+
+def test_ring_bookkeeping_matches_oracle():
+    abi, orc = load_abi(), load_oracle()
+    eles, param = rings.ring(50)
+    steps, nbytes = lib.lattice_check(eles, param)
+    assert 0 < nbytes < 64 * 1024   # identical cells pack into a small table
+    for e, s in zip(eles, steps):
+        n_or = orc.oracle_element_num_steps(ctypes.byref(e), ctypes.byref(param))
+        if e.key in (abi.SEXTUPOLE, abi.RFCAVITY):
+            assert s == n_or
+        else:
+            assert s == 1
+
+
+def test_config1_ring_packs_and_sextupoles_use_one_step():
+    eles, param = rings.ring(200, fringe=True, multipole_sigma=1e-4)
+    steps, nbytes = lib.lattice_check(eles, param)
+    assert nbytes < 200 * 1024
+    abi = load_abi()
+    assert all(s == 1 for e, s in zip(eles, steps) if e.key == abi.SEXTUPOLE)
+
+
+@pytest.mark.parametrize("bad", ["elec", "pitch", "bend_offset", "abs_time"])
+def test_unsupported_inputs_fail_loudly(bad):
+    abi = load_abi()
+    p = abi.electron_param(3e9)
+    e = abi.default_element(abi.QUADRUPOLE, l=0.4, k1=0.5)
+    if bad == "elec":
+        e.b_pole_elec[1] = 1e3
+    elif bad == "pitch":
+        e.y_pitch = 1e-3
+    elif bad == "bend_offset":
+        e = abi.default_element(abi.SBEND, l=1.0, g=0.01, x_offset=1e-3)
+    else:
+        p.absolute_time_tracking = 1
+    with pytest.raises(lib.BmadGpuError) as ei:
+        lib.lattice_check([e], p)
+    assert ei.value.code == abi.EUNSUPPORTED
+
+
+def test_optics_of_benchmark_ring_is_stable():
+    eles, _ = rings.ring(50)
+    tw = rings.periodic_optics(eles)
+    assert 0 < tw["tune_a"] < 1 and 0 < tw["tune_b"] < 1
+    assert tw["beta_a"] > 0 and tw["beta_b"] > 0
