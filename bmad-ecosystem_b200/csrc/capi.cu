@@ -111,10 +111,13 @@ Globals make_globals(const bmadgpu_param& p) {
   g.beta0 = p.p0c / p.e_tot;
   g.max_ap = p.max_aperture_limit;
   g.mass2 = p.mass * p.mass;
+  // low_energy_z_correction.f90:43-45 constants, same expressions
   double me = p.mass / p.e_tot;
-  g.me2 = me * me;
-  g.lez_f = g.beta0 * g.beta0 * (2 * g.beta0 * g.beta0 - g.me2 / 2);
+  g.lez_me2 = me * me;
+  g.lez_b02 = g.beta0 * g.beta0;
+  g.lez_f = g.lez_b02 * (2 * g.lez_b02 - g.lez_me2 / 2);
   g.lez_thresh = 3e-7 * p.e_tot;
+  g.charge = p.charge;
   return g;
 }
 
@@ -232,6 +235,7 @@ int bmadgpu_ctx_create(int32_t device, bmadgpu_ctx** out) {
   cudaDeviceProp prop;
   CUDA_TRY(cudaGetDeviceProperties(&prop, device));
   if (prop.major < 10) return fail(BMADGPU_EUNSUPPORTED, "needs an sm_100 (Blackwell B200) device");
+  CUDA_TRY(upload_constants());
   bmadgpu_ctx* c = new (std::nothrow) bmadgpu_ctx();
   if (!c) return fail(BMADGPU_ENOMEM, "host allocation failed");
   c->device = device;

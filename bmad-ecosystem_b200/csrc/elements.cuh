@@ -1,0 +1,161 @@
+// elements.cuh -- per-element bodies and the track1 wrapper (shared by the kernels and the
+// test-only host check build).
+#pragma once
+#include "maps.cuh"
+
+namespace bmadgpu {
+
+// ---- element bodies (track1_bmad dispatch, bmad/low_level/track1_bmad.f90:64-272) ----------
+
+BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b, const Globals& G) {
+  // track_a_quadrupole, bmad/low_level/track_a_quadrupole.f90 (fringe_type none)
+  const int np = h.n_pole;
+  const double* kh = b + 3;
+  const double* kf = kh + 2 * np;
+  const double* mis = b + 3 + 4 * np;
+  const bool has_t = h.flags & F_TILT;
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
+  if (np) ab_kicks(p, kh, np);
+  const double b1 = b[0], length = b[1], step_len = b[2];
+  for (int i = 1; i <= h.n_step; i++) {
+    quad_step(p, b1, length, step_len, G);
+    if (np) ab_kicks(p, i == h.n_step ? kh : kf, np);
+  }
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
+}
+
+BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b) {
+  // track_a_thick_multipole, bmad/low_level/track_a_thick_multipole.f90:18-133
+  const int np = h.n_pole;
+  const double* kh = b + 1;
+  const double* kf = kh + 2 * np;
+  const double* mis = b + 1 + 4 * np;
+  const bool has_t = h.flags & F_TILT;
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
+  if (np) ab_kicks(p, kh, np);
+  const double step_len = b[0];
+  for (int i = 1; i <= h.n_step; i++) {
+    drift(p, step_len);
+    if (np) ab_kicks(p, i == h.n_step ? kh : kf, np);
+  }
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
+}
+
+BG_HD void bend_kick(Particle& p, const double* __restrict__ b, int np, double coef, const Globals& G) {
+  // apply_multipole_kicks (magnetic, exact_multipoles = off), track_a_bend.f90:360-397
+  double B1, B2;
+  ab_field(p, b + SB_FIXED, np, b[11], B1, B2);
+  double f_coef = coef * G.charge * (1 + b[1] * p.x) * kCLight / G.p0c;
+  p.px = p.px - f_coef * B2;
+  p.py = p.py + f_coef * B1;
+}
+
+BG_HD void body_bend(Particle& p, const EleHdr& h, const double* __restrict__ b, const Globals& G) {
+  // track_a_bend, bmad/low_level/track_a_bend.f90:18-333
+  const int np = h.n_pole;
+  const double* mis = b + SB_FIXED + 2 * np;
+  if (h.flags & F_MISALIGN) tilt(p, mis[2], mis[3]);   // ref_tilt, offset_particle.f90:263-266
+  if (h.flags & F_EDGE_IN) hwang_edge(p, b + SB_EDGE_IN, true);
+  if (orbit_too_large(p, G)) return;
+  if (np) bend_kick(p, b, np, 0.5, G);
+  for (int n = 1; n <= h.n_step; n++) {
+    if (h.flags & F_BEND_K1) {
+      bend_k1_step(p, b);
+      p.z = p.z + low_energy_z(p, b[0], G);
+    } else if (h.flags & F_BEND_DRIFT) {
+      drift(p, b[0]);
+    } else {
+      if (!bend_exact_step(p, b, G)) return;
+    }
+    if (np) bend_kick(p, b, np, n == h.n_step ? 0.5 : 1.0, G);
+  }
+  if (orbit_too_large(p, G)) return;
+  if (h.flags & F_EDGE_OUT) hwang_edge(p, b + SB_EDGE_OUT, false);
+  if (h.flags & F_MISALIGN) tilt(p, mis[2], -mis[3]);
+}
+
+BG_HD void body_thin(Particle& p, const EleHdr& h, const double* __restrict__ b) {
+  // multipole / ab_multipole, track1_bmad.f90:142-166 with multipole_kicks (multipole_mod.f90:32-51).
+  // Block: per order n < n_pole: [knl, cos(tilt), sin(tilt), tilt == 0]; then misalign.
+  const int np = h.n_pole;
+  const double* mis = b + 4 * np;
+  if (h.flags & F_MISALIGN) offset_set(p, mis, false);
+  for (int n = 0; n < np; n++) {
+    const double* q = b + 4 * n;
+    double knl = q[0];
+    if (knl == 0) continue;
+    if (n == 0 && (h.flags & F_REF_ORB_N0)) {  // multipole_mod.f90:250-255
+      double c = q[1], s = q[2];
+      double x = p.x, y = p.y;
+      p.px = p.px + 1.0 * knl * c * p.pz;
+      p.py = p.py + 1.0 * knl * s * p.pz;
+      p.z = p.z - 1.0 * knl * (c * x + s * y);
+      continue;
+    }
+    thin_kick(p, knl, n, q[3] != 0, q[1], q[2]);
+  }
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, false);
+}
+
+BG_HD void body_rf(Particle& p, const EleHdr& h, const double* __restrict__ b, const Globals& G) {
+  // track_a_rfcavity, bmad/low_level/track_a_rfcavity.f90:17-146 (relative time tracking)
+  const int np = h.n_pole;
+  const double* kh = b + RF_FIXED;
+  const double* mis = kh + 2 * np;
+  const bool has_t = h.flags & F_TILT;
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
+  if (np) ab_kicks(p, kh, np);
+  const double voltage = b[0], f = b[1], slice_len = b[4];
+  const int n_slice = h.n_step;
+  double phase = rf_phase(p, b[2], f, b[3]);
+  for (int i = 0; i <= n_slice; i++) {
+    double dE = 1.0 * voltage * sin(phase) / n_slice;
+    if (i == 0 || i == n_slice) dE = dE / 2;
+    energy_kick(p, dE, G);
+    if (p.pz == -1) {
+      p.state = S_LOST_PZ;
+      return;
+    }
+    if (i != n_slice) {
+      refresh(p, G);
+      double z = p.z;
+      drift(p, slice_len);
+      phase = phase + kTwoPi * f * (p.z - z) / (kCLight * p.beta);
+    }
+  }
+  refresh(p, G);
+  if (np) ab_kicks(p, kh, np);
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
+}
+
+// track1 around one element: entrance orbit/aperture checks, body, exit checks
+// (track1.f90:179-196, 221-236, 289-329). Returns 0 if the particle survived, else its
+// coord%location at the loss. The entrance orbit_too_large test repeats the previous element's
+// exit test on unchanged coordinates, so it runs only for the first element of a launch.
+BG_HD int track1(Particle& p, const EleHdr& h, const double* __restrict__ pool,
+                                      const ApRec* __restrict__ ap, const Globals& G, bool entry_check) {
+  if (entry_check && orbit_too_large(p, G)) return L_UPSTREAM;
+  if (h.flags & F_AP_ENTRANCE) {
+    aperture(p, ap[h.ap_index], h.flags & F_AP_ELLIPTICAL);
+    if (p.state != S_ALIVE) return L_UPSTREAM;
+  }
+  const double* b = pool + h.param;
+  switch (h.kind) {
+    case K_DRIFT: drift(p, b[0]); break;
+    case K_QUAD: body_quad(p, h, b, G); break;
+    case K_THICK: body_thick(p, h, b); break;
+    case K_SBEND: body_bend(p, h, b, G); break;
+    case K_THIN: body_thin(p, h, b); break;
+    case K_RFCAV: body_rf(p, h, b, G); break;
+    default: break;  // K_MARKER
+  }
+  if (orbit_too_large(p, G)) return L_UPSTREAM;
+  if (p.state != S_ALIVE) return L_INSIDE;
+  if (h.flags & F_AP_EXIT) {
+    aperture(p, ap[h.ap_index], h.flags & F_AP_ELLIPTICAL);
+    if (p.state != S_ALIVE) return L_DOWNSTREAM;
+  }
+  return 0;
+}
+
+}  // namespace bmadgpu

@@ -169,6 +169,18 @@ void tilt_ab(double tilt, double* a, double* b, int ix_pole_max) {
   }
 }
 
+// multipole1_ab_to_kt, bmad/low_level/multipole1_ab_to_kt.f90:17
+void ab_to_kt(double an, double bn, int n, double* knl, double* tn) {
+  if (an == 0 && bn == 0) { *knl = 0; *tn = 0; return; }
+  *knl = factorial(n) * std::sqrt(an * an + bn * bn);
+  *tn = -std::atan2(an, bn) / (n + 1);
+  if (2 * (n + 1) * std::fabs(*tn) > kPi) {
+    *knl = -*knl;
+    double sgn = (*tn < 0) ? -1.0 : 1.0;
+    *tn = sgn * (std::fabs(*tn) - kPi / (n + 1));
+  }
+}
+
 // pull_this_b1 (multipole_ele_to_ab.f90:664-676)
 double pull_b1(double* a, double* b, int* ix_pole_max) {
   double b1 = b[1];
@@ -286,6 +298,33 @@ void push_kicks(std::vector<double>& blk, const double* a, const double* b, int 
 
 }  // namespace
 
+void build_cmulti_tables(double cm[22][22], double cf[22][22]) {
+  // c_multi.f90:38-63: binomials normalised by n!, sign - for m mod 4 in {0, 3}
+  double c[22][22], nf[22];
+  for (int i = 0; i < 22; i++)
+    for (int j = 0; j < 22; j++) c[i][j] = 0;
+  c[0][0] = 1;
+  for (int in = 1; in < 22; in++) {
+    c[in][0] = 1;
+    c[in][in] = 1;
+    for (int im = 1; im <= in - 1; im++) c[in][im] = c[in - 1][im - 1] + c[in - 1][im];
+  }
+  nf[0] = 1;
+  for (int in = 0; in < 22; in++) {
+    if (in > 0) nf[in] = in * nf[in - 1];
+    for (int im = 0; im <= in; im++) {
+      c[in][im] = c[in][im] / nf[in];
+      if (im % 4 == 0) c[in][im] = -c[in][im];
+      if (im % 4 == 3) c[in][im] = -c[in][im];
+    }
+  }
+  for (int i = 0; i < 22; i++)
+    for (int j = 0; j < 22; j++) {
+      cf[i][j] = c[i][j];
+      cm[i][j] = c[i][j] * nf[i];
+    }
+}
+
 int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p, PackedLattice& out,
                  std::string& err) {
   try {
@@ -387,8 +426,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           if (ix_mag_max > -1) n_step = std::max(nint(std::fabs(e.l) / ds_step), 1);
           double r_step = 1.0 / n_step;
           double step_len = e.l * r_step;
-          double b1_l = (e.l != 0) ? b1 / e.l : 0.0;
-          blk = {b1_l, std::sqrt(std::fabs(b1_l)), step_len};
+          blk = {b1, e.l, step_len};
           if (ix_mag_max > -1) {
             flags |= F_KICKS;
             h.n_pole = (uint8_t)(ix_mag_max + 1);
@@ -445,7 +483,8 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           double angle = g * step_len;
           double gl = g * step_len;
           blk = {step_len, g, g_tot, dg, angle, std::cos(angle), std::sin(angle), sinc0(angle), cosc0(angle),
-                 (gl * gl) * sincc0(angle), (b1 != 0 && e.l != 0) ? b1 / e.l : 0.0, r_step};
+                 (gl * gl) * sincc0(angle), (b1 != 0 && e.l != 0) ? b1 / e.l : 0.0,
+                 r_step * p.p0c / (2.99792458e8 * p.charge)};
           if (b1 != 0) flags |= F_BEND_K1;
           else if ((g == 0 && dg == 0) || step_len == 0) flags |= F_BEND_DRIFT;
           // Hwang edge coefficients (fringe_mod.f90:262-290); bend_edge_kick acts for
@@ -486,40 +525,32 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
         }
         case BMADGPU_MULTIPOLE: case BMADGPU_AB_MULTIPOLE: {  // track1_bmad.f90:142-166
           h.kind = K_THIN;
-          double knl0 = 0, c0 = 1, s0 = 0;
-          mag_ab(e, tilt_tot, 0, a, b, &ix_mag_max);
-          if (key == BMADGPU_AB_MULTIPOLE) {
-            tilt_ab(tilt_tot, a, b, ix_mag_max);
+          double knl[kNPole], tn[kNPole];
+          for (int n = 0; n < kNPole; n++) { knl[n] = 0; tn[n] = 0; }
+          if (key == BMADGPU_MULTIPOLE) {
+            // multipole_ele_to_kt.f90: knl = knl_pole, tilt = tilt_pole + tilt_tot
+            for (int n = 0; n < kNPole; n++) { knl[n] = e.a_pole[n]; tn[n] = e.b_pole[n] + tilt_tot; }
+            if (e.a_pole[0] != 0) flags |= F_REF_ORB_N0;
           } else {
-            // multipole_ele_to_kt: tilt(n) = tn + tilt_tot; redo the kt -> ab conversion with it
-            for (int n = 0; n < kNPole; n++) {
-              a[n] = 0;
-              b[n] = 0;
-              double knl = e.a_pole[n], tn = e.b_pole[n] + tilt_tot;
-              if (knl == 0) continue;
-              if (n == 0) {
-                knl0 = knl;
-                if (tn != 0) { c0 = std::cos(tn); s0 = std::sin(tn); }
-                flags |= F_REF_ORB_N0;
-                continue;
-              }
-              double angle = -tn * (n + 1);
-              b[n] = knl * std::cos(angle) / factorial(n);
-              a[n] = knl * std::sin(angle) / factorial(n);
-            }
-            ix_mag_max = max_nonzero(a, b, kNPole - 1);
+            // multipole_ele_to_ab(use_ele_tilt = T) then multipole_ab_to_kt
+            mag_ab(e, tilt_tot, 0, a, b, &ix_mag_max);
+            tilt_ab(tilt_tot, a, b, ix_mag_max);
+            if (ix_mag_max > -1)
+              for (int n = 0; n < kNPole; n++) ab_to_kt(a[n], b[n], n, &knl[n], &tn[n]);
           }
-          blk = {knl0, c0, s0};
-          if (ix_mag_max > -1) {
-            flags |= F_KICKS;
-            h.n_pole = (uint8_t)(ix_mag_max + 1);
-            push_kicks(blk, a, b, ix_mag_max + 1, 1.0);
+          int top = -1;
+          for (int n = 0; n < kNPole; n++)
+            if (knl[n] != 0) top = n;
+          blk.clear();
+          for (int n = 0; n <= top; n++) {
+            bool tz = (tn[n] == 0);
+            blk.insert(blk.end(), {knl[n], tz ? 1.0 : std::cos(tn[n]), tz ? 0.0 : std::sin(tn[n]), tz ? 1.0 : 0.0});
           }
-          if (e.tilt != 0 || e.x_offset != 0 || e.y_offset != 0) {
-            if (e.x_offset != 0 || e.y_offset != 0) {
-              mis = {e.x_offset, e.y_offset, 1.0, 0.0};  // set_tilt = .false.
-              flags |= F_MISALIGN;
-            }
+          if (top >= 0) flags |= F_KICKS;
+          h.n_pole = (uint8_t)(top + 1);
+          if (e.x_offset != 0 || e.y_offset != 0) {
+            mis = {e.x_offset, e.y_offset, 1.0, 0.0};  // offset_particle with set_tilt = .false.
+            flags |= F_MISALIGN;
           }
           break;
         }

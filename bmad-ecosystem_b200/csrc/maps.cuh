@@ -1,66 +1,91 @@
 // maps.cuh -- FP64 device maps of Bmad's bmad_standard tracking, one particle per thread.
 //
-// Each function restates one reference routine (cited) on a particle held in registers. The
-// element invariants come precomputed from the packed table (lattice.cpp). Quantities that
-// depend on the particle only through pz (1/(1+pz), the drift's reference-motion term, the
-// low-energy z-correction slope) are cached in the particle and refreshed when the energy
-// changes, instead of being recomputed in every element as the reference does. Where an
-// identity replaces a transcendental (the exact bend), the comment says so; results agree with
-// the reference's operation order to rounding (tested against the oracle to 1e-12).
+// Each function restates one reference routine (cited) on a particle held in registers, with
+// the reference's operand order: in long-term tracking, rounding that differs systematically
+// from the reference (a product regrouped around near-constant factors rounds the same way for
+// every particle and every element) accumulates coherently turn after turn. Element invariants
+// that the reference recomputes from element attributes alone come precomputed from the packed
+// table with the same expressions, hence bit-identical. Functions of pz alone that the reference
+// recomputes per element with the same expression are cached in the particle (refresh()).
+// The kernels are compiled without FMA contraction, so on the device the results differ from the
+// reference only through the device libm (sin, cos, asin, atan2, sinh, cosh).
 #pragma once
+#include <math.h>
 #include <stdint.h>
 
 #include "table.h"
+
+// The maps compile for the device (the product) and, for the test-only host check build
+// (hostcheck.cpp: op counting and algorithm checks on CPU), for the host.
+#if defined(__CUDACC__)
+#define BG_HD __host__ __device__ __forceinline__
+#else
+#define BG_HD inline
+#endif
 
 namespace bmadgpu {
 
 constexpr double kPi = 3.141592653589793238462643383279;
 constexpr double kTwoPi = 2 * kPi;
 constexpr double kCLight = 2.99792458e8;
+constexpr int kNPole = 22;
 
 enum : int { S_ALIVE = 1, S_LOST = 2, S_NEG_X = 3, S_POS_X = 4, S_NEG_Y = 5, S_POS_Y = 6, S_LOST_PZ = 8 };
 enum : int { L_UPSTREAM = 1, L_DOWNSTREAM = 2, L_INSIDE = 3 };
 
-struct Globals {            // branch constants (lat_param_struct / bmad_com)
-  double p0c, e_tot, mass, beta0, max_ap;
-  double mass2;             // mass^2
-  double lez_f, me2;        // low_energy_z_correction: beta0^2 (2 beta0^2 - (m/E)^2/2), (m/E)^2
-  double lez_thresh;        // 3e-7 * e_tot
-};
+
+// Signed binomial tables of c_multi.f90:38-63: c(n,m) (c_full) and c(n,m) * n! (no_n_fact = T),
+// built on the host with the reference's operation sequence and uploaded once per device.
+#if defined(__CUDACC__)
+__constant__ double c_cmulti[kNPole][kNPole];
+__constant__ double c_cfull[kNPole][kNPole];
+#define BG_CMULTI(n, m) c_cmulti[n][m]
+#define BG_CFULL(n, m) c_cfull[n][m]
+#else
+extern double h_cmulti[kNPole][kNPole];
+extern double h_cfull[kNPole][kNPole];
+#define BG_CMULTI(n, m) h_cmulti[n][m]
+#define BG_CFULL(n, m) h_cfull[n][m]
+#endif
 
 struct Particle {
   double x, px, y, py, z, pz, beta;
   int state;
-  // cached functions of pz (and beta), refreshed by refresh()
-  double inv_rel;           // 1 / (1 + pz)
-  double dzb;               // sqrt_one(m^2 (2 pz + pz^2) / ((p0c (1+pz))^2 + m^2)) = beta/beta_ref - 1
-  double sq_inv;            // sqrt(1 / (1 + pz))
-  double lez;               // low_energy_z_correction per unit length
+  // functions of pz (and beta) the reference evaluates with the same expression in each
+  // element; refreshed by refresh() whenever pz or beta change
+  double dzb;               // sqrt_one(mc2**2 (2 pz + pz**2) / ((p0c (1+pz))**2 + mc2**2))  (drift dz)
+  double e_factor;          // 1 / (1 + pz)                                                  (hwang edge)
+  double lez_a;             // 1 - 3 (pz beta0**2)/2 + pz**2 f   or  beta - beta0           (low-energy dz)
+  bool lez_series;          // series branch of low_energy_z_correction
 };
 
-__device__ __forceinline__ double sqrt_one(double x) {  // sim_utils/special_functions/sqrt_one.f90
+BG_HD double sqrt_one(double x) {  // sim_utils/special_functions/sqrt_one.f90
   double sq = sqrt(1 + x);
-  return x / (sq + 1);
+  double rad = sq + 1;
+  return x / rad;
 }
 
-__device__ __forceinline__ void refresh(Particle& p, const Globals& g) {
-  double rel = 1 + p.pz;
-  p.inv_rel = 1.0 / rel;
-  double pr = g.p0c * rel;
-  p.dzb = sqrt_one((g.mass2 * (2 * p.pz + p.pz * p.pz)) / (pr * pr + g.mass2));
-  p.sq_inv = sqrt(p.inv_rel);
+BG_HD void refresh(Particle& p, const Globals& g) {
+  double delta = p.pz;
+  double rel_pc = 1 + delta;
+  double pr = g.p0c * rel_pc;
+  p.dzb = sqrt_one((g.mass2 * (2 * delta + delta * delta)) / (pr * pr + g.mass2));
+  p.e_factor = 1 / (1 + p.pz);
   // low_energy_z_correction.f90:43-52
   double b0pz = g.beta0 * p.pz;
-  if (g.mass * (b0pz * b0pz) < g.lez_thresh) {
-    double b02 = g.beta0 * g.beta0;
-    p.lez = p.pz * (1 - 3 * (p.pz * b02) / 2 + (p.pz * p.pz) * g.lez_f) * g.me2;
-  } else {
-    p.lez = (p.beta - g.beta0) / g.beta0;
-  }
+  p.lez_series = g.mass * (b0pz * b0pz) < g.lez_thresh;
+  if (p.lez_series) p.lez_a = 1 - 3 * (p.pz * g.lez_b02) / 2 + (p.pz * p.pz) * g.lez_f;
+  else p.lez_a = p.beta - g.beta0;
+}
+
+// low_energy_z_correction, bmad/low_level/low_energy_z_correction.f90:22-57
+BG_HD double low_energy_z(const Particle& p, double ds, const Globals& g) {
+  if (p.lez_series) return ds * p.pz * p.lez_a * g.lez_me2;
+  return ds * p.lez_a / g.beta0;
 }
 
 // orbit_too_large, bmad/low_level/orbit_too_large.f90:26-120
-__device__ __forceinline__ bool orbit_too_large(Particle& p, const Globals& g) {
+BG_HD bool orbit_too_large(Particle& p, const Globals& g) {
   if (p.x > g.max_ap) { p.state = S_POS_X; return true; }
   if (-p.x > g.max_ap) { p.state = S_NEG_X; return true; }
   if (p.y > g.max_ap) { p.state = S_POS_Y; return true; }
@@ -76,14 +101,14 @@ __device__ __forceinline__ bool orbit_too_large(Particle& p, const Globals& g) {
   return false;
 }
 
-// check_aperture_limit (rectangular / elliptical branch), check_aperture_limit.f90:286-324
-__device__ __forceinline__ void aperture(Particle& p, const ApRec& a, bool elliptical) {
+// check_aperture_limit (rectangular / elliptical branch), check_aperture_limit.f90:256-324
+BG_HD void aperture(Particle& p, const ApRec& a, bool elliptical) {
   double xp = p.x, yp = p.y;
   if (elliptical) {
     double rx = xp / a.x2_lim, ry = yp / a.y2_lim;
     double r = rx * rx + ry * ry;
     if (r < 1) return;
-    if (fabs(rx) > fabs(ry)) p.state = (xp > 0) ? S_POS_X : S_NEG_X;
+    if (fabs(xp / a.x2_lim) > fabs(yp / a.y2_lim)) p.state = (xp > 0) ? S_POS_X : S_NEG_X;
     else p.state = (yp > 0) ? S_POS_Y : S_NEG_Y;
     return;
   }
@@ -109,70 +134,138 @@ __device__ __forceinline__ void aperture(Particle& p, const ApRec& a, bool ellip
   }
 }
 
-// track_a_drift, bmad/low_level/track_a_drift.f90:25-116 (direction = +1, with ref. motion).
-// sqrt_one(-pxy2)/ps = -pxy2 / (ps (1 + ps)); the first z term is the cached p.dzb.
-__device__ __forceinline__ void drift(Particle& p, double L) {
-  if (L == 0) return;
-  double px_rel = p.px * p.inv_rel;
-  double py_rel = p.py * p.inv_rel;
+// track_a_drift, bmad/low_level/track_a_drift.f90:25-116 (direction = +1, with reference
+// motion). sqrt(1 + (-pxy2)) equals ps_rel exactly, so sqrt_one(-pxy2) reuses it.
+BG_HD void drift(Particle& p, double length) {
+  if (length == 0) return;
+  double rel_pc = 1 + p.pz;
+  double px_rel = p.px / rel_pc;
+  double py_rel = p.py / rel_pc;
   double pxy2 = px_rel * px_rel + py_rel * py_rel;
   if (pxy2 >= 1) { p.state = S_LOST_PZ; return; }
-  double ps = sqrt(1 - pxy2);
-  double r = 1.0 / (ps * (1 + ps));
-  double inv_ps = (1 + ps) * r;
-  p.x = p.x + L * px_rel * inv_ps;
-  p.y = p.y + L * py_rel * inv_ps;
-  double dz = (p.beta > 0) ? L * (p.dzb - pxy2 * r) : L * (1 - inv_ps);
+  double ps_rel = sqrt(1 - pxy2);
+  p.x = p.x + length * px_rel / ps_rel;
+  p.y = p.y + length * py_rel / ps_rel;
+  double dz;
+  if (p.beta > 0) {
+    double so = -pxy2 / (ps_rel + 1);  // sqrt_one(-pxy2)
+    dz = length * (p.dzb + so / ps_rel);
+  } else {
+    dz = length * (1 - 1 / ps_rel);
+  }
   p.z = p.z + dz;
 }
 
-// Drift without reference motion (offset_particle.f90:279-282, include_ref_motion = F).
-__device__ __forceinline__ void drift_no_ref(Particle& p, double L) {
-  double px_rel = p.px * p.inv_rel, py_rel = p.py * p.inv_rel;
-  double pxy2 = px_rel * px_rel + py_rel * py_rel;
-  if (pxy2 >= 1) { p.state = S_LOST_PZ; return; }
-  double ps = sqrt(1 - pxy2);
-  p.x = p.x + L * px_rel / ps;
-  p.y = p.y + L * py_rel / ps;
-  p.z = p.z - L / ps;
-}
-
-// Sum of ab_multipole_kick over n < n_pole (multipole_mod.f90:314-401) as one complex Horner
-// evaluation: kx - i ky = -sum_n (b_n + i a_n) (x + i y)^n. c = [(b_0, a_0), (b_1, a_1), ...].
-__device__ __forceinline__ void multipole_kick_sum(const double* __restrict__ c, int n_pole, double x, double y,
-                                                   double& kx, double& ky) {
-  double pr = c[2 * (n_pole - 1)], pi = c[2 * (n_pole - 1) + 1];
-  for (int n = n_pole - 2; n >= 0; n--) {
-    double nr = pr * x - pi * y + c[2 * n];
-    double ni = pr * y + pi * x + c[2 * n + 1];
-    pr = nr;
-    pi = ni;
+// x**m for a run-time integer m by binary powering (the lowering gfortran uses), mexp.f90
+BG_HD double mexp(double x, int m) {
+  if (m < 0) return 0;
+  if (m == 0) return 1;
+  unsigned n = (unsigned)m;
+  double y = (n % 2) ? x : 1;
+  while (n >>= 1) {
+    x = x * x;
+    if (n % 2) y = y * x;
   }
-  kx = -pr;
-  ky = pi;
+  return y;
 }
 
-// ab_multipole_kicks (multipole_mod.f90:82-121), magnetic, coefficients pre-scaled.
-__device__ __forceinline__ void kicks(Particle& p, const double* __restrict__ c, int n_pole) {
-  double kx, ky;
-  multipole_kick_sum(c, n_pole, p.x, p.y, kx, ky);
-  p.px = p.px + kx;
-  p.py = p.py + ky;
+// ab_multipole_kicks (multipole_mod.f90:82-121), magnetic, with ab_multipole_kick
+// (multipole_mod.f90:314-376) for each order. c: (b_n * scale, a_n * scale), n < n_pole.
+BG_HD void ab_kicks(Particle& p, const double* __restrict__ c, int n_pole) {
+  double kx_tot = 0, ky_tot = 0;
+  const double x = p.x, y = p.y;
+  for (int n = 0; n < n_pole; n++) {
+    const double b2 = c[2 * n], a2 = c[2 * n + 1];
+    double kx = 0, ky = 0;
+    if (!(a2 == 0 && b2 == 0)) {
+      for (int m = 0; m <= n; m += 2) {
+        double f = BG_CMULTI(n, m) * mexp(x, n - m) * mexp(y, m);
+        kx = kx + b2 * f;
+        ky = ky - a2 * f;
+      }
+      for (int m = 1; m <= n; m += 2) {
+        double f = BG_CMULTI(n, m) * mexp(x, n - m) * mexp(y, m);
+        kx = kx + a2 * f;
+        ky = ky + b2 * f;
+      }
+    }
+    kx_tot = kx_tot + kx;
+    ky_tot = ky_tot + ky;
+  }
+  p.px = p.px + kx_tot;
+  p.py = p.py + ky_tot;
 }
 
-// tilt_coords, bmad/code/tilt_coords.f90:18-53 (cos/sin precomputed)
-__device__ __forceinline__ void tilt(Particle& p, double c, double s) {
+// Unscaled ab_multipole_kick sums for the bend field (ele_orientation = 0), track_a_bend.f90:366-379.
+BG_HD void ab_field(const Particle& p, const double* __restrict__ c, int n_pole, double f_p0c, double& B1,
+                    double& B2) {
+  B1 = 0;
+  B2 = 0;
+  const double x = p.x, y = p.y;
+  for (int n = 0; n < n_pole; n++) {
+    const double b = c[2 * n], a = c[2 * n + 1];
+    if (a == 0 && b == 0) continue;
+    double kx = 0, ky = 0;
+    for (int m = 0; m <= n; m += 2) {
+      double f = BG_CMULTI(n, m) * mexp(x, n - m) * mexp(y, m);
+      kx = kx + b * f;
+      ky = ky - a * f;
+    }
+    for (int m = 1; m <= n; m += 2) {
+      double f = BG_CMULTI(n, m) * mexp(x, n - m) * mexp(y, m);
+      kx = kx + a * f;
+      ky = ky + b * f;
+    }
+    B1 = B1 + f_p0c * ky;
+    B2 = B2 - f_p0c * kx;
+  }
+}
+
+// multipole_kick (multipole_mod.f90:203-286), magnetic, n >= 1, tilt given by cos/sin (t_zero
+// when the tilt is exactly zero).
+BG_HD void thin_kick(Particle& p, double knl, int n, bool t_zero, double cos_ang, double sin_ang) {
+  double x, y;
+  if (t_zero) {
+    x = p.x;
+    y = p.y;
+  } else {
+    x = p.x * cos_ang + p.y * sin_ang;
+    y = -p.x * sin_ang + p.y * cos_ang;
+  }
+  double x_terms[kNPole], y_terms[kNPole];
+  x_terms[n] = 1.0;
+  y_terms[0] = 1.0;
+  for (int m = 1; m <= n; m++) {
+    x_terms[n - m] = x_terms[n - m + 1] * x;
+    y_terms[m] = y_terms[m - 1] * y;
+  }
+  double x_value = 0, y_value = 0;
+  for (int m = 0; m <= n; m += 2) x_value = x_value + BG_CFULL(n, m) * x_terms[m] * y_terms[m];
+  for (int m = 1; m <= n; m += 2) y_value = y_value + BG_CFULL(n, m) * x_terms[m] * y_terms[m];
+  double x_vel = 1.0 * knl * x_value;
+  double y_vel = 1.0 * knl * y_value;
+  if (t_zero) {
+    p.px = p.px + x_vel;
+    p.py = p.py + y_vel;
+  } else {
+    p.px = p.px + x_vel * cos_ang - y_vel * sin_ang;
+    p.py = p.py + x_vel * sin_ang + y_vel * cos_ang;
+  }
+}
+
+// tilt_coords, bmad/code/tilt_coords.f90:18-53 (cos/sin precomputed; Fortran matmul order)
+BG_HD void tilt(Particle& p, double c, double s) {
   double x = p.x, y = p.y, px = p.px, py = p.py;
-  p.x = c * x + s * y;
-  p.y = -s * x + c * y;
-  p.px = c * px + s * py;
-  p.py = -s * px + c * py;
+  p.x = (0 + c * x) + s * y;
+  p.y = (0 + -s * x) + c * y;
+  p.px = (0 + c * px) + s * py;
+  p.py = (0 + -s * px) + c * py;
 }
 
-// offset_particle set/unset for straight elements with x/y offsets and tilt
-// (offset_particle.f90:201-330, 374-459 with zero pitches and z_offset: the transforms reduce to
-// exact shifts plus the pz-loss test).
-__device__ __forceinline__ void offset_set(Particle& p, const double* __restrict__ m, bool has_tilt) {
+// offset_particle set/unset for straight elements with x/y offsets and tilt, no pitches or
+// z_offset (offset_particle.f90:201-330, 374-459): the transforms reduce to exact shifts, the
+// pz-loss test and tilt_coords; no drift to the edge is needed (s_body = s_target).
+BG_HD void offset_set(Particle& p, const double* __restrict__ m, bool has_tilt) {
   if (m[0] != 0 || m[1] != 0) {
     p.x = p.x - m[0];
     p.y = p.y - m[1];
@@ -181,7 +274,7 @@ __device__ __forceinline__ void offset_set(Particle& p, const double* __restrict
   }
   if (has_tilt) tilt(p, m[2], m[3]);
 }
-__device__ __forceinline__ void offset_unset(Particle& p, const double* __restrict__ m, bool has_tilt) {
+BG_HD void offset_unset(Particle& p, const double* __restrict__ m, bool has_tilt) {
   if (has_tilt) tilt(p, m[2], -m[3]);
   if (m[0] != 0 || m[1] != 0) {
     double rel_p = 1 + p.pz;
@@ -191,57 +284,54 @@ __device__ __forceinline__ void offset_unset(Particle& p, const double* __restri
   }
 }
 
-// sinh and cosh of a non-negative argument from one expm1.
-__device__ __forceinline__ void sinh_cosh(double a, double& sh, double& ch) {
-  double em = expm1(a);
-  double ep = em + 1;
-  double inv = 1.0 / ep;
-  sh = 0.5 * em * (1 + inv);
-  ch = 1 + 0.5 * em * em * inv;
+// quad_mat2_calc, bmad/low_level/quad_mat2_calc.f90:22-61 (mat2 and z_coef)
+BG_HD void quad_mat2(double k1, double length, double rel_p, double& m11, double& m12, double& m21,
+                     double& m22, double& z0, double& z1, double& z2) {
+  double sqrt_k = sqrt(fabs(k1));
+  double sk_l = sqrt_k * length;
+  double cx, sx;
+  if (fabs(sk_l) < 1e-10) {
+    double k_l2 = k1 * (length * length);
+    cx = 1 + k_l2 / 2;
+    sx = (1 + k_l2 / 6) * length;
+  } else if (k1 < 0) {
+    cx = cos(sk_l);
+    sx = sin(sk_l) / sqrt_k;
+  } else {
+    cx = cosh(sk_l);
+    sx = sinh(sk_l) / sqrt_k;
+  }
+  m11 = cx;
+  m12 = sx / rel_p;
+  m21 = k1 * sx * rel_p;
+  m22 = cx;
+  z0 = k1 * (-cx * sx + length) / 4;
+  z1 = -k1 * (sx * sx) / (2 * rel_p);
+  z2 = -(cx * sx + length) / (4 * (rel_p * rel_p));
 }
 
-// One body step of track_a_quadrupole (track_a_quadrupole.f90:95-120) with quad_mat2_calc
-// (quad_mat2_calc.f90:22-61) for both planes. b1_l = b1/L, sqrt_bl = sqrt(|b1/L|).
-__device__ __forceinline__ void quad_step(Particle& p, double b1_l, double sqrt_bl, double step_len) {
-  double k1 = b1_l * p.inv_rel;             // k1 = b1 / (L (1 + pz))
-  double sqrt_k = sqrt_bl * p.sq_inv;
-  double sk_l = sqrt_k * step_len;
-  double cx, sx, cy, sy;                    // x plane uses -k1, y plane +k1
-  if (fabs(sk_l) < 1e-10) {
-    double k_l2 = k1 * (step_len * step_len);
-    cx = 1 - k_l2 / 2;
-    sx = (1 - k_l2 / 6) * step_len;
-    cy = 1 + k_l2 / 2;
-    sy = (1 + k_l2 / 6) * step_len;
-  } else {
-    double st, ct, sh, ch;
-    sincos(sk_l, &st, &ct);
-    sinh_cosh(sk_l, sh, ch);
-    double inv_sk = 1.0 / sqrt_k;
-    if (k1 > 0) {           // x focusing (-k1 < 0), y defocusing
-      cx = ct; sx = st * inv_sk; cy = ch; sy = sh * inv_sk;
-    } else {
-      cx = ch; sx = sh * inv_sk; cy = ct; sy = st * inv_sk;
-    }
-  }
-  double ir = p.inv_rel;
-  double ir2 = ir * ir;
-  double zx0 = -k1 * (-cx * sx + step_len) / 4, zx1 = k1 * (sx * sx) * ir / 2, zx2 = -(cx * sx + step_len) * ir2 / 4;
-  double zy0 = k1 * (-cy * sy + step_len) / 4, zy1 = -k1 * (sy * sy) * ir / 2, zy2 = -(cy * sy + step_len) * ir2 / 4;
+// One body step of track_a_quadrupole (track_a_quadrupole.f90:95-120); b1 and length are the
+// element's (charge_dir = 1).
+BG_HD void quad_step(Particle& p, double b1, double length, double step_len, const Globals& G) {
+  double rel_p = 1 + p.pz;
+  double k1 = b1 / (length * rel_p);
+  double ax, bx, cx_, dx, zx0, zx1, zx2, ay, by, cy, dy, zy0, zy1, zy2;
+  quad_mat2(-k1, step_len, rel_p, ax, bx, cx_, dx, zx0, zx1, zx2);
+  quad_mat2(k1, step_len, rel_p, ay, by, cy, dy, zy0, zy1, zy2);
   double x = p.x, px = p.px, y = p.y, py = p.py;
   p.z = p.z + (zx0 * (x * x) + zx1 * x * px + zx2 * (px * px) + zy0 * (y * y) + zy1 * y * py + zy2 * (py * py));
-  p.x = cx * x + sx * ir * px;
-  p.px = -b1_l * sx * x + cx * px;          // mat2(2,1) = k sx rel_p with k = -k1
-  p.y = cy * y + sy * ir * py;
-  p.py = b1_l * sy * y + cy * py;
-  p.z = p.z + step_len * p.lez;
+  p.x = (0 + ax * x) + bx * px;
+  p.px = (0 + cx_ * x) + dx * px;
+  p.y = (0 + ay * y) + by * py;
+  p.py = (0 + cy * y) + dy * py;
+  p.z = p.z + low_energy_z(p, step_len, G);
 }
 
 // hwang_bend_edge_kick, bmad/modules/fringe_mod.f90:241-419 (time_dir = +1).
-// e: [gt, gt2, gs2, k1_tane, fg_factor, g_tot, gt*g_tot*(1 + 2 tan_e^2)]
-__device__ __forceinline__ void hwang_edge(Particle& p, const double* __restrict__ e, bool entering) {
+// e: [gt, gt2, gs2, k1_tane, fg_factor, g_tot, gt*g_tot*(1 + 2 tan_e**2)]
+BG_HD void hwang_edge(Particle& p, const double* __restrict__ e, bool entering) {
   double gt = e[0], gt2 = e[1], gs2 = e[2], k1t = e[3], fg = e[4], gtot = e[5], cdpx = e[6];
-  double ef = p.inv_rel;
+  double ef = p.e_factor;
   double v1 = p.x, v2 = p.px, v3 = p.y, v4 = p.py;
   double v11 = v1 * v1, v33 = v3 * v3;
   double dx, dpx, dy, dpy, dz;
@@ -262,40 +352,48 @@ __device__ __forceinline__ void hwang_edge(Particle& p, const double* __restrict
          (v33 * fg + (v11 * v1) * (4.0 * k1t - gt * gt2) / 6.0 + 0.5 * v1 * v33 * (-4.0 * k1t + gt * gs2) -
           (v11 * v2 - 2.0 * v1 * v3 * v4) * gt2 + v2 * v33 * gs2);
   }
-  p.x = v1 + dx;
-  p.px = v2 + (dpx + gt * v1);
-  p.y = v3 + dy;
-  p.py = v4 + (dpy - gt * v3);
-  p.z = p.z + dz;
+  p.x = v1 + 1.0 * dx;
+  p.px = v2 + 1.0 * (dpx + gt * v1);
+  p.y = v3 + 1.0 * dy;
+  p.py = v4 + 1.0 * (dpy - gt * v3);
+  p.z = p.z + 1.0 * dz;
 }
 
-// sbend_body_with_k1_map, track_a_bend.f90:500-659 (ending coordinates only)
-__device__ __forceinline__ void bend_k1_step(Particle& p, const double* __restrict__ b) {
-  double length = b[0], g = b[1], g_tot = b[2], k1 = b[10];   // k1 = b1 / L
+// sbend_body_with_k1_map, track_a_bend.f90:500-659 (ending coordinates only).
+// b: bend parameter block (table.h); k1 = b1 / L in b[10], the step length in b[0].
+BG_HD void bend_k1_step(Particle& p, const double* __restrict__ b) {
+  double length = b[0], g = b[1], g_tot = b[2], k1 = b[10];
   double rel_p = 1 + p.pz, rel_p2 = rel_p * rel_p;
   double k_x = k1 + g * g_tot;
   double x_c = (g * rel_p - g_tot) / k_x;
   double om_x = sqrt(fabs(k_x) / rel_p), om_y = sqrt(fabs(k1) / rel_p);
-  double tau_x = k_x > 0 ? -1.0 : 1.0, tau_y = k1 > 0 ? 1.0 : -1.0;
-  if (k_x == 0) tau_x = -1.0;
-  if (k1 == 0) tau_y = 1.0;
+  double tau_x = (k_x >= 0) ? -1.0 : 1.0, tau_y = (k1 >= 0) ? 1.0 : -1.0;
   double s_x, c_x, z2, s_y, c_y, arg = om_x * length;
   if (arg < 1e-6) {
-    s_x = (1 + tau_x * (arg * arg) / 6) * length; c_x = 1 + tau_x * (arg * arg) / 2; z2 = g * (length * length) / (2 * rel_p);
+    s_x = (1 + tau_x * (arg * arg) / 6) * length;
+    c_x = 1 + tau_x * (arg * arg) / 2;
+    z2 = g * (length * length) / (2 * rel_p);
   } else if (k_x > 0) {
-    double s, c; sincos(arg, &s, &c); s_x = s / om_x; c_x = c; z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
+    s_x = sin(arg) / om_x;
+    c_x = cos(arg);
+    z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
   } else {
-    double s, c; sinh_cosh(arg, s, c); s_x = s / om_x; c_x = c; z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
+    s_x = sinh(arg) / om_x;
+    c_x = cosh(arg);
+    z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
   }
   arg = om_y * length;
   if (arg < 1e-6) {
-    s_y = (1 + tau_y * (arg * arg) / 6) * length; c_y = 1 + tau_y * (arg * arg) / 2;
+    s_y = (1 + tau_y * (arg * arg) / 6) * length;
+    c_y = 1 + tau_y * (arg * arg) / 2;
   } else if (k1 < 0) {
-    double s, c; sincos(arg, &s, &c); s_y = s / om_y; c_y = c;
+    s_y = sin(om_y * length) / om_y;
+    c_y = cos(om_y * length);
   } else {
-    double s, c; sinh_cosh(arg, s, c); s_y = s / om_y; c_y = c;
+    s_y = sinh(om_y * length) / om_y;
+    c_y = cosh(om_y * length);
   }
-  double r1 = p.x - x_c, r2 = p.px, r3 = p.y, r4 = p.py;
+  double r1 = p.x - x_c, r2 = p.px, r3 = p.y, r4 = p.py, r5 = p.z;
   double z0 = -g * x_c * length, z1 = -g * s_x;
   double ox2 = om_x * om_x, oy2 = om_y * om_y;
   double z11 = tau_x * ox2 * (length - c_x * s_x) / 4, z12 = -tau_x * ox2 * (s_x * s_x) / (2 * rel_p);
@@ -306,18 +404,17 @@ __device__ __forceinline__ void bend_k1_step(Particle& p, const double* __restri
   p.px = tau_x * ox2 * rel_p * s_x * r1 + c_x * r2;
   p.y = c_y * r3 + s_y * r4 / rel_p;
   p.py = tau_y * oy2 * rel_p * s_y * r3 + c_y * r4;
-  p.z = p.z + z0 + z1 * r1 + z2 * r2 + z11 * (r1 * r1) + z12 * r1 * r2 + z22 * (r2 * r2) + z33 * (r3 * r3) +
-        z34 * r3 * r4 + z44 * (r4 * r4);
+  p.z = r5 + 1.0 * 1.0 * z0 + z1 * r1 + z2 * r2 + z11 * (r1 * r1) + z12 * r1 * r2 + z22 * (r2 * r2) +
+        z33 * (r3 * r3) + z34 * r3 * r4 + z44 * (r4 * r4);
 }
 
 // Exact sbend body step, track_a_bend.f90:121-209. Returns false if the particle was lost.
-// phi_1 = asin(px/pt) and theta = atan2(L_u, -L_v) enter only through their sines and cosines
-// except in sinc(angle_p/2); angle_p/2 = angle + phi_1 - theta is recovered as asin of its sine.
-__device__ __forceinline__ bool bend_exact_step(Particle& p, const double* __restrict__ b, const Globals& G) {
+BG_HD bool bend_exact_step(Particle& p, const double* __restrict__ b, const Globals& G) {
   double step_len = b[0], g = b[1], g_tot = b[2], dg = b[3], angle = b[4];
   double cos_a = b[5], sin_a = b[6], sinc_a = b[7], cosc_a = b[8], gl2_sincc = b[9];
   double x = p.x, px = p.px, y = p.y, py = p.py, z = p.z, pz = p.pz;
   double rel_p = 1 + pz;
+  double rel_p2 = rel_p * rel_p;
   if (dg == 0 && fabs(x * g) < 1e-9 && fabs(px) < 1e-9 && fabs(py) < 1e-9 && fabs(pz) < 1e-9) {
     // semi-linear map near the zero orbit, track_a_bend.f90:136-159
     double ll = step_len;
@@ -330,16 +427,15 @@ __device__ __forceinline__ bool bend_exact_step(Particle& p, const double* __res
     p.z = -g * ll * sinc_a * x - g * (ll * ll) * cosc_a * px + z + m56 * pz;
     return true;
   }
-  double pt = sqrt(rel_p * rel_p - py * py);
+  double pt = sqrt(rel_p2 - py * py);
   if (fabs(px) > pt) { p.state = S_LOST_PZ; return false; }
-  double inv_pt = 1.0 / pt;
-  double g_p = g_tot * inv_pt;
-  double s1 = px * inv_pt;                        // sin(phi_1)
-  double c1 = sqrt((1 - s1) * (1 + s1));          // cos(phi_1) >= 0
-  double cos_plus = cos_a * c1 - sin_a * s1;      // cos(angle + phi_1)
-  double sin_plus = sin_a * c1 + cos_a * s1;      // sin(angle + phi_1)
-  double ls = (1 + g * x) * step_len * sinc_a;
-  double alpha = 2 * sin_plus * ls - g_p * (ls * ls);
+  double g_p = g_tot / pt;
+  double phi_1 = asin(px / pt);
+  double cos_plus = cos(angle + phi_1);
+  double sin_plus = sin(angle + phi_1);
+  double gx1 = 1 + g * x;
+  double ls = gx1 * step_len * sinc_a;
+  double alpha = 2 * gx1 * sin_plus * step_len * sinc_a - g_p * (ls * ls);
   double r = cos_plus * cos_plus + g_p * alpha;
   if (r < 0 || (fabs(g_p) < 1e-5 && fabs(cos_plus) < 1e-5)) {
     p.state = S_LOST;
@@ -347,52 +443,51 @@ __device__ __forceinline__ bool bend_exact_step(Particle& p, const double* __res
     return false;
   }
   double rad = sqrt(r);
-  double xi = (cos_plus > 0) ? alpha / (rad + cos_plus) : (rad - cos_plus) / g_p;
-  double x_new = x * cos_a - (step_len * step_len) * g * cosc_a + xi;
-  p.x = x_new;
-  if (fabs(x_new) > G.max_ap) { p.state = S_LOST; return false; }
-  double L_u = xi;
-  double L_v = -(step_len * sinc_a + x * sin_a);
-  double L_c = sqrt(L_v * L_v + L_u * L_u);
-  double inv_lc = 1.0 / L_c;
-  double st = L_u * inv_lc, ct = -L_v * inv_lc;   // sin, cos of theta = atan2(L_u, -L_v)
-  double sin_u = sin_plus * ct - cos_plus * st;   // sin(angle_p / 2)
-  double u;
-  if (fabs(sin_u) < 0.7) {
-    u = asin(sin_u);
+  double xi;
+  if (cos_plus > 0) {
+    double denom = rad + cos_plus;
+    xi = alpha / denom;
   } else {
-    u = angle + asin(s1) - atan2(L_u, -L_v);
+    double denom = rad - cos_plus;
+    xi = denom / g_p;
   }
-  double sinc_u = (fabs(u) < 1e-8) ? 1.0 : sin(u) / u;
-  double L_p = L_c / sinc_u;
-  double s2t = 2 * st * ct, c2t = (ct - st) * (ct + st);
-  p.px = pt * (s2t * cos_plus - c2t * sin_plus);  // pt sin(phi_1 + angle - angle_p)
-  p.y = y + py * L_p * inv_pt;
-  p.z = z + p.beta * step_len / G.beta0 - rel_p * L_p * inv_pt;
+  p.x = x * cos_a - (step_len * step_len) * g * cosc_a + xi;
+  if (fabs(p.x) > G.max_ap) { p.state = S_LOST; return false; }
+  double L_u = xi;
+  double L_v = -1 * (step_len * sinc_a + x * sin_a);
+  double L_c = sqrt(L_v * L_v + L_u * L_u);
+  double angle_p = 2 * (angle + phi_1 - 1 * atan2(L_u, -L_v));
+  double hp = angle_p / 2;
+  double L_p = 1 * L_c / ((fabs(hp) < 1e-8) ? 1.0 : sin(hp) / hp);
+  p.px = pt * sin(phi_1 + angle - angle_p);
+  p.y = y + py * L_p / pt;
+  p.z = z + p.beta * step_len / G.beta0 - rel_p * L_p / pt;
   return true;
 }
 
 // apply_energy_kick, bmad/low_level/apply_energy_kick.f90:23-74
-__device__ __forceinline__ void energy_kick(Particle& p, double dE, const Globals& G) {
-  double pc = (1 + p.pz) * G.p0c;
+BG_HD void energy_kick(Particle& p, double dE, const Globals& G) {
+  double mc2 = G.mass;
+  double p0c = G.p0c;
+  double pc = (1 + p.pz) * p0c;
   double beta_old = p.beta;
   double E_old = pc / p.beta;
   double E_new = E_old + dE;
-  if (E_new < G.mass) {
+  if (E_new < mc2) {
     p.pz = -1;
     p.beta = 0;
     p.state = S_LOST_PZ;
     return;
   }
   p.pz = p.pz + (1 + p.pz) * sqrt_one((2 * E_old * dE + dE * dE) / (pc * pc));
-  double pc_new = G.p0c * (1 + p.pz);
+  double pc_new = p0c * (1 + p.pz);
   double beta_new = pc_new / E_new;
   p.z = p.z * beta_new / beta_old;
   p.beta = beta_new;
 }
 
 // modulo2 (sim_utils/special_functions/modulo2_mod.f90:85-100): x + 2 n amp in [-amp, amp)
-__device__ __forceinline__ double modulo2(double x, double amp) {
+BG_HD double modulo2(double x, double amp) {
   double two = 2 * amp;
   double r = fmod(x, two);
   if (r != 0 && ((r < 0) != (two < 0))) r += two;
@@ -400,16 +495,16 @@ __device__ __forceinline__ double modulo2(double x, double amp) {
   return r;
 }
 
-// RF phase of track_a_rfcavity.f90:78-86 with particle_rf_time (relative time). The reference
-// evaluates twopi*(phi0 - t*f) in real(qp) and rounds once; here t*f and the subtraction are
-// carried in double-double so the rounded result matches.
-__device__ __forceinline__ double rf_phase(const Particle& p, double phi0, double f, double twopi_mp) {
+// RF phase of track_a_rfcavity.f90:78-86 with particle_rf_time (particle_rf_time.f90:89, 115).
+// The reference evaluates twopi*(phi0 - t*f) in real(qp) and rounds once; t*f and the
+// subtraction are carried here in double-double (exact product by fma, two-sum), then rounded.
+BG_HD double rf_phase(const Particle& p, double phi0, double f, double twopi_mp) {
   double time = -p.z / (p.beta * kCLight);
   double amp = 0.5 / f;
-  if (!(fabs(time) < amp)) time = modulo2(time, amp);
+  if (!(fabs(time) < amp)) time = modulo2(time, amp);   // qp fold; identity for |t| < 1/(2f)
   double pr = time * f;
   double pe = fma(time, f, -pr);
-  double s = phi0 - pr;                           // two-sum of phi0 and -pr
+  double s = phi0 - pr;
   double bb = s - phi0;
   double err = (phi0 - (s - bb)) + (-pr - bb);
   double lo = err - pe;

@@ -53,14 +53,14 @@ struct ApRec {             // 32 bytes: rectangular/elliptical limits (x1_lim = 
 
 // Parameter block layouts (indices in doubles from EleHdr::param).
 // K_DRIFT:  [0] L
-// K_QUAD:   [0] b1/L  [1] sqrt(|b1/L|)  [2] step_len  then kicks, then misalign
+// K_QUAD:   [0] b1  [1] L  [2] step_len  then kicks, then misalign
 // K_THICK:  [0] step_len  then kicks, then misalign
 // K_SBEND:  [0] step_len [1] g [2] g_tot [3] dg [4] angle [5] cos_a [6] sin_a [7] sinc_a
-//           [8] cosc_a [9] (g step_len)^2 sincc_a [10] k1 = b1/L [11] r_step
+//           [8] cosc_a [9] (g step_len)^2 sincc_a [10] k1 = b1/L [11] f_p0c = r_step p0c/(c q)
 //           [12..18] entrance edge: gt gt2 gs2 k1_tane fg_factor g_tot gt*g_tot*(1+2tan^2)
 //           [19..25] exit edge:     (same)
 //           then kicks (bend form: plain b_n, a_n), then misalign (ref_tilt only: cos, sin)
-// K_THIN:   [0] knl0 [1] cos0 [2] sin0 then kicks (plain b_n, a_n)
+// K_THIN:   per order n < n_pole: [knl, cos(tilt), sin(tilt), tilt == 0], then misalign
 // K_RFCAV:  [0] voltage [1] rf_frequency [2] phi0 [3] twopi*phi0_multipass [4] slice_len
 //           [5] n_slice  then kicks (half kicks 0.5*r_step), then misalign
 // kicks: n_pole pairs for the end (half) kick followed, for K_QUAD/K_THICK, by n_pole pairs for
@@ -78,5 +78,20 @@ struct TableInfo {
   uint32_t total_bytes;    // whole image, 16-aligned
   double turn_ref_time;    // sum of delta_ref_time over the elements
 };
+
+struct Globals {            // branch constants (lat_param_struct / bmad_com) and derived terms
+  double p0c, e_tot, mass, beta0, max_ap;
+  double mass2;             // mass**2
+  double lez_b02;           // beta0**2           (low_energy_z_correction.f90:44)
+  double lez_f;             // beta0**2 * (2 * beta0**2 - (mass / e_tot)**2 / 2)
+  double lez_me2;           // (mass / e_tot)**2
+  double lez_thresh;        // 3d-7 * e_tot
+  double charge;            // charge_of(species)
+};
+
+
+// Signed binomial tables of c_multi.f90:38-63 (cm: no_n_fact = T, cf: c(n,m)), computed with the
+// reference's operation sequence.
+void build_cmulti_tables(double cm[22][22], double cf[22][22]);
 
 }  // namespace bmadgpu

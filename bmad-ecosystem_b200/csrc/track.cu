@@ -15,6 +15,7 @@
 
 #include <cuda_runtime.h>
 
+#include "elements.cuh"
 #include "track.cuh"
 
 namespace bmadgpu {
@@ -62,157 +63,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 __device__ __forceinline__ void load_hdr(const EleHdr* hdr, int i, EleHdr& h) {
   uint4 raw = *reinterpret_cast<const uint4*>(hdr + i);
   h = *reinterpret_cast<const EleHdr*>(&raw);
-}
-
-// ---- element bodies (track1_bmad dispatch, bmad/low_level/track1_bmad.f90:64-272) ----------
-
-__device__ __forceinline__ void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b) {
-  // track_a_quadrupole, bmad/low_level/track_a_quadrupole.f90
-  const int np = h.n_pole;
-  const double* kh = b + 3;
-  const double* kf = kh + 2 * np;
-  const double* mis = b + 3 + 4 * np;
-  const bool has_t = h.flags & F_TILT;
-  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
-  if (np) kicks(p, kh, np);
-  const double b1_l = b[0], sqrt_bl = b[1], step_len = b[2];
-  for (int i = 1; i <= h.n_step; i++) {
-    quad_step(p, b1_l, sqrt_bl, step_len);
-    if (np) kicks(p, i == h.n_step ? kh : kf, np);
-  }
-  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
-}
-
-__device__ __forceinline__ void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b) {
-  // track_a_thick_multipole, bmad/low_level/track_a_thick_multipole.f90:18-133
-  const int np = h.n_pole;
-  const double* kh = b + 1;
-  const double* kf = kh + 2 * np;
-  const double* mis = b + 1 + 4 * np;
-  const bool has_t = h.flags & F_TILT;
-  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
-  if (np) kicks(p, kh, np);
-  const double step_len = b[0];
-  for (int i = 1; i <= h.n_step; i++) {
-    drift(p, step_len);
-    if (np) kicks(p, i == h.n_step ? kh : kf, np);
-  }
-  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
-}
-
-__device__ __forceinline__ void bend_kick(Particle& p, const double* __restrict__ b, int np, double coef) {
-  // apply_multipole_kicks (magnetic, exact_multipoles = off), track_a_bend.f90:338-411:
-  // the field form reduces to coef * r_step * (1 + g x) * (kx, ky).
-  double kx, ky;
-  multipole_kick_sum(b + SB_FIXED, np, p.x, p.y, kx, ky);
-  double f = coef * b[11] * (1 + b[1] * p.x);
-  p.px = p.px + f * kx;
-  p.py = p.py + f * ky;
-}
-
-__device__ __forceinline__ void body_bend(Particle& p, const EleHdr& h, const double* __restrict__ b,
-                                          const Globals& G) {
-  // track_a_bend, bmad/low_level/track_a_bend.f90:18-333
-  const int np = h.n_pole;
-  const double* mis = b + SB_FIXED + 2 * np;
-  if (h.flags & F_MISALIGN) offset_set(p, mis, true);  // ref_tilt rotation
-  if (h.flags & F_EDGE_IN) hwang_edge(p, b + SB_EDGE_IN, true);
-  if (orbit_too_large(p, G)) return;
-  if (np) bend_kick(p, b, np, 0.5);
-  for (int n = 1; n <= h.n_step; n++) {
-    if (h.flags & F_BEND_K1) {
-      bend_k1_step(p, b);
-      p.z = p.z + b[0] * p.lez;
-    } else if (h.flags & F_BEND_DRIFT) {
-      drift(p, b[0]);
-    } else {
-      if (!bend_exact_step(p, b, G)) return;
-    }
-    if (np) bend_kick(p, b, np, n == h.n_step ? 0.5 : 1.0);
-  }
-  if (orbit_too_large(p, G)) return;
-  if (h.flags & F_EDGE_OUT) hwang_edge(p, b + SB_EDGE_OUT, false);
-  if (h.flags & F_MISALIGN) offset_unset(p, mis, true);
-}
-
-__device__ __forceinline__ void body_thin(Particle& p, const EleHdr& h, const double* __restrict__ b) {
-  // multipole / ab_multipole, track1_bmad.f90:142-166 with multipole_kicks (multipole_mod.f90:32-51)
-  const int np = h.n_pole;
-  const double* mis = b + 3 + 2 * np;
-  if (h.flags & F_MISALIGN) offset_set(p, mis, false);
-  if (h.flags & F_REF_ORB_N0) {  // multipole_mod.f90:250-255
-    double knl = b[0], c0 = b[1], s0 = b[2];
-    double x = p.x, y = p.y;
-    p.px = p.px + knl * c0 * p.pz;
-    p.py = p.py + knl * s0 * p.pz;
-    p.z = p.z - knl * (c0 * x + s0 * y);
-  }
-  if (np) kicks(p, b + 3, np);
-  if (h.flags & F_MISALIGN) offset_unset(p, mis, false);
-}
-
-__device__ __forceinline__ void body_rf(Particle& p, const EleHdr& h, const double* __restrict__ b,
-                                        const Globals& G) {
-  // track_a_rfcavity, bmad/low_level/track_a_rfcavity.f90:17-146 (relative time tracking)
-  const int np = h.n_pole;
-  const double* kh = b + RF_FIXED;
-  const double* mis = kh + 2 * np;
-  const bool has_t = h.flags & F_TILT;
-  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
-  if (np) kicks(p, kh, np);
-  const double voltage = b[0], f = b[1], slice_len = b[4];
-  const int n_slice = h.n_step;
-  double phase = rf_phase(p, b[2], f, b[3]);
-  double sin_ph = sin(phase);
-  for (int i = 0; i <= n_slice; i++) {
-    double dE = voltage * sin_ph / n_slice;
-    if (i == 0 || i == n_slice) dE = dE / 2;
-    energy_kick(p, dE, G);
-    if (p.pz == -1) {
-      p.state = S_LOST_PZ;
-      return;
-    }
-    if (i != n_slice) {
-      refresh(p, G);
-      double z0 = p.z;
-      drift(p, slice_len);
-      phase = phase + kTwoPi * f * (p.z - z0) / (kCLight * p.beta);
-      sin_ph = sin(phase);
-    }
-  }
-  refresh(p, G);
-  if (np) kicks(p, kh, np);
-  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
-}
-
-// track1 around one element: entrance orbit/aperture checks, body, exit checks
-// (track1.f90:179-196, 221-236, 289-329). Returns 0 if the particle survived, else its
-// coord%location at the loss. The entrance orbit_too_large test repeats the previous element's
-// exit test on unchanged coordinates, so it runs only for the first element of a launch.
-__device__ __forceinline__ int track1(Particle& p, const EleHdr& h, const double* __restrict__ pool,
-                                      const ApRec* __restrict__ ap, const Globals& G, bool entry_check) {
-  if (entry_check && orbit_too_large(p, G)) return L_UPSTREAM;
-  if (h.flags & F_AP_ENTRANCE) {
-    aperture(p, ap[h.ap_index], h.flags & F_AP_ELLIPTICAL);
-    if (p.state != S_ALIVE) return L_UPSTREAM;
-  }
-  const double* b = pool + h.param;
-  switch (h.kind) {
-    case K_DRIFT: drift(p, b[0]); break;
-    case K_QUAD: body_quad(p, h, b); break;
-    case K_THICK: body_thick(p, h, b); break;
-    case K_SBEND: body_bend(p, h, b, G); break;
-    case K_THIN: body_thin(p, h, b); break;
-    case K_RFCAV: body_rf(p, h, b, G); break;
-    default: break;  // K_MARKER
-  }
-  if (orbit_too_large(p, G)) return L_UPSTREAM;
-  if (p.state != S_ALIVE) return L_INSIDE;
-  if (h.flags & F_AP_EXIT) {
-    aperture(p, ap[h.ap_index], h.flags & F_AP_ELLIPTICAL);
-    if (p.state != S_ALIVE) return L_DOWNSTREAM;
-  }
-  return 0;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -363,6 +213,14 @@ __global__ void k_compact(const int32_t* __restrict__ state, const int32_t* __re
 }  // namespace
 
 int table_fits_smem(uint32_t table_bytes) { return table_bytes <= 200 * 1024; }
+
+cudaError_t upload_constants() {
+  double cm[22][22], cf[22][22];
+  build_cmulti_tables(cm, cf);
+  cudaError_t e = cudaMemcpyToSymbol(c_cmulti, cm, sizeof(cm));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyToSymbol(c_cfull, cf, sizeof(cf));
+}
 
 cudaError_t launch_track(const TrackArgs& a, const LaunchCfg& cfg, int sm_count, cudaStream_t stream) {
   int stage = (cfg.stage_smem && table_fits_smem(a.table_bytes)) ? 1 : 0;

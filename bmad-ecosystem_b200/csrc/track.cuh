@@ -3,7 +3,6 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "maps.cuh"
 #include "table.h"
 
 namespace bmadgpu {
@@ -37,6 +36,7 @@ struct LaunchCfg {
 };
 
 int table_fits_smem(uint32_t table_bytes);
+cudaError_t upload_constants();
 cudaError_t launch_track(const TrackArgs& a, const LaunchCfg& cfg, int sm_count, cudaStream_t stream);
 
 // Warp-ballot stream compaction of the live particles: live_out gets the indices (taken from

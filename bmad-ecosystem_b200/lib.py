@@ -185,12 +185,13 @@ class HostBunch:
     bunch_struct. vec is [6, n] C-contiguous so vec[i] is coordinate i of every particle."""
 
     def __init__(self, vec, beta, state=None, t=None, track_losses=True):
-        self.vec = np.ascontiguousarray(vec, dtype=np.float64)
+        # own copies: tracking updates these arrays in place
+        self.vec = np.array(vec, dtype=np.float64, order="C", copy=True)
         n = self.vec.shape[1]
-        self.beta = np.ascontiguousarray(beta, dtype=np.float64)
+        self.beta = np.array(beta, dtype=np.float64, copy=True)
         self.state = (np.full(n, abi.ALIVE, dtype=np.int32) if state is None
-                      else np.ascontiguousarray(state, dtype=np.int32))
-        self.t = None if t is None else np.ascontiguousarray(t, dtype=np.float64)
+                      else np.array(state, dtype=np.int32, copy=True))
+        self.t = None if t is None else np.array(t, dtype=np.float64, copy=True)
         if track_losses:
             self.ix_ele = np.full(n, -1, dtype=np.int32)
             self.ix_turn = np.full(n, -1, dtype=np.int32)

@@ -34,7 +34,44 @@ def rel_err(got, want, floor):
     return np.abs(got - want) / np.maximum(np.abs(want), floor)
 
 
-def coord_floor(vec, frac=1e-3):
-    """A per-coordinate floor for relative errors: frac * RMS of the coordinate over the bunch."""
+def coord_floor(vec, frac=1.0):
+    """Per-coordinate scale for relative errors: frac * RMS of the coordinate over the bunch.
+    A coordinate passing near zero has no meaningful relative error of its own; its error is
+    measured against the coordinate's spread in the bunch."""
     rms = np.sqrt(np.mean(vec * vec, axis=1))
     return np.maximum(frac * rms, 1e-30)[:, None]
+
+
+_NOISE = None
+
+
+def noise_track(elements, param, vec, n_turns):
+    """Track with the host build of the device code whose transcendental results are moved by one
+    ulp for about half of the calls (csrc/hostcheck_noise.cpp): the spread that 1-ulp libm
+    differences alone produce, against which the GPU (CUDA libm vs glibc) is judged."""
+    global _NOISE
+    import os
+    import subprocess
+    from conftest import ROOT
+    abi = load_abi()
+    if _NOISE is None:
+        path = os.path.join(ROOT, "bmad-ecosystem_b200", "_build", "libbmadgpu_hostnoise.so")
+        if not os.path.exists(path):
+            subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "bmad-ecosystem_b200", "csrc"),
+                                   "hostcheck-lib"])
+        _NOISE = ctypes.CDLL(path)
+    arr = abi.element_array(elements) if not isinstance(elements, ctypes.Array) else elements
+    vec = np.array(vec, dtype=np.float64, copy=True)
+    n = vec.shape[1]
+    pc = param.p0c * (1 + vec[5])
+    beta = np.ascontiguousarray(np.where(vec[5] == 0, param.p0c / param.e_tot,
+                                         pc / np.sqrt(pc * pc + param.mass * param.mass)))
+    state = np.full(n, abi.ALIVE, dtype=np.int32)
+    b = abi.Bunch(n, vec.ctypes.data, beta.ctypes.data, None, state.ctypes.data, None, None, None)
+    assert _NOISE.bmadgpu_hostcheck_noise_track(arr, len(arr), ctypes.byref(param), ctypes.byref(b), n_turns) == 0
+    return dict(vec=vec, beta=beta, state=state)
+
+
+def per_particle_err(got, want):
+    """Max over coordinates of the RMS-relative error, per particle."""
+    return rel_err(got, want, coord_floor(want)).max(axis=0)
