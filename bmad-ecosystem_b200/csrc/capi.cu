@@ -59,6 +59,7 @@ struct bmadgpu_ctx {
   int64_t mom_cap = 0;
   int32_t* d_i32 = nullptr;       // state, ix_ele, ix_turn, location: 4 * cap
   bmadgpu_tuning tuning;
+  int64_t launches = 0;           // kernel launches enqueued
 };
 
 struct bmadgpu_lattice {
@@ -151,6 +152,7 @@ int track_device(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch
   if (d_moments) CUDA_TRY(cudaMemsetAsync(d_moments, 0, (size_t)n_turns * BMADGPU_N_MOMENTS * sizeof(double), c->stream));
   k_set_i64<<<1, 1, 0, c->stream>>>(c->d_nwork, b->n);
   CUDA_TRY(cudaGetLastError());
+  c->launches++;
   TrackArgs a;
   std::memset(&a, 0, sizeof(a));
   a.table = lat->d_table;
@@ -184,10 +186,12 @@ int track_device(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch
     a.live = live;
     a.moments = d_moments ? d_moments + (int64_t)done * BMADGPU_N_MOMENTS : nullptr;
     CUDA_TRY(launch_track(a, cfg, c->sm_count, c->stream));
+    c->launches++;
     if (compact && done + nt < n_turns) {
       int nxt = live ? 1 - cur : 0;
       if (!live) nxt = 1;  // first compaction: identity list -> list 1
       CUDA_TRY(launch_compact(b->state, live, c->d_nwork + cur, b->n, c->d_live[nxt], c->d_nwork + nxt, c->stream));
+      c->launches++;
       live = c->d_live[nxt];
       cur = nxt;
     }
@@ -275,6 +279,16 @@ int bmadgpu_ctx_synchronize(bmadgpu_ctx* c) {
   CUDA_TRY(cudaSetDevice(c->device));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   return check_err_flag(c);
+}
+
+int64_t bmadgpu_ctx_launch_count(const bmadgpu_ctx* c) { return c ? c->launches : -1; }
+
+int bmadgpu_measure_fp64_peak(bmadgpu_ctx* c, double* flops_per_s) {
+  if (!c || !flops_per_s) return fail(BMADGPU_EINVAL, "NULL argument");
+  CUDA_TRY(cudaSetDevice(c->device));
+  CUDA_TRY(measure_fp64_peak(c->sm_count, c->stream, flops_per_s));
+  c->launches += 2;
+  return BMADGPU_OK;
 }
 
 int bmadgpu_ctx_set_tuning(bmadgpu_ctx* c, const bmadgpu_tuning* t) {

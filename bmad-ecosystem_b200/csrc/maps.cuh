@@ -18,16 +18,16 @@
 // The maps compile for the device (the product) and, for the test-only host check build
 // (hostcheck.cpp: op counting and algorithm checks on CPU), for the host.
 #if defined(__CUDACC__)
-#define BG_HD __host__ __device__ __forceinline__
+#define BG_HD __device__ __forceinline__
 #else
 #define BG_HD inline
 #endif
 
 namespace bmadgpu {
 
-constexpr double kPi = 3.141592653589793238462643383279;
-constexpr double kTwoPi = 2 * kPi;
-constexpr double kCLight = 2.99792458e8;
+constexpr real_const kPi = 3.141592653589793238462643383279;
+constexpr real_const kTwoPi = 2 * kPi;
+constexpr real_const kCLight = 2.99792458e8;
 constexpr int kNPole = 22;
 
 enum : int { S_ALIVE = 1, S_LOST = 2, S_NEG_X = 3, S_POS_X = 4, S_NEG_Y = 5, S_POS_Y = 6, S_LOST_PZ = 8 };

@@ -12,6 +12,9 @@
 
 namespace bmadgpu {
 
+// Plain double for compile-time constants (stays double in the op-counting host build).
+typedef double real_const;
+
 enum Kind : uint8_t {
   K_MARKER = 0,  // no map (reference time only)
   K_DRIFT = 1,   // track_a_drift

@@ -210,7 +210,47 @@ __global__ void k_compact(const int32_t* __restrict__ state, const int32_t* __re
   }
 }
 
+// FP64 peak probe: 8 independent DFMA chains per thread, register resident.
+__global__ void k_fp64_peak(double* out, int iters, double a, double b) {
+  double r[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) r[k] = threadIdx.x * 1e-9 + k;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) r[k] = fma(r[k], a, b);
+  }
+  double s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) s += r[k];
+  if (s == 123.456) out[0] = s;  // keeps the chains live
+}
+
 }  // namespace
+
+cudaError_t measure_fp64_peak(int sm_count, cudaStream_t stream, double* flops_per_s) {
+  double* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(double));
+  if (e != cudaSuccess) return e;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int block = 256, iters = 1 << 14;
+  const int grid = sm_count * 8;
+  k_fp64_peak<<<grid, block, 0, stream>>>(d, 64, 0.999999, 1e-7);  // warm-up
+  cudaEventRecord(e0, stream);
+  k_fp64_peak<<<grid, block, 0, stream>>>(d, iters, 0.999999, 1e-7);
+  cudaEventRecord(e1, stream);
+  e = cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  if (e != cudaSuccess) return e;
+  double flops = 2.0 * 8 * (double)iters * block * (double)grid;
+  *flops_per_s = flops / (ms * 1e-3);
+  return cudaGetLastError();
+}
 
 int table_fits_smem(uint32_t table_bytes) { return table_bytes <= 200 * 1024; }
 

@@ -37,6 +37,7 @@ struct LaunchCfg {
 
 int table_fits_smem(uint32_t table_bytes);
 cudaError_t upload_constants();
+cudaError_t measure_fp64_peak(int sm_count, cudaStream_t stream, double* flops_per_s);
 cudaError_t launch_track(const TrackArgs& a, const LaunchCfg& cfg, int sm_count, cudaStream_t stream);
 
 // Warp-ballot stream compaction of the live particles: live_out gets the indices (taken from

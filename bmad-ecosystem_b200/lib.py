@@ -59,6 +59,8 @@ def load(path=LIB_PATH):
         "bmadgpu_track_bunch_device": ([V, V, P(abi.Bunch), C.c_int32, C.c_int32, C.c_int32, C.c_int32, V],
                                        C.c_int),
         "bmadgpu_track1_bunch": ([V, V, P(abi.Bunch), C.c_int32, C.c_int32], C.c_int),
+        "bmadgpu_ctx_launch_count": ([V], C.c_int64),
+        "bmadgpu_measure_fp64_peak": ([V, P(C.c_double)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name, None)
@@ -132,6 +134,16 @@ class Context:
         cur.update(kw)
         t = Tuning(cur["block"], cur["ctas_per_sm"], cur["stage_smem"], cur["turns_per_launch"], cur["compact"])
         check(load().bmadgpu_ctx_set_tuning(self._h, C.byref(t)))
+
+    @property
+    def launch_count(self):
+        return load().bmadgpu_ctx_launch_count(self._h)
+
+    def measure_fp64_peak(self):
+        """FP64 FLOP/s of a DFMA-chain kernel on every SM of this device."""
+        f = C.c_double()
+        check(load().bmadgpu_measure_fp64_peak(self._h, C.byref(f)))
+        return f.value
 
     def close(self):
         if self._h:

@@ -201,6 +201,13 @@ int bmadgpu_ctx_get_tuning(const bmadgpu_ctx* ctx, bmadgpu_tuning* tuning);
  * (cudaStream_t, returned as void*). */
 int bmadgpu_ctx_info(const bmadgpu_ctx* ctx, int32_t* device, int32_t* sm_count, void** stream);
 
+/* Kernel launches this context has enqueued since it was created (all kernels of this library). */
+int64_t bmadgpu_ctx_launch_count(const bmadgpu_ctx* ctx);
+
+/* Measures the device's FP64 FMA throughput with a register-resident DFMA chain on every SM
+ * (2 flops per FMA), a roofline denominator; *flops_per_s receives FLOP/s. */
+int bmadgpu_measure_fp64_peak(bmadgpu_ctx* ctx, double* flops_per_s);
+
 /* sizeof() of the ABI structs as this library was compiled, for binding checks. */
 int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning */
 
