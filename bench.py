@@ -304,7 +304,7 @@ def run_ours(args):
             try:
                 tj = json.load(open(prof))
                 if tj.get("workload") == args.workload:
-                    traffic = tj["dram_bytes_per_particle_turn"] * total_pt / args.steps
+                    traffic = tj["dram_bytes_per_particle_per_launch"] * n
             except (ValueError, KeyError):
                 traffic = None
         out = {
