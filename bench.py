@@ -203,21 +203,9 @@ def run_ours(args):
                          t["ix_ele"].data_ptr(), t["ix_turn"].data_ptr(), t["location"].data_ptr())
         return t, view
 
-    # launch shape: short untimed trial of the candidates on this device and ring
-    cands = [dict(block=b, stage_smem=s) for b in (128, 256) for s in (1, 0)]
-    best, best_ms = None, 1e30
-    for cnd in cands:
-        ctx.set_tuning(**cnd)
-        t, v = device_bunch()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        lib.check(lib.load().bmadgpu_track_bunch_device(ctx.handle, lat.handle, ctypes.byref(v), 0, lat.n_ele, 0, 1, None))
-        e1.record(stream)
-        ctx.synchronize()
-        ms = e0.elapsed_time(e1)
-        if ms < best_ms:
-            best, best_ms = cnd, ms
-    ctx.set_tuning(**best)
+    # launch shape: the library's autotuner (one-turn trials on a copy of the bunch)
+    t, v = device_bunch()
+    best = lib.autotune(ctx, lat, v)
 
     t, v = device_bunch()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2

@@ -60,6 +60,11 @@ struct bmadgpu_ctx {
   int32_t* d_i32 = nullptr;       // state, ix_ele, ix_turn, location: 4 * cap
   bmadgpu_tuning tuning;
   int64_t launches = 0;           // kernel launches enqueued
+  // autotuner trial copies
+  int64_t tune_cap = 0;
+  double* d_tvec = nullptr;
+  double* d_tbeta = nullptr;
+  int32_t* d_tstate = nullptr;
 };
 
 struct bmadgpu_lattice {
@@ -269,6 +274,9 @@ int bmadgpu_ctx_destroy(bmadgpu_ctx* c) {
   cudaFree(c->d_t);
   cudaFree(c->d_i32);
   cudaFree(c->d_mom);
+  cudaFree(c->d_tvec);
+  cudaFree(c->d_tbeta);
+  cudaFree(c->d_tstate);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return BMADGPU_OK;
@@ -438,6 +446,72 @@ int bmadgpu_track_bunch(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadgpu_bunc
     CUDA_TRY(cudaMemcpyAsync(moments, c->d_mom, (size_t)n_turns * BMADGPU_N_MOMENTS * sizeof(double),
                              cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
+  return check_err_flag(c);
+}
+
+int bmadgpu_autotune(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch* b, int64_t sample_n,
+                     bmadgpu_tuning* chosen) {
+  if (!c || !lat || !b) return fail(BMADGPU_EINVAL, "NULL argument");
+  int r = check_bunch(b);
+  if (r) return r;
+  CUDA_TRY(cudaSetDevice(c->device));
+  int64_t m = std::min<int64_t>(b->n, sample_n > 0 ? sample_n : (int64_t)c->sm_count * 2048);
+  if (m <= 0) return fail(BMADGPU_EINVAL, "empty bunch");
+  if (m > c->tune_cap) {
+    cudaFree(c->d_tvec);
+    cudaFree(c->d_tbeta);
+    cudaFree(c->d_tstate);
+    c->d_tvec = nullptr; c->d_tbeta = nullptr; c->d_tstate = nullptr;
+    c->tune_cap = 0;
+    if (cudaMalloc(&c->d_tvec, (size_t)m * 6 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->d_tbeta, (size_t)m * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->d_tstate, (size_t)m * sizeof(int32_t)) != cudaSuccess)
+      return fail(BMADGPU_ENOMEM, "cannot allocate autotuner trial buffers");
+    c->tune_cap = m;
+  }
+  bmadgpu_bunch t;
+  std::memset(&t, 0, sizeof(t));
+  t.n = m;
+  t.vec = c->d_tvec;
+  t.beta = c->d_tbeta;
+  t.state = c->d_tstate;
+  const bmadgpu_tuning saved = c->tuning;
+  struct Cand { int block, ctas, stage; };
+  static const Cand cands[] = {{128, 0, 0}, {128, 4, 0}, {128, 5, 0}, {128, 6, 0}, {256, 0, 0}, {256, 2, 0},
+                               {256, 3, 0}, {64, 8, 0},  {64, 12, 0}, {128, 0, 1}, {128, 4, 1}, {256, 2, 1}};
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  float best_ms = 1e30f;
+  bmadgpu_tuning best = saved;
+  for (const Cand& k : cands) {
+    if (k.stage && !table_fits_smem(lat->pk.info.total_bytes)) continue;
+    CUDA_TRY(cudaMemcpy2DAsync(t.vec, m * sizeof(double), b->vec, b->n * sizeof(double), m * sizeof(double), 6,
+                               cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(t.beta, b->beta, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(t.state, b->state, m * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
+    c->tuning = bmadgpu_tuning{k.block, k.ctas, k.stage, 0, 0, {0, 0, 0}};
+    CUDA_TRY(cudaEventRecord(e0, c->stream));
+    r = track_device(c, lat, &t, 0, (int32_t)lat->pk.info.n_ele, 0, 1, nullptr);
+    CUDA_TRY(cudaEventRecord(e1, c->stream));
+    if (r) {
+      c->tuning = saved;
+      return r;
+    }
+    CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c->tuning;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  best.turns_per_launch = saved.turns_per_launch;
+  best.compact = saved.compact;
+  c->tuning = best;
+  if (chosen) *chosen = best;
   return check_err_flag(c);
 }
 

@@ -8,18 +8,19 @@ namespace bmadgpu {
 // ---- element bodies (track1_bmad dispatch, bmad/low_level/track1_bmad.f90:64-272) ----------
 
 BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b, const Globals& G) {
-  // track_a_quadrupole, bmad/low_level/track_a_quadrupole.f90 (fringe_type none)
+  // track_a_quadrupole, bmad/low_level/track_a_quadrupole.f90 (fringe_type none); the kick
+  // before the body and the kick after each step share one call site.
   const int np = h.n_pole;
   const double* kh = b + 3;
   const double* kf = kh + 2 * np;
   const double* mis = b + 3 + 4 * np;
   const bool has_t = h.flags & F_TILT;
   if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
-  if (np) ab_kicks(p, kh, np);
   const double b1 = b[0], length = b[1], step_len = b[2];
-  for (int i = 1; i <= h.n_step; i++) {
-    quad_step(p, b1, length, step_len, G);
-    if (np) ab_kicks(p, i == h.n_step ? kh : kf, np);
+  const int n_step = h.n_step;
+  for (int i = 0; i <= n_step; i++) {
+    if (i > 0) quad_step(p, b1, length, step_len, G);
+    if (np) ab_kicks(p, (i == 0 || i == n_step) ? kh : kf, np);
   }
   if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
 }
@@ -32,11 +33,11 @@ BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b
   const double* mis = b + 1 + 4 * np;
   const bool has_t = h.flags & F_TILT;
   if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
-  if (np) ab_kicks(p, kh, np);
   const double step_len = b[0];
-  for (int i = 1; i <= h.n_step; i++) {
-    drift(p, step_len);
-    if (np) ab_kicks(p, i == h.n_step ? kh : kf, np);
+  const int n_step = h.n_step;
+  for (int i = 0; i <= n_step; i++) {
+    if (i > 0) drift(p, step_len);
+    if (np) ab_kicks(p, (i == 0 || i == n_step) ? kh : kf, np);
   }
   if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
 }

@@ -169,11 +169,69 @@ BG_HD double mexp(double x, int m) {
   return y;
 }
 
-// ab_multipole_kicks (multipole_mod.f90:82-121), magnetic, with ab_multipole_kick
-// (multipole_mod.f90:314-376) for each order. c: (b_n * scale, a_n * scale), n < n_pole.
-BG_HD void ab_kicks(Particle& p, const double* __restrict__ c, int n_pole) {
-  double kx_tot = 0, ky_tot = 0;
-  const double x = p.x, y = p.y;
+// Powers x**k, k = 0..N, with exactly the roundings of mexp's binary powering: x**k is the product
+// of the repeated squares x, x**2, x**4, x**8 selected by the set bits of k, taken from the lowest
+// bit up, so the squares can be shared between exponents without changing any result.
+template <int N>
+BG_HD void mexp_table(double x, double* __restrict__ xp) {
+  double sq[4];
+  sq[0] = x;
+#pragma unroll
+  for (int i = 1; i < 4; i++) sq[i] = sq[i - 1] * sq[i - 1];
+  xp[0] = 1;
+#pragma unroll
+  for (int k = 1; k <= N; k++) {
+    double y = 0;
+    bool started = false;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      if ((k >> i) & 1) {
+        y = started ? y * sq[i] : sq[i];
+        started = true;
+      }
+    }
+    xp[k] = y;
+  }
+}
+
+// Sum over orders n < NP of ab_multipole_kick (multipole_mod.f90:314-376), as ab_multipole_kicks
+// accumulates it (:103-115). c: (b_n * scale, a_n * scale). Terms whose coefficient is exactly
+// zero add an exact zero in the reference and are skipped.
+template <int NP>
+BG_HD void ab_kick_sum(double x, double y, const double* __restrict__ c, double& kx_tot, double& ky_tot) {
+  double xp[NP], yp[NP];
+  mexp_table<NP - 1>(x, xp);
+  mexp_table<NP - 1>(y, yp);
+  kx_tot = 0;
+  ky_tot = 0;
+#pragma unroll
+  for (int n = 0; n < NP; n++) {
+    const double b2 = c[2 * n], a2 = c[2 * n + 1];
+    double kx = 0, ky = 0;
+    if (!(a2 == 0 && b2 == 0)) {
+#pragma unroll
+      for (int m = 0; m <= n; m += 2) {
+        double f = BG_CMULTI(n, m) * xp[n - m] * yp[m];
+        if (b2 != 0) kx = kx + b2 * f;
+        if (a2 != 0) ky = ky - a2 * f;
+      }
+#pragma unroll
+      for (int m = 1; m <= n; m += 2) {
+        double f = BG_CMULTI(n, m) * xp[n - m] * yp[m];
+        if (a2 != 0) kx = kx + a2 * f;
+        if (b2 != 0) ky = ky + b2 * f;
+      }
+    }
+    kx_tot = kx_tot + kx;
+    ky_tot = ky_tot + ky;
+  }
+}
+
+// Any order count: the reference's loop with run-time powers.
+BG_HD void ab_kick_sum_any(double x, double y, const double* __restrict__ c, int n_pole, double& kx_tot,
+                           double& ky_tot) {
+  kx_tot = 0;
+  ky_tot = 0;
   for (int n = 0; n < n_pole; n++) {
     const double b2 = c[2 * n], a2 = c[2 * n + 1];
     double kx = 0, ky = 0;
@@ -192,11 +250,35 @@ BG_HD void ab_kicks(Particle& p, const double* __restrict__ c, int n_pole) {
     kx_tot = kx_tot + kx;
     ky_tot = ky_tot + ky;
   }
+}
+
+BG_HD void ab_kick_dispatch(double x, double y, const double* __restrict__ c, int n_pole, double& kx, double& ky) {
+  switch (n_pole) {
+    case 1: ab_kick_sum<1>(x, y, c, kx, ky); break;
+    case 2: ab_kick_sum<2>(x, y, c, kx, ky); break;
+    case 3: ab_kick_sum<3>(x, y, c, kx, ky); break;
+    case 4: ab_kick_sum<4>(x, y, c, kx, ky); break;
+    case 5: ab_kick_sum<5>(x, y, c, kx, ky); break;
+    case 6: ab_kick_sum<6>(x, y, c, kx, ky); break;
+    case 7: ab_kick_sum<7>(x, y, c, kx, ky); break;
+    case 8: ab_kick_sum<8>(x, y, c, kx, ky); break;
+    case 9: ab_kick_sum<9>(x, y, c, kx, ky); break;
+    case 10: ab_kick_sum<10>(x, y, c, kx, ky); break;
+    case 11: ab_kick_sum<11>(x, y, c, kx, ky); break;
+    default: ab_kick_sum_any(x, y, c, n_pole, kx, ky); break;
+  }
+}
+
+// ab_multipole_kicks (multipole_mod.f90:82-121), magnetic, coefficients pre-scaled.
+BG_HD void ab_kicks(Particle& p, const double* __restrict__ c, int n_pole) {
+  double kx_tot, ky_tot;
+  ab_kick_dispatch(p.x, p.y, c, n_pole, kx_tot, ky_tot);
   p.px = p.px + kx_tot;
   p.py = p.py + ky_tot;
 }
 
-// Unscaled ab_multipole_kick sums for the bend field (ele_orientation = 0), track_a_bend.f90:366-379.
+// Field of the bend multipoles (ab_multipole_kick with ele_orientation = 0, unscaled) as
+// track_a_bend's apply_multipole_kicks sums it (track_a_bend.f90:366-379).
 BG_HD void ab_field(const Particle& p, const double* __restrict__ c, int n_pole, double f_p0c, double& B1,
                     double& B2) {
   B1 = 0;

@@ -91,8 +91,8 @@ __device__ void add_moments(const Particle& p, bool alive, double* __restrict__ 
   }
 }
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_track(const TrackArgs a, int stage_smem) {
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_track(const TrackArgs a, int stage_smem) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t bar;
   const uint8_t* tbl = a.table;
@@ -262,25 +262,41 @@ cudaError_t upload_constants() {
   return cudaMemcpyToSymbol(c_cfull, cf, sizeof(cf));
 }
 
+// Kernel variants: threads per CTA x minimum resident CTAs per SM (the register budget per
+// thread follows: 65536 / (BLOCK * MINB), capped at 255).
+struct Variant {
+  int block, minb;
+  const void* fn;
+};
+static const Variant kVariants[] = {
+    {64, 8, (const void*)k_track<64, 8>},    {64, 12, (const void*)k_track<64, 12>},
+    {128, 3, (const void*)k_track<128, 3>},  {128, 4, (const void*)k_track<128, 4>},
+    {128, 5, (const void*)k_track<128, 5>},
+    {128, 6, (const void*)k_track<128, 6>},  {256, 2, (const void*)k_track<256, 2>},
+    {256, 1, (const void*)k_track<256, 1>},  {256, 3, (const void*)k_track<256, 3>},
+    {512, 1, (const void*)k_track<512, 1>},
+};
+
 cudaError_t launch_track(const TrackArgs& a, const LaunchCfg& cfg, int sm_count, cudaStream_t stream) {
   int stage = (cfg.stage_smem && table_fits_smem(a.table_bytes)) ? 1 : 0;
   size_t smem = stage ? a.table_bytes : 0;
-  const void* fn;
-  switch (cfg.block) {
-    case 64: fn = (const void*)k_track<64>; break;
-    case 128: fn = (const void*)k_track<128>; break;
-    case 256: fn = (const void*)k_track<256>; break;
-    case 512: fn = (const void*)k_track<512>; break;
-    default: return cudaErrorInvalidValue;
+  // ctas_per_sm selects the register budget: the variant with the largest minimum CTA count
+  // not above it (0: the most registers per thread)
+  const Variant* v = nullptr;
+  for (const Variant& k : kVariants) {
+    if (k.block != cfg.block) continue;
+    if (cfg.ctas_per_sm > 0 && k.minb > cfg.ctas_per_sm) continue;
+    if (!v || (cfg.ctas_per_sm > 0 ? k.minb > v->minb : k.minb < v->minb)) v = &k;
   }
+  if (!v) return cudaErrorInvalidValue;
+  const void* fn = v->fn;
   cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   int per_sm = 0;
   err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, cfg.block, smem);
   if (err != cudaSuccess) return err;
   if (per_sm < 1) per_sm = 1;
-  if (cfg.ctas_per_sm > 0 && cfg.ctas_per_sm < per_sm) per_sm = cfg.ctas_per_sm;
-  // Persistent grid: at most one full wave; every CTA strides over the particle range.
+  // Persistent grid: one full wave; every CTA strides over the particle range.
   int64_t grid = (int64_t)sm_count * per_sm;
   void* args[] = {(void*)&a, (void*)&stage};
   return cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(cfg.block), args, smem, stream);

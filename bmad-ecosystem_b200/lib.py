@@ -61,6 +61,7 @@ def load(path=LIB_PATH):
         "bmadgpu_track1_bunch": ([V, V, P(abi.Bunch), C.c_int32, C.c_int32], C.c_int),
         "bmadgpu_ctx_launch_count": ([V], C.c_int64),
         "bmadgpu_measure_fp64_peak": ([V, P(C.c_double)], C.c_int),
+        "bmadgpu_autotune": ([V, V, P(abi.Bunch), C.c_int64, P(Tuning)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name, None)
@@ -240,6 +241,15 @@ def track_bunch(ctx, lat, bunch, n_turns=1, ix_start=0, ix_end=None, turn0=0, mo
     check(lib.bmadgpu_track_bunch(ctx.handle, lat.handle, C.byref(v), ix_start, ix_end, turn0, n_turns,
                                   mom.ctypes.data if mom is not None else None))
     return mom
+
+
+def autotune(ctx, lat, device_bunch_view, sample_n=0):
+    """Run the library's launch-shape autotuner on a device-resident bunch view (abi.Bunch of
+    device pointers); returns the chosen tuning (also set on the context)."""
+    t = Tuning()
+    check(load().bmadgpu_autotune(ctx.handle, lat.handle, C.byref(device_bunch_view), sample_n, C.byref(t)))
+    return dict(block=t.block, ctas_per_sm=t.ctas_per_sm, stage_smem=t.stage_smem,
+                turns_per_launch=t.turns_per_launch, compact=t.compact)
 
 
 def track1_bunch(ctx, lat, bunch, ix_ele, turn=0):

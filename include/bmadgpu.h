@@ -197,6 +197,13 @@ typedef struct bmadgpu_tuning {
 int bmadgpu_ctx_set_tuning(bmadgpu_ctx* ctx, const bmadgpu_tuning* tuning);
 int bmadgpu_ctx_get_tuning(const bmadgpu_ctx* ctx, bmadgpu_tuning* tuning);
 
+/* Autotuner: times one-turn trial launches of every launch shape (threads per CTA, register
+ * budget via resident CTAs per SM, element table staged in shared memory or read through L1) on
+ * a copy of the first min(n, sample_n) particles of a device-resident bunch, sets the fastest
+ * as the context's tuning and returns it in *chosen (nullable). The bunch is not modified. */
+int bmadgpu_autotune(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const bmadgpu_bunch* device_bunch,
+                     int64_t sample_n, bmadgpu_tuning* chosen);
+
 /* Device the context runs on, its SM count, and the CUDA stream it enqueues work on
  * (cudaStream_t, returned as void*). */
 int bmadgpu_ctx_info(const bmadgpu_ctx* ctx, int32_t* device, int32_t* sm_count, void** stream);

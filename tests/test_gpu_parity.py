@@ -211,3 +211,29 @@ def test_launch_shapes_agree(ctx, tuning):
     alt = gpu_track(ctx, eles, p, vec, 25, **tuning)
     for k in ("vec", "beta", "state", "ix_ele", "ix_turn", "location"):
         assert np.array_equal(base[k], alt[k]), k
+
+
+@pytest.mark.parametrize("variant", [dict(block=128, ctas_per_sm=6), dict(block=256, ctas_per_sm=0),
+                                     dict(block=64, ctas_per_sm=12), dict(block=512, ctas_per_sm=0)])
+def test_register_budget_variants_are_bitwise_identical(ctx, variant):
+    eles, p = rings.ring(200, fringe=True, multipole_sigma=1e-4)
+    vec = rings.matched_gaussian(eles, 2000, seed=4, scale=4.0)
+    base = gpu_track(ctx, eles, p, vec, 3)
+    alt = gpu_track(ctx, eles, p, vec, 3, **variant)
+    for k in ("vec", "beta", "state"):
+        assert np.array_equal(base[k], alt[k]), k
+
+
+def test_autotuner_leaves_bunch_untouched(ctx):
+    import torch
+    eles, p = rings.ring(50)
+    lat = lib.Lattice(ctx, eles, p)
+    hb = lib.HostBunch.from_vec(rings.matched_gaussian(eles, 50000, seed=1), p)
+    d = {k: torch.from_numpy(getattr(hb, k)).cuda() for k in ("vec", "beta", "state")}
+    torch.cuda.synchronize()
+    v = abi.Bunch(hb.n, d["vec"].data_ptr(), d["beta"].data_ptr(), None, d["state"].data_ptr(), None, None, None)
+    chosen = lib.autotune(ctx, lat, v)
+    assert chosen["block"] in (64, 128, 256, 512)
+    assert np.array_equal(d["vec"].cpu().numpy(), hb.vec)
+    assert np.array_equal(d["state"].cpu().numpy(), hb.state)
+    ctx.set_tuning(block=128, ctas_per_sm=0, stage_smem=1, turns_per_launch=0, compact=0)
