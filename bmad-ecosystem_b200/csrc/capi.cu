@@ -217,6 +217,49 @@ int check_err_flag(bmadgpu_ctx* c) {
 
 }  // namespace
 
+namespace bmadgpu {
+
+int noalloc_fail(int code, const char* msg) { return fail(code, msg); }
+
+// Argument checks and kernel arguments for bmadgpu_track_bunch_device_noalloc (noalloc.cu); makes
+// the context's device current. Allocates nothing.
+int noalloc_prepare(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch* b, TrackArgs* a,
+                    LaunchCfg* cfg, int* sm_count, cudaStream_t* stream, int64_t** launches) {
+  if (!c) return fail(BMADGPU_EINVAL, "ctx is NULL");
+  int r = check_bunch(b);
+  if (r) return r;
+  if ((r = check_range(lat, 0, (int32_t)(lat ? lat->pk.info.n_ele : 1), 0))) return r;
+  if (lat->device != c->device) return fail(BMADGPU_EINVAL, "lattice and context are on different devices");
+  CUDA_TRY(cudaSetDevice(c->device));
+  std::memset(a, 0, sizeof(*a));
+  a->table = lat->d_table;
+  a->table_bytes = lat->pk.info.total_bytes;
+  a->hdr_bytes = lat->pk.info.hdr_bytes;
+  a->ap_bytes = lat->pk.info.ap_bytes;
+  a->ix_start = 0;
+  a->ix_end = (int32_t)lat->pk.info.n_ele;
+  a->ld = b->n;
+  a->vec = b->vec;
+  a->beta = b->beta;
+  a->t = b->t;
+  a->state = b->state;
+  a->ix_ele = b->ix_ele;
+  a->ix_turn = b->ix_turn;
+  a->location = b->location;
+  a->ref_prefix = lat->d_prefix;
+  a->G = lat->G;
+  a->err_flag = c->d_err;
+  cfg->block = c->tuning.block;
+  cfg->ctas_per_sm = c->tuning.ctas_per_sm;
+  cfg->stage_smem = c->tuning.stage_smem != 0;
+  *sm_count = c->sm_count;
+  *stream = c->stream;
+  *launches = &c->launches;
+  return BMADGPU_OK;
+}
+
+}  // namespace bmadgpu
+
 extern "C" {
 
 int bmadgpu_abi_version(void) { return BMADGPU_ABI_VERSION; }

@@ -177,6 +177,24 @@ int bmadgpu_track_bunch_device(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bma
                                int32_t ix_start, int32_t ix_end, int32_t turn0, int32_t n_turns,
                                double* moments);
 
+/* Largest bunch bmadgpu_track_bunch_device_noalloc accepts. */
+#define BMADGPU_NOALLOC_MAX_PARTICLES 262144
+
+/* No counterpart in the reference (an addition for callers that cannot allocate).
+ * Same tracking as bmadgpu_track_bunch_device over the whole lattice (ix_start = 0,
+ * ix_end = n_ele, no moments), with the live-particle list compacted every turns_per_launch
+ * turns (0 = one launch), but allocating nothing: its scratch (two index lists and their
+ * lengths, 2 MiB) is a fixed device array inside the library, for callers that cannot call
+ * cudaMalloc mid-run -- code inside CUDA stream capture, or programs whose memory pool owns the
+ * GPU's memory. Every bunch pointer is device memory; the context and lattice already exist.
+ * Limits: at most BMADGPU_NOALLOC_MAX_PARTICLES particles (BMADGPU_EINVAL otherwise). The
+ * array is shared by all calls on a device and keeps the last call's contents (the lengths are
+ * reset by each call); calls that overlap on the GPU race and must be serialised. The first
+ * call on each device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current: make that first call before any stream capture. */
+int bmadgpu_track_bunch_device_noalloc(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* bunch,
+                                       int32_t turn0, int32_t n_turns, int32_t turns_per_launch);
+
 /* The per-element hook: one element for the whole bunch, the work of track1_bunch_hom
  * (beam_utils.f90:32-172) for bmad_standard elements. ix_ele is 0-based. */
 int bmadgpu_track1_bunch(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* bunch,
