@@ -1,0 +1,263 @@
+!+
+! Module bmadgpu_mod
+!
+! Fortran binding of the B200 tracker (include/bmadgpu.h) for Bmad programs. It installs a
+! track1_bunch hook (bmad/custom/track1_bunch_hook.f90:25-43, pointer at
+! bmad/modules/bmad_routine_interface.f90:4034, called by track1_bunch at
+! bmad/multiparticle/beam_mod.f90:263-266) and offers a ring-level routine for the turn loop of
+! long_term_tracking (bsim/modules/lt_tracking_mod.f90:1631-1713).
+!
+! Marshalling follows cpp_bmad_interface's coord_to_c / coord_to_f2 idiom
+! (cpp_bmad_interface/code/bmad_cpp_convert_mod.f90:1767-1844): component by component into
+! structure-of-arrays buffers, since coord_struct is not C interoperable (real(qp) time,
+! allocatables).
+!
+! This file is compiled with the caller's Bmad build (gfortran/ifort with bmad modules on the
+! include path) and linked with libbmadgpu.so; it has not been compiled in this repository
+! (no Fortran compiler in the build image).
+!-
+
+module bmadgpu_mod
+
+use bmad
+use, intrinsic :: iso_c_binding
+
+implicit none
+
+integer, parameter :: bmadgpu_n_pole = 22
+
+type, bind(c) :: bmadgpu_element_t
+  integer(c_int32_t) :: key, is_on, fringe_type, fringe_at, aperture_at, aperture_type
+  integer(c_int32_t) :: num_steps, scale_multipoles, field_master, exact_multipoles, orientation, reserved
+  real(c_double) :: l, k1, k2, k3, g, dg, e1, e2, fint, fintx, hgap, hgapx
+  real(c_double) :: tilt, ref_tilt, roll, x_offset, y_offset, z_offset, x_pitch, y_pitch
+  real(c_double) :: hkick, vkick
+  real(c_double) :: x1_limit, x2_limit, y1_limit, y2_limit
+  real(c_double) :: voltage, rf_frequency, phi0, phi0_multipass
+  real(c_double) :: ds_step, r0_mag, r0_elec
+  real(c_double) :: delta_ref_time
+  real(c_double) :: a_pole(0:bmadgpu_n_pole-1), b_pole(0:bmadgpu_n_pole-1)
+  real(c_double) :: a_pole_elec(0:bmadgpu_n_pole-1), b_pole_elec(0:bmadgpu_n_pole-1)
+end type
+
+type, bind(c) :: bmadgpu_param_t
+  real(c_double) :: p0c, e_tot, mass, charge, max_aperture_limit, default_ds_step
+  integer(c_int32_t) :: aperture_limit_on, absolute_time_tracking, radiation_on, reserved
+end type
+
+type, bind(c) :: bmadgpu_bunch_t
+  integer(c_int64_t) :: n
+  type(c_ptr) :: vec, beta, t, state, ix_ele, ix_turn, location
+end type
+
+interface
+  integer(c_int) function bmadgpu_ctx_create(device, ctx) bind(c, name='bmadgpu_ctx_create')
+    import
+    integer(c_int32_t), value :: device
+    type(c_ptr) :: ctx
+  end function
+  integer(c_int) function bmadgpu_lattice_create(ctx, eles, n_ele, param, lat) bind(c, name='bmadgpu_lattice_create')
+    import
+    type(c_ptr), value :: ctx
+    type(bmadgpu_element_t) :: eles(*)
+    integer(c_int32_t), value :: n_ele
+    type(bmadgpu_param_t) :: param
+    type(c_ptr) :: lat
+  end function
+  integer(c_int) function bmadgpu_track_bunch(ctx, lat, bunch, ix_start, ix_end, turn0, n_turns, moments) &
+                                                                              bind(c, name='bmadgpu_track_bunch')
+    import
+    type(c_ptr), value :: ctx, lat
+    type(bmadgpu_bunch_t) :: bunch
+    integer(c_int32_t), value :: ix_start, ix_end, turn0, n_turns
+    type(c_ptr), value :: moments
+  end function
+  integer(c_int) function bmadgpu_track1_bunch(ctx, lat, bunch, ix_ele, turn) bind(c, name='bmadgpu_track1_bunch')
+    import
+    type(c_ptr), value :: ctx, lat
+    type(bmadgpu_bunch_t) :: bunch
+    integer(c_int32_t), value :: ix_ele, turn
+  end function
+  type(c_ptr) function bmadgpu_last_error() bind(c, name='bmadgpu_last_error')
+    import
+  end function
+end interface
+
+type(c_ptr), save :: gpu_ctx = c_null_ptr, gpu_lat = c_null_ptr
+integer, save :: gpu_branch = 0, gpu_turn = 0
+
+contains
+
+!+
+! Subroutine bmadgpu_install (lat, ix_branch, err)
+!
+! Packs branch%ele(1:n_ele_track) into the device element table and points
+! track1_bunch_hook_ptr at bmadgpu_track1_bunch_hook. Elements outside the device path make
+! bmadgpu_lattice_create return an error and nothing is installed.
+!-
+
+subroutine bmadgpu_install (lat, ix_branch, err)
+
+type (lat_struct), target :: lat
+integer ix_branch
+logical err
+type (branch_struct), pointer :: branch
+type (bmadgpu_element_t), allocatable :: eles(:)
+type (bmadgpu_param_t) param
+integer i, n
+
+err = .true.
+branch => lat%branch(ix_branch)
+n = branch%n_ele_track
+allocate (eles(n))
+do i = 1, n
+  call pack_element(branch%ele(i), eles(i))
+enddo
+
+param%p0c = branch%ele(0)%value(p0c$)
+param%e_tot = branch%ele(0)%value(e_tot$)
+param%mass = mass_of(branch%param%particle)
+param%charge = charge_of(branch%param%particle)
+param%max_aperture_limit = bmad_com%max_aperture_limit
+param%default_ds_step = bmad_com%default_ds_step
+param%aperture_limit_on = merge(1, 0, bmad_com%aperture_limit_on)
+param%absolute_time_tracking = merge(1, 0, bmad_com%absolute_time_tracking)
+param%radiation_on = merge(1, 0, bmad_com%radiation_damping_on .or. bmad_com%radiation_fluctuations_on .or. &
+                                 bmad_com%spin_tracking_on)
+param%reserved = 0
+
+if (.not. c_associated(gpu_ctx)) then
+  if (bmadgpu_ctx_create(0_c_int32_t, gpu_ctx) /= 0) return
+endif
+if (bmadgpu_lattice_create(gpu_ctx, eles, int(n, c_int32_t), param, gpu_lat) /= 0) return
+gpu_branch = ix_branch
+track1_bunch_hook_ptr => bmadgpu_track1_bunch_hook
+err = .false.
+
+end subroutine bmadgpu_install
+
+!+
+! Subroutine pack_element (ele, e)
+! One bmadgpu_element from ele%value(...) and the multipole arrays.
+!-
+
+subroutine pack_element (ele, e)
+
+type (ele_struct) ele
+type (bmadgpu_element_t) e
+
+e%key = ele%key;  e%is_on = merge(1, 0, ele%is_on)
+e%fringe_type = nint(ele%value(fringe_type$));  e%fringe_at = nint(ele%value(fringe_at$))
+e%aperture_at = ele%aperture_at;  e%aperture_type = ele%aperture_type
+e%num_steps = nint(ele%value(num_steps$));  e%scale_multipoles = merge(1, 0, ele%scale_multipoles)
+e%field_master = merge(1, 0, ele%field_master);  e%exact_multipoles = nint(ele%value(exact_multipoles$))
+e%orientation = ele%orientation;  e%reserved = 0
+e%l = ele%value(l$);  e%k1 = ele%value(k1$);  e%k2 = ele%value(k2$);  e%k3 = ele%value(k3$)
+e%g = ele%value(g$);  e%dg = ele%value(dg$);  e%e1 = ele%value(e1$);  e%e2 = ele%value(e2$)
+e%fint = ele%value(fint$);  e%fintx = ele%value(fintx$);  e%hgap = ele%value(hgap$);  e%hgapx = ele%value(hgapx$)
+e%tilt = ele%value(tilt_tot$);  e%ref_tilt = ele%value(ref_tilt_tot$);  e%roll = ele%value(roll_tot$)
+e%x_offset = ele%value(x_offset_tot$);  e%y_offset = ele%value(y_offset_tot$);  e%z_offset = ele%value(z_offset_tot$)
+e%x_pitch = ele%value(x_pitch_tot$);  e%y_pitch = ele%value(y_pitch_tot$)
+e%hkick = ele%value(hkick$);  e%vkick = ele%value(vkick$)
+e%x1_limit = ele%value(x1_limit$);  e%x2_limit = ele%value(x2_limit$)
+e%y1_limit = ele%value(y1_limit$);  e%y2_limit = ele%value(y2_limit$)
+e%voltage = ele%value(voltage$);  e%rf_frequency = ele%value(rf_frequency$)
+e%phi0 = ele%value(phi0$);  e%phi0_multipass = ele%value(phi0_multipass$)
+e%ds_step = ele%value(ds_step$);  e%r0_mag = ele%value(r0_mag$);  e%r0_elec = ele%value(r0_elec$)
+e%delta_ref_time = ele%value(delta_ref_time$)
+e%a_pole = 0;  e%b_pole = 0;  e%a_pole_elec = 0;  e%b_pole_elec = 0
+if (associated(ele%a_pole)) then
+  e%a_pole = ele%a_pole(0:bmadgpu_n_pole-1);  e%b_pole = ele%b_pole(0:bmadgpu_n_pole-1)
+endif
+if (associated(ele%a_pole_elec)) then
+  e%a_pole_elec = ele%a_pole_elec(0:bmadgpu_n_pole-1);  e%b_pole_elec = ele%b_pole_elec(0:bmadgpu_n_pole-1)
+endif
+
+end subroutine pack_element
+
+!+
+! Subroutine bmadgpu_track1_bunch_hook (bunch, ele, err, centroid, direction, finished, bunch_track)
+! The track1_bunch_hook_def procedure: tracks the bunch through ele on the GPU.
+!-
+
+subroutine bmadgpu_track1_bunch_hook (bunch, ele, err, centroid, direction, finished, bunch_track)
+
+type (bunch_struct), target :: bunch
+type (ele_struct), target :: ele
+logical err, finished
+type (coord_struct), optional :: centroid(0:)
+integer, optional :: direction
+type (bunch_track_struct), optional :: bunch_track
+
+finished = .false.
+err = .false.
+if (integer_option(1, direction) /= 1 .or. present(bunch_track)) return   ! Bmad's own code path
+if (ele%ix_branch /= gpu_branch .or. ele%ix_ele < 1) return
+call track_on_gpu (bunch, ele%ix_ele - 1, ele%ix_ele, 1, err)
+finished = .not. err
+
+end subroutine bmadgpu_track1_bunch_hook
+
+!+
+! Subroutine bmadgpu_track_turns (bunch, n_turns, err)
+! All elements of the installed branch, n_turns times (the element and turn loops of
+! track_bunch / ltt_run_beam_mode in one call).
+!-
+
+subroutine bmadgpu_track_turns (bunch, n_turns, n_ele_track, err)
+
+type (bunch_struct), target :: bunch
+integer n_turns, n_ele_track
+logical err
+
+call track_on_gpu (bunch, 0, n_ele_track, n_turns, err)
+
+end subroutine bmadgpu_track_turns
+
+subroutine track_on_gpu (bunch, ix_start, ix_end, n_turns, err)
+
+type (bunch_struct), target :: bunch
+integer ix_start, ix_end, n_turns
+logical err
+real(c_double), allocatable, target :: vec(:,:), beta(:), t(:)
+integer(c_int32_t), allocatable, target :: state(:), ix_ele(:), ix_turn(:), location(:)
+type (bmadgpu_bunch_t) b
+integer j, n, i
+
+n = size(bunch%particle)
+allocate (vec(n, 6), beta(n), t(n), state(n), ix_ele(n), ix_turn(n), location(n))
+do j = 1, n
+  do i = 1, 6
+    vec(j, i) = bunch%particle(j)%vec(i)
+  enddo
+  beta(j) = bunch%particle(j)%beta
+  t(j) = real(bunch%particle(j)%t, c_double)
+  state(j) = bunch%particle(j)%state
+enddo
+ix_ele = -1;  ix_turn = -1;  location = 0
+b%n = n
+b%vec = c_loc(vec);  b%beta = c_loc(beta);  b%t = c_loc(t);  b%state = c_loc(state)
+b%ix_ele = c_loc(ix_ele);  b%ix_turn = c_loc(ix_turn);  b%location = c_loc(location)
+err = (bmadgpu_track_bunch(gpu_ctx, gpu_lat, b, int(ix_start, c_int32_t), int(ix_end, c_int32_t), &
+                           int(gpu_turn, c_int32_t), int(n_turns, c_int32_t), c_null_ptr) /= 0)
+if (err) return
+do j = 1, n
+  do i = 1, 6
+    bunch%particle(j)%vec(i) = vec(j, i)
+  enddo
+  bunch%particle(j)%beta = beta(j)
+  bunch%particle(j)%t = t(j)
+  bunch%particle(j)%state = state(j)
+  if (ix_ele(j) >= 0) then        ! lost in this call
+    bunch%particle(j)%ix_ele = ix_ele(j) + 1
+    bunch%particle(j)%location = location(j)
+  else
+    bunch%particle(j)%location = downstream_end$
+  endif
+enddo
+bunch%n_live = count(bunch%particle%state == alive$)
+bunch%charge_live = sum(bunch%particle%charge, mask = (bunch%particle%state == alive$))
+
+end subroutine track_on_gpu
+
+end module bmadgpu_mod
