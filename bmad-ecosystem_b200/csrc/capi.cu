@@ -13,13 +13,11 @@
 #include <new>
 #include <string>
 
-#include "../../include/bmadgpu.h"
-#include "lattice.h"
-#include "track.cuh"
+#include "capi_internal.h"
 
 using namespace bmadgpu;
 
-namespace {
+namespace bmadgpu {
 
 thread_local std::string g_last_error;
 
@@ -32,51 +30,11 @@ int cuda_fail(cudaError_t e, const char* what) {
   return fail(BMADGPU_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-#define CUDA_TRY(call)                                  \
-  do {                                                  \
-    cudaError_t e_ = (call);                            \
-    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
-  } while (0)
-
-__global__ void k_set_i64(int64_t* p, int64_t v) { *p = v; }
-
-}  // namespace
-
-struct bmadgpu_ctx {
-  int device = 0;
-  int sm_count = 0;
-  cudaStream_t stream = nullptr;
-  int32_t* d_err = nullptr;
-  int64_t* d_nwork = nullptr;     // [2] live-list lengths
-  int32_t* d_live[2] = {nullptr, nullptr};
-  int64_t live_cap = 0;
-  // staging for the host-pointer API
-  int64_t cap = 0;
-  double* d_vec = nullptr;
-  double* d_beta = nullptr;
-  double* d_t = nullptr;
-  double* d_mom = nullptr;
-  int64_t mom_cap = 0;
-  int32_t* d_i32 = nullptr;       // state, ix_ele, ix_turn, location: 4 * cap
-  bmadgpu_tuning tuning;
-  int64_t launches = 0;           // kernel launches enqueued
-  // autotuner trial copies
-  int64_t tune_cap = 0;
-  double* d_tvec = nullptr;
-  double* d_tbeta = nullptr;
-  int32_t* d_tstate = nullptr;
-};
-
-struct bmadgpu_lattice {
-  int device = 0;
-  PackedLattice pk;
-  uint8_t* d_table = nullptr;
-  double* d_prefix = nullptr;
-  Globals G;
-  bmadgpu_param param;
-};
+}  // namespace bmadgpu
 
 namespace {
+
+__global__ void k_set_i64(int64_t* p, int64_t v) { *p = v; }
 
 int ensure_live(bmadgpu_ctx* c, int64_t n) {
   if (n <= c->live_cap) return BMADGPU_OK;
@@ -107,24 +65,6 @@ int ensure_staging(bmadgpu_ctx* c, int64_t n) {
     return fail(BMADGPU_ENOMEM, "cannot allocate device particle buffers");
   c->cap = n;
   return BMADGPU_OK;
-}
-
-Globals make_globals(const bmadgpu_param& p) {
-  Globals g;
-  g.p0c = p.p0c;
-  g.e_tot = p.e_tot;
-  g.mass = p.mass;
-  g.beta0 = p.p0c / p.e_tot;
-  g.max_ap = p.max_aperture_limit;
-  g.mass2 = p.mass * p.mass;
-  // low_energy_z_correction.f90:43-45 constants, same expressions
-  double me = p.mass / p.e_tot;
-  g.lez_me2 = me * me;
-  g.lez_b02 = g.beta0 * g.beta0;
-  g.lez_f = g.lez_b02 * (2 * g.lez_b02 - g.lez_me2 / 2);
-  g.lez_thresh = 3e-7 * p.e_tot;
-  g.charge = p.charge;
-  return g;
 }
 
 int check_bunch(const bmadgpu_bunch* b) {
@@ -204,6 +144,28 @@ int track_device(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch
   return BMADGPU_OK;
 }
 
+}  // namespace
+
+namespace bmadgpu {
+
+Globals make_globals(const bmadgpu_param& p) {
+  Globals g;
+  g.p0c = p.p0c;
+  g.e_tot = p.e_tot;
+  g.mass = p.mass;
+  g.beta0 = p.p0c / p.e_tot;
+  g.max_ap = p.max_aperture_limit;
+  g.mass2 = p.mass * p.mass;
+  // low_energy_z_correction.f90:43-45 constants, same expressions
+  double me = p.mass / p.e_tot;
+  g.lez_me2 = me * me;
+  g.lez_b02 = g.beta0 * g.beta0;
+  g.lez_f = g.lez_b02 * (2 * g.lez_b02 - g.lez_me2 / 2);
+  g.lez_thresh = 3e-7 * p.e_tot;
+  g.charge = p.charge;
+  return g;
+}
+
 int check_err_flag(bmadgpu_ctx* c) {
   int32_t h = 0;
   CUDA_TRY(cudaMemcpyAsync(&h, c->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
@@ -214,10 +176,6 @@ int check_err_flag(bmadgpu_ctx* c) {
   }
   return BMADGPU_OK;
 }
-
-}  // namespace
-
-namespace bmadgpu {
 
 int noalloc_fail(int code, const char* msg) { return fail(code, msg); }
 
@@ -272,6 +230,7 @@ int64_t bmadgpu_sizeof(int32_t which) {
     case 1: return (int64_t)sizeof(bmadgpu_param);
     case 2: return (int64_t)sizeof(bmadgpu_bunch);
     case 3: return (int64_t)sizeof(bmadgpu_tuning);
+    case 4: return (int64_t)sizeof(bmadgpu_batch_tuning);
   }
   return -1;
 }

@@ -15,55 +15,14 @@
 
 #include <cuda_runtime.h>
 
-#include "elements.cuh"
+#include "particle.cuh"
+#include "tma.cuh"
 #include "track.cuh"
+#include "batch.cuh"
 
 namespace bmadgpu {
 
 namespace {
-
-constexpr uint32_t kBulkChunk = 32768;
-constexpr int kSpinLimit = 1 << 22;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// 1-D bulk copy global -> this CTA's shared memory (no multicast), completion on an mbarrier.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ void load_hdr(const EleHdr* hdr, int i, EleHdr& h) {
-  uint4 raw = *reinterpret_cast<const uint4*>(hdr + i);
-  h = *reinterpret_cast<const EleHdr*>(&raw);
-}
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -101,16 +60,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_track(const TrackArgs a, int st
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
-      mbar_arrive_expect_tx(&bar, a.table_bytes);
-      for (uint32_t off = 0; off < a.table_bytes; off += kBulkChunk) {
-        uint32_t n = a.table_bytes - off < kBulkChunk ? a.table_bytes - off : kBulkChunk;
-        bulk_g2s(smem + off, a.table + off, n, &bar);
-      }
+      stage_table_issue(smem, a.table, a.table_bytes, &bar);
     }
-    bool ok = false;
-    for (int it = 0; it < kSpinLimit; ++it) {
-      if (mbar_try_wait(&bar, 0)) { ok = true; break; }
-    }
+    const bool ok = mbar_wait_bounded(&bar, 0);
     // Every thread must agree; a timed-out copy falls back to reading the table from global
     // memory and raises the error flag for the host.
     staged = __syncthreads_and(ok);
@@ -122,8 +74,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_track(const TrackArgs a, int st
   const double* pool = reinterpret_cast<const double*>(tbl + a.hdr_bytes + a.ap_bytes);
   const Globals G = a.G;
   const int64_t n_work = *a.n_work;
-  const int64_t ld = a.ld;
   const double seg_ref = a.ref_prefix[a.ix_end] - a.ref_prefix[a.ix_start];
+
+  const SoA soa{a.vec, a.beta, a.t, a.state, a.ix_ele, a.ix_turn, a.location, a.ld};
 
   for (int64_t base = (int64_t)blockIdx.x * BLOCK; base < n_work; base += (int64_t)gridDim.x * BLOCK) {
     const int64_t w = base + threadIdx.x;
@@ -131,65 +84,20 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_track(const TrackArgs a, int st
     const int64_t j = valid ? (a.live ? (int64_t)a.live[w] : w) : 0;
     Particle p;
     p.state = 0;
-    if (valid) {
-      p.x = a.vec[j];
-      p.px = a.vec[ld + j];
-      p.y = a.vec[2 * ld + j];
-      p.py = a.vec[3 * ld + j];
-      p.z = a.vec[4 * ld + j];
-      p.pz = a.vec[5 * ld + j];
-      p.beta = a.beta[j];
-      p.state = a.state[j];
-    }
+    if (valid) load_particle(soa, j, p);
     bool alive = valid && p.state == S_ALIVE;
     const double z_in = p.z, beta_in = p.beta;
-    int lost_loc = 0, lost_ele = -1, lost_turn = -1;
+    LossInfo li;
     if (alive) refresh(p, G);
     for (int turn = 0; turn < a.n_turns; ++turn) {
-      if (alive) {
-        for (int ie = a.ix_start; ie < a.ix_end; ++ie) {
-          EleHdr h;
-          load_hdr(hdr, ie, h);
-          int loc = track1(p, h, pool, ap, G, turn == 0 && ie == a.ix_start);
-          if (loc) {
-            alive = false;
-            lost_loc = loc;
-            lost_ele = ie;
-            lost_turn = a.turn0 + turn;
-            break;
-          }
-        }
-      }
+      if (alive) alive = track_turn(p, hdr, pool, ap, G, a.ix_start, a.ix_end, turn == 0, a.turn0 + turn, li);
       if (a.moments) add_moments(p, alive, a.moments + (int64_t)turn * 28);
     }
-    if (valid && (alive || lost_loc)) {
-      a.vec[j] = p.x;
-      a.vec[ld + j] = p.px;
-      a.vec[2 * ld + j] = p.y;
-      a.vec[3 * ld + j] = p.py;
-      a.vec[4 * ld + j] = p.z;
-      a.vec[5 * ld + j] = p.pz;
-      a.beta[j] = p.beta;
-      a.state[j] = p.state;
-      if (a.t && beta_in > 0) {
-        // t + z/(beta c) advances by delta_ref_time in every element (track_a_*: orbit%t update),
-        // so the time follows from the reference time elapsed.
-        double elapsed = alive ? a.n_turns * seg_ref
-                               : (lost_turn - a.turn0) * seg_ref + (a.ref_prefix[lost_ele] - a.ref_prefix[a.ix_start]);
-        double tb = (p.beta > 0) ? p.z / (p.beta * kCLight) : 0.0;
-        a.t[j] = a.t[j] + (z_in / (beta_in * kCLight) + elapsed - tb);
-      }
-      if (!alive) {
-        if (a.ix_ele) a.ix_ele[j] = lost_ele;
-        if (a.ix_turn) a.ix_turn[j] = lost_turn;
-        if (a.location) a.location[j] = lost_loc;
-      }
-    }
+    if (valid) store_particle(soa, j, p, alive, li, z_in, beta_in, a.n_turns, a.turn0, seg_ref, a.ref_prefix, a.ix_start);
   }
   if (stage_smem && !staged) {
     // Let our own bulk copy drain (bounded) before the CTA's shared memory is released.
-    for (int it = 0; it < kSpinLimit; ++it)
-      if (mbar_try_wait(&bar, 0)) break;
+    mbar_wait_bounded(&bar, 0);
   }
 }
 
@@ -255,11 +163,14 @@ cudaError_t measure_fp64_peak(int sm_count, cudaStream_t stream, double* flops_p
 int table_fits_smem(uint32_t table_bytes) { return table_bytes <= 200 * 1024; }
 
 cudaError_t upload_constants() {
+  // the __constant__ tables exist once per translation unit: fill this one's and the batch kernel's
   double cm[22][22], cf[22][22];
   build_cmulti_tables(cm, cf);
   cudaError_t e = cudaMemcpyToSymbol(c_cmulti, cm, sizeof(cm));
   if (e != cudaSuccess) return e;
-  return cudaMemcpyToSymbol(c_cfull, cf, sizeof(cf));
+  e = cudaMemcpyToSymbol(c_cfull, cf, sizeof(cf));
+  if (e != cudaSuccess) return e;
+  return batch_upload_constants();
 }
 
 // Kernel variants: threads per CTA x minimum resident CTAs per SM (the register budget per

@@ -28,6 +28,14 @@ class Tuning(C.Structure):
                 ("turns_per_launch", C.c_int32), ("compact", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("block", C.c_int32), ("ctas_per_sm", C.c_int32), ("particles_per_thread", C.c_int32),
+                ("turns_per_launch", C.c_int32), ("stage_smem", C.c_int32), ("use_graph", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
+
+
+_BATCH_FIELDS = ("block", "ctas_per_sm", "particles_per_thread", "turns_per_launch", "stage_smem", "use_graph")
+
 _lib = None
 
 
@@ -62,6 +70,15 @@ def load(path=LIB_PATH):
         "bmadgpu_ctx_launch_count": ([V], C.c_int64),
         "bmadgpu_measure_fp64_peak": ([V, P(C.c_double)], C.c_int),
         "bmadgpu_autotune": ([V, V, P(abi.Bunch), C.c_int64, P(Tuning)], C.c_int),
+        "bmadgpu_batch_create": ([V, C.c_int32, P(V), P(C.c_int64), P(V)], C.c_int),
+        "bmadgpu_batch_destroy": ([V], C.c_int),
+        "bmadgpu_batch_view": ([V, C.c_int32, P(abi.Bunch)], C.c_int),
+        "bmadgpu_batch_upload": ([V, C.c_int32, P(abi.Bunch)], C.c_int),
+        "bmadgpu_batch_download": ([V, C.c_int32, P(abi.Bunch)], C.c_int),
+        "bmadgpu_batch_track": ([V, C.c_int32, C.c_int32], C.c_int),
+        "bmadgpu_batch_set_tuning": ([V, P(BatchTuning)], C.c_int),
+        "bmadgpu_batch_get_tuning": ([V, P(BatchTuning)], C.c_int),
+        "bmadgpu_batch_autotune": ([V, C.c_int32, P(BatchTuning)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name, None)
@@ -89,7 +106,7 @@ def check(code):
 def check_layout():
     """Compare ctypes struct sizes with the compiled library's sizeof()."""
     lib = load()
-    for i, st in enumerate((abi.Element, abi.Param, abi.Bunch, Tuning)):
+    for i, st in enumerate((abi.Element, abi.Param, abi.Bunch, Tuning, BatchTuning)):
         if lib.bmadgpu_sizeof(i) != C.sizeof(st):
             raise BmadGpuError(abi.EINVAL, "ABI size mismatch for %s" % st.__name__)
 
@@ -256,3 +273,121 @@ def track1_bunch(ctx, lat, bunch, ix_ele, turn=0):
     """One element for the whole bunch: the work of track1_bunch / track1_bunch_hom."""
     v = bunch.view()
     check(load().bmadgpu_track1_bunch(ctx.handle, lat.handle, C.byref(v), ix_ele, turn))
+
+
+class Batch:
+    """Many lattice variants with their own particle counts, tracked together (bmadgpu_batch):
+    one persistent launch per batch of turns, fed by a device work queue, replayed as a CUDA
+    graph. The batch owns the device particle state; ``upload``/``download`` move a variant's
+    particles (v = -1: all variants, concatenated in variant order)."""
+
+    def __init__(self, ctx, lattices, counts):
+        lib = load()
+        self.ctx = ctx
+        self.lattices = list(lattices)
+        self.counts = [int(c) for c in counts]
+        if len(self.lattices) != len(self.counts):
+            raise BmadGpuError(abi.EINVAL, "one particle count per lattice")
+        n = len(self.lattices)
+        hl = (C.c_void_p * n)(*[l.handle.value for l in self.lattices])
+        hc = (C.c_int64 * n)(*self.counts)
+        self._h = C.c_void_p()
+        check(lib.bmadgpu_batch_create(ctx.handle, n, hl, hc, C.byref(self._h)))
+        self.offsets = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def n_var(self):
+        return len(self.counts)
+
+    @property
+    def total(self):
+        return int(self.offsets[-1])
+
+    def view(self, v=-1):
+        """Device pointers (abi.Bunch) of variant v, or of the whole batch."""
+        b = abi.Bunch()
+        check(load().bmadgpu_batch_view(self._h, v, C.byref(b)))
+        return b
+
+    def upload(self, v, bunch):
+        """Copy a HostBunch into variant v (v = -1: a HostBunch of all particles in batch layout).
+        The copy is queued on the context stream; keep ``bunch`` alive until the next
+        synchronisation (download or ctx.synchronize)."""
+        hv = bunch.view()
+        check(load().bmadgpu_batch_upload(self._h, v, C.byref(hv)))
+
+    def download(self, v, bunch):
+        hv = bunch.view()
+        check(load().bmadgpu_batch_download(self._h, v, C.byref(hv)))
+
+    def track(self, n_turns, turn0=0):
+        """Queue n_turns turns of every variant (asynchronous; download or ctx.synchronize waits)."""
+        check(load().bmadgpu_batch_track(self._h, turn0, n_turns))
+
+    def get_tuning(self):
+        t = BatchTuning()
+        check(load().bmadgpu_batch_get_tuning(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k in _BATCH_FIELDS}
+
+    def set_tuning(self, **kw):
+        cur = self.get_tuning()
+        cur.update(kw)
+        t = BatchTuning(*[cur[k] for k in _BATCH_FIELDS])
+        check(load().bmadgpu_batch_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, sample_turns=0):
+        t = BatchTuning()
+        check(load().bmadgpu_batch_autotune(self._h, sample_turns, C.byref(t)))
+        return {k: getattr(t, k) for k in _BATCH_FIELDS}
+
+    def close(self):
+        if self._h:
+            load().bmadgpu_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def concat_bunches(bunches):
+    """One HostBunch holding the given bunches one after another, in the batch layout
+    (each bunch's [6, n] block contiguous)."""
+    n = sum(b.n for b in bunches)
+    out = HostBunch(np.zeros((6, n)), np.zeros(n))
+    flat = out.vec.reshape(-1)
+    at = 0
+    for b in bunches:
+        flat[6 * at:6 * (at + b.n)] = b.vec.reshape(-1)
+        out.beta[at:at + b.n] = b.beta
+        out.state[at:at + b.n] = b.state
+        at += b.n
+    out.t = np.zeros(n)
+    at = 0
+    for b in bunches:
+        if b.t is not None:
+            out.t[at:at + b.n] = b.t
+        at += b.n
+    return out
+
+
+def split_bunch(whole, counts):
+    """Inverse of concat_bunches: per-variant HostBunch copies from a batch-layout HostBunch."""
+    flat = whole.vec.reshape(-1)
+    out, at = [], 0
+    for n in counts:
+        b = HostBunch(flat[6 * at:6 * (at + n)].reshape(6, n), whole.beta[at:at + n],
+                      state=whole.state[at:at + n], t=None if whole.t is None else whole.t[at:at + n])
+        for f in ("ix_ele", "ix_turn", "location"):
+            src = getattr(whole, f)
+            if src is not None:
+                setattr(b, f, np.array(src[at:at + n], copy=True))
+        out.append(b)
+        at += n
+    return out

@@ -234,7 +234,59 @@ int64_t bmadgpu_ctx_launch_count(const bmadgpu_ctx* ctx);
 int bmadgpu_measure_fp64_peak(bmadgpu_ctx* ctx, double* flops_per_s);
 
 /* sizeof() of the ABI structs as this library was compiled, for binding checks. */
-int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning */
+int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning, 4 batch tuning */
+
+/* ---- Batched tracking of many lattice variants -------------------------------------------
+ * No single counterpart in the reference: it replaces a loop of long_term_tracking runs
+ * (bsim/modules/lt_tracking_mod.f90:1571-1715, each a track_bunch per turn) over lattice
+ * variants and dynamic-aperture grids (bmad/modules/dynamic_aperture_mod.f90:284-398), with
+ * every variant's particles tracked in one persistent kernel launch per batch of turns.
+ *
+ * A batch holds n_var (lattice, particle count) pairs and owns the device particle state of
+ * all of them: one structure-of-arrays block per variant, laid out one after another
+ * (vec: variant v's [6][n_v] block follows variant v-1's; beta, t, state, ix_ele, ix_turn and
+ * location likewise). Each launch hands out work items -- (variant, tile of live particles) --
+ * from a device counter; CTAs stage the item's element table in shared memory when the variant
+ * changes. Between launches the surviving particles of each variant are compacted (fused in the
+ * tracking kernel: warp ballot + one atomic per warp). The launch sequence of a call is captured
+ * once into a CUDA graph and replayed. Results per particle are bit-identical to
+ * bmadgpu_track_bunch_device on the same variant with the same turns_per_launch. */
+typedef struct bmadgpu_batch bmadgpu_batch;
+
+typedef struct bmadgpu_batch_tuning {
+  int32_t block;                /* threads per CTA: 64, 128, 256 or 512 */
+  int32_t ctas_per_sm;          /* register budget as in bmadgpu_tuning (0 = most registers) */
+  int32_t particles_per_thread; /* particles a thread tracks per work item: tile = block x this */
+  int32_t turns_per_launch;     /* turns per launch, compaction in between; 0 = one launch */
+  int32_t stage_smem;           /* stage each variant's element table in shared memory */
+  int32_t use_graph;            /* replay each call's launch sequence as a CUDA graph */
+  int32_t reserved[2];
+} bmadgpu_batch_tuning;
+
+/* counts[v] particles for lattices[v] (all lattices on the context's device; a lattice may
+ * appear more than once). Device state starts zeroed. */
+int bmadgpu_batch_create(bmadgpu_ctx* ctx, int32_t n_var, const bmadgpu_lattice* const* lattices,
+                         const int64_t* counts, bmadgpu_batch** out);
+int bmadgpu_batch_destroy(bmadgpu_batch* batch);
+/* Device pointers of variant v's particles (v = -1: the whole batch, n = total count). */
+int bmadgpu_batch_view(const bmadgpu_batch* batch, int32_t v, bmadgpu_bunch* device_view);
+/* Copies variant v (v = -1: all variants, in the batch layout) from host memory; enqueued on the
+ * context stream, so the host buffers must stay valid until the next synchronisation. Fields
+ * passed as NULL (t, ix_ele, ix_turn, location) are left as they are on the device. */
+int bmadgpu_batch_upload(bmadgpu_batch* batch, int32_t v, const bmadgpu_bunch* host);
+/* Copies variant v (v = -1: all) to host memory and waits for it. */
+int bmadgpu_batch_download(bmadgpu_batch* batch, int32_t v, bmadgpu_bunch* host);
+/* Tracks every variant's live particles through its whole lattice for n_turns turns numbered
+ * from turn0; enqueued on the context stream (bmadgpu_ctx_synchronize waits and reports a
+ * staging time-out). */
+int bmadgpu_batch_track(bmadgpu_batch* batch, int32_t turn0, int32_t n_turns);
+int bmadgpu_batch_set_tuning(bmadgpu_batch* batch, const bmadgpu_batch_tuning* tuning);
+int bmadgpu_batch_get_tuning(const bmadgpu_batch* batch, bmadgpu_batch_tuning* tuning);
+/* Autotuner: times trial calls of sample_turns turns (0: 8) for every launch shape, then
+ * particles per thread, then turns per launch, on the batch's current state, which it restores
+ * after each trial; sets the fastest and returns it in *chosen (nullable). */
+int bmadgpu_batch_autotune(bmadgpu_batch* batch, int32_t sample_turns, bmadgpu_batch_tuning* chosen);
+
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,213 @@
+"""Batched tracking of many lattice variants (bmadgpu_batch_*): one persistent launch per batch
+of turns over all variants, a device work queue, compaction fused into the tracking kernel,
+CUDA-graph replay.
+
+Checks: every variant's result is bit-identical to the plain single-lattice path on the same
+variant with the same turns per launch (same per-particle device code); the batch agrees with the
+oracle within the one-turn tolerance of test_gpu_parity; launch shape, particles per thread,
+table staging and graph replay do not change any bit; ragged, empty and single-particle
+variants; the autotuner leaves the state untouched; bad arguments fail with EINVAL."""
+import importlib
+
+import numpy as np
+import pytest
+
+from conftest import load_abi
+from helpers import coord_floor, oracle_track, rel_err
+
+pytestmark = pytest.mark.gpu
+lib = importlib.import_module("bmad-ecosystem_b200.lib")
+rings = importlib.import_module("bmad-ecosystem_b200.rings")
+abi = load_abi()
+
+FIELDS = ("vec", "beta", "state", "ix_ele", "ix_turn", "location", "t")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = lib.Context(0)
+    yield c
+    c.close()
+
+
+def variant_inputs(counts, n_cells=10, seed0=100):
+    """Perturbed rings (strengths, offsets, tilts) with dynamic-aperture grids out to 25 mm, so
+    some particles are lost within the first turns and compaction has work to do."""
+    out = []
+    for i, n in enumerate(counts):
+        eles, param = rings.perturbed_ring(n_cells, seed=seed0 + i)
+        vec = rings.da_grid(n) if n > 0 else np.zeros((6, 0))
+        rng = np.random.default_rng(seed0 + i)
+        t = rng.normal(0.0, 1e-9, n)
+        out.append((eles, param, vec, t))
+    return out
+
+
+def host_bunch(param, vec, t):
+    return lib.HostBunch.from_vec(vec, param, t=t)
+
+
+def run_batch(ctx, inputs, calls, **tuning):
+    lats = [lib.Lattice(ctx, e, p) for e, p, _, _ in inputs]
+    counts = [v.shape[1] for _, _, v, _ in inputs]
+    batch = lib.Batch(ctx, lats, counts)
+    if tuning:
+        batch.set_tuning(**tuning)
+    for i, (_, p, v, t) in enumerate(inputs):
+        batch.upload(i, host_bunch(p, v, t))
+    for turn0, n in calls:
+        batch.track(n, turn0=turn0)
+    res = []
+    for i, (_, p, v, t) in enumerate(inputs):
+        b = host_bunch(p, v, t)
+        batch.download(i, b)
+        res.append({f: getattr(b, f) for f in FIELDS})
+    batch.close()
+    return res
+
+
+def run_plain(ctx, inputs, calls, turns_per_launch):
+    ctx.set_tuning(block=128, ctas_per_sm=0, stage_smem=1, turns_per_launch=turns_per_launch, compact=1)
+    res = []
+    for e, p, v, t in inputs:
+        b = host_bunch(p, v, t)
+        if b.n:
+            lat = lib.Lattice(ctx, e, p)
+            for turn0, n in calls:
+                lib.track_bunch(ctx, lat, b, n_turns=n, turn0=turn0)
+        res.append({f: getattr(b, f) for f in FIELDS})
+    ctx.set_tuning(block=128, ctas_per_sm=0, stage_smem=1, turns_per_launch=0, compact=0)
+    return res
+
+
+def assert_identical(a, b, fields=FIELDS):
+    for i, (x, y) in enumerate(zip(a, b)):
+        for f in fields:
+            assert np.array_equal(x[f], y[f]), "variant %d field %s differs" % (i, f)
+
+
+COUNTS = [700, 1, 0, 2500, 333, 64]
+
+
+def test_batch_bit_identical_to_plain(ctx):
+    inputs = variant_inputs(COUNTS)
+    calls = [(0, 12)]
+    got = run_batch(ctx, inputs, calls, turns_per_launch=5)
+    want = run_plain(ctx, inputs, calls, turns_per_launch=5)
+    assert_identical(got, want)
+    lost = sum(int(np.sum(r["state"] != abi.ALIVE)) for r in got)
+    alive = sum(int(np.sum(r["state"] == abi.ALIVE)) for r in got)
+    assert lost > 0 and alive > 0   # the grid reaches beyond the aperture
+
+
+def test_batch_against_oracle(ctx):
+    inputs = variant_inputs([257, 96], n_cells=6, seed0=7)
+    got = run_batch(ctx, inputs, [(0, 2)], turns_per_launch=1)
+    for (e, p, v, t), g in zip(inputs, got):
+        o = oracle_track(e, p, v, 2, t=t)
+        assert np.array_equal(g["state"], o["state"])
+        lost = o["state"] != abi.ALIVE
+        assert np.array_equal(g["ix_ele"][lost], o["ix_ele"][lost])
+        assert np.array_equal(g["ix_turn"][lost], o["ix_turn"][lost])
+        assert np.array_equal(g["location"][lost], o["location"][lost])
+        alive = ~lost
+        fl = coord_floor(o["vec"][:, alive])
+        err = rel_err(g["vec"][:, alive], o["vec"][:, alive], fl)
+        assert err.max() <= 1e-11, err.max()
+
+
+@pytest.mark.parametrize("tuning", [
+    dict(block=64, ctas_per_sm=8, particles_per_thread=1, stage_smem=1, use_graph=1),
+    dict(block=256, ctas_per_sm=2, particles_per_thread=3, stage_smem=0, use_graph=1),
+    dict(block=512, ctas_per_sm=1, particles_per_thread=2, stage_smem=1, use_graph=0),
+    dict(block=128, ctas_per_sm=4, particles_per_thread=8, stage_smem=0, use_graph=0),
+])
+def test_batch_tuning_does_not_change_results(ctx, tuning):
+    inputs = variant_inputs(COUNTS, seed0=300)
+    calls = [(0, 9)]
+    ref = run_batch(ctx, inputs, calls, block=128, ctas_per_sm=0, particles_per_thread=1, turns_per_launch=4,
+                    stage_smem=1, use_graph=1)
+    got = run_batch(ctx, inputs, calls, turns_per_launch=4, **tuning)
+    assert_identical(got, ref)
+
+
+def test_batch_graph_replay_and_turn_numbers(ctx):
+    """Two calls of the same length replay one captured graph; turn numbers continue from turn0."""
+    inputs = variant_inputs([900, 40, 1500], seed0=500)
+    calls = [(0, 6), (6, 6), (12, 6)]
+    g = run_batch(ctx, inputs, calls, turns_per_launch=3, use_graph=1)
+    n = run_batch(ctx, inputs, calls, turns_per_launch=3, use_graph=0)
+    assert_identical(g, n)
+    p = run_plain(ctx, inputs, calls, turns_per_launch=3)
+    assert_identical(g, p)
+    turns = np.concatenate([r["ix_turn"][r["state"] != abi.ALIVE] for r in g])
+    assert turns.size and turns.min() >= 0 and turns.max() <= 17
+
+
+def test_batch_turns_per_launch_changes_no_coordinate(ctx):
+    """Compaction interval: coordinates and loss records are identical; t is recomputed per
+    launch from the reference time, so it may differ in the last bits."""
+    inputs = variant_inputs(COUNTS, seed0=900)
+    a = run_batch(ctx, inputs, [(0, 10)], turns_per_launch=0)
+    b = run_batch(ctx, inputs, [(0, 10)], turns_per_launch=3)
+    assert_identical(a, b, fields=("vec", "beta", "state", "ix_ele", "ix_turn", "location"))
+    for x, y in zip(a, b):
+        if x["t"].size:
+            assert np.max(np.abs(x["t"] - y["t"]) / np.maximum(np.abs(y["t"]), 1e-9)) < 1e-12
+
+
+def test_batch_autotune_keeps_state(ctx):
+    inputs = variant_inputs([3000, 17, 800], seed0=11)
+    lats = [lib.Lattice(ctx, e, p) for e, p, _, _ in inputs]
+    batch = lib.Batch(ctx, lats, [v.shape[1] for _, _, v, _ in inputs])
+    bunches = [host_bunch(p, v, t) for _, p, v, t in inputs]
+    for i, b in enumerate(bunches):
+        batch.upload(i, b)
+    chosen = batch.autotune(sample_turns=4)
+    assert chosen["block"] in (64, 128, 256, 512)
+    assert 1 <= chosen["turns_per_launch"] <= 4
+    for i, (_, p, v, t) in enumerate(inputs):
+        b = host_bunch(p, v, t)
+        b.vec[:] = 0
+        batch.download(i, b)
+        assert np.array_equal(b.vec, bunches[i].vec)
+        assert np.array_equal(b.state, bunches[i].state)
+        assert np.array_equal(b.t, bunches[i].t)
+    batch.close()
+
+
+def test_batch_whole_upload_download(ctx):
+    inputs = variant_inputs([100, 0, 55], seed0=21)
+    lats = [lib.Lattice(ctx, e, p) for e, p, _, _ in inputs]
+    counts = [v.shape[1] for _, _, v, _ in inputs]
+    batch = lib.Batch(ctx, lats, counts)
+    parts = [host_bunch(p, v, t) for _, p, v, t in inputs]
+    whole = lib.concat_bunches(parts)
+    batch.upload(-1, whole)
+    batch.track(3)
+    out = lib.HostBunch(np.zeros((6, whole.n)), np.zeros(whole.n), t=np.zeros(whole.n))
+    batch.download(-1, out)
+    per = run_batch(ctx, inputs, [(0, 3)])
+    for got, want in zip(lib.split_bunch(out, counts), per):
+        for f in ("vec", "beta", "state", "t", "ix_ele", "ix_turn", "location"):
+            assert np.array_equal(getattr(got, f), want[f]), f
+    batch.close()
+
+
+def test_batch_bad_arguments(ctx):
+    e, p = rings.ring(2)
+    lat = lib.Lattice(ctx, e, p)
+    with pytest.raises(lib.BmadGpuError) as ex:
+        lib.Batch(ctx, [lat], [-1])
+    assert ex.value.code == abi.EINVAL
+    batch = lib.Batch(ctx, [lat], [10])
+    with pytest.raises(lib.BmadGpuError):
+        batch.view(1)
+    wrong = lib.HostBunch(np.zeros((6, 11)), np.ones(11))
+    with pytest.raises(lib.BmadGpuError):
+        batch.upload(0, wrong)
+    with pytest.raises(lib.BmadGpuError):
+        batch.set_tuning(block=96)
+    with pytest.raises(lib.BmadGpuError):
+        batch.set_tuning(particles_per_thread=0)
+    batch.close()
