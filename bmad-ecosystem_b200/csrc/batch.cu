@@ -178,6 +178,12 @@ __global__ void k_batch_set_turns(BatchVar* vars, int n_var, int turn0, int n_tu
   }
 }
 
+__global__ void k_batch_init_list(int32_t* __restrict__ list, int64_t n, unsigned long long* __restrict__ count) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    list[i] = (int32_t)i;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *count = (unsigned long long)n;
+}
+
 struct Variant {
   int block, minb;
   const void* fn;
@@ -245,6 +251,14 @@ cudaError_t batch_launch_set_turns(BatchVar* vars, int32_t n_var, int32_t turn0,
   if (blocks < 1) blocks = 1;
   if (blocks > 1024) blocks = 1024;
   k_batch_set_turns<<<blocks, 256, 0, stream>>>(vars, n_var, turn0, n_turns);
+  return cudaGetLastError();
+}
+
+cudaError_t batch_launch_init_list(int32_t* list, int64_t n, unsigned long long* count, cudaStream_t stream) {
+  int64_t blocks = (n + 255) / 256;
+  if (blocks < 1) blocks = 1;
+  if (blocks > 1024) blocks = 1024;
+  k_batch_init_list<<<(unsigned)blocks, 256, 0, stream>>>(list, n, count);
   return cudaGetLastError();
 }
 

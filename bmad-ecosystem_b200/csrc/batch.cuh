@@ -70,4 +70,7 @@ cudaError_t batch_launch_plan(const BatchVar* vars, int32_t n_var, int32_t tile,
 cudaError_t batch_launch_set_turns(BatchVar* vars, int32_t n_var, int32_t turn0, int32_t n_turns,
                                    cudaStream_t stream);
 
+// A job's first live list: list[i] = i for i < n, *count = n.
+cudaError_t batch_launch_init_list(int32_t* list, int64_t n, unsigned long long* count, cudaStream_t stream);
+
 }  // namespace bmadgpu

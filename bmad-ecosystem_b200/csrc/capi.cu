@@ -231,6 +231,9 @@ int64_t bmadgpu_sizeof(int32_t which) {
     case 2: return (int64_t)sizeof(bmadgpu_bunch);
     case 3: return (int64_t)sizeof(bmadgpu_tuning);
     case 4: return (int64_t)sizeof(bmadgpu_batch_tuning);
+    case 5: return (int64_t)sizeof(bmadgpu_server_config);
+    case 6: return (int64_t)sizeof(bmadgpu_job_info);
+    case 7: return (int64_t)sizeof(bmadgpu_server_stats);
   }
   return -1;
 }

@@ -106,7 +106,8 @@ def check(code):
 def check_layout():
     """Compare ctypes struct sizes with the compiled library's sizeof()."""
     lib = load()
-    for i, st in enumerate((abi.Element, abi.Param, abi.Bunch, Tuning, BatchTuning)):
+    for i, st in enumerate((abi.Element, abi.Param, abi.Bunch, Tuning, BatchTuning, ServerConfig, JobInfo,
+                            ServerStats)):
         if lib.bmadgpu_sizeof(i) != C.sizeof(st):
             raise BmadGpuError(abi.EINVAL, "ABI size mismatch for %s" % st.__name__)
 
@@ -391,3 +392,148 @@ def split_bunch(whole, counts):
         out.append(b)
         at += n
     return out
+
+
+# ---- serving ---------------------------------------------------------------------------------
+
+class ServerConfig(C.Structure):
+    _fields_ = [("max_particles", C.c_int64), ("hbm_fraction", C.c_double), ("max_jobs", C.c_int32),
+                ("element_steps", C.c_int32), ("target_live", C.c_int64), ("policy", C.c_int32),
+                ("block", C.c_int32), ("ctas_per_sm", C.c_int32), ("stage_smem", C.c_int32),
+                ("reserved", C.c_int32 * 4)]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("rounds", C.c_int32), ("t_submit", C.c_double), ("t_admit", C.c_double),
+                ("t_done", C.c_double), ("particle_turns", C.c_int64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("jobs_submitted", C.c_int64), ("jobs_done", C.c_int64), ("rounds", C.c_int64),
+                ("particle_turns", C.c_int64), ("elapsed_s", C.c_double), ("latency_p50_s", C.c_double),
+                ("latency_p99_s", C.c_double), ("latency_max_s", C.c_double), ("capacity", C.c_int64),
+                ("peak_resident", C.c_int64)]
+
+
+SERVE_SRPT, SERVE_FIFO = 0, 1
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELLED = 0, 1, 2, 3
+
+
+def _serve_sigs(lib):
+    P, V = C.POINTER, C.c_void_p
+    sig = {
+        "bmadgpu_server_create": ([V, P(ServerConfig), P(V)], C.c_int),
+        "bmadgpu_server_destroy": ([V], C.c_int),
+        "bmadgpu_server_submit": ([V, V, P(abi.Bunch), C.c_int32, C.c_int32, P(C.c_int64)], C.c_int),
+        "bmadgpu_server_job": ([V, C.c_int64, P(JobInfo)], C.c_int),
+        "bmadgpu_server_wait": ([V, C.c_int64, C.c_double], C.c_int),
+        "bmadgpu_server_get_stats": ([V, P(ServerStats)], C.c_int),
+        "bmadgpu_host_alloc": ([C.c_int64, P(V)], C.c_int),
+        "bmadgpu_host_free": ([V], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    return lib
+
+
+class PinnedBunch(HostBunch):
+    """HostBunch whose arrays live in page-locked host memory (bmadgpu_host_alloc), so the
+    server's copies of it run asynchronously and overlap with tracking."""
+
+    def __init__(self, vec, beta, state=None, t=None, track_losses=True):
+        lib = _serve_sigs(load())
+        vec = np.asarray(vec, dtype=np.float64)
+        n = vec.shape[1]
+        self._blocks = []
+
+        def alloc(shape, dtype):
+            nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+            p = C.c_void_p()
+            check(lib.bmadgpu_host_alloc(max(nbytes, 8), C.byref(p)))
+            self._blocks.append(p.value)
+            buf = (C.c_char * max(nbytes, 8)).from_address(p.value)
+            return np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+        self.vec = alloc((6, n), np.float64)
+        self.vec[:] = vec
+        self.beta = alloc((n,), np.float64)
+        self.beta[:] = beta
+        self.state = alloc((n,), np.int32)
+        self.state[:] = abi.ALIVE if state is None else state
+        self.t = None
+        if t is not None:
+            self.t = alloc((n,), np.float64)
+            self.t[:] = t
+        if track_losses:
+            self.ix_ele = alloc((n,), np.int32)
+            self.ix_ele[:] = -1
+            self.ix_turn = alloc((n,), np.int32)
+            self.ix_turn[:] = -1
+            self.location = alloc((n,), np.int32)
+            self.location[:] = 0
+        else:
+            self.ix_ele = self.ix_turn = self.location = None
+
+    def free(self):
+        lib = load()
+        for p in self._blocks:
+            lib.bmadgpu_host_free(p)
+        self._blocks = []
+        self.vec = self.beta = self.state = self.t = self.ix_ele = self.ix_turn = self.location = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching tracking server (bmadgpu_server): jobs of any lattice, particle count
+    and turn count are submitted at any time and tracked together, with the particle state and the
+    lattice tables resident on the device. ``submit`` returns a job id; the bunch is written back
+    in place when the job is done."""
+
+    def __init__(self, ctx, **cfg):
+        lib = _serve_sigs(load())
+        self.ctx = ctx
+        c = ServerConfig()
+        for k, v in cfg.items():
+            setattr(c, k, v)
+        self._h = C.c_void_p()
+        check(lib.bmadgpu_server_create(ctx.handle, C.byref(c), C.byref(self._h)))
+        self._keep = {}
+
+    def submit(self, lat, bunch, n_turns, turn0=0):
+        v = bunch.view()
+        jid = C.c_int64()
+        check(load().bmadgpu_server_submit(self._h, lat.handle, C.byref(v), turn0, n_turns, C.byref(jid)))
+        self._keep[jid.value] = (lat, bunch)
+        return jid.value
+
+    def job(self, jid):
+        i = JobInfo()
+        check(load().bmadgpu_server_job(self._h, jid, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in JobInfo._fields_}
+
+    def wait(self, jid=-1, timeout=3600.0):
+        check(load().bmadgpu_server_wait(self._h, jid, timeout))
+
+    def stats(self):
+        s = ServerStats()
+        check(load().bmadgpu_server_get_stats(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in ServerStats._fields_}
+
+    def close(self):
+        if self._h:
+            load().bmadgpu_server_destroy(self._h)
+            self._h = C.c_void_p()
+            self._keep = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

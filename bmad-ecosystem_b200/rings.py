@@ -192,3 +192,35 @@ def da_grid(n, delta_values=(-0.01, 0.0, 0.01), r_max=0.025, n_rays=None):
         vec[0, k] = r_max * (k % 97 + 1) / 97
         k += 1
     return vec
+
+
+def fma_grid(n, x_max=0.02, y_max=0.01, delta=0.0):
+    """Frequency-map grid: particles on an nx x ny grid of starting amplitudes
+    (0, x_max] x (0, y_max] at momentum deviation delta, as frequency_map scans the x-y plane
+    (bsim/frequency_map/frequency_map.f90:183-330). Returns vec[6, n]."""
+    vec = np.zeros((6, n))
+    if n == 0:
+        return vec
+    nx = max(1, int(round(math.sqrt(n * x_max / y_max))))
+    ny = max(1, -(-n // nx))
+    k = np.arange(n)
+    vec[0] = x_max * (k % nx + 1) / nx
+    vec[2] = y_max * (k // nx + 1) / ny
+    vec[5] = delta
+    return vec
+
+
+def serving_stream(n_jobs, seed=0, mean_gap=5e-3, cells=(50, 100, 200, 400), n_range=(256, 262144),
+                   turn_range=(64, 4096)):
+    """A Poisson request stream of tracking jobs: arrival time, base ring (cells), perturbation
+    seed, particle count and turn count (both log-uniform), and kind ('gauss' or 'fma')."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(mean_gap, n_jobs))
+    out = []
+    for i in range(n_jobs):
+        n = int(round(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))))
+        turns = int(round(math.exp(rng.uniform(math.log(turn_range[0]), math.log(turn_range[1])))))
+        out.append(dict(arrival=float(t[i]), cells=int(cells[rng.integers(len(cells))]),
+                        variant_seed=int(rng.integers(1 << 30)), n=n, turns=turns,
+                        kind="gauss" if rng.random() < 0.5 else "fma"))
+    return out

@@ -234,7 +234,8 @@ int64_t bmadgpu_ctx_launch_count(const bmadgpu_ctx* ctx);
 int bmadgpu_measure_fp64_peak(bmadgpu_ctx* ctx, double* flops_per_s);
 
 /* sizeof() of the ABI structs as this library was compiled, for binding checks. */
-int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning, 4 batch tuning */
+int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning, 4 batch tuning,
+                                           5 server config, 6 job info, 7 server stats */
 
 /* ---- Batched tracking of many lattice variants -------------------------------------------
  * No single counterpart in the reference: it replaces a loop of long_term_tracking runs
@@ -286,6 +287,75 @@ int bmadgpu_batch_get_tuning(const bmadgpu_batch* batch, bmadgpu_batch_tuning* t
  * particles per thread, then turns per launch, on the batch's current state, which it restores
  * after each trial; sets the fastest and returns it in *chosen (nullable). */
 int bmadgpu_batch_autotune(bmadgpu_batch* batch, int32_t sample_turns, bmadgpu_batch_tuning* chosen);
+
+/* ---- Serving: continuous batching of tracking jobs -----------------------------------------
+ * No counterpart in the reference: it serves the jobs that Bmad programs run one at a time --
+ * long_term_tracking bunch runs (bsim/modules/lt_tracking_mod.f90:1571-1715), dynamic-aperture
+ * scans (bmad/modules/dynamic_aperture_mod.f90:284-398), frequency-map grids
+ * (bsim/frequency_map/frequency_map.f90:183-330) -- as requests arriving at any time.
+ *
+ * A server owns a resident particle arena in device memory, sized at creation from the free HBM,
+ * and a worker thread. Submitted jobs wait in a queue; the worker admits them (shortest remaining
+ * work first, or in arrival order) while job slots, arena space and the live-particle target
+ * allow, uploads their particles on a copy stream while the current round runs, and runs rounds:
+ * one persistent batched launch in which every resident job advances max(1, element_steps /
+ * n_ele) turns (the batched kernel, with fused compaction). Jobs finished after a round are
+ * copied back into the caller's host arrays on the copy stream, overlapping the next round, and
+ * their slot and arena space go to waiting jobs. Lattice tables stay resident (the caller's
+ * lattice objects must outlive the jobs that use them). A job's result is bit-identical to the
+ * plain path run alone with turns_per_launch equal to the job's turns per round. */
+typedef struct bmadgpu_server bmadgpu_server;
+
+enum { BMADGPU_SERVE_SRPT = 0, BMADGPU_SERVE_FIFO = 1 };
+enum { BMADGPU_JOB_QUEUED = 0, BMADGPU_JOB_RUNNING = 1, BMADGPU_JOB_DONE = 2, BMADGPU_JOB_CANCELLED = 3 };
+
+typedef struct bmadgpu_server_config {
+  int64_t max_particles;   /* resident particle capacity; 0 = hbm_fraction of the free device memory */
+  double hbm_fraction;     /* share of free device memory the arena may take (0: 0.5) */
+  int32_t max_jobs;        /* jobs resident at once (0: 4096) */
+  int32_t element_steps;   /* element passes per particle per round (0: 4096) */
+  int64_t target_live;     /* no admission while this many live particles are resident (0: 1,048,576) */
+  int32_t policy;          /* BMADGPU_SERVE_SRPT or BMADGPU_SERVE_FIFO */
+  int32_t block;           /* round kernel shape as bmadgpu_batch_tuning (0: 64) */
+  int32_t ctas_per_sm;     /* (0 with block 0: 12) */
+  int32_t stage_smem;      /* stage element tables of up to 64 KiB in shared memory */
+  int32_t reserved[4];
+} bmadgpu_server_config;
+
+typedef struct bmadgpu_job_info {
+  int32_t status;          /* BMADGPU_JOB_* */
+  int32_t rounds;          /* rounds the job took part in */
+  double t_submit, t_admit, t_done;  /* seconds on the server's clock (-1 when not reached) */
+  int64_t particle_turns;  /* turns tracked summed over particles (lost ones up to their loss) */
+} bmadgpu_job_info;
+
+typedef struct bmadgpu_server_stats {
+  int64_t jobs_submitted, jobs_done, rounds, particle_turns;
+  double elapsed_s;        /* first submission to the last completion */
+  double latency_p50_s, latency_p99_s, latency_max_s;  /* t_done - t_submit over finished jobs */
+  int64_t capacity;        /* resident particle capacity */
+  int64_t peak_resident;   /* most particles resident at once */
+} bmadgpu_server_stats;
+
+/* cfg may be NULL (all defaults). The server runs on the context's device with its own streams. */
+int bmadgpu_server_create(bmadgpu_ctx* ctx, const bmadgpu_server_config* cfg, bmadgpu_server** out);
+/* Cancels queued jobs, lets resident ones finish, stops the worker and frees the server. */
+int bmadgpu_server_destroy(bmadgpu_server* server);
+/* Queues a job: the bunch (host memory; pinned memory from bmadgpu_host_alloc lets its copies
+ * overlap with tracking) is tracked through the whole lattice for n_turns turns numbered from
+ * turn0 and written back in place. The bunch arrays must stay valid and untouched until the job is
+ * done. BMADGPU_ENOMEM if the bunch can never fit the arena, BMADGPU_EBUSY if the queue is full. */
+int bmadgpu_server_submit(bmadgpu_server* server, const bmadgpu_lattice* lat, bmadgpu_bunch* bunch, int32_t turn0,
+                          int32_t n_turns, int64_t* job_id);
+int bmadgpu_server_job(bmadgpu_server* server, int64_t job_id, bmadgpu_job_info* info);
+/* Waits until the job (job_id = -1: every submitted job) is done or cancelled; BMADGPU_ETIMEDOUT
+ * after timeout_s seconds. Also reports an error the worker met. */
+int bmadgpu_server_wait(bmadgpu_server* server, int64_t job_id, double timeout_s);
+int bmadgpu_server_get_stats(bmadgpu_server* server, bmadgpu_server_stats* stats);
+
+/* Page-locked host memory for bunch arrays (cudaHostAlloc / cudaFreeHost). */
+int bmadgpu_host_alloc(int64_t bytes, void** ptr);
+int bmadgpu_host_free(void* ptr);
 
 
 #ifdef __cplusplus

@@ -4,7 +4,7 @@ CUDA-graph replay.
 
 Checks: every variant's result is bit-identical to the plain single-lattice path on the same
 variant with the same turns per launch (same per-particle device code); the batch agrees with the
-oracle within the one-turn tolerance of test_gpu_parity; launch shape, particles per thread,
+oracle within the spread of 1-ulp libm differences, with bit-exact losses; launch shape, particles per thread,
 table staging and graph replay do not change any bit; ragged, empty and single-particle
 variants; the autotuner leaves the state untouched; bad arguments fail with EINVAL."""
 import importlib
@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from conftest import load_abi
-from helpers import coord_floor, oracle_track, rel_err
+from helpers import noise_track, oracle_track, per_particle_err
 
 pytestmark = pytest.mark.gpu
 lib = importlib.import_module("bmad-ecosystem_b200.lib")
@@ -101,19 +101,25 @@ def test_batch_bit_identical_to_plain(ctx):
 
 
 def test_batch_against_oracle(ctx):
+    """Losses bit-exact; coordinates within the spread that 1-ulp libm differences alone cause
+    (the grid reaches the dynamic aperture, where the sextupoles amplify ulps fastest), and
+    never above 1e-10 of the coordinate's RMS after two turns."""
     inputs = variant_inputs([257, 96], n_cells=6, seed0=7)
     got = run_batch(ctx, inputs, [(0, 2)], turns_per_launch=1)
     for (e, p, v, t), g in zip(inputs, got):
         o = oracle_track(e, p, v, 2, t=t)
+        z = noise_track(e, p, v, 2)
         assert np.array_equal(g["state"], o["state"])
         lost = o["state"] != abi.ALIVE
         assert np.array_equal(g["ix_ele"][lost], o["ix_ele"][lost])
         assert np.array_equal(g["ix_turn"][lost], o["ix_turn"][lost])
         assert np.array_equal(g["location"][lost], o["location"][lost])
         alive = ~lost
-        fl = coord_floor(o["vec"][:, alive])
-        err = rel_err(g["vec"][:, alive], o["vec"][:, alive], fl)
-        assert err.max() <= 1e-11, err.max()
+        eg = per_particle_err(g["vec"][:, alive], o["vec"][:, alive])
+        ez = per_particle_err(z["vec"][:, alive], o["vec"][:, alive])
+        assert eg.max() <= 1e-10, eg.max()
+        assert eg.max() <= 4 * ez.max() + 1e-12, (eg.max(), ez.max())
+        assert np.median(eg) <= 4 * np.median(ez) + 1e-13, (np.median(eg), np.median(ez))
 
 
 @pytest.mark.parametrize("tuning", [
