@@ -178,9 +178,8 @@ BG_HD void vjp_tilt(double c, double s, Adj& a) {
 BG_HD void vjp_bend_exact(const Particle& p, const double* __restrict__ b, Adj& a, const Globals& G) {
   double l = b[0], g = b[1], g_tot = b[2], dg = b[3], angle = b[4];
   double cos_a = b[5], sin_a = b[6], sinc_a = b[7], cosc_a = b[8], gl2_sincc = b[9];
-  double x = p.x, px = p.px, py = p.py, z = p.z, pz = p.pz;
+  double x = p.x, px = p.px, py = p.py, pz = p.pz;
   double rel = 1 + pz;
-  (void)z;
   if (dg == 0 && fabs(x * g) < 1e-9 && fabs(px) < 1e-9 && fabs(py) < 1e-9 && fabs(pz) < 1e-9) {
     double rpp = rel * G.p0c;
     double den = rpp * rpp + G.mass2;
@@ -352,8 +351,14 @@ struct AdjTape {
   BG_HD void push(const Particle& p) { in[n++] = p; }
 };
 
+#if defined(__CUDACC__)
+#define BG_HOST_DEVICE __host__ __device__ inline
+#else
+#define BG_HOST_DEVICE inline
+#endif
+
 // Which element bodies the adjoint covers (elements.cuh forms). 0 if supported.
-BG_HD int adj_supported(const EleHdr& h) {
+BG_HOST_DEVICE int adj_supported(const EleHdr& h) {
   switch (h.kind) {
     case K_MARKER:
     case K_DRIFT:

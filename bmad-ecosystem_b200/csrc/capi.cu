@@ -341,6 +341,7 @@ int bmadgpu_lattice_create(bmadgpu_ctx* c, const bmadgpu_element* eles, int32_t 
   }
   L->device = c->device;
   L->param = *param;
+  L->eles.assign(eles, eles + n_ele);
   L->G = make_globals(*param);
   cudaSetDevice(c->device);
   size_t nb = L->pk.image.size();

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/bmadgpu.h"
 #include "lattice.h"
@@ -56,5 +57,6 @@ struct bmadgpu_lattice {
   double* d_prefix = nullptr;
   bmadgpu::Globals G;
   bmadgpu_param param;
+  std::vector<bmadgpu_element> eles;  // the element records as given (attribute look-ups)
 };
 

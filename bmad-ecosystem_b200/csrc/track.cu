@@ -21,6 +21,10 @@
 #include "batch.cuh"
 
 namespace bmadgpu {
+cudaError_t adjoint_upload_constants();  // adjoint.cu
+}
+
+namespace bmadgpu {
 
 namespace {
 
@@ -170,7 +174,9 @@ cudaError_t upload_constants() {
   if (e != cudaSuccess) return e;
   e = cudaMemcpyToSymbol(c_cfull, cf, sizeof(cf));
   if (e != cudaSuccess) return e;
-  return batch_upload_constants();
+  e = batch_upload_constants();
+  if (e != cudaSuccess) return e;
+  return adjoint_upload_constants();
 }
 
 // Kernel variants: threads per CTA x minimum resident CTAs per SM (the register budget per

@@ -537,3 +537,26 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ---- differentiation -------------------------------------------------------------------------
+
+def loss_grad(ctx, lat, bunch, n_turns, param_ele, checkpoint_every=16):
+    """loss = mean over the bunch of x^2 + y^2 (particles alive after n_turns) and its gradient
+    with respect to the strengths (k1 / k2 / k3) of the elements param_ele, by the library's
+    adjoint kernel. The bunch (HostBunch) is not modified. Returns (loss, grad ndarray)."""
+    lib = load()
+    if not hasattr(lib, "_loss_grad_sig"):
+        lib.bmadgpu_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(abi.Bunch), C.c_int32, C.c_int32,
+                                          C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double)]
+        lib.bmadgpu_loss_grad.restype = C.c_int
+        lib._loss_grad_sig = True
+    idx = np.ascontiguousarray(param_ele, dtype=np.int32)
+    grad = np.zeros(len(idx))
+    loss = C.c_double()
+    v = bunch.view()
+    check(lib.bmadgpu_loss_grad(ctx.handle, lat.handle, C.byref(v), n_turns, checkpoint_every, len(idx),
+                                idx.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(loss),
+                                grad.ctypes.data_as(C.POINTER(C.c_double))))
+    return loss.value, grad

@@ -353,6 +353,23 @@ int bmadgpu_server_job(bmadgpu_server* server, int64_t job_id, bmadgpu_job_info*
 int bmadgpu_server_wait(bmadgpu_server* server, int64_t job_id, double timeout_s);
 int bmadgpu_server_get_stats(bmadgpu_server* server, bmadgpu_server_stats* stats);
 
+/* ---- Differentiation ------------------------------------------------------------------------
+ * No counterpart in the reference, which has no derivative of tracking with respect to element
+ * strengths other than Tao's one-sided finite differences (tao/code/tao_dmerit_mod.f90:162-180).
+ *
+ * loss = (1/n) sum over the particles still alive after n_turns of (x^2 + y^2), tracking the host
+ * bunch (vec, beta, state; left unchanged) through the whole lattice from turn 0. grad[i] =
+ * d(loss)/d(k) for element param_ele[i] (0-based): k1 of a quadrupole, k2 of a sextupole, k3 of
+ * an octupole; the element's strength must be non-zero and its other field coefficients must scale
+ * with it (no hkick/vkick; multipoles only with scale_multipoles). Computed by a hand-written
+ * adjoint of the element maps, one thread per particle, with a checkpoint every checkpoint_every
+ * turns and recomputation in between. Lattices with edge fringe, bends with k1 or multipoles,
+ * thin multipoles or elements of more than 16 steps give BMADGPU_EUNSUPPORTED. Lost particles
+ * leave the loss (the set of survivors is held fixed). */
+int bmadgpu_loss_grad(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const bmadgpu_bunch* host_bunch, int32_t n_turns,
+                      int32_t checkpoint_every, int32_t n_param, const int32_t* param_ele, double* loss,
+                      double* grad);
+
 /* Page-locked host memory for bunch arrays (cudaHostAlloc / cudaFreeHost). */
 int bmadgpu_host_alloc(int64_t bytes, void** ptr);
 int bmadgpu_host_free(void* ptr);
