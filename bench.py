@@ -15,6 +15,19 @@ the whole bunch included every step.
 --impl reference: the reference algorithm's CPU implementation (the C++ oracle restating the
 Fortran track1_bunch path, OpenMP over particles) on the host cores, bounded samples.
 
+Further workloads (one JSON line each, same keys):
+  batch256  256 perturbed 50-cell rings (strengths, offsets, tilts per variant seed), each with a
+            dynamic-aperture grid of log-uniform [1024, 65536] particles, 2048 turns; a step is the
+            whole job from the initial grids through the batched path (one persistent launch per
+            batch of turns, CUDA-graph replay, autotuned). Beside it: the plain kernel run variant
+            by variant on a random sample of the variants (ratio estimate of its aggregate).
+  serve     the Poisson request stream of tracking jobs (mean gap 5 ms; 50/100/200/400-cell
+            perturbed rings; log-uniform [256, 262144] particles and [64, 4096] turns; Gaussian or
+            frequency-map grid), the first --jobs jobs, through the continuous-batching server from
+            host memory; p50/p99 latency; beside it the plain kernel on a sample of the same jobs.
+  adjoint   d(loss)/d(100 quadrupole k1, 100 sextupole k2) on the 50-cell ring, 4096 particles,
+            256 turns, checkpoints every 16 turns; a step is one gradient.
+
 Multi-GPU: one process per GPU (torchrun); each rank tracks its own bunch (particles never
 interact: weak scaling, no collective on the data path); the timing is the max over ranks.
 """
@@ -173,6 +186,21 @@ def op_count(eles, p, scale):
     return sum(per), dict(zip(["add", "mul", "div", "sqrt", "transcendental"], per))
 
 
+def combine_ranks(total_ms, total_pt, e2e_s, e2e_pt, world, dev):
+    """Whole-job figures over ranks: the slowest rank's times (max) and every rank's
+    particle-turns (sum); each rank tracks its own particles (weak scaling)."""
+    import torch
+    import torch.distributed as dist
+    vals = torch.tensor([total_ms, float(total_pt), e2e_s, float(e2e_pt)], dtype=torch.float64, device=dev)
+    if world == 1:
+        return total_ms, float(total_pt), e2e_s, float(e2e_pt)
+    mx = vals.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = vals.clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return mx[0].item(), sm[1].item(), mx[2].item(), sm[3].item()
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -269,15 +297,7 @@ def run_ours(args):
         e2e_pt += int(alive1.sum()) * T + int((hb_e2e.ix_turn[lost_now] - turn + 1).sum())
         turn += T
     bytes_per = 6 * 8 + 8 + 4 * 4
-    vals = torch.tensor([total_ms, float(total_pt), e2e_s, float(e2e_pt)], dtype=torch.float64, device=dev)
-    if world > 1:
-        mx = vals.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = vals.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        total_ms_max, total_pt_sum, e2e_s_max, e2e_pt_sum = mx[0].item(), sm[1].item(), mx[2].item(), sm[3].item()
-    else:
-        total_ms_max, total_pt_sum, e2e_s_max, e2e_pt_sum = total_ms, float(total_pt), e2e_s, float(e2e_pt)
+    total_ms_max, total_pt_sum, e2e_s_max, e2e_pt_sum = combine_ranks(total_ms, total_pt, e2e_s, e2e_pt, world, dev)
     value = total_pt_sum / (total_ms_max / 1e3)
     e2e_value = e2e_pt_sum / e2e_s_max
 
@@ -320,6 +340,247 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def _timed(ctx, fn):
+    """Device time of fn() on the context stream (CUDA events, synchronised both sides)."""
+    import torch
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.synchronize()
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    ctx.synchronize()
+    return e0.elapsed_time(e1) / 1e3
+
+
+def _particle_turns(state, ix_turn, turn0, n_turns):
+    alive = state == abi.ALIVE
+    lost = ~alive & (ix_turn >= turn0)
+    return int(alive.sum()) * n_turns + int((ix_turn[lost] - turn0 + 1).sum())
+
+
+def _flush_l2(dev):
+    import torch
+    buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    buf.fill_(1.0)
+    torch.cuda.synchronize()
+
+
+def run_batch(args):
+    """256 lattice variants, dynamic-aperture grids, 2048 turns, batched path vs plain kernel."""
+    import torch
+    lib = importlib.import_module(PKG + ".lib")
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    n_var, n_turns = args.variants, 2048 if args.turns_per_step == 10 else args.turns_per_step
+    rng = np.random.default_rng(2)
+    counts = np.exp(rng.uniform(math.log(1024), math.log(65536), n_var)).astype(np.int64)
+    ctx = lib.Context(0)
+    lats, bunches = [], []
+    for v in range(n_var):
+        e, p = rings.perturbed_ring(50, seed=1000 + v)
+        lats.append(lib.Lattice(ctx, e, p))
+        bunches.append(lib.HostBunch.from_vec(rings.da_grid(int(counts[v])), p))
+    whole = lib.concat_bunches(bunches)
+    pinned = lib.PinnedBunch(whole.vec, whole.beta, state=whole.state, t=whole.t)
+    batch = lib.Batch(ctx, lats, counts)
+    batch.upload(-1, pinned)
+    tuning = batch.autotune(sample_turns=32)
+    out_b = lib.HostBunch(np.zeros((6, whole.n)), np.zeros(whole.n), t=np.zeros(whole.n))
+
+    def one_step(timed):
+        batch.upload(-1, pinned)
+        ctx.synchronize()
+        _flush_l2(dev)
+        s = _timed(ctx, lambda: batch.track(n_turns))
+        batch.download(-1, out_b)
+        return s, _particle_turns(out_b.state, out_b.ix_turn, 0, n_turns)
+
+    for _ in range(args.warmup):
+        one_step(False)
+    clocks = ClockSampler(0)
+    l0 = ctx.launch_count
+    tot_s, tot_pt = 0.0, 0
+    for _ in range(args.steps):
+        sec, pt = one_step(True)
+        tot_s += sec
+        tot_pt += pt
+    launches = ctx.launch_count - l0
+    clk = clocks.stop()
+    value = tot_pt / tot_s
+    # end to end: host arrays in, results out, every step, through the public API
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        batch.upload(-1, pinned)
+        batch.track(n_turns)
+        batch.download(-1, out_b)
+        e2e_s += time.perf_counter() - t0
+    e2e = tot_pt / e2e_s
+    # plain kernel, variant by variant, on a random sample (device-resident, its own autotuned
+    # launch shape, the batch's compaction interval)
+    sample = np.random.default_rng(5).choice(n_var, size=min(args.plain_sample, n_var), replace=False)
+    big = int(np.argmax(counts))
+    bt = {k: torch.from_numpy(np.array(getattr(bunches[big], k))).to(dev) for k in ("vec", "beta", "state")}
+    plain_tuning = lib.autotune(ctx, lats[big], abi.Bunch(bunches[big].n, bt["vec"].data_ptr(), bt["beta"].data_ptr(),
+                                                          None, bt["state"].data_ptr(), None, None, None))
+    ctx.set_tuning(turns_per_launch=tuning["turns_per_launch"], compact=1)
+    p_s, p_pt = 0.0, 0
+    for v in sample:
+        b = bunches[v]
+        t = {k: torch.from_numpy(np.array(getattr(b, k))).to(dev) for k in ("vec", "beta", "state", "ix_ele", "ix_turn",
+                                                                          "location")}
+        view = abi.Bunch(b.n, t["vec"].data_ptr(), t["beta"].data_ptr(), None, t["state"].data_ptr(),
+                         t["ix_ele"].data_ptr(), t["ix_turn"].data_ptr(), t["location"].data_ptr())
+        _flush_l2(dev)
+        sec = _timed(ctx, lambda: lib.check(lib.load().bmadgpu_track_bunch_device(
+            ctx.handle, lats[v].handle, ctypes.byref(view), 0, lats[v].n_ele, 0, n_turns, None)))
+        p_s += sec
+        p_pt += _particle_turns(t["state"].cpu().numpy(), t["ix_turn"].cpu().numpy(), 0, n_turns)
+    plain = p_pt / p_s
+    out = {
+        "metric": "particle-turns/s (FP64, batched 256-variant DA job)", "value": value, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (perturbed rings, dynamic-aperture grids)",
+        "config": {"workload": "batch256: %d perturbed 50-cell rings, %d particles (log-uniform 1024-65536 per "
+                               "variant), %d turns from the initial grids per step" % (n_var, int(counts.sum()), n_turns),
+                   "tuning": tuning, "l2": "flushed before each step (256 MiB write)"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(whole.n) * (8 * 8 + 4 * 4),
+                "d2h_bytes_per_step": int(whole.n) * (8 * 8 + 4 * 4)},
+        "plain_kernel": {"value": plain, "unit": UNIT, "ratio": value / plain,
+                         "sample": "%d of %d variants, each tracked alone (device-resident, autotuned shape %s, "
+                                   "compaction every %d turns), %.1f s" % (len(sample), n_var, plain_tuning,
+                                                                          tuning["turns_per_launch"], p_s)},
+        "gpu_launches": launches, "clocks": clk,
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_serve(args):
+    """The Poisson stream of tracking jobs through the continuous-batching server."""
+    import threading
+    import torch
+    lib = importlib.import_module(PKG + ".lib")
+    torch.cuda.set_device(0)
+    ctx = lib.Context(0)
+    stream = rings.serving_stream(args.jobs, seed=3)
+    jobs = []
+    t_prep = time.time()
+    for j in stream:
+        e, p = rings.perturbed_ring(j["cells"], seed=j["variant_seed"])
+        lat = lib.Lattice(ctx, e, p)
+        if j["kind"] == "gauss":
+            vec = rings.matched_gaussian(e, j["n"], seed=j["variant_seed"] % 100000)
+        else:
+            vec = rings.fma_grid(j["n"])
+        hb = lib.HostBunch.from_vec(vec, p)
+        jobs.append((j, lat, vec, hb.beta))
+    t_prep = time.time() - t_prep
+
+    def pinned_inputs():
+        return [lib.PinnedBunch(vec, beta) for (_, _, vec, beta) in jobs]
+
+    def run_stream(bunches):
+        srv = lib.Server(ctx)
+        start = time.perf_counter()
+        for (j, lat, _, _), b in zip(jobs, bunches):
+            dt = start + j["arrival"] - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            srv.submit(lat, b, j["turns"])
+        srv.wait(-1, timeout=7200)
+        st = srv.stats()
+        srv.close()
+        return st
+
+    # warm-up: a server with the first few jobs of the stream, shortened to 8 turns each
+    warm = lib.Server(ctx)
+    warm_b = [lib.PinnedBunch(vec, beta) for (_, _, vec, beta) in jobs[:3]]
+    for (j, lat, _, _), b in zip(jobs[:3], warm_b):
+        warm.submit(lat, b, 8)
+    warm.wait(-1, timeout=600)
+    warm.close()
+    clocks = ClockSampler(0)
+    l0 = ctx.launch_count
+    st = run_stream(pinned_inputs())
+    clk = clocks.stop()
+    value = st["particle_turns"] / st["elapsed_s"]
+    # plain kernel: jobs one after another (host buffers, synchronous), on a random sample
+    ctx.set_tuning(block=64, ctas_per_sm=12, stage_smem=0, turns_per_launch=64, compact=1)
+    sample = np.random.default_rng(7).choice(len(jobs), size=min(args.plain_sample, len(jobs)), replace=False)
+    p_s, p_pt = 0.0, 0
+    for k in sample:
+        j, lat, vec, beta = jobs[k]
+        b = lib.HostBunch(vec, beta)
+        t0 = time.perf_counter()
+        lib.track_bunch(ctx, lat, b, n_turns=j["turns"])
+        p_s += time.perf_counter() - t0
+        p_pt += _particle_turns(b.state, b.ix_turn, 0, j["turns"])
+    plain = p_pt / p_s
+    n_part = sum(j["n"] for j, _, _, _ in jobs)
+    out = {
+        "metric": "particle-turns/s (FP64, served mixed request stream)", "value": value, "unit": UNIT, "n_gpus": 1,
+        "steps": 1, "warmup": 1, "ms_per_step": 1e3 * st["elapsed_s"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (Poisson stream, perturbed rings, Gaussian / frequency-map grids)",
+        "config": {"workload": "serve: first %d jobs of the 2000-job stream (mean gap 5 ms), %d particles, "
+                               "50/100/200/400-cell rings" % (len(jobs), n_part),
+                   "host_prep_s": t_prep},
+        "latency_s": {"p50": st["latency_p50_s"], "p99": st["latency_p99_s"], "max": st["latency_max_s"]},
+        "server": {k: st[k] for k in ("jobs_done", "rounds", "particle_turns", "capacity", "peak_resident")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": n_part * (8 * 8 + 4 * 4),
+                "d2h_bytes_per_step": n_part * (8 * 8 + 4 * 4)},
+        "plain_kernel": {"value": plain, "unit": UNIT, "ratio": value / plain,
+                         "sample": "%d of %d jobs, one after another through bmadgpu_track_bunch (host buffers), "
+                                   "%.1f s" % (len(sample), len(jobs), p_s)},
+        "gpu_launches": ctx.launch_count - l0, "clocks": clk,
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_adjoint(args):
+    """Gradient of the tracking loss with respect to 200 strengths by the adjoint kernel."""
+    import torch
+    lib = importlib.import_module(PKG + ".lib")
+    torch.cuda.set_device(0)
+    ctx = lib.Context(0)
+    eles, p = rings.ring(50)
+    vec = rings.matched_gaussian(eles, 4096, seed=2)
+    param_ele = [i for i, e in enumerate(eles) if e.key in (abi.QUADRUPOLE, abi.SEXTUPOLE)]
+    lat = lib.Lattice(ctx, eles, p)
+    b = lib.HostBunch.from_vec(vec, p)
+    for _ in range(args.warmup):
+        lib.loss_grad(ctx, lat, b, 256, param_ele, 16)
+    clocks = ClockSampler(0)
+    l0 = ctx.launch_count
+    secs = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        loss, grad = lib.loss_grad(ctx, lat, b, 256, param_ele, 16)
+        secs.append(time.perf_counter() - t0)
+    clk = clocks.stop()
+    fd_check = None
+    gold = os.path.join(ROOT, "tests", "golden", "adjoint_config4_fd.json")
+    if os.path.exists(gold):
+        d = json.load(open(gold))
+        fd_check = [{"slot": e["slot"], "attr": e["attr"], "h": e["h"], "fd": e["fd"], "adjoint": float(grad[e["slot"]]),
+                     "rel_diff": abs(float(grad[e["slot"]]) - e["fd"]) / abs(e["fd"])} for e in d["entries"]]
+    s = sum(secs) / len(secs)
+    out = {
+        "metric": "gradient evaluations/s (FP64 adjoint, 200 strengths)", "value": 1 / s, "unit": "gradients/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * s, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded matched Gaussian bunch)",
+        "config": {"workload": "adjoint: 50-cell ring, 4096 particles, 256 turns, loss mean(x^2+y^2), "
+                               "d/d(100 quad k1, 100 sextupole k2), checkpoints every 16 turns"},
+        "forward_equivalent": {"value": 4096 * 256 / s, "unit": "particle-turns/s (forward part of the sweep)"},
+        "e2e": {"value": 1 / s, "unit": "gradients/s", "h2d_bytes_per_step": 4096 * (8 * 8 + 4),
+                "d2h_bytes_per_step": 8 * 201},
+        "loss": loss, "fd_check": fd_check, "gpu_launches": ctx.launch_count - l0, "clocks": clk,
+    }
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -353,7 +614,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["ring200", "ring50"], default="ring200")
+    ap.add_argument("--workload", choices=["ring200", "ring50", "batch256", "serve", "adjoint"], default="ring200")
+    ap.add_argument("--jobs", type=int, default=200, help="serve: number of jobs of the stream")
+    ap.add_argument("--variants", type=int, default=256, help="batch256: number of lattice variants")
+    ap.add_argument("--plain-sample", type=int, default=12, help="batch256/serve: variants/jobs timed on the plain path")
     ap.add_argument("--turns-per-step", type=int, default=10)
     ap.add_argument("--particles", type=int, default=0)
     args = ap.parse_args()
@@ -361,6 +625,12 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch256":
+        run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_ours(args)
 

@@ -1,7 +1,9 @@
 """Differentiation on the GPU (bmadgpu_loss_grad, autograd.TrackingLoss): d(loss)/d(quadrupole
 k1, sextupole k2) by the hand-written adjoint kernel.
 
-  - the device adjoint equals the host build of the same code (libm differences only);
+  - the device adjoint equals the host build of the same code up to the device libm's ulp
+    differences, amplified by the tracking as in the forward parity tests (loss 1e-10, gradient
+    1e-8 of the largest component);
   - it matches central finite differences of the oracle (the reference restatement) to 1e-6:
     quadrupoles at h = 1e-5 relative, sextupoles (gradients ~1e4 times smaller) at h = 5e-3; at
     the benchmark's h = 1e-7 the differences themselves carry ~1e-5 rounding noise;
@@ -55,11 +57,11 @@ def test_device_adjoint_equals_host_build(ctx):
     param_ele = [i for i, _ in names]
     loss_g, grad_g = gpu_loss_grad(ctx, eles, p, vec, 20, 7, param_ele)
     loss_h, grad_h, _, _ = host_loss_grad(ha, eles, p, vec, 20, 7)
-    assert abs(loss_g - loss_h) <= 1e-12 * abs(loss_h)
+    assert abs(loss_g - loss_h) <= 1e-10 * abs(loss_h)
     quads = np.array([k == "k1" for _, k in names])
     for fam in (quads, ~quads):
         rel = np.abs(grad_g[fam] - grad_h[fam]) / np.max(np.abs(grad_h[fam]))
-        assert rel.max() < 1e-9, rel.max()
+        assert rel.max() < 1e-8, rel.max()
 
 
 def test_gradient_matches_oracle_finite_differences(ctx):
@@ -103,13 +105,17 @@ def test_autograd_function_and_descent(ctx):
     loss = autograd.TrackingLoss.apply(k, prob)
     loss.backward()
     l0, g0 = gpu_loss_grad(ctx, eles, p, vec, 16, 8, param_ele)
-    assert float(loss) == l0
+    assert float(loss.detach()) == l0
     assert np.array_equal(k.grad.numpy(), g0)
-    # one small step against the gradient lowers the loss
+    # a small step against the gradient lowers the loss by what the gradient predicts
     with torch.no_grad():
-        k2 = k - 1e-4 * k.grad / k.grad.abs().max() * k.abs().max()
+        g = k.grad
+        alpha = 1e-6 * float(k.abs().max()) / float(g.abs().max())
+        k2 = k - alpha * g
     l1 = float(autograd.TrackingLoss.apply(k2, prob))
+    predicted = -alpha * float((g * g).sum())
     assert l1 < l0
+    assert abs((l1 - l0) - predicted) < 0.05 * abs(predicted), (l1 - l0, predicted)
 
 
 def test_unsupported_forms_refused(ctx):
@@ -124,3 +130,22 @@ def test_unsupported_forms_refused(ctx):
     with pytest.raises(lib.BmadGpuError) as ex:
         lib.loss_grad(ctx, lat, b, 4, [0])       # a drift has no strength
     assert ex.value.code == abi.EINVAL
+
+
+def test_full_size_gradient_matches_oracle_differences(ctx):
+    """The differentiation workload at full size (50-cell ring, 4096 particles, 256 turns,
+    checkpoints every 16) against the oracle's fourth-order central differences committed in
+    tests/golden/adjoint_config4_fd.json (tests/golden/make_adjoint_fd.py): <= 1e-6 relative. The
+    second-order differences at h = 1e-7 carry the tracking's rounding noise and are compared at
+    1e-4."""
+    import json
+    import os
+    from conftest import ROOT
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "adjoint_config4_fd.json")))
+    eles, p = rings.ring(d["n_cells"])
+    vec = rings.matched_gaussian(eles, d["n_particles"], seed=d["seed"])
+    loss, grad = gpu_loss_grad(ctx, eles, p, vec, d["n_turns"], 16, d["param_ele"])
+    assert abs(loss - d["loss"]) <= 1e-9 * d["loss"]
+    for e in d["entries"]:
+        rel = abs(grad[e["slot"]] - e["fd"]) / abs(e["fd"])
+        assert rel <= (1e-6 if e["order"] == 4 else 1e-4), (e, grad[e["slot"]], rel)
