@@ -39,11 +39,13 @@ _BATCH_FIELDS = ("block", "ctas_per_sm", "particles_per_thread", "turns_per_laun
 _lib = None
 
 
-def load(path=LIB_PATH):
-    """Load the shared library (built by csrc/Makefile). Raises if it is missing."""
+def load(path=None):
+    """Load the shared library (built by csrc/Makefile; BMADGPU_LIBRARY overrides the path).
+    Raises if it is missing."""
     global _lib
     if _lib is not None:
         return _lib
+    path = path or os.environ.get("BMADGPU_LIBRARY") or LIB_PATH
     if not os.path.exists(path):
         raise BmadGpuError(abi.EINVAL, "libbmadgpu.so not built: run make -C bmad-ecosystem_b200/csrc")
     lib = C.CDLL(path)
