@@ -83,6 +83,10 @@ int check_range(const bmadgpu_lattice* lat, int32_t ix_start, int32_t ix_end, in
   return BMADGPU_OK;
 }
 
+}  // namespace
+
+namespace bmadgpu {
+
 // Core device-side tracking: all bunch pointers are device pointers.
 int track_device(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch* b, int32_t ix_start,
                  int32_t ix_end, int32_t turn0, int32_t n_turns, double* d_moments) {
@@ -144,9 +148,6 @@ int track_device(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch
   return BMADGPU_OK;
 }
 
-}  // namespace
-
-namespace bmadgpu {
 
 Globals make_globals(const bmadgpu_param& p) {
   Globals g;
@@ -234,6 +235,8 @@ int64_t bmadgpu_sizeof(int32_t which) {
     case 5: return (int64_t)sizeof(bmadgpu_server_config);
     case 6: return (int64_t)sizeof(bmadgpu_job_info);
     case 7: return (int64_t)sizeof(bmadgpu_server_stats);
+    case 8: return (int64_t)sizeof(bmadgpu_bunch_data);
+    case 9: return (int64_t)sizeof(bmadgpu_ltt_params);
   }
   return -1;
 }

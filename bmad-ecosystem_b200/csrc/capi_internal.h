@@ -17,6 +17,11 @@ int cuda_fail(cudaError_t e, const char* what);
 Globals make_globals(const bmadgpu_param& p);
 // Reads and clears the context's device error flag (synchronises the context stream).
 int check_err_flag(bmadgpu_ctx* c);
+// Enqueues n_turns of tracking of a device-resident bunch on the context stream with the
+// context's tuning (chunks of turns_per_launch, live-list compaction between them); d_moments,
+// if not NULL, receives the per-turn sums [n_turns][28].
+int track_device(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch* b, int32_t ix_start,
+                 int32_t ix_end, int32_t turn0, int32_t n_turns, double* d_moments);
 }  // namespace bmadgpu
 
 #define CUDA_TRY(call)                                            \

@@ -109,7 +109,7 @@ def check_layout():
     """Compare ctypes struct sizes with the compiled library's sizeof()."""
     lib = load()
     for i, st in enumerate((abi.Element, abi.Param, abi.Bunch, Tuning, BatchTuning, ServerConfig, JobInfo,
-                            ServerStats)):
+                            ServerStats, BunchData, LttParams)):
         if lib.bmadgpu_sizeof(i) != C.sizeof(st):
             raise BmadGpuError(abi.EINVAL, "ABI size mismatch for %s" % st.__name__)
 
@@ -562,3 +562,70 @@ def loss_grad(ctx, lat, bunch, n_turns, param_ele, checkpoint_every=16):
                                 idx.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(loss),
                                 grad.ctypes.data_as(C.POINTER(C.c_double))))
     return loss.value, grad
+
+
+# ---- long-term tracking outputs --------------------------------------------------------------
+
+class BunchData(C.Structure):
+    _fields_ = [("n_live", C.c_int64), ("t", C.c_double), ("sigma_t", C.c_double), ("p0c", C.c_double),
+                ("centroid", C.c_double * 6), ("sigma_vec", C.c_double * 21), ("sig1", C.c_double * 6),
+                ("skew", C.c_double * 3), ("kurt", C.c_double * 3), ("sigma", C.c_double * 36),
+                ("emit", C.c_double * 3), ("norm_emit", C.c_double * 3), ("proj_emit", C.c_double * 3),
+                ("proj_beta", C.c_double * 3), ("proj_alpha", C.c_double * 3), ("eta", C.c_double * 2),
+                ("etap", C.c_double * 2), ("emit_valid", C.c_int32), ("reserved", C.c_int32)]
+
+    def as_dict(self):
+        out = {}
+        for f, _ in self._fields_:
+            v = getattr(self, f)
+            out[f] = np.array(v[:]) if hasattr(v, "_length_") else v
+        return out
+
+
+class LttParams(C.Structure):
+    _fields_ = [("n_turns", C.c_int32), ("averages_every_n_turns", C.c_int32), ("particle_every_n_turns", C.c_int32),
+                ("output_only_last_turns", C.c_int32), ("only_live_particles_out", C.c_int32),
+                ("reserved", C.c_int32), ("dead_cutoff", C.c_double), ("averages_file", C.c_char_p),
+                ("phase_space_file", C.c_char_p)]
+
+
+def _ltt_sigs(lib):
+    P, V = C.POINTER, C.c_void_p
+    for name, args in (("bmadgpu_bunch_stats", [V, V, P(abi.Bunch), P(BunchData)]),
+                       ("bmadgpu_bunch_data_from_sums", [P(C.c_double), C.c_double, C.c_double, P(BunchData)]),
+                       ("bmadgpu_ltt_run", [V, V, P(abi.Bunch), P(LttParams), P(C.c_int32)])):
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    return lib
+
+
+def bunch_data_from_sums(sums, p0c, mass):
+    """Host-only: the bunch data from the 63 two-pass sums (no GPU needed)."""
+    lib = _ltt_sigs(load())
+    s = np.ascontiguousarray(sums, dtype=np.float64)
+    bd = BunchData()
+    check(lib.bmadgpu_bunch_data_from_sums(s.ctypes.data_as(C.POINTER(C.c_double)), p0c, mass, C.byref(bd)))
+    return bd.as_dict()
+
+
+def bunch_stats(ctx, lat, device_view):
+    """Bunch data (ltt_calc_bunch_data) of a device-resident bunch."""
+    lib = _ltt_sigs(load())
+    bd = BunchData()
+    check(lib.bmadgpu_bunch_stats(ctx.handle, lat.handle, C.byref(device_view), C.byref(bd)))
+    return bd.as_dict()
+
+
+def ltt_run(ctx, lat, bunch, n_turns, averages_file=None, phase_space_file=None, averages_every_n_turns=-1,
+            particle_every_n_turns=-1, output_only_last_turns=0, only_live_particles_out=True, dead_cutoff=1.0):
+    """long_term_tracking's beam mode for a HostBunch (updated in place); returns turns tracked."""
+    lib = _ltt_sigs(load())
+    p = LttParams(n_turns, averages_every_n_turns, particle_every_n_turns, output_only_last_turns,
+                  1 if only_live_particles_out else 0, 0, dead_cutoff,
+                  averages_file.encode() if averages_file else None,
+                  phase_space_file.encode() if phase_space_file else None)
+    done = C.c_int32()
+    v = bunch.view()
+    check(lib.bmadgpu_ltt_run(ctx.handle, lat.handle, C.byref(v), C.byref(p), C.byref(done)))
+    return done.value

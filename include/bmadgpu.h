@@ -235,7 +235,8 @@ int bmadgpu_measure_fp64_peak(bmadgpu_ctx* ctx, double* flops_per_s);
 
 /* sizeof() of the ABI structs as this library was compiled, for binding checks. */
 int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning, 4 batch tuning,
-                                           5 server config, 6 job info, 7 server stats */
+                                           5 server config, 6 job info, 7 server stats,
+                                           8 bunch data, 9 ltt params */
 
 /* ---- Batched tracking of many lattice variants -------------------------------------------
  * No single counterpart in the reference: it replaces a loop of long_term_tracking runs
@@ -369,6 +370,52 @@ int bmadgpu_server_get_stats(bmadgpu_server* server, bmadgpu_server_stats* stats
 int bmadgpu_loss_grad(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const bmadgpu_bunch* host_bunch, int32_t n_turns,
                       int32_t checkpoint_every, int32_t n_param, const int32_t* param_ele, double* loss,
                       double* grad);
+
+/* ---- Long-term tracking outputs ------------------------------------------------------------
+ * Bunch data of ltt_calc_bunch_data / calc_bunch_params (bsim/modules/lt_tracking_mod.f90:
+ * 2369-2451, bmad/multiparticle/beam_utils.f90:1326-1690) over the live particles. */
+typedef struct bmadgpu_bunch_data {
+  int64_t n_live;
+  double t, sigma_t, p0c;       /* <t>, rms t, reference momentum */
+  double centroid[6];           /* <vec> */
+  double sigma_vec[21];         /* <v_i v_j> - <v_i><v_j>, i <= j, with the round-off zeroing rule (ltt .sigma) */
+  double sig1[6];               /* sqrt of its diagonal */
+  double skew[3], kurt[3];      /* x, y, z: <d^3>/sig^3 and <d^4>/sig^4 - 3 (n_live >= 10) */
+  double sigma[36];             /* centred sigma matrix <(v - <v>)(v - <v>)^T> */
+  double emit[3], norm_emit[3]; /* normal-mode a, b, c emittances (eigenvalues of sigma.S), n_live >= 6 */
+  double proj_emit[3], proj_beta[3], proj_alpha[3];  /* projected x, y, z (dispersion removed) */
+  double eta[2], etap[2];       /* x, y dispersion from the sigma matrix */
+  int32_t emit_valid;           /* 1 if the normal-mode analysis succeeded */
+  int32_t reserved;
+} bmadgpu_bunch_data;
+
+/* Bunch data of a device-resident bunch (two-pass device sums, deterministic reduction order). */
+int bmadgpu_bunch_stats(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const bmadgpu_bunch* device_bunch,
+                        bmadgpu_bunch_data* data);
+/* Host-only: bunch data from the 63 sums of the two passes (count, sum v, sum t, sum t^2,
+ * sum v_i v_j; centred sum d_i d_j, sum d^3, sum d^4), for callers with their own sums. */
+int bmadgpu_bunch_data_from_sums(const double* sums, double p0c, double mass, bmadgpu_bunch_data* data);
+
+/* ltt_run_beam_mode (lt_tracking_mod.f90:1571-1715) for one bunch with bmad_standard tracking:
+ * n_turns turns with the reference's stop conditions (no particle left; lost count reaching
+ * nint(dead_cutoff * n)), writing the averages files (<averages_file>.ave / .sigma / .emit, the
+ * reference's columns and number formats) and phase-space files (<phase_space_file> with the turn
+ * number, zero-padded, appended or put in place of '#'). Output schedules as the reference's
+ * *_output_every_n_turns: -1 last turn only, 0 first and last turn, n > 0 every n turns. The host
+ * bunch is updated to the final state; *turns_done receives the turns tracked. */
+typedef struct bmadgpu_ltt_params {
+  int32_t n_turns;
+  int32_t averages_every_n_turns;
+  int32_t particle_every_n_turns;
+  int32_t output_only_last_turns;   /* > 0: outputs only within the last this-many turns */
+  int32_t only_live_particles_out;  /* phase-space files list only live particles */
+  int32_t reserved;
+  double dead_cutoff;               /* 0 means 1 (the reference default) */
+  const char* averages_file;        /* NULL or "": no averages output */
+  const char* phase_space_file;     /* NULL or "": no phase-space output */
+} bmadgpu_ltt_params;
+int bmadgpu_ltt_run(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* host_bunch,
+                    const bmadgpu_ltt_params* params, int32_t* turns_done);
 
 /* Page-locked host memory for bunch arrays (cudaHostAlloc / cudaFreeHost). */
 int bmadgpu_host_alloc(int64_t bytes, void** ptr);

@@ -1,0 +1,143 @@
+"""numpy restatement of the long-term-tracking bunch data (test infrastructure, the checker):
+
+  ltt_calc_bunch_data            bsim/modules/lt_tracking_mod.f90:2369-2421
+  calc_bunch_params              bmad/multiparticle/beam_utils.f90:1326-1431
+  calc_bunch_sigma_matrix_etc    beam_utils.f90:1757-1844 (two passes, centred sums)
+  calc_emittances_and_twiss_from_sigma_matrix  beam_utils.f90:1454-1690 (projected Twiss)
+  mat_eigen                      sim_utils/matrix/mat_eigen.f90:37-187 (LAPACK geev through
+                                 numpy.linalg.eig, pairing and the greedy plane sort)
+
+Also the per-particle sums the device computes, for the host-only reduction test, and readers of
+the averages / phase-space files."""
+import numpy as np
+
+
+def two_pass_sums(vec, t, state):
+    """The 63 sums of the device's two passes, summed sequentially in particle order."""
+    alive = state == 1
+    v = vec[:, alive]
+    tt = t[alive] if t is not None else np.zeros(v.shape[1])
+    n = v.shape[1]
+    s1 = [float(n)] + [float(np.sum(v[i])) for i in range(6)] + [float(np.sum(tt)), float(np.sum(tt * tt))]
+    for i in range(6):
+        for j in range(i, 6):
+            s1.append(float(np.sum(v[i] * v[j])))
+    a = np.array(s1[1:7]) / n if n else np.zeros(6)
+    d = v - a[:, None]
+    s2 = []
+    for i in range(6):
+        for j in range(i, 6):
+            s2.append(float(np.sum(d[i] * d[j])))
+    s2 += [float(np.sum(d[i] ** 3)) for i in range(6)]
+    s2 += [float(np.sum(d[i] ** 4)) for i in range(6)]
+    return np.array(s1 + s2)
+
+
+def mat_eigen_emittances(sigma_s):
+    """Normal-mode emittances as mat_eigen + calc_emittances_and_twiss_from_sigma_matrix give them:
+    aimag of the odd eigenvalue of each pair after the sort and the normalisation flip."""
+    n = sigma_s.shape[0]
+    nn = n // 2
+    w, vr = np.linalg.eig(sigma_s)
+    # LAPACK (geev) returns complex-conjugate pairs in adjacent slots, positive imaginary part first
+    pairs = [(2 * k, 2 * k + 1) for k in range(nn)]
+    amp = np.zeros((nn, nn))
+    for ii, (p, q) in enumerate(pairs):
+        v = vr[:, p]
+        re, im = v.real, v.imag
+        for kk in range(nn):
+            amp[kk, ii] = np.sum(re[2 * kk:2 * kk + 2] ** 2) + np.sum(im[2 * kk:2 * kk + 2] ** 2)
+        amp[:, ii] /= np.sum(amp[:, ii])
+    sort = np.zeros(nn, int)
+    for _ in range(nn):
+        amp2 = amp.copy()
+        dmax = np.zeros(nn)
+        for jj in range(nn):
+            m = int(np.argmax(amp2[jj]))
+            amp2[jj, m] = -1
+            m2 = int(np.argmax(amp2[jj]))
+            dmax[jj] = amp[jj, m] - amp[jj, m2]
+        k = int(np.argmax(dmax))
+        m = int(np.argmax(amp[k]))
+        sort[m] = k
+        amp[k, :] = 0
+        amp[:, m] = 0
+    emit = np.zeros(3)
+    for ii, (p, q) in enumerate(pairs):
+        emit[sort[ii]] = abs(w[p].imag)
+    return emit
+
+
+def bunch_data(vec, t, state, p0c, mass):
+    """Dict of the bunch data fields (same names as lib.BunchData)."""
+    alive = state == 1
+    n = int(np.sum(alive))
+    out = dict(n_live=n, p0c=p0c)
+    if n == 0:
+        return out
+    v = vec[:, alive]
+    tt = t[alive] if t is not None else np.zeros(n)
+    avg = v.sum(axis=1) / n
+    out["centroid"] = avg
+    out["t"] = tt.sum() / n
+    out["sigma_t"] = np.sqrt(max(0.0, (tt * tt).sum() / n - out["t"] ** 2))
+    d = v - avg[:, None]
+    sig = (d @ d.T) / n
+    out["sigma"] = sig
+    f_emit = p0c * (1 + avg[5]) / mass
+    pe, pb, pa = np.zeros(3), np.zeros(3), np.zeros(3)
+    eta, etap = np.zeros(2), np.zeros(2)
+    for p, (i, j, xd, pxd) in enumerate([(0, 1, sig[0, 5], sig[1, 5]), (2, 3, sig[2, 5], sig[3, 5]),
+                                          (4, 5, 0.0, 0.0)]):
+        x2, px2, xpx = sig[i, i], sig[j, j], sig[i, j]
+        if sig[5, 5] != 0:
+            if p < 2:
+                eta[p], etap[p] = xd / sig[5, 5], pxd / sig[5, 5]
+            x2, xpx, px2 = x2 - xd ** 2 / sig[5, 5], xpx - xd * pxd / sig[5, 5], px2 - pxd ** 2 / sig[5, 5]
+        e = np.sqrt(max(0.0, x2 * px2 - xpx ** 2))
+        pe[p] = e
+        if e != 0:
+            pa[p], pb[p] = -xpx / e, x2 / e
+    out.update(proj_emit=pe, proj_beta=pb, proj_alpha=pa, eta=eta, etap=etap)
+    if n >= 6:
+        S = np.zeros((6, 6))
+        for k in range(3):
+            S[2 * k + 1, 2 * k] = -1
+            S[2 * k, 2 * k + 1] = 1
+        ss = sig @ S
+        cut = 1e-20 * np.max(np.abs(sig))
+        dim = 4 if (abs(sig[4, 4]) < cut or abs(sig[5, 5]) < cut) else 6
+        out["emit"] = mat_eigen_emittances(ss[:dim, :dim])
+        out["norm_emit"] = out["emit"] * f_emit
+    if n < 10:
+        return out
+    s_sum = v.sum(axis=1)
+    sv, sig1 = [], np.zeros(6)
+    for i in range(6):
+        for j in range(i, 6):
+            x = np.sum(v[i] * v[j]) / n - s_sum[i] * s_sum[j] / n ** 2
+            if abs(x) < 1e-15 * abs(s_sum[i] * s_sum[j]) / n:
+                x = 0.0
+            sv.append(x)
+            if i == j:
+                sig1[i] = np.sqrt(max(0.0, x))
+    out["sigma_vec"] = np.array(sv)
+    out["sig1"] = sig1
+    skew, kurt = np.zeros(3), np.zeros(3)
+    for p, i in enumerate((0, 2, 4)):
+        if sig1[i] != 0:
+            ave = s_sum[i] / n
+            skew[p] = np.sum((v[i] - ave) ** 3) / (n * sig1[i] ** 3)
+            kurt[p] = np.sum((v[i] - ave) ** 4) / (n * sig1[i] ** 4) - 3.0
+    out.update(skew=skew, kurt=kurt)
+    return out
+
+
+def read_table(path):
+    """Rows of numbers of an LTT output file (comment lines start with '#')."""
+    rows = []
+    for line in open(path):
+        if line.startswith("#") or not line.strip():
+            continue
+        rows.append(line.split())
+    return rows

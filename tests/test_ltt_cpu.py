@@ -1,0 +1,60 @@
+"""Long-term-tracking bunch data on CPU: the library's host reduction (bunchdata.cpp, through
+bmadgpu_bunch_data_from_sums, which needs no GPU) against the numpy restatement of
+ltt_calc_bunch_data / calc_bunch_params / mat_eigen (tests/ltt_reference.py) on synthetic
+bunches: uncoupled and coupled (x-y and x-z), with and without an energy spread, with lost
+particles, and below the 10- and 6-particle thresholds of the reference."""
+import importlib
+
+import numpy as np
+import pytest
+
+from ltt_reference import bunch_data, two_pass_sums
+
+lib = importlib.import_module("bmad-ecosystem_b200.lib")
+abi = importlib.import_module("bmad-ecosystem_b200.abi")
+
+P0C, MASS = 3e9, 0.51099895069e6
+
+
+def bunch(n, seed, couple=0.0, sig_pz=1e-3, lost_frac=0.0):
+    rng = np.random.default_rng(seed)
+    r = rng.standard_normal((6, n))
+    sig = np.array([3e-4, 2e-5, 4e-5, 3e-6, 3e-3, sig_pz])
+    v = r * sig[:, None]
+    v[0] += 1.5 * v[5]                      # dispersion
+    v[2] += couple * v[0]                   # x-y coupling
+    v[1] -= 0.3 * v[0] / 10                 # alpha
+    v[4] += couple * 5 * v[0]               # x-z correlation
+    v += np.array([1e-5, -2e-7, 3e-6, 1e-8, 2e-4, 1e-5])[:, None]
+    t = rng.normal(1e-6, 1e-11, n)
+    state = np.ones(n, np.int32)
+    state[rng.random(n) < lost_frac] = 4
+    return v, t, state
+
+
+@pytest.mark.parametrize("case", [dict(n=5000, seed=1), dict(n=5000, seed=2, couple=0.05),
+                                  dict(n=20000, seed=3, couple=0.2, lost_frac=0.1),
+                                  dict(n=3000, seed=4, sig_pz=0.0), dict(n=8, seed=5), dict(n=5, seed=6)])
+def test_host_reduction_matches_reference(case):
+    v, t, st = bunch(**case)
+    got = lib.bunch_data_from_sums(two_pass_sums(v, t, st), P0C, MASS)
+    want = bunch_data(v, t, st, P0C, MASS)
+    assert got["n_live"] == want["n_live"]
+    keys = ["centroid", "t", "sigma_t", "sigma", "proj_emit", "proj_beta", "proj_alpha", "eta", "etap",
+            "sigma_vec", "sig1", "skew", "kurt", "emit", "norm_emit"]
+    if case.get("sig_pz", 1e-3) == 0.0:
+        # <pz.pz> is rounding noise: dispersion and projected Twiss divide by it in both codes
+        keys = [k for k in keys if not k.startswith("proj_") and k not in ("eta", "etap")]
+    for k in keys:
+        if k not in want:
+            assert np.all(np.asarray(got[k]) == 0), k      # not computed below the thresholds
+            continue
+        g, w = np.asarray(got[k], float).ravel(), np.asarray(want[k], float).ravel()
+        if k == "sigma":
+            g = g.reshape(6, 6).ravel()
+        scale = np.max(np.abs(w)) if np.any(w) else 1.0
+        assert np.allclose(g, w, rtol=1e-10, atol=1e-12 * scale), (k, g, w)
+    if want["n_live"] >= 6:
+        assert got["emit_valid"] == 1
+        if case.get("sig_pz", 1e-3) == 0.0:
+            assert got["emit"][2] == 0.0     # no energy spread: transverse modes only (dim = 4)

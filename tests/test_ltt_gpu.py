@@ -1,0 +1,120 @@
+"""Long-term tracking outputs on the GPU (bmadgpu_bunch_stats, bmadgpu_ltt_run):
+
+  - the device two-pass sums give the same bunch data as the numpy restatement of
+    ltt_calc_bunch_data on the same particles;
+  - ltt_run's averages files (.ave, .sigma, .emit) and phase-space files hold, at every output
+    turn, what the oracle's tracking to that turn gives through the restated statistics, to the
+    printed precision (es14.6 / es16.8), and the reference's column layout;
+  - the stop conditions: with dead_cutoff, tracking ends at the first turn where the lost count
+    reaches nint(dead_cutoff * n), as the reference's turn loop does, and no output is written for
+    that turn."""
+import glob
+import importlib
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_abi
+from helpers import oracle_track
+from ltt_reference import bunch_data, read_table
+
+pytestmark = pytest.mark.gpu
+lib = importlib.import_module("bmad-ecosystem_b200.lib")
+rings = importlib.import_module("bmad-ecosystem_b200.rings")
+abi = load_abi()
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = lib.Context(0)
+    yield c
+    c.close()
+
+
+def close(got, want, rel, what):
+    got, want = np.asarray(got, float), np.asarray(want, float)
+    scale = np.maximum(np.abs(want), 1e-300)
+    assert np.all(np.abs(got - want) <= rel * scale + 1e-300), (what, got, want)
+
+
+def test_device_stats_match_reference(ctx):
+    eles, p = rings.ring(50)
+    vec = rings.matched_gaussian(eles, 50000, seed=11, scale=2.0)
+    hb = lib.HostBunch.from_vec(vec, p, t=np.random.default_rng(1).normal(0, 1e-11, 50000))
+    lat = lib.Lattice(ctx, eles, p)
+    lib.track_bunch(ctx, lat, hb, n_turns=7)
+    dev = torch.device("cuda", 0)
+    t = {k: torch.from_numpy(np.array(getattr(hb, k))).to(dev) for k in ("vec", "beta", "t", "state")}
+    view = abi.Bunch(hb.n, t["vec"].data_ptr(), t["beta"].data_ptr(), t["t"].data_ptr(), t["state"].data_ptr(),
+                     None, None, None)
+    got = lib.bunch_stats(ctx, lat, view)
+    want = bunch_data(hb.vec, hb.t, hb.state, p.p0c, p.mass)
+    assert got["n_live"] == want["n_live"]
+    for k in ("centroid", "t", "sigma_t", "sigma_vec", "sig1", "skew", "kurt", "proj_emit", "emit"):
+        w = np.asarray(want[k], float).ravel()
+        g = np.asarray(got[k], float).ravel()
+        assert np.allclose(g, w, rtol=1e-9, atol=1e-13 * np.max(np.abs(w))), (k, g, w)
+
+
+def test_ltt_run_outputs_match_oracle(ctx, tmp_path):
+    eles, p = rings.ring(50)
+    n, n_turns = 3000, 20
+    vec = rings.matched_gaussian(eles, n, seed=4, scale=4.0)
+    hb = lib.HostBunch.from_vec(vec, p, t=np.zeros(n))
+    lat = lib.Lattice(ctx, eles, p)
+    base = str(tmp_path / "run")
+    done = lib.ltt_run(ctx, lat, hb, n_turns, averages_file=base, phase_space_file=str(tmp_path / "ps#.dat"),
+                       averages_every_n_turns=5, particle_every_n_turns=10)
+    assert done == n_turns
+    ave, sig, emi = (read_table(base + ext) for ext in (".ave", ".sigma", ".emit"))
+    turns = [int(r[0]) for r in ave]
+    assert turns == [0, 5, 10, 15, 20]
+    for line in open(base + ".sigma"):
+        if line.startswith("##") and "Turn" in line:
+            assert "<x.x>" in line and "<pz.pz>" in line
+    for row_a, row_s, row_e in zip(ave, sig, emi):
+        T = int(row_a[0])
+        o = oracle_track(eles, p, vec, T, t=np.zeros(n)) if T > 0 else dict(
+            vec=vec, t=np.zeros(n), state=np.ones(n, np.int32))
+        w = bunch_data(o["vec"], o["t"], o["state"], p.p0c, p.mass)
+        assert int(row_a[1]) == w["n_live"] == int(row_s[1]) == int(row_e[1])
+        close([float(x) for x in row_a[7:13]], w["centroid"], 2e-6, "centroid T=%d" % T)
+        close([float(x) for x in row_a[15:21]], w["sig1"], 2e-6, "sig1 T=%d" % T)
+        close([float(x) for x in row_s[3:24]], w["sigma_vec"], 2e-6, "sigma T=%d" % T)
+        close([float(x) for x in row_e[3:6]], w["emit"], 2e-6, "emit T=%d" % T)
+        close([float(x) for x in row_e[6:9]], w["kurt"], 2e-5, "kurt T=%d" % T)
+    files = sorted(glob.glob(str(tmp_path / "ps*.dat")))
+    assert [os.path.basename(f) for f in files] == ["ps00.dat", "ps10.dat", "ps20.dat"]
+    rows = read_table(str(tmp_path / "ps10.dat"))
+    o = oracle_track(eles, p, vec, 10, t=np.zeros(n))
+    alive = np.nonzero(o["state"] == abi.ALIVE)[0]
+    assert [int(r[0]) - 1 for r in rows] == list(alive)          # only live particles, 1-based index
+    assert all(int(r[1]) == 10 and r[-1] == "Alive" for r in rows)
+    coords = np.array([[float(x) for x in r[2:8]] for r in rows]).T
+    scale = np.sqrt(np.mean(o["vec"][:, alive] ** 2, axis=1))[:, None]
+    assert np.max(np.abs(coords - o["vec"][:, alive]) / scale) < 1e-7
+
+
+def test_dead_cutoff_stops_at_the_reference_turn(ctx, tmp_path):
+    eles, p = rings.ring(50)
+    n, n_turns = 4000, 40
+    vec = rings.da_grid(n, r_max=0.02)
+    o = oracle_track(eles, p, vec, n_turns)
+    lost_turn = np.where(o["state"] != abi.ALIVE, o["ix_turn"], n_turns + 1)
+    cutoff = 0.3
+    limit = int(np.rint(cutoff * n))
+    # after turn i the lost count is #(lost_turn <= i); the loop exits after the first such turn
+    stop = next(i + 1 for i in range(n_turns) if np.sum(lost_turn <= i) >= limit)
+    assert stop < n_turns
+    hb = lib.HostBunch.from_vec(vec, p)
+    lat = lib.Lattice(ctx, eles, p)
+    base = str(tmp_path / "cut")
+    done = lib.ltt_run(ctx, lat, hb, n_turns, averages_file=base, averages_every_n_turns=1, dead_cutoff=cutoff)
+    assert done == stop
+    turns = [int(r[0]) for r in read_table(base + ".ave")]
+    assert turns == list(range(0, stop))            # nothing written for the stopping turn
+    o2 = oracle_track(eles, p, vec, stop)
+    assert np.array_equal(hb.state, o2["state"])
+    assert np.array_equal(hb.ix_turn[hb.state != abi.ALIVE], o2["ix_turn"][o2["state"] != abi.ALIVE])
