@@ -118,3 +118,10 @@ def test_dead_cutoff_stops_at_the_reference_turn(ctx, tmp_path):
     o2 = oracle_track(eles, p, vec, stop)
     assert np.array_equal(hb.state, o2["state"])
     assert np.array_equal(hb.ix_turn[hb.state != abi.ALIVE], o2["ix_turn"][o2["state"] != abi.ALIVE])
+    # the same with outputs only at the end: the stop falls inside one long chunk, which is re-run
+    # from its start for exactly the turns up to the stop
+    hb2 = lib.HostBunch.from_vec(vec, p)
+    done2 = lib.ltt_run(ctx, lat, hb2, n_turns, averages_file=str(tmp_path / "cut2"), dead_cutoff=cutoff)
+    assert done2 == stop
+    assert np.array_equal(hb2.vec, hb.vec) and np.array_equal(hb2.state, hb.state)
+    assert read_table(str(tmp_path / "cut2.ave")) == []          # the last turn was never reached
