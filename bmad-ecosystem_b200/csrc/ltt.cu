@@ -313,6 +313,16 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
   const int n_ele = (int)lat->pk.info.n_ele;
   const std::string ave_base = P->averages_file ? P->averages_file : "";
   const std::string ps_base = P->phase_space_file ? P->phase_space_file : "";
+  const std::string beam_base = P->beam_file ? P->beam_file : "";
+  if (P->ix_turn_start < 0 || P->ix_turn_start > P->n_turns) return fail(BMADGPU_EINVAL, "ix_turn_start out of range");
+  // ltt_write_beam_file's schedule: every beam_every_n_turns turns, and always at n_turns
+  auto wants_beam = [&](int turn) {
+    if (beam_base.empty()) return false;
+    const int nt = P->beam_every_n_turns;
+    if (nt > 0 && P->output_only_last_turns > 0 && P->n_turns - turn >= P->output_only_last_turns) return false;
+    if ((nt <= 0 || turn % nt != 0) && turn != P->n_turns) return false;
+    return true;
+  };
   const double cutoff = P->dead_cutoff > 0 ? P->dead_cutoff : 1.0;
   const int64_t dead_limit = (int64_t)std::llround(cutoff * (double)n);
   DevBunch cur, save;
@@ -377,16 +387,48 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
     }
     return BMADGPU_OK;
   };
+  auto beam_output = [&](int turn) -> int {
+    if (!wants_beam(turn)) return BMADGPU_OK;
+    std::vector<double> bv(6 * n), bb(n), bt(n);
+    std::vector<int32_t> bs(n), be(n), bl(n);
+    bmadgpu_bunch h;
+    h.n = n;
+    h.vec = bv.data();
+    h.beta = bb.data();
+    h.t = bt.data();
+    h.state = bs.data();
+    h.ix_ele = be.data();
+    h.ix_turn = nullptr;
+    h.location = bl.data();
+    CUDA_TRY(cudaMemcpyAsync(h.vec, cur.b.vec, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(h.beta, cur.b.beta, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(h.t, cur.b.t, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(h.state, cur.b.state, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(h.ix_ele, cur.b.ix_ele, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(h.location, cur.b.location, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    // "<stem>-<turn, zero-padded to the digits of n_turns><.ext>"
+    const int width = (int)std::log10(P->n_turns + 0.1) + 1;
+    char num[32];
+    std::snprintf(num, sizeof num, "%0*d", width, turn);
+    std::string name;
+    const size_t dot = beam_base.find_last_of('.');
+    name = dot == std::string::npos ? beam_base + "-" + num : beam_base.substr(0, dot) + "-" + num + beam_base.substr(dot);
+    if (bmadgpu_beam_write_ascii(name.c_str(), &h, &lat->param, 0.0, P->beam_exact ? BMADGPU_BEAM_EXACT : 0))
+      return fail(BMADGPU_EINVAL, "cannot write the beam file " + name);
+    return BMADGPU_OK;
+  };
 
-  int r = outputs(0);
+  int r = P->ix_turn_start == 0 ? outputs(0) : BMADGPU_OK;
   if (r) return r;
-  int turn = 0;
+  int turn = P->ix_turn_start;
   bool stopped = false;
   while (turn < P->n_turns && !stopped) {
     int next = turn + 1;
     while (next < P->n_turns && next - turn < kChunk &&
            !(wants(P->averages_every_n_turns, P->output_only_last_turns, P->n_turns, next) && !ave_base.empty()) &&
-           !(wants(P->particle_every_n_turns, P->output_only_last_turns, P->n_turns, next) && !ps_base.empty()))
+           !(wants(P->particle_every_n_turns, P->output_only_last_turns, P->n_turns, next) && !ps_base.empty()) &&
+           !wants_beam(next))
       ++next;
     const int chunk = next - turn;
     CUDA_TRY(copy_bunch(save.b, cur.b, cudaMemcpyDeviceToDevice, s, true, true));
@@ -412,6 +454,7 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
     }
     turn = next;
     if ((r = outputs(turn))) return r;
+    if ((r = beam_output(turn))) return r;
   }
   // final state back to the caller
   bmadgpu_bunch out = *hb;

@@ -585,8 +585,9 @@ class BunchData(C.Structure):
 class LttParams(C.Structure):
     _fields_ = [("n_turns", C.c_int32), ("averages_every_n_turns", C.c_int32), ("particle_every_n_turns", C.c_int32),
                 ("output_only_last_turns", C.c_int32), ("only_live_particles_out", C.c_int32),
-                ("reserved", C.c_int32), ("dead_cutoff", C.c_double), ("averages_file", C.c_char_p),
-                ("phase_space_file", C.c_char_p)]
+                ("ix_turn_start", C.c_int32), ("beam_every_n_turns", C.c_int32), ("beam_exact", C.c_int32),
+                ("dead_cutoff", C.c_double), ("averages_file", C.c_char_p), ("phase_space_file", C.c_char_p),
+                ("beam_file", C.c_char_p)]
 
 
 def _ltt_sigs(lib):
@@ -618,14 +619,47 @@ def bunch_stats(ctx, lat, device_view):
 
 
 def ltt_run(ctx, lat, bunch, n_turns, averages_file=None, phase_space_file=None, averages_every_n_turns=-1,
-            particle_every_n_turns=-1, output_only_last_turns=0, only_live_particles_out=True, dead_cutoff=1.0):
-    """long_term_tracking's beam mode for a HostBunch (updated in place); returns turns tracked."""
+            particle_every_n_turns=-1, output_only_last_turns=0, only_live_particles_out=True, dead_cutoff=1.0,
+            beam_file=None, beam_every_n_turns=-1, beam_exact=False, ix_turn_start=0):
+    """long_term_tracking's beam mode for a HostBunch (updated in place); returns the turn reached."""
     lib = _ltt_sigs(load())
     p = LttParams(n_turns, averages_every_n_turns, particle_every_n_turns, output_only_last_turns,
-                  1 if only_live_particles_out else 0, 0, dead_cutoff,
-                  averages_file.encode() if averages_file else None,
-                  phase_space_file.encode() if phase_space_file else None)
+                  1 if only_live_particles_out else 0, ix_turn_start, beam_every_n_turns, 1 if beam_exact else 0,
+                  dead_cutoff, averages_file.encode() if averages_file else None,
+                  phase_space_file.encode() if phase_space_file else None,
+                  beam_file.encode() if beam_file else None)
     done = C.c_int32()
     v = bunch.view()
     check(lib.bmadgpu_ltt_run(ctx.handle, lat.handle, C.byref(v), C.byref(p), C.byref(done)))
     return done.value
+
+
+BEAM_ALIVE_ONLY, BEAM_APPEND, BEAM_EXACT = 1, 2, 4
+
+
+def beam_write(path, bunch, param, s_position=0.0, flags=0):
+    """Bmad ASCII (version 4) beam file of a HostBunch."""
+    lib = load()
+    lib.bmadgpu_beam_write_ascii.argtypes = [C.c_char_p, C.POINTER(abi.Bunch), C.POINTER(abi.Param), C.c_double,
+                                             C.c_int32]
+    v = bunch.view()
+    check_host(lib.bmadgpu_beam_write_ascii(path.encode(), C.byref(v), C.byref(param), s_position, flags))
+
+
+def beam_read(path, param):
+    """HostBunch from a Bmad ASCII beam file (version 4, or the older ASCII::3 layout)."""
+    lib = load()
+    lib.bmadgpu_beam_read_ascii.argtypes = [C.c_char_p, C.POINTER(abi.Param), C.POINTER(abi.Bunch),
+                                            C.POINTER(C.c_int64)]
+    n = C.c_int64()
+    check_host(lib.bmadgpu_beam_read_ascii(path.encode(), C.byref(param), None, C.byref(n)))
+    b = HostBunch(np.zeros((6, n.value)), np.zeros(n.value), t=np.zeros(n.value))
+    v = b.view()
+    check_host(lib.bmadgpu_beam_read_ascii(path.encode(), C.byref(param), C.byref(v), C.byref(n)))
+    return b
+
+
+def check_host(code):
+    """Status check for the host-only calls (they set no last-error message)."""
+    if code != 0:
+        raise BmadGpuError(code, "host call failed")

@@ -397,7 +397,7 @@ int bmadgpu_bunch_stats(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const bmad
 int bmadgpu_bunch_data_from_sums(const double* sums, double p0c, double mass, bmadgpu_bunch_data* data);
 
 /* ltt_run_beam_mode (lt_tracking_mod.f90:1571-1715) for one bunch with bmad_standard tracking:
- * n_turns turns with the reference's stop conditions (no particle left; lost count reaching
+ * turns ix_turn_start .. n_turns - 1 with the reference's stop conditions (no particle left; lost count reaching
  * nint(dead_cutoff * n)), writing the averages files (<averages_file>.ave / .sigma / .emit, the
  * reference's columns and number formats) and phase-space files (<phase_space_file> with the turn
  * number, zero-padded, appended or put in place of '#'). Output schedules as the reference's
@@ -409,13 +409,31 @@ typedef struct bmadgpu_ltt_params {
   int32_t particle_every_n_turns;
   int32_t output_only_last_turns;   /* > 0: outputs only within the last this-many turns */
   int32_t only_live_particles_out;  /* phase-space files list only live particles */
-  int32_t reserved;
+  int32_t ix_turn_start;            /* turn number of the bunch as given (resume from a beam file) */
+  int32_t beam_every_n_turns;       /* beam files every n turns (and at n_turns); -1: at n_turns only */
+  int32_t beam_exact;               /* beam files with 17 digits and beta (bit-exact resume) */
   double dead_cutoff;               /* 0 means 1 (the reference default) */
   const char* averages_file;        /* NULL or "": no averages output */
   const char* phase_space_file;     /* NULL or "": no phase-space output */
+  const char* beam_file;            /* NULL or "": no beam files; "<stem>-<turn><.ext>" as ltt_write_beam_file names them */
 } bmadgpu_ltt_params;
 int bmadgpu_ltt_run(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* host_bunch,
                     const bmadgpu_ltt_params* params, int32_t* turns_done);
+
+/* ---- Beam files (checkpoint / resume) -------------------------------------------------------
+ * Bmad's ASCII beam file, version 4 (write_ascii_beam_file / read_beam_ascii,
+ * bmad/multiparticle/beam_file_io.f90:112-300, 834-1282). Host-only; no GPU needed. */
+enum { BMADGPU_BEAM_ALIVE_ONLY = 1, BMADGPU_BEAM_APPEND = 2, BMADGPU_BEAM_EXACT = 4 };
+/* Writes one bunch; flags: ALIVE_ONLY (skip lost particles), APPEND, EXACT (17 significant
+ * digits and a beta column, so a resumed run continues bit for bit; otherwise the reference's
+ * es23.15). ix_ele is written 1-based as Bmad numbers elements (0 for particles not lost). */
+int bmadgpu_beam_write_ascii(const char* path, const bmadgpu_bunch* host_bunch, const bmadgpu_param* param,
+                             double s_position, int32_t flags);
+/* Reads a file written as above (or by Bmad): with host_bunch NULL or host_bunch->vec NULL only
+ * *n_particle is set; otherwise host_bunch->n must equal it and the arrays are filled (beta from
+ * the file's beta column, else from pz as init_coord computes it). */
+int bmadgpu_beam_read_ascii(const char* path, const bmadgpu_param* param, bmadgpu_bunch* host_bunch,
+                            int64_t* n_particle);
 
 /* Page-locked host memory for bunch arrays (cudaHostAlloc / cudaFreeHost). */
 int bmadgpu_host_alloc(int64_t bytes, void** ptr);

@@ -125,3 +125,26 @@ def test_dead_cutoff_stops_at_the_reference_turn(ctx, tmp_path):
     assert done2 == stop
     assert np.array_equal(hb2.vec, hb.vec) and np.array_equal(hb2.state, hb.state)
     assert read_table(str(tmp_path / "cut2.ave")) == []          # the last turn was never reached
+
+
+def test_checkpoint_and_resume_continue_bit_for_bit(ctx, tmp_path):
+    """Beam files every 8 turns (exact layout); resuming from the turn-16 file reaches the same
+    final bunch as the uninterrupted run, bit for bit (the reference resumes LTT from a beam file
+    with ix_turn_start the same way)."""
+    eles, p = rings.ring(50)
+    n, n_turns = 2000, 24
+    vec = rings.matched_gaussian(eles, n, seed=8, scale=4.0)
+    lat = lib.Lattice(ctx, eles, p)
+    full = lib.HostBunch.from_vec(vec, p, t=np.zeros(n))
+    assert lib.ltt_run(ctx, lat, full, n_turns, beam_file=str(tmp_path / "beam.dat"), beam_every_n_turns=8,
+                       beam_exact=True) == n_turns
+    names = sorted(os.path.basename(f) for f in glob.glob(str(tmp_path / "beam-*.dat")))
+    assert names == ["beam-08.dat", "beam-16.dat", "beam-24.dat"]
+    b = lib.beam_read(str(tmp_path / "beam-16.dat"), p)
+    assert lib.ltt_run(ctx, lat, b, n_turns, ix_turn_start=16) == n_turns
+    for f in ("vec", "beta", "t", "state", "ix_ele", "location"):
+        assert np.array_equal(getattr(b, f), getattr(full, f)), f
+    late = (full.state != abi.ALIVE) & (full.ix_turn >= 16)
+    assert np.array_equal(b.ix_turn[late], full.ix_turn[late])
+    final = lib.beam_read(str(tmp_path / "beam-24.dat"), p)
+    assert np.array_equal(final.vec, full.vec) and np.array_equal(final.state, full.state)
