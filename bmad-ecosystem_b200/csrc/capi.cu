@@ -237,6 +237,8 @@ int64_t bmadgpu_sizeof(int32_t which) {
     case 7: return (int64_t)sizeof(bmadgpu_server_stats);
     case 8: return (int64_t)sizeof(bmadgpu_bunch_data);
     case 9: return (int64_t)sizeof(bmadgpu_ltt_params);
+    case 10: return (int64_t)sizeof(bmadgpu_da_params);
+    case 11: return (int64_t)sizeof(bmadgpu_da_point);
   }
   return -1;
 }

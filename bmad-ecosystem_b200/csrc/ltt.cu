@@ -409,8 +409,8 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
     CUDA_TRY(cudaStreamSynchronize(s));
     // "<stem>-<turn, zero-padded to the digits of n_turns><.ext>"
     const int width = (int)std::log10(P->n_turns + 0.1) + 1;
-    char num[32];
-    std::snprintf(num, sizeof num, "%0*d", width, turn);
+    std::string num = std::to_string(turn);
+    if ((int)num.size() < width) num = std::string(width - num.size(), '0') + num;
     std::string name;
     const size_t dot = beam_base.find_last_of('.');
     name = dot == std::string::npos ? beam_base + "-" + num : beam_base.substr(0, dot) + "-" + num + beam_base.substr(dot);

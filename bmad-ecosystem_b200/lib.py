@@ -109,7 +109,7 @@ def check_layout():
     """Compare ctypes struct sizes with the compiled library's sizeof()."""
     lib = load()
     for i, st in enumerate((abi.Element, abi.Param, abi.Bunch, Tuning, BatchTuning, ServerConfig, JobInfo,
-                            ServerStats, BunchData, LttParams)):
+                            ServerStats, BunchData, LttParams, DaParams, DaPoint)):
         if lib.bmadgpu_sizeof(i) != C.sizeof(st):
             raise BmadGpuError(abi.EINVAL, "ABI size mismatch for %s" % st.__name__)
 
@@ -663,3 +663,32 @@ def check_host(code):
     """Status check for the host-only calls (they set no last-error message)."""
     if code != 0:
         raise BmadGpuError(code, "host call failed")
+
+
+# ---- dynamic aperture ------------------------------------------------------------------------
+
+class DaParams(C.Structure):
+    _fields_ = [("x_init", C.c_double), ("y_init", C.c_double), ("abs_accuracy", C.c_double),
+                ("rel_accuracy", C.c_double), ("n_turn", C.c_int32), ("max_iterations", C.c_int32)]
+
+
+class DaPoint(C.Structure):
+    _fields_ = [("x", C.c_double), ("y", C.c_double), ("i_turn", C.c_int32), ("ix_ele", C.c_int32),
+                ("plane", C.c_int32), ("iterations", C.c_int32)]
+
+
+def da_scan(ctx, lat, theta, n_turn, x_init=1e-3, y_init=1e-3, abs_accuracy=1e-5, rel_accuracy=0.0, orb0=None,
+            max_iterations=0):
+    """Dynamic-aperture points along rays theta (dynamic_aperture_point for all rays at once).
+    Returns a list of dicts (x, y, i_turn, ix_ele, plane, iterations)."""
+    lib = load()
+    lib.bmadgpu_da_scan.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double), C.POINTER(DaParams), C.POINTER(DaPoint)]
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    n = len(th)
+    o = None if orb0 is None else np.ascontiguousarray(orb0, dtype=np.float64).reshape(n, 6)
+    pts = (DaPoint * max(n, 1))()
+    prm = DaParams(x_init, y_init, abs_accuracy, rel_accuracy, n_turn, max_iterations)
+    check(lib.bmadgpu_da_scan(ctx.handle, lat.handle, n, th.ctypes.data_as(C.POINTER(C.c_double)),
+                              None if o is None else o.ctypes.data_as(C.POINTER(C.c_double)), C.byref(prm), pts))
+    return [{f: getattr(pts[i], f) for f, _ in DaPoint._fields_} for i in range(n)]

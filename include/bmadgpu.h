@@ -236,7 +236,7 @@ int bmadgpu_measure_fp64_peak(bmadgpu_ctx* ctx, double* flops_per_s);
 /* sizeof() of the ABI structs as this library was compiled, for binding checks. */
 int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning, 4 batch tuning,
                                            5 server config, 6 job info, 7 server stats,
-                                           8 bunch data, 9 ltt params */
+                                           8 bunch data, 9 ltt params, 10 da params, 11 da point */
 
 /* ---- Batched tracking of many lattice variants -------------------------------------------
  * No single counterpart in the reference: it replaces a loop of long_term_tracking runs
@@ -419,6 +419,31 @@ typedef struct bmadgpu_ltt_params {
 } bmadgpu_ltt_params;
 int bmadgpu_ltt_run(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* host_bunch,
                     const bmadgpu_ltt_params* params, int32_t* turns_done);
+
+/* ---- Dynamic aperture ------------------------------------------------------------------------
+ * dynamic_aperture_point (bmad/modules/dynamic_aperture_mod.f90:284-398) for many rays at once:
+ * along the ray (x, y) = (cos theta x_init, sin theta y_init) s, starting at s = 1, a trial
+ * particle (start orbit + (x, 0, y, 0, 0, 0)) is tracked n_turn turns; survival doubles s until a
+ * loss brackets the aperture, then the bracket is halved until it is within
+ * 2 (abs_accuracy + r rel_accuracy). Every iteration tracks the trial particles of all unfinished
+ * rays in one launch and updates the searches on the device. */
+typedef struct bmadgpu_da_params {
+  double x_init, y_init;            /* aperture_param%x_init, %y_init [m] */
+  double abs_accuracy, rel_accuracy;
+  int32_t n_turn;
+  int32_t max_iterations;           /* per ray (0: 200); the reference loops without limit */
+} bmadgpu_da_params;
+typedef struct bmadgpu_da_point {
+  double x, y;                      /* the aperture point relative to the start orbit */
+  int32_t i_turn;                   /* turn of the last loss (counted from 1, as the reference) */
+  int32_t ix_ele;                   /* element of that loss (0-based) */
+  int32_t plane;                    /* its state code (lost_neg_x, ...) */
+  int32_t iterations;
+} bmadgpu_da_point;
+/* orb0: [n_rays][6] start orbits (e.g. closed orbit, or an energy offset per ray), or NULL for
+ * zero. BMADGPU_ETIMEDOUT if a ray reached 1 m or the iteration limit (its point is still set). */
+int bmadgpu_da_scan(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, int32_t n_rays, const double* theta,
+                    const double* orb0, const bmadgpu_da_params* params, bmadgpu_da_point* points);
 
 /* ---- Beam files (checkpoint / resume) -------------------------------------------------------
  * Bmad's ASCII beam file, version 4 (write_ascii_beam_file / read_beam_ascii,
