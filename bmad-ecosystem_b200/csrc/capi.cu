@@ -239,6 +239,8 @@ int64_t bmadgpu_sizeof(int32_t which) {
     case 9: return (int64_t)sizeof(bmadgpu_ltt_params);
     case 10: return (int64_t)sizeof(bmadgpu_da_params);
     case 11: return (int64_t)sizeof(bmadgpu_da_point);
+    case 12: return (int64_t)sizeof(bmadgpu_twiss);
+    case 13: return (int64_t)sizeof(bmadgpu_beam_init);
   }
   return -1;
 }

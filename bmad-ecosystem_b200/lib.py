@@ -109,7 +109,7 @@ def check_layout():
     """Compare ctypes struct sizes with the compiled library's sizeof()."""
     lib = load()
     for i, st in enumerate((abi.Element, abi.Param, abi.Bunch, Tuning, BatchTuning, ServerConfig, JobInfo,
-                            ServerStats, BunchData, LttParams, DaParams, DaPoint)):
+                            ServerStats, BunchData, LttParams, DaParams, DaPoint, Twiss, BeamInit)):
         if lib.bmadgpu_sizeof(i) != C.sizeof(st):
             raise BmadGpuError(abi.EINVAL, "ABI size mismatch for %s" % st.__name__)
 
@@ -692,3 +692,129 @@ def da_scan(ctx, lat, theta, n_turn, x_init=1e-3, y_init=1e-3, abs_accuracy=1e-5
     check(lib.bmadgpu_da_scan(ctx.handle, lat.handle, n, th.ctypes.data_as(C.POINTER(C.c_double)),
                               None if o is None else o.ctypes.data_as(C.POINTER(C.c_double)), C.byref(prm), pts))
     return [{f: getattr(pts[i], f) for f, _ in DaPoint._fields_} for i in range(n)]
+
+
+# ---- optics: closed orbit, one-turn matrix, periodic Twiss, matched beam ---------------------
+
+TWISS_OK, TWISS_IN_STOP_BAND, TWISS_NON_SYMPLECTIC, TWISS_UNSTABLE, TWISS_UNSTABLE_A, TWISS_UNSTABLE_B = 1, 2, 3, 4, 5, 6
+
+
+class Twiss(C.Structure):
+    _fields_ = ([(n, C.c_double) for n in (
+        "beta_a alpha_a gamma_a phi_a beta_b alpha_b gamma_b phi_b "
+        "eta_a etap_a deta_ds_a eta_b etap_b deta_ds_b eta_x etap_x deta_ds_x eta_y etap_y deta_ds_y").split()]
+        + [("c_mat", C.c_double * 4), ("gamma_c", C.c_double), ("growth_rate", C.c_double),
+           ("symp_error", C.c_double), ("status", C.c_int32), ("reserved", C.c_int32)])
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("c_mat", "reserved")}
+        d["c_mat"] = np.array(self.c_mat[:]).reshape(2, 2)
+        return d
+
+
+class BeamInit(C.Structure):
+    _fields_ = ([(n, C.c_double) for n in "a_emit b_emit sig_z sig_pz dpz_dz sig_z_jitter sig_pz_jitter".split()]
+                + [("center", C.c_double * 6), ("center_jitter", C.c_double * 6), ("sigma_cutoff", C.c_double),
+                   ("seed", C.c_uint64), ("renorm_center", C.c_int32), ("renorm_sigma", C.c_int32)])
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def one_turn_matrix(ctx, lat, orbit, rf_on=True):
+    """(mat[6, 6], orbit after one turn) about `orbit` by central differences of device tracking."""
+    lib = load()
+    lib.bmadgpu_one_turn_matrix.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_int32,
+                                            C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    o = np.ascontiguousarray(orbit, dtype=np.float64).copy()
+    end, mat = np.zeros(6), np.zeros(36)
+    check(lib.bmadgpu_one_turn_matrix(ctx.handle, lat.handle, _dptr(o), 1 if rf_on else 0, _dptr(end), _dptr(mat)))
+    return mat.reshape(6, 6), end
+
+
+def closed_orbit(ctx, lat, dim=0, guess=None, rel_tol=0.0, abs_tol=0.0, max_iter=0):
+    """closed_orbit_calc at the lattice start: (orbit[6], one-turn matrix[6, 6], iterations)."""
+    lib = load()
+    lib.bmadgpu_closed_orbit.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double), C.c_double, C.c_double, C.c_int32,
+                                         C.POINTER(C.c_int32)]
+    o = np.zeros(6) if guess is None else np.ascontiguousarray(guess, dtype=np.float64).copy()
+    mat = np.zeros(36)
+    it = C.c_int32()
+    check(lib.bmadgpu_closed_orbit(ctx.handle, lat.handle, dim, _dptr(o), _dptr(mat), rel_tol, abs_tol, max_iter,
+                                   C.byref(it)))
+    return o, mat.reshape(6, 6), it.value
+
+
+def twiss_from_mat6(mat, orb0=None):
+    """Periodic Twiss of a one-turn matrix (host-only); a dict of the bmadgpu_twiss fields."""
+    lib = load()
+    lib.bmadgpu_twiss_from_mat6.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(Twiss)]
+    m = np.ascontiguousarray(mat, dtype=np.float64).reshape(36)
+    o = None if orb0 is None else np.ascontiguousarray(orb0, dtype=np.float64)
+    tw = Twiss()
+    check_host(lib.bmadgpu_twiss_from_mat6(_dptr(m), None if o is None else _dptr(o), C.byref(tw)))
+    return tw.as_dict()
+
+
+def philox4x32_10(counter, key):
+    """The Philox4x32-10 block function of the beam generator (host-only)."""
+    lib = load()
+    ctr = (C.c_uint32 * 4)(*counter)
+    k = (C.c_uint32 * 2)(*key)
+    out = (C.c_uint32 * 4)()
+    check_host(lib.bmadgpu_philox4x32_10(ctr, k, out))
+    return [int(v) for v in out]
+
+
+def gaussian_deviates(ctx, seed, n, sigma_cutoff=0.0):
+    """The deviates the beam generator draws for (seed, sigma_cutoff, n): array [6 * n + 8]."""
+    import torch
+    lib = load()
+    lib.bmadgpu_gaussian_deviates.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.c_int64, C.c_void_p]
+    d = torch.empty(6 * n + 8, dtype=torch.float64, device="cuda:%d" % ctx.device)
+    check(lib.bmadgpu_gaussian_deviates(ctx.handle, seed, sigma_cutoff, n, d.data_ptr()))
+    return d.cpu().numpy()
+
+
+def beam_init_gaussian(ctx, param, twiss, n, seed=0, a_emit=1e-9, b_emit=10e-12, sig_z=3e-3, sig_pz=1e-3,
+                       dpz_dz=0.0, sig_z_jitter=0.0, sig_pz_jitter=0.0, center=None, center_jitter=None,
+                       sigma_cutoff=0.0, renorm_center=True, renorm_sigma=True, normals=None, orbit=None):
+    """Matched Gaussian bunch of n particles generated on the device (init_bunch_distribution with
+    RAN_GAUSS); returns a HostBunch (vec, beta, t, state). twiss: a Twiss or its dict."""
+    import torch
+    lib = load()
+    lib.bmadgpu_beam_init_gaussian.argtypes = [C.c_void_p, C.POINTER(abi.Param), C.POINTER(Twiss),
+                                               C.POINTER(BeamInit), C.c_void_p, C.POINTER(C.c_double),
+                                               C.POINTER(abi.Bunch)]
+    if isinstance(twiss, dict):
+        tw = Twiss()
+        for f, _ in Twiss._fields_:
+            if f == "c_mat":
+                tw.c_mat[:] = list(np.asarray(twiss["c_mat"], float).ravel())
+            elif f in twiss:
+                setattr(tw, f, twiss[f])
+    else:
+        tw = twiss
+    bi = BeamInit(a_emit, b_emit, sig_z, sig_pz, dpz_dz, sig_z_jitter, sig_pz_jitter)
+    bi.center[:] = list(center) if center is not None else [0.0] * 6
+    bi.center_jitter[:] = list(center_jitter) if center_jitter is not None else [0.0] * 6
+    bi.sigma_cutoff, bi.seed = sigma_cutoff, seed
+    bi.renorm_center, bi.renorm_sigma = int(bool(renorm_center)), int(bool(renorm_sigma))
+    dev = "cuda:%d" % ctx.device
+    vec = torch.empty(6 * n, dtype=torch.float64, device=dev)
+    beta = torch.empty(n, dtype=torch.float64, device=dev)
+    t = torch.empty(n, dtype=torch.float64, device=dev)
+    state = torch.empty(n, dtype=torch.int32, device=dev)
+    nd = None
+    if normals is not None:
+        nd = torch.from_numpy(np.ascontiguousarray(normals, dtype=np.float64)).to(dev)
+        assert nd.numel() == 6 * n + 8
+    o = None if orbit is None else np.ascontiguousarray(orbit, dtype=np.float64)
+    view = abi.Bunch(n, vec.data_ptr(), beta.data_ptr(), t.data_ptr(), state.data_ptr(), None, None, None)
+    check(lib.bmadgpu_beam_init_gaussian(ctx.handle, C.byref(param), C.byref(tw), C.byref(bi),
+                                         None if nd is None else nd.data_ptr(), None if o is None else _dptr(o),
+                                         C.byref(view)))
+    return HostBunch(vec.cpu().numpy().reshape(6, n), beta.cpu().numpy(), state=state.cpu().numpy(),
+                     t=t.cpu().numpy())

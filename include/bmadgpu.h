@@ -236,7 +236,8 @@ int bmadgpu_measure_fp64_peak(bmadgpu_ctx* ctx, double* flops_per_s);
 /* sizeof() of the ABI structs as this library was compiled, for binding checks. */
 int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning, 4 batch tuning,
                                            5 server config, 6 job info, 7 server stats,
-                                           8 bunch data, 9 ltt params, 10 da params, 11 da point */
+                                           8 bunch data, 9 ltt params, 10 da params, 11 da point,
+                                           12 twiss, 13 beam init */
 
 /* ---- Batched tracking of many lattice variants -------------------------------------------
  * No single counterpart in the reference: it replaces a loop of long_term_tracking runs
@@ -444,6 +445,77 @@ typedef struct bmadgpu_da_point {
  * zero. BMADGPU_ETIMEDOUT if a ray reached 1 m or the iteration limit (its point is still set). */
 int bmadgpu_da_scan(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, int32_t n_rays, const double* theta,
                     const double* orb0, const bmadgpu_da_params* params, bmadgpu_da_point* points);
+
+/* ---- Optics: closed orbit, one-turn matrix, periodic Twiss, matched beam ---------------------
+ * What long_term_tracking computes before it tracks (twiss_and_track, lt_tracking_mod.f90:562,
+ * and ltt_init_beam_distribution, lt_tracking_mod.f90:1548-1561). Matrices are 6x6 row-major:
+ * mat[i*6 + j] = Fortran mat6(i+1, j+1). */
+
+/* One-turn matrix about `orbit` [6] by fourth-order central differences of one turn of device
+ * tracking (25 particles in one launch), apertures off; rf_on = 0 tracks every rfcavity as
+ * switched off (the matrix twiss_at_start.f90:29 uses). orbit_end [6] (nullable) receives the
+ * tracked orbit. Replaces transfer_matrix_calc after lat_make_mat6 (closed_orbit_calc.f90:787-788). */
+int bmadgpu_one_turn_matrix(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const double* orbit, int32_t rf_on,
+                            double* orbit_end, double* mat);
+/* Closed orbit at the lattice start (closed_orbit_calc, closed_orbit_calc.f90:192-862), forward
+ * direction. dim = 4: transverse at the fixed pz = orbit[5], RF off, z starts at 0; 5: RF off,
+ * pz adjusted until z closes; 6: full 6D with RF on; 0: 6 if any cavity is on, else 4. orbit [6]
+ * is the initial guess in and the closed orbit out; mat [36] (nullable) receives the one-turn
+ * matrix there. Stops when |f(x)_i - x_i| < |x_i| rel_tol + abs_tol for the fitted coordinates
+ * (<= 0: bmad_com's 1e-9 and 1e-12); max_iter <= 0: 100. BMADGPU_ETIMEDOUT if not converged. */
+int bmadgpu_closed_orbit(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, int32_t dim, double* orbit, double* mat,
+                         double rel_tol, double abs_tol, int32_t max_iter, int32_t* iterations);
+
+/* Status codes of the Twiss calculation (matrix_status, bmad_struct.f90:186-187). */
+enum {
+  BMADGPU_TWISS_OK = 1, BMADGPU_TWISS_IN_STOP_BAND = 2, BMADGPU_TWISS_NON_SYMPLECTIC = 3,
+  BMADGPU_TWISS_UNSTABLE = 4, BMADGPU_TWISS_UNSTABLE_A = 5, BMADGPU_TWISS_UNSTABLE_B = 6
+};
+/* ele%a, ele%b, ele%x, ele%y, ele%c_mat, ele%gamma_c as twiss_from_mat6 fills them. phi_a/phi_b
+ * are the one-turn phase advances in [0, 2 pi) (the tunes times 2 pi). */
+typedef struct bmadgpu_twiss {
+  double beta_a, alpha_a, gamma_a, phi_a;
+  double beta_b, alpha_b, gamma_b, phi_b;
+  double eta_a, etap_a, deta_ds_a, eta_b, etap_b, deta_ds_b;   /* normal-mode dispersion */
+  double eta_x, etap_x, deta_ds_x, eta_y, etap_y, deta_ds_y;   /* lab-frame dispersion */
+  double c_mat[4];            /* c_mat(1,1), (1,2), (2,1), (2,2) */
+  double gamma_c;
+  double growth_rate;         /* when not stable */
+  double symp_error;          /* mat_symp_error of the 4x4 block */
+  int32_t status;             /* BMADGPU_TWISS_* */
+  int32_t reserved;
+} bmadgpu_twiss;
+/* Periodic Twiss from a one-turn matrix (twiss_from_mat6.f90:24, mat_symp_decouple.f90:22,
+ * twiss_from_mat2.f90:19); orb0 [6] (nullable) is the orbit for the deta_ds terms. Host-only.
+ * Returns BMADGPU_OK with tw->status telling whether the optics are stable. */
+int bmadgpu_twiss_from_mat6(const double* mat, const double* orb0, bmadgpu_twiss* tw);
+
+/* beam_init_struct fields of a Gaussian bunch (beam_init_struct, bmad_struct.f90). */
+typedef struct bmadgpu_beam_init {
+  double a_emit, b_emit;      /* geometric emittances [m] */
+  double sig_z, sig_pz;
+  double dpz_dz;
+  double sig_z_jitter, sig_pz_jitter;
+  double center[6];
+  double center_jitter[6];
+  double sigma_cutoff;        /* random_sigma_cutoff: <= 0 none */
+  uint64_t seed;              /* Philox4x32-10 key */
+  int32_t renorm_center;
+  int32_t renorm_sigma;
+} bmadgpu_beam_init;
+/* Fills the device bunch (n = bunch->n particles) with a Gaussian beam matched to tw
+ * (init_bunch_distribution with RAN_GAUSS in all planes, beam_utils.f90:328-535, 551-721), plus
+ * orbit [6] (nullable) as add_closed_orbit_to_init_position adds it. Deviates: normals (device,
+ * nullable) = [6*n] SoA per particle, then the sig_z and sig_pz jitters, then the 6 centre jitters
+ * ([6*n + 8] in all); NULL draws them on the device from a counter-based Philox4x32-10 stream keyed
+ * by bi->seed (deviate k of particle i from counter (i, attempt, k)). */
+int bmadgpu_beam_init_gaussian(bmadgpu_ctx* ctx, const bmadgpu_param* param, const bmadgpu_twiss* tw,
+                               const bmadgpu_beam_init* bi, const double* normals, const double* orbit,
+                               bmadgpu_bunch* device_bunch);
+/* The deviates bmadgpu_beam_init_gaussian draws for (seed, sigma_cutoff, n): d_out [6*n + 8] (device). */
+int bmadgpu_gaussian_deviates(bmadgpu_ctx* ctx, uint64_t seed, double sigma_cutoff, int64_t n, double* d_out);
+/* The Philox4x32-10 block function those deviates come from (host-only): out = philox(counter [4], key [2]). */
+int bmadgpu_philox4x32_10(const uint32_t* counter, const uint32_t* key, uint32_t* out);
 
 /* ---- Beam files (checkpoint / resume) -------------------------------------------------------
  * Bmad's ASCII beam file, version 4 (write_ascii_beam_file / read_beam_ascii,
