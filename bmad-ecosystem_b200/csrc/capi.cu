@@ -241,6 +241,8 @@ int64_t bmadgpu_sizeof(int32_t which) {
     case 11: return (int64_t)sizeof(bmadgpu_da_point);
     case 12: return (int64_t)sizeof(bmadgpu_twiss);
     case 13: return (int64_t)sizeof(bmadgpu_beam_init);
+    case 14: return (int64_t)sizeof(bmadgpu_fma_params);
+    case 15: return (int64_t)sizeof(bmadgpu_fma_point);
   }
   return -1;
 }

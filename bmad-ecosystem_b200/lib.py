@@ -5,6 +5,7 @@ over turns, ``track1_bunch`` the per-element hook (beam_mod.f90:238). Errors rai
 ``BmadGpuError`` with the library's last-error message; nothing here falls back to a CPU path.
 """
 import ctypes as C
+import math
 import os
 import re
 
@@ -109,7 +110,7 @@ def check_layout():
     """Compare ctypes struct sizes with the compiled library's sizeof()."""
     lib = load()
     for i, st in enumerate((abi.Element, abi.Param, abi.Bunch, Tuning, BatchTuning, ServerConfig, JobInfo,
-                            ServerStats, BunchData, LttParams, DaParams, DaPoint, Twiss, BeamInit)):
+                            ServerStats, BunchData, LttParams, DaParams, DaPoint, Twiss, BeamInit, FmaParams, FmaPoint)):
         if lib.bmadgpu_sizeof(i) != C.sizeof(st):
             raise BmadGpuError(abi.EINVAL, "ABI size mismatch for %s" % st.__name__)
 
@@ -818,3 +819,125 @@ def beam_init_gaussian(ctx, param, twiss, n, seed=0, a_emit=1e-9, b_emit=10e-12,
                                          C.byref(view)))
     return HostBunch(vec.cpu().numpy().reshape(6, n), beta.cpu().numpy(), state=state.cpu().numpy(),
                      t=t.cpu().numpy())
+
+
+# ---- frequency-map analysis ------------------------------------------------------------------
+
+class FmaParams(C.Structure):
+    _fields_ = [("n_turn", C.c_int32), ("fft_turns", C.c_int32), ("z_cut", C.c_int32), ("reserved", C.c_int32),
+                ("rf_frequency", C.c_double), ("norm", C.c_double * 36), ("orbit", C.c_double * 6),
+                ("tune_a", C.c_double), ("tune_b", C.c_double)]
+
+
+class FmaPoint(C.Structure):
+    _fields_ = [("tune", C.c_double * 6), ("status", C.c_int32), ("turn_lost", C.c_int32), ("ix_ele", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+def mat_eigen(mat):
+    """Eigenvalues and eigenvectors (rows) of a one-turn matrix paired and ordered by plane as
+    mat_eigen does (sim_utils/matrix/mat_eigen.f90:37-187) for stable modes: LAPACK geev, pairs
+    assigned to the plane they live in, the odd member of each pair the one of positive
+    symplectic norm, phase normalised."""
+    m = np.asarray(mat, float)
+    n = m.shape[0]
+    nn = n // 2
+    w, vr = np.linalg.eig(m)
+    if np.any(w.imag == 0):
+        raise BmadGpuError(abi.EINVAL, "unstable mode: no complex eigenvalue pair")
+    pos = [p for p in range(n) if w[p].imag > 0]
+    amp = np.zeros((nn, nn))
+    for ii, p in enumerate(pos):
+        re, im = vr[:, p].real, vr[:, p].imag
+        for kk in range(nn):
+            amp[kk, ii] = np.sum(re[2 * kk:2 * kk + 2] ** 2) + np.sum(im[2 * kk:2 * kk + 2] ** 2)
+        amp[:, ii] /= np.sum(amp[:, ii])
+    sort = np.zeros(nn, int)
+    for _ in range(nn):
+        amp2 = amp.copy()
+        dmax = np.zeros(nn)
+        for j in range(nn):
+            mx = int(np.argmax(amp2[j]))
+            amp2[j, mx] = -1
+            dmax[j] = amp[j, mx] - amp[j, int(np.argmax(amp2[j]))]
+        k = int(np.argmax(dmax))
+        mx = int(np.argmax(amp[k]))
+        sort[mx] = k
+        amp[k, :] = 0
+        amp[:, mx] = 0
+    vals = np.zeros(n, complex)
+    vecs = np.zeros((n, n), complex)
+    for ii, p in enumerate(pos):
+        j = 2 * sort[ii]
+        e1, e2 = np.conj(vr[:, p]), vr[:, p]
+        l1, l2 = np.conj(w[p]), w[p]
+        fnorm = sum(2 * np.imag(np.conj(e1[jj]) * e1[jj + 1]) for jj in range(0, n, 2))
+        if fnorm < 0:
+            e1, e2, l1, l2, fnorm = e2, e1, l2, l1, -fnorm
+        sgn = 1 / math.sqrt(fnorm) if abs(e1[j]) == 0 else abs(e1[j]) / (math.sqrt(fnorm) * e1[j])
+        vals[j], vals[j + 1] = l1, l2
+        vecs[j], vecs[j + 1] = sgn * e1, np.conj(sgn) * e2
+    return vals, vecs
+
+
+def fma_normalization(mat6):
+    """The matrix frequency_map applies to (vec - co) each turn (frequency_map.f90:200-212): with
+    mat6(6,5) == 0 the inverse of the decoupling V on (x, px, y, py); otherwise the inverse of T,
+    whose rows are the real and minus imaginary parts of the ordered eigenvectors (as psv Tinv)."""
+    m = np.asarray(mat6, float)
+    if m[5, 4] == 0:
+        tw = twiss_from_mat6(m)
+        Cm, g = tw["c_mat"], tw["gamma_c"]
+        Vinv = np.eye(6)
+        Vinv[:2, :2] = Vinv[2:4, 2:4] = g * np.eye(2)
+        Vinv[:2, 2:4] = -Cm
+        Vinv[2:4, :2] = np.array([[Cm[1, 1], -Cm[0, 1]], [-Cm[1, 0], Cm[0, 0]]])
+        return Vinv
+    _, vecs = mat_eigen(m)
+    T = np.zeros((6, 6))
+    for i in range(0, 6, 2):
+        T[i] = vecs[i].real
+        T[i + 1] = -vecs[i].imag
+    return np.linalg.inv(T).T
+
+
+def fma(ctx, lat, offsets, n_turn, fft_turns=0, z_cut=True, rf_frequency=0.0, orbit=None, norm=None, tunes=None):
+    """frequency_map for particles at closed orbit + offsets[n, 6]. The closed orbit, the
+    normalisation and the ring tunes default to what the reference computes (twiss_and_track with
+    the RF on). Returns (tunes[n, 6], status[n], turn_lost[n], ix_ele[n])."""
+    lib = load()
+    lib.bmadgpu_fma.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(FmaParams),
+                                C.POINTER(FmaPoint)]
+    off = np.ascontiguousarray(offsets, dtype=np.float64).reshape(-1, 6)
+    n = off.shape[0]
+    if orbit is None:
+        orbit = closed_orbit(ctx, lat)[0]
+    if norm is None:
+        norm = fma_normalization(one_turn_matrix(ctx, lat, orbit, rf_on=True)[0])
+    if tunes is None:
+        tw = twiss_from_mat6(one_turn_matrix(ctx, lat, orbit, rf_on=False)[0], orbit)
+        tunes = (tw["phi_a"] / (2 * math.pi), tw["phi_b"] / (2 * math.pi))
+    P = FmaParams(n_turn, fft_turns, 1 if z_cut else 0, 0, rf_frequency)
+    P.norm[:] = list(np.asarray(norm, float).ravel())
+    P.orbit[:] = list(np.asarray(orbit, float))
+    P.tune_a, P.tune_b = tunes
+    pts = (FmaPoint * max(n, 1))()
+    check(lib.bmadgpu_fma(ctx.handle, lat.handle, n, _dptr(off), C.byref(P), pts))
+    q = np.array([pts[i].tune[:] for i in range(n)]).reshape(n, 6)
+    st = np.array([pts[i].status for i in range(n)], np.int32)
+    tl = np.array([pts[i].turn_lost for i in range(n)], np.int32)
+    ie = np.array([pts[i].ix_ele for i in range(n)], np.int32)
+    return q, st, tl, ie
+
+
+def fma_write(path, offsets, tunes, status, append=False):
+    """The reference's .fm table (host-only)."""
+    lib = load()
+    lib.bmadgpu_fma_write.argtypes = [C.c_char_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(FmaPoint), C.c_int32]
+    off = np.ascontiguousarray(offsets, dtype=np.float64).reshape(-1, 6)
+    n = off.shape[0]
+    pts = (FmaPoint * max(n, 1))()
+    for i in range(n):
+        pts[i].tune[:] = list(np.asarray(tunes[i], float))
+        pts[i].status = int(status[i])
+    check_host(lib.bmadgpu_fma_write(path.encode(), n, _dptr(off), pts, 1 if append else 0))

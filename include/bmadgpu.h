@@ -237,7 +237,7 @@ int bmadgpu_measure_fp64_peak(bmadgpu_ctx* ctx, double* flops_per_s);
 int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning, 4 batch tuning,
                                            5 server config, 6 job info, 7 server stats,
                                            8 bunch data, 9 ltt params, 10 da params, 11 da point,
-                                           12 twiss, 13 beam init */
+                                           12 twiss, 13 beam init, 14 fma params, 15 fma point */
 
 /* ---- Batched tracking of many lattice variants -------------------------------------------
  * No single counterpart in the reference: it replaces a loop of long_term_tracking runs
@@ -516,6 +516,37 @@ int bmadgpu_beam_init_gaussian(bmadgpu_ctx* ctx, const bmadgpu_param* param, con
 int bmadgpu_gaussian_deviates(bmadgpu_ctx* ctx, uint64_t seed, double sigma_cutoff, int64_t n, double* d_out);
 /* The Philox4x32-10 block function those deviates come from (host-only): out = philox(counter [4], key [2]). */
 int bmadgpu_philox4x32_10(const uint32_t* counter, const uint32_t* key, uint32_t* out);
+
+/* ---- Frequency-map analysis -----------------------------------------------------------------
+ * frequency_map (bsim/frequency_map/frequency_map.f90:197-376) for all particles at once: start at
+ * orbit + offset, n_turn turns of tracking with the normalised coordinates recorded every turn, then
+ * per particle the Hanning-windowed spectra of x + i px, y + i py, z - i pz over the first and the
+ * last fft_turns turns and calc_tune's interpolated peak (frequency_map.f90:364-375). */
+typedef struct bmadgpu_fma_params {
+  int32_t n_turn;
+  int32_t fft_turns;          /* 0: n_turn / 2 (at most 4096) */
+  int32_t z_cut;              /* stop a particle whose |z - z_co| exceeds a quarter RF wavelength */
+  int32_t reserved;
+  double rf_frequency;        /* for z_cut; <= 0: the lowest frequency of the lattice's cavities */
+  double norm[36];            /* psv_norm = norm (vec - orbit), row-major: V^-1 (uncoupled RF-off
+                                 matrix) or Tinv^T from the eigenvectors, as the reference chooses */
+  double orbit[6];            /* closed orbit co(0) */
+  double tune_a, tune_b;      /* ring tunes phi/2pi: below 0.5 the x/y results are 1 - Q as there */
+} bmadgpu_fma_params;
+typedef struct bmadgpu_fma_point {
+  double tune[6];             /* Qx0, Qy0, Qz0 (first fft_turns turns), Qx1, Qy1, Qz1 (last) */
+  int32_t status;             /* 0 tunes computed, 1 lost, 2 outside the RF bucket */
+  int32_t turn_lost;          /* turn (from 1) where status was set */
+  int32_t ix_ele;             /* element of the loss (0-based), status 1 */
+  int32_t reserved;
+} bmadgpu_fma_point;
+/* offsets: [n_particles][6] start offsets from the closed orbit. */
+int bmadgpu_fma(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, int32_t n_particles, const double* offsets,
+                const bmadgpu_fma_params* params, bmadgpu_fma_point* points);
+/* The reference's .fm table for these particles (host-only): header unless append, then
+ * '(12e14.5)' rows, '*' tune columns for status 2, no row for lost particles. */
+int bmadgpu_fma_write(const char* path, int32_t n_particles, const double* offsets,
+                      const bmadgpu_fma_point* points, int32_t append);
 
 /* ---- Beam files (checkpoint / resume) -------------------------------------------------------
  * Bmad's ASCII beam file, version 4 (write_ascii_beam_file / read_beam_ascii,
