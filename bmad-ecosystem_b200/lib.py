@@ -941,3 +941,19 @@ def fma_write(path, offsets, tunes, status, append=False):
         pts[i].tune[:] = list(np.asarray(tunes[i], float))
         pts[i].status = int(status[i])
     check_host(lib.bmadgpu_fma_write(path.encode(), n, _dptr(off), pts, 1 if append else 0))
+
+
+def naff(ctx, signals, n_comp, zero_first=False):
+    """NAFF of complex signals [n_signals, n_samples] on the device: (freqs [n, n_comp],
+    amps [n, n_comp] complex) as naff_mod's naff returns them."""
+    lib = load()
+    lib.bmadgpu_naff.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double), C.c_int32, C.c_int32,
+                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    sig = np.atleast_2d(np.asarray(signals, dtype=np.complex128))
+    n, m = sig.shape
+    data = np.ascontiguousarray(sig).view(np.float64)
+    freqs = np.zeros((n, n_comp))
+    amps = np.zeros((n, n_comp), np.complex128)
+    check(lib.bmadgpu_naff(ctx.handle, n, m, _dptr(data), n_comp, 1 if zero_first else 0, _dptr(freqs),
+                           amps.view(np.float64).ctypes.data_as(C.POINTER(C.c_double))))
+    return freqs, amps

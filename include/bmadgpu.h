@@ -548,6 +548,16 @@ int bmadgpu_fma(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, int32_t n_particle
 int bmadgpu_fma_write(const char* path, int32_t n_particles, const double* offsets,
                       const bmadgpu_fma_point* points, int32_t append);
 
+/* NAFF frequency decomposition (naff, sim_utils/math/naff.f90:72-131) of n_signals complex
+ * signals of n_samples points each (4..4096; any length): cdata [n_signals][n_samples] as
+ * interleaved (re, im) doubles, Fortran complex(rp) layout, in host memory. Per signal n_comp
+ * components: freqs [n_signals][n_comp] in units of 2 pi (data ~ amp exp(-2 pi i f t)), amps
+ * [n_signals][n_comp] interleaved complex. zero_first: the first component is f = 0. As in the
+ * reference, a signal whose points are all equal gets freqs 0, and a failed peak estimate leaves
+ * the remaining freqs at -1. One CTA per signal on the device. */
+int bmadgpu_naff(bmadgpu_ctx* ctx, int32_t n_signals, int32_t n_samples, const double* cdata, int32_t n_comp,
+                 int32_t zero_first, double* freqs, double* amps);
+
 /* ---- Beam files (checkpoint / resume) -------------------------------------------------------
  * Bmad's ASCII beam file, version 4 (write_ascii_beam_file / read_beam_ascii,
  * bmad/multiparticle/beam_file_io.f90:112-300, 834-1282). Host-only; no GPU needed. */
