@@ -23,7 +23,31 @@ namespace bmadgpu {
 
 namespace {
 
-template <int BLOCK, int MINB>
+// One turn's record of a frequency-map job (the per-turn step of frequency_map.f90:288-312):
+// the stop test against a quarter RF wavelength, then psv_norm = norm (vec - co). Kept out of
+// line so the record's registers do not weigh on the tracking loop of every other variant.
+__device__ __noinline__ void fma_record(const BatchVar& v, int64_t j, int32_t t_rel, double x, double px, double y,
+                                        double py, double z, double pz) {
+  if (v.rec_state[j] != 0) return;
+  const double* q = v.rec_par;
+  const double psv[6] = {x - q[36], px - q[37], y - q[38], py - q[39], z - q[40], pz - q[41]};
+  const double z_limit = q[42];
+  if (z_limit > 0 && (fabs(psv[4]) > z_limit || (t_rel == v.rec_turns - 1 && !(fabs(z) < z_limit)))) {
+    v.rec_state[j] = 2;
+    v.rec_state[v.n + j] = t_rel + 1;
+    return;
+  }
+  const int64_t n = v.n;
+  for (int r = 0; r < 6; r++) {
+    double s = 0;
+    for (int k = 0; k < 6; k++) s = s + q[r * 6 + k] * psv[k];
+    v.rec[((int64_t)r * v.rec_turns + t_rel) * n + j] = s;
+  }
+}
+
+// REC: the instantiation for rounds that hold a frequency-map job; every other launch uses the
+// REC = false code, which has no record path at all.
+template <int BLOCK, int MINB, bool REC>
 __global__ void __launch_bounds__(BLOCK, MINB) k_batch_track(const BatchArgs a, int ppt) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -108,8 +132,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_batch_track(const BatchArgs a, 
       LossInfo li;
       if (alive) {
         refresh(p, G);
-        for (int turn = 0; turn < nt && alive; ++turn)
+        for (int turn = 0; turn < nt && alive; ++turn) {
           alive = track_turn(p, hdr, pool, ap, G, 0, n_ele, turn == 0, turn_no0 + turn, li);
+          if (REC && sv.rec && alive)
+            fma_record(sv, j, turn_no0 + turn - sv.rec_turn0, p.x, p.px, p.y, p.py, p.z, p.pz);
+        }
       }
       if (valid) store_particle(soa, j, p, alive, li, z_in, beta_in, nt, turn_no0, seg_ref, sv.ref_prefix, 0);
       if (a.live_out) {
@@ -187,14 +214,15 @@ __global__ void k_batch_init_list(int32_t* __restrict__ list, int64_t n, unsigne
 struct Variant {
   int block, minb;
   const void* fn;
+  const void* fn_rec;
 };
+#define BG_BATCH_VARIANT(B, M) {B, M, (const void*)k_batch_track<B, M, false>, (const void*)k_batch_track<B, M, true>}
 const Variant kVariants[] = {
-    {64, 8, (const void*)k_batch_track<64, 8>},    {64, 12, (const void*)k_batch_track<64, 12>},
-    {128, 3, (const void*)k_batch_track<128, 3>},  {128, 4, (const void*)k_batch_track<128, 4>},
-    {128, 5, (const void*)k_batch_track<128, 5>},  {128, 6, (const void*)k_batch_track<128, 6>},
-    {256, 1, (const void*)k_batch_track<256, 1>},  {256, 2, (const void*)k_batch_track<256, 2>},
-    {256, 3, (const void*)k_batch_track<256, 3>},  {512, 1, (const void*)k_batch_track<512, 1>},
+    BG_BATCH_VARIANT(64, 8),  BG_BATCH_VARIANT(64, 12), BG_BATCH_VARIANT(128, 3), BG_BATCH_VARIANT(128, 4),
+    BG_BATCH_VARIANT(128, 5), BG_BATCH_VARIANT(128, 6), BG_BATCH_VARIANT(256, 1), BG_BATCH_VARIANT(256, 2),
+    BG_BATCH_VARIANT(256, 3), BG_BATCH_VARIANT(512, 1),
 };
+#undef BG_BATCH_VARIANT
 
 }  // namespace
 
@@ -219,11 +247,19 @@ cudaError_t batch_resolve(const BatchLaunch& cfg, uint32_t smem_bytes, int sm_co
   if (!v || cfg.particles_per_thread < 1) return cudaErrorInvalidValue;
   cudaError_t err = cudaFuncSetAttribute(v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
   if (err != cudaSuccess) return err;
+  err = cudaFuncSetAttribute(v->fn_rec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  if (err != cudaSuccess) return err;
   int per_sm = 0;
   err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v->fn, cfg.block, smem_bytes);
   if (err != cudaSuccess) return err;
   if (per_sm < 1) per_sm = 1;
+  int per_sm_rec = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_rec, v->fn_rec, cfg.block, smem_bytes);
+  if (err != cudaSuccess) return err;
+  if (per_sm_rec < 1) per_sm_rec = 1;
   out->fn = v->fn;
+  out->fn_rec = v->fn_rec;
+  out->grid_rec = sm_count * per_sm_rec;
   out->block = cfg.block;
   out->grid = sm_count * per_sm;
   out->ppt = cfg.particles_per_thread;
@@ -231,9 +267,11 @@ cudaError_t batch_resolve(const BatchLaunch& cfg, uint32_t smem_bytes, int sm_co
   return cudaSuccess;
 }
 
-cudaError_t batch_launch_track(const BatchKernel& k, const BatchArgs& a, cudaStream_t stream) {
+cudaError_t batch_launch_track(const BatchKernel& k, const BatchArgs& a, cudaStream_t stream, bool record) {
   int ppt = k.ppt;
   void* args[] = {(void*)&a, (void*)&ppt};
+  if (record)
+    return cudaLaunchKernel(k.fn_rec, dim3((unsigned)k.grid_rec), dim3((unsigned)k.block), args, k.smem, stream);
   return cudaLaunchKernel(k.fn, dim3((unsigned)k.grid), dim3((unsigned)k.block), args, k.smem, stream);
 }
 

@@ -18,6 +18,13 @@ struct BatchVar {
   int32_t turn0;              // turn number of call-relative turn 0
   int32_t n_turns;            // turns of the current call for this variant
   Globals G;
+  // Frequency-map job (serving): after every turn the normalised coordinates of each surviving
+  // particle go to rec [6][rec_turns][n]; nullptr for every other variant.
+  double* rec;
+  const double* rec_par;      // norm [36] (row-major), closed orbit [6], z_limit (0: no z cut)
+  int32_t* rec_state;         // [n] 0 recording, 2 stopped outside the RF bucket; [n, 2n) its turn
+  int32_t rec_turn0;          // turn number of the job's first turn
+  int32_t rec_turns;          // the job's turn count
 };
 
 // Arguments of one launch of k_batch_track: call-relative turns [turn_off, turn_off + n_turns),
@@ -55,11 +62,14 @@ struct BatchKernel {
   const void* fn = nullptr;
   int block = 0, grid = 0, ppt = 1;
   uint32_t smem = 0;
+  const void* fn_rec = nullptr;  // the same shape with the frequency-map record path
+  int grid_rec = 0;
 };
 
 cudaError_t batch_upload_constants();
 cudaError_t batch_resolve(const BatchLaunch& cfg, uint32_t smem_bytes, int sm_count, BatchKernel* out);
-cudaError_t batch_launch_track(const BatchKernel& k, const BatchArgs& a, cudaStream_t stream);
+// record: use the instantiation with the frequency-map record path (rounds with an FMA job).
+cudaError_t batch_launch_track(const BatchKernel& k, const BatchArgs& a, cudaStream_t stream, bool record = false);
 // Work plan for a launch: tile_prefix from the live counts (or the variants' sizes when
 // identity is set), restricted to variants with turns left after turn_off; zeroes the queue
 // counter and the next launch's counts (n_zero, nullable).

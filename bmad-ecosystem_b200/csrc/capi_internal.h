@@ -22,6 +22,11 @@ int check_err_flag(bmadgpu_ctx* c);
 // if not NULL, receives the per-turn sums [n_turns][28].
 int track_device(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch* b, int32_t ix_start,
                  int32_t ix_end, int32_t turn0, int32_t n_turns, double* d_moments);
+// Frequency-map tunes of n particles from their record hist [6][n_turn][n] (fma.cu): fstate[i]
+// = 1 where state[i] is not alive, else rec_state[i]; tunes [n][6] where fstate is 0.
+cudaError_t fma_launch_tunes(const double* hist, int64_t n, int32_t n_turn, int32_t N, const int32_t* state,
+                             const int32_t* rec_state, int32_t* fstate, int32_t flip_a, int32_t flip_b, double* tunes,
+                             int sm_count, cudaStream_t s);
 }  // namespace bmadgpu
 
 #define CUDA_TRY(call)                                            \

@@ -187,7 +187,33 @@ __global__ void k_fma_start(const double* __restrict__ off, const double* __rest
   }
 }
 
+__global__ void k_fma_status(const int32_t* __restrict__ state, const int32_t* __restrict__ rec_state, int64_t n,
+                             int32_t* __restrict__ fstate) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    fstate[i] = state[i] != BMADGPU_ALIVE ? 1 : rec_state[i];
+}
+
 }  // namespace
+
+namespace bmadgpu {
+
+cudaError_t fma_launch_tunes(const double* hist, int64_t n, int32_t n_turn, int32_t N, const int32_t* state,
+                             const int32_t* rec_state, int32_t* fstate, int32_t flip_a, int32_t flip_b, double* tunes,
+                             int sm_count, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if (N < 2 || N > kMaxFftTurns || N > n_turn) return cudaErrorInvalidValue;
+  const size_t smem = sizeof(double) * 4 * N;
+  cudaError_t e = cudaSuccess;
+  if (smem > 48 * 1024) e = cudaFuncSetAttribute(k_fma_tunes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sm_count * 8));
+  k_fma_status<<<grid, 256, 0, s>>>(state, rec_state, n, fstate);
+  k_fma_tunes<<<(unsigned)(n * 6), kTuneThreads, smem, s>>>(hist, n, n_turn, N, fstate, flip_a, flip_b, tunes);
+  return cudaGetLastError();
+}
+
+}  // namespace bmadgpu
 
 extern "C" int bmadgpu_fma(bmadgpu_ctx* c, const bmadgpu_lattice* lat, int32_t n_particles, const double* offsets,
                            const bmadgpu_fma_params* P, bmadgpu_fma_point* out) {

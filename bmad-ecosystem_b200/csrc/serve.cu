@@ -48,6 +48,11 @@ constexpr size_t kBytesPerParticle = 8 * sizeof(double) + 4 * sizeof(int32_t) + 
 constexpr uint32_t kServeStageBytes = 64 * 1024;
 constexpr int kRoundsInFlight = 2;
 constexpr size_t kMaxQueued = 1 << 20;
+constexpr int kRecPar = 48;  // norm [36], closed orbit [6], z_limit, padding
+
+// Record-arena layout of a frequency-map job of n particles and T turns (in doubles): the record
+// [6][T][n], the parameters, the tunes [n][6], rec_state [2n] (int32) and fstate [n] (int32).
+int64_t rec_doubles(int64_t n, int64_t T) { return 6 * T * n + kRecPar + 6 * n + n + n; }
 
 double now_s() {
   using namespace std::chrono;
@@ -116,6 +121,14 @@ struct Job {
   double t_submit = -1, t_admit = -1, t_done = -1;
   int64_t particle_turns = 0;
   cudaEvent_t ev_up = nullptr, ev_down = nullptr;
+  // frequency-map job: record range [rec_off, rec_off + rec_len) of the record arena (doubles),
+  // parameters, result staging (pinned: tunes [6n] then rec_state [2n]) and the caller's points
+  bool fma = false;
+  int64_t rec_off = -1, rec_len = 0;
+  int32_t fft_turns = 0, flip_a = 0, flip_b = 0;
+  double rec_par[kRecPar] = {};
+  void* h_fma = nullptr;
+  bmadgpu_fma_point* fma_out = nullptr;
   double work() const { return (double)host.n * (double)(n_turns - done_turns) * (double)lat->pk.info.n_ele; }
 };
 
@@ -148,6 +161,10 @@ struct bmadgpu_server {
   unsigned long long* h_cnt[kRoundsInFlight] = {nullptr, nullptr};
   BatchKernel kern;
   uint32_t smem = 0;
+  // record arena for frequency-map jobs (doubles)
+  double* d_rec = nullptr;
+  int64_t rec_capacity = 0;
+  RangeAlloc rec_arena;
   // bookkeeping (guarded by mu)
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -204,6 +221,17 @@ BatchVar make_var(const Job& j) {
   return v;
 }
 
+// The record pointers of a frequency-map job's descriptor.
+void set_rec(BatchVar& v, const Job& j, double* d_rec) {
+  const int64_t n = j.host.n, T = j.n_turns;
+  double* base = d_rec + j.rec_off;
+  v.rec = base;
+  v.rec_par = base + 6 * T * n;
+  v.rec_state = reinterpret_cast<int32_t*>(base + 6 * T * n + kRecPar + 6 * n);
+  v.rec_turn0 = j.turn0;
+  v.rec_turns = j.n_turns;
+}
+
 // Copies a job's particles into its arena range (copy stream) and records ev_up.
 bool upload(bmadgpu_server* s, Job& j) {
   const int64_t n = j.host.n, off = j.off, C = s->capacity;
@@ -221,6 +249,13 @@ bool upload(bmadgpu_server* s, Job& j) {
   if (j.host.ix_ele) SRV_TRY(cudaMemcpyAsync(ie, j.host.ix_ele, ni, cudaMemcpyHostToDevice, st));
   if (j.host.ix_turn) SRV_TRY(cudaMemcpyAsync(it, j.host.ix_turn, ni, cudaMemcpyHostToDevice, st));
   if (j.host.location) SRV_TRY(cudaMemcpyAsync(lo, j.host.location, ni, cudaMemcpyHostToDevice, st));
+  if (j.fma) {
+    BatchVar v;
+    std::memset(&v, 0, sizeof(v));
+    set_rec(v, j, s->d_rec);
+    SRV_TRY(cudaMemcpyAsync(const_cast<double*>(v.rec_par), j.rec_par, sizeof(j.rec_par), cudaMemcpyHostToDevice, st));
+    SRV_TRY(cudaMemsetAsync(v.rec_state, 0, 2 * ni, st));
+  }
   SRV_TRY(cudaEventRecord(j.ev_up, st));
   return true;
 }
@@ -238,8 +273,42 @@ bool download(bmadgpu_server* s, Job& j, cudaEvent_t after) {
   if (j.host.ix_turn) SRV_TRY(cudaMemcpyAsync(j.host.ix_turn, s->d_i32 + 2 * C + off, ni, cudaMemcpyDeviceToHost, st));
   if (j.host.location)
     SRV_TRY(cudaMemcpyAsync(j.host.location, s->d_i32 + 3 * C + off, ni, cudaMemcpyDeviceToHost, st));
+  if (j.fma) {
+    // the tunes of the job's record, on the copy stream after the job's last round
+    BatchVar v;
+    std::memset(&v, 0, sizeof(v));
+    set_rec(v, j, s->d_rec);
+    double* tunes = v.rec + 6 * (int64_t)j.n_turns * n + kRecPar;
+    int32_t* fstate = v.rec_state + 2 * n;
+    SRV_TRY(fma_launch_tunes(v.rec, n, j.n_turns, j.fft_turns, s->d_i32 + off, v.rec_state, fstate, j.flip_a,
+                             j.flip_b, tunes, s->ctx->sm_count, st));
+    SRV_TRY(cudaMemcpyAsync(j.h_fma, tunes, 6 * nd, cudaMemcpyDeviceToHost, st));
+    SRV_TRY(cudaMemcpyAsync((double*)j.h_fma + 6 * n, v.rec_state, 2 * ni, cudaMemcpyDeviceToHost, st));
+  }
   SRV_TRY(cudaEventRecord(j.ev_down, st));
   return true;
+}
+
+// The caller's frequency-map points from the downloaded bunch and the staged tunes.
+void fill_fma(const Job& j) {
+  const int64_t n = j.host.n;
+  const double* tunes = (const double*)j.h_fma;
+  const int32_t* rs = (const int32_t*)(tunes + 6 * n);
+  for (int64_t i = 0; i < n; ++i) {
+    bmadgpu_fma_point& o = j.fma_out[i];
+    std::memset(&o, 0, sizeof(o));
+    if (rs[i] != 0) {  // stopped outside the bucket first (recording only runs while alive)
+      o.status = rs[i];
+      o.turn_lost = rs[n + i];
+      o.ix_ele = -1;
+    } else if (j.host.state[i] != 1) {
+      o.status = 1;
+      o.turn_lost = j.host.ix_turn ? j.host.ix_turn[i] - j.turn0 + 1 : -1;
+      o.ix_ele = j.host.ix_ele ? j.host.ix_ele[i] : -1;
+    } else {
+      for (int k = 0; k < 6; ++k) o.tune[k] = tunes[i * 6 + k];
+    }
+  }
 }
 
 int64_t count_particle_turns(const Job& j) {
@@ -284,6 +353,15 @@ void worker_main(bmadgpu_server* s) {
         if (s->cfg.policy == BMADGPU_SERVE_FIFO) break;
         continue;  // a smaller job may still fit
       }
+      if (j.fma) {
+        const int64_t roff = s->rec_arena.alloc(j.rec_len);
+        if (roff < 0) {
+          s->arena.release(off, j.host.n);
+          if (s->cfg.policy == BMADGPU_SERVE_FIFO) break;
+          continue;
+        }
+        j.rec_off = roff;
+      }
       j.slot = (int32_t)(free_slot - s->slot_job.begin());
       j.off = off;
       *free_slot = id;
@@ -301,6 +379,7 @@ void worker_main(bmadgpu_server* s) {
     const int buf = (int)(r % kRoundsInFlight);
     int32_t n_var = 0;
     std::vector<int64_t> round_jobs;
+    bool round_records = false;
     for (int32_t slot = 0; slot < (int32_t)s->slot_job.size(); ++slot) {
       const int64_t id = s->slot_job[slot];
       BatchVar& hv = s->h_vars[buf][slot];
@@ -309,6 +388,7 @@ void worker_main(bmadgpu_server* s) {
       Job& j = s->jobs[id];
       n_var = slot + 1;
       hv = make_var(j);
+      if (j.fma) set_rec(hv, j, s->d_rec);
       const int32_t left = j.n_turns - j.done_turns;
       if (left <= 0 || j.retiring || j.live == 0) continue;
       const int32_t k = std::min(left, j.per_round);
@@ -318,6 +398,7 @@ void worker_main(bmadgpu_server* s) {
       j.rounds++;
       j.last_round = r;
       round_jobs.push_back(id);
+      round_records = round_records || j.fma;
     }
     const bool stopping = s->stop;
     lk.unlock();
@@ -372,7 +453,7 @@ void worker_main(bmadgpu_server* s) {
                cudaSuccess &&
            batch_launch_plan(s->d_vars, n_var, a.tile, 0, false, a.n_in, s->d_prefix, s->d_queue, a.n_out, c) ==
                cudaSuccess &&
-           batch_launch_track(s->kern, a, c) == cudaSuccess &&
+           batch_launch_track(s->kern, a, c, round_records) == cudaSuccess &&
            cudaMemcpyAsync(s->h_cnt[buf], a.n_out, sizeof(unsigned long long) * n_var, cudaMemcpyDeviceToHost, c) ==
                cudaSuccess &&
            cudaEventCreateWithFlags(&rd.done, cudaEventDisableTiming) == cudaSuccess &&
@@ -425,6 +506,7 @@ void worker_main(bmadgpu_server* s) {
         // copy stream, and no round in flight has work for this job.
         s->slot_job[j.slot] = -1;
         s->arena.release(j.off, j.host.n);
+        if (j.fma) s->rec_arena.release(j.rec_off, j.rec_len);
         lk.unlock();
         retiring.push_back(jp);
       }
@@ -446,6 +528,7 @@ void worker_main(bmadgpu_server* s) {
         return;
       }
       const int64_t pt = count_particle_turns(j);
+      if (j.fma) fill_fma(j);
       lk.lock();
       j.particle_turns = pt;
       j.t_done = now_s();
@@ -548,6 +631,20 @@ int bmadgpu_server_create(bmadgpu_ctx* c, const bmadgpu_server_config* cfg_in, b
          cudaHostAlloc(&s->h_cnt[i], J * sizeof(unsigned long long), cudaHostAllocPortable) == cudaSuccess;
   ok = ok && cudaMemset(s->d_cnt, 0, 2 * J * sizeof(unsigned long long)) == cudaSuccess;
   if (ok) {
+    // record arena for frequency-map jobs: record_mib, or a quarter of what is free now
+    size_t free2 = 0, total2 = 0;
+    ok = cudaMemGetInfo(&free2, &total2) == cudaSuccess;
+    const double want = cfg.record_mib > 0 ? (double)cfg.record_mib * 1048576.0 : 0.25 * (double)free2;
+    const int64_t cap_rec = (int64_t)(std::min(want, 0.9 * (double)free2) / sizeof(double));
+    if (ok && cap_rec > 0 && cudaMalloc(&s->d_rec, (size_t)cap_rec * sizeof(double)) == cudaSuccess) {
+      s->rec_capacity = cap_rec;
+      s->rec_arena.reset(cap_rec);
+    } else {
+      cudaGetLastError();
+      s->rec_arena.reset(0);
+    }
+  }
+  if (ok) {
     s->smem = cfg.stage_smem ? kServeStageBytes : 0;
     BatchLaunch bl;
     bl.block = cfg.block;
@@ -584,7 +681,9 @@ int bmadgpu_server_destroy(bmadgpu_server* s) {
   for (auto& kv : s->jobs) {
     if (kv.second.ev_up) cudaEventDestroy(kv.second.ev_up);
     if (kv.second.ev_down) cudaEventDestroy(kv.second.ev_down);
+    if (kv.second.h_fma) cudaFreeHost(kv.second.h_fma);
   }
+  cudaFree(s->d_rec);
   cudaFree(s->d_vec);
   cudaFree(s->d_beta);
   cudaFree(s->d_t);
@@ -605,13 +704,20 @@ int bmadgpu_server_destroy(bmadgpu_server* s) {
   return BMADGPU_OK;
 }
 
-int bmadgpu_server_submit(bmadgpu_server* s, const bmadgpu_lattice* lat, bmadgpu_bunch* b, int32_t turn0,
-                          int32_t n_turns, int64_t* job_id) {
+}  // extern "C"
+
+namespace {
+
+// Queues a job (fma: a frequency-map job with its prepared fields; nullptr otherwise).
+int submit_job(bmadgpu_server* s, const bmadgpu_lattice* lat, bmadgpu_bunch* b, int32_t turn0, int32_t n_turns,
+               const Job* fma, int64_t* job_id) {
   if (!s || !lat || !b || !job_id) return fail(BMADGPU_EINVAL, "NULL argument");
   if (b->n < 0 || n_turns < 0) return fail(BMADGPU_EINVAL, "negative particle or turn count");
   if (b->n > 0 && (!b->vec || !b->beta || !b->state)) return fail(BMADGPU_EINVAL, "bunch vec/beta/state NULL");
   if (lat->device != s->ctx->device) return fail(BMADGPU_EINVAL, "lattice and server are on different devices");
   if (b->n > s->capacity) return fail(BMADGPU_ENOMEM, "the bunch is larger than the server's particle arena");
+  if (fma && fma->rec_len > s->rec_capacity)
+    return fail(BMADGPU_ENOMEM, "the frequency-map record is larger than the server's record arena");
   cudaEvent_t up = nullptr, down = nullptr;
   CUDA_TRY(cudaSetDevice(s->ctx->device));
   CUDA_TRY(cudaEventCreateWithFlags(&up, cudaEventDisableTiming));
@@ -619,18 +725,24 @@ int bmadgpu_server_submit(bmadgpu_server* s, const bmadgpu_lattice* lat, bmadgpu
     cudaEventDestroy(up);
     return fail(BMADGPU_ECUDA, "cudaEventCreate failed");
   }
-  std::lock_guard<std::mutex> lk(s->mu);
-  if (s->err_code) {
+  void* h_fma = nullptr;
+  if (fma && b->n > 0 &&
+      cudaHostAlloc(&h_fma, (size_t)b->n * (6 * sizeof(double) + 2 * sizeof(int32_t)), cudaHostAllocPortable) !=
+          cudaSuccess) {
     cudaEventDestroy(up);
     cudaEventDestroy(down);
-    return fail(s->err_code, s->err_msg);
+    return fail(BMADGPU_ENOMEM, "cudaHostAlloc failed");
   }
-  if (s->stop || s->queued.size() >= kMaxQueued) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->err_code || s->stop || s->queued.size() >= kMaxQueued) {
     cudaEventDestroy(up);
     cudaEventDestroy(down);
+    if (h_fma) cudaFreeHost(h_fma);
+    if (s->err_code) return fail(s->err_code, s->err_msg);
     return fail(BMADGPU_EBUSY, "server queue is full or stopping");
   }
   Job j;
+  if (fma) j = *fma;
   j.id = s->next_id++;
   j.lat = lat;
   j.host = *b;
@@ -640,6 +752,7 @@ int bmadgpu_server_submit(bmadgpu_server* s, const bmadgpu_lattice* lat, bmadgpu
   j.t_submit = now_s();
   j.ev_up = up;
   j.ev_down = down;
+  j.h_fma = h_fma;
   if (s->t_first < 0) s->t_first = j.t_submit;
   s->submitted++;
   if (b->n == 0 || n_turns == 0) {
@@ -657,6 +770,45 @@ int bmadgpu_server_submit(bmadgpu_server* s, const bmadgpu_lattice* lat, bmadgpu
   s->cv_work.notify_all();
   s->cv_done.notify_all();
   return BMADGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bmadgpu_server_submit(bmadgpu_server* s, const bmadgpu_lattice* lat, bmadgpu_bunch* b, int32_t turn0,
+                          int32_t n_turns, int64_t* job_id) {
+  return submit_job(s, lat, b, turn0, n_turns, nullptr, job_id);
+}
+
+int bmadgpu_server_submit_fma(bmadgpu_server* s, const bmadgpu_lattice* lat, bmadgpu_bunch* b, int32_t turn0,
+                              int32_t n_turns, const bmadgpu_fma_params* P, bmadgpu_fma_point* points,
+                              int64_t* job_id) {
+  if (!s || !lat || !b || !P || (b->n > 0 && !points)) return fail(BMADGPU_EINVAL, "NULL argument");
+  if (n_turns < 2) return fail(BMADGPU_EINVAL, "a frequency-map job needs at least 2 turns");
+  Job f;
+  f.fma = true;
+  f.fft_turns = P->fft_turns > 0 ? P->fft_turns : n_turns / 2;
+  if (f.fft_turns < 2 || f.fft_turns > n_turns || f.fft_turns > 4096)
+    return fail(BMADGPU_EINVAL, "fft_turns must be in [2, min(n_turns, 4096)]");
+  f.flip_a = P->tune_a < 0.5;
+  f.flip_b = P->tune_b < 0.5;
+  std::memcpy(f.rec_par, P->norm, sizeof(double) * 36);
+  std::memcpy(f.rec_par + 36, P->orbit, sizeof(double) * 6);
+  double z_limit = 0;
+  if (P->z_cut) {  // frequency_map.f90:99-119
+    double fr = P->rf_frequency;
+    if (fr <= 0) {
+      fr = 0;
+      for (const auto& e : lat->eles)
+        if (e.key == BMADGPU_RFCAVITY) fr = (fr == 0) ? e.rf_frequency : std::fmin(fr, e.rf_frequency);
+    }
+    if (fr > 0) z_limit = 0.25 * (299792458.0 / fr);
+  }
+  f.rec_par[42] = z_limit;
+  f.rec_len = rec_doubles(b->n, n_turns);
+  f.fma_out = points;
+  return submit_job(s, lat, b, turn0, n_turns, &f, job_id);
 }
 
 int bmadgpu_server_job(bmadgpu_server* s, int64_t id, bmadgpu_job_info* info) {

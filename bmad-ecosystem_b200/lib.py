@@ -403,7 +403,7 @@ class ServerConfig(C.Structure):
     _fields_ = [("max_particles", C.c_int64), ("hbm_fraction", C.c_double), ("max_jobs", C.c_int32),
                 ("element_steps", C.c_int32), ("target_live", C.c_int64), ("policy", C.c_int32),
                 ("block", C.c_int32), ("ctas_per_sm", C.c_int32), ("stage_smem", C.c_int32),
-                ("reserved", C.c_int32 * 4)]
+                ("record_mib", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class JobInfo(C.Structure):
@@ -515,6 +515,35 @@ class Server:
         check(load().bmadgpu_server_submit(self._h, lat.handle, C.byref(v), turn0, n_turns, C.byref(jid)))
         self._keep[jid.value] = (lat, bunch)
         return jid.value
+
+    def submit_fma(self, lat, bunch, n_turns, norm, orbit, tunes, fft_turns=0, z_cut=True, rf_frequency=0.0,
+                   turn0=0):
+        """A frequency-map job: bunch holds closed orbit + offsets; norm, orbit and tunes as
+        fma_setup gives them. fma_result(jid) has the tunes once the job is done."""
+        lib = load()
+        lib.bmadgpu_server_submit_fma.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(abi.Bunch), C.c_int32, C.c_int32,
+                                                  C.POINTER(FmaParams), C.POINTER(FmaPoint), C.POINTER(C.c_int64)]
+        P = FmaParams(n_turns, fft_turns, 1 if z_cut else 0, 0, rf_frequency)
+        P.norm[:] = list(np.asarray(norm, float).ravel())
+        P.orbit[:] = list(np.asarray(orbit, float))
+        P.tune_a, P.tune_b = tunes
+        pts = (FmaPoint * max(bunch.n, 1))()
+        v = bunch.view()
+        jid = C.c_int64()
+        check(lib.bmadgpu_server_submit_fma(self._h, lat.handle, C.byref(v), turn0, n_turns, C.byref(P), pts,
+                                            C.byref(jid)))
+        self._keep[jid.value] = (lat, bunch, P, pts)
+        return jid.value
+
+    def fma_result(self, jid):
+        """(tunes [n, 6], status [n], turn_lost [n], ix_ele [n]) of a finished frequency-map job."""
+        _, bunch, _, pts = self._keep[jid]
+        n = bunch.n
+        q = np.array([pts[i].tune[:] for i in range(n)]).reshape(n, 6)
+        st = np.array([pts[i].status for i in range(n)], np.int32)
+        tl = np.array([pts[i].turn_lost for i in range(n)], np.int32)
+        ie = np.array([pts[i].ix_ele for i in range(n)], np.int32)
+        return q, st, tl, ie
 
     def job(self, jid):
         i = JobInfo()
@@ -901,22 +930,29 @@ def fma_normalization(mat6):
     return np.linalg.inv(T).T
 
 
+def fma_setup(ctx, lat):
+    """(closed orbit, normalisation, ring tunes) as frequency_map computes them before its grid
+    loop (twiss_and_track with the RF on, frequency_map.f90:128-212)."""
+    orbit = closed_orbit(ctx, lat)[0]
+    norm = fma_normalization(one_turn_matrix(ctx, lat, orbit, rf_on=True)[0])
+    tw = twiss_from_mat6(one_turn_matrix(ctx, lat, orbit, rf_on=False)[0], orbit)
+    return orbit, norm, (tw["phi_a"] / (2 * math.pi), tw["phi_b"] / (2 * math.pi))
+
+
 def fma(ctx, lat, offsets, n_turn, fft_turns=0, z_cut=True, rf_frequency=0.0, orbit=None, norm=None, tunes=None):
     """frequency_map for particles at closed orbit + offsets[n, 6]. The closed orbit, the
-    normalisation and the ring tunes default to what the reference computes (twiss_and_track with
-    the RF on). Returns (tunes[n, 6], status[n], turn_lost[n], ix_ele[n])."""
+    normalisation and the ring tunes default to what the reference computes (fma_setup).
+    Returns (tunes[n, 6], status[n], turn_lost[n], ix_ele[n])."""
     lib = load()
     lib.bmadgpu_fma.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(FmaParams),
                                 C.POINTER(FmaPoint)]
     off = np.ascontiguousarray(offsets, dtype=np.float64).reshape(-1, 6)
     n = off.shape[0]
-    if orbit is None:
-        orbit = closed_orbit(ctx, lat)[0]
-    if norm is None:
-        norm = fma_normalization(one_turn_matrix(ctx, lat, orbit, rf_on=True)[0])
-    if tunes is None:
-        tw = twiss_from_mat6(one_turn_matrix(ctx, lat, orbit, rf_on=False)[0], orbit)
-        tunes = (tw["phi_a"] / (2 * math.pi), tw["phi_b"] / (2 * math.pi))
+    if orbit is None or norm is None or tunes is None:
+        o, nm, tn = fma_setup(ctx, lat)
+        orbit = o if orbit is None else orbit
+        norm = nm if norm is None else norm
+        tunes = tn if tunes is None else tunes
     P = FmaParams(n_turn, fft_turns, 1 if z_cut else 0, 0, rf_frequency)
     P.norm[:] = list(np.asarray(norm, float).ravel())
     P.orbit[:] = list(np.asarray(orbit, float))

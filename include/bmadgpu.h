@@ -321,7 +321,9 @@ typedef struct bmadgpu_server_config {
   int32_t block;           /* round kernel shape as bmadgpu_batch_tuning (0: 64) */
   int32_t ctas_per_sm;     /* (0 with block 0: 12) */
   int32_t stage_smem;      /* stage element tables of up to 64 KiB in shared memory */
-  int32_t reserved[4];
+  int32_t record_mib;      /* record arena of frequency-map jobs in MiB (0: a quarter of the device
+                              memory still free after the particle arena) */
+  int32_t reserved[3];
 } bmadgpu_server_config;
 
 typedef struct bmadgpu_job_info {
@@ -349,6 +351,17 @@ int bmadgpu_server_destroy(bmadgpu_server* server);
  * done. BMADGPU_ENOMEM if the bunch can never fit the arena, BMADGPU_EBUSY if the queue is full. */
 int bmadgpu_server_submit(bmadgpu_server* server, const bmadgpu_lattice* lat, bmadgpu_bunch* bunch, int32_t turn0,
                           int32_t n_turns, int64_t* job_id);
+/* A frequency-map job (frequency_map.f90:197-376 for these particles): bunch holds the start
+ * coordinates (closed orbit + grid offsets), tracked n_turns turns like any job, while every turn's
+ * normalised coordinates are recorded on the device (params: normalisation, closed orbit, z_cut,
+ * fft_turns, ring tunes; params->n_turn is not used). When the job completes, points [n] hold each
+ * particle's tunes or its status as bmadgpu_fma gives them, and the bunch arrays its final
+ * coordinates. The record (48 B per particle-turn) comes from the server's record arena. */
+struct bmadgpu_fma_params;
+struct bmadgpu_fma_point;
+int bmadgpu_server_submit_fma(bmadgpu_server* server, const bmadgpu_lattice* lat, bmadgpu_bunch* bunch, int32_t turn0,
+                              int32_t n_turns, const struct bmadgpu_fma_params* params,
+                              struct bmadgpu_fma_point* points, int64_t* job_id);
 int bmadgpu_server_job(bmadgpu_server* server, int64_t job_id, bmadgpu_job_info* info);
 /* Waits until the job (job_id = -1: every submitted job) is done or cancelled; BMADGPU_ETIMEDOUT
  * after timeout_s seconds. Also reports an error the worker met. */
