@@ -472,33 +472,55 @@ def run_serve(args):
         lat = lib.Lattice(ctx, e, p)
         if j["kind"] == "gauss":
             vec = rings.matched_gaussian(e, j["n"], seed=j["variant_seed"] % 100000)
+            j["fma"] = None
         else:
-            vec = rings.fma_grid(j["n"])
+            # frequency-map job: grid offsets from the closed orbit, with the reference's set-up
+            orbit, norm, tunes = lib.fma_setup(ctx, lat)
+            vec = rings.fma_grid(j["n"]) + orbit[:, None]
+            j["fma"] = (norm, orbit, tunes)
         hb = lib.HostBunch.from_vec(vec, p)
         jobs.append((j, lat, vec, hb.beta))
     t_prep = time.time() - t_prep
+    n_fma = sum(1 for j, _, _, _ in jobs if j["fma"] is not None)
 
     def pinned_inputs():
         return [lib.PinnedBunch(vec, beta) for (_, _, vec, beta) in jobs]
 
+    def server():
+        # a quarter of HBM for resident particles, most of the rest for frequency-map records
+        free_b = torch.cuda.mem_get_info(0)[0]
+        return lib.Server(ctx, hbm_fraction=0.25, record_mib=int(0.6 * free_b / 2 ** 20))
+
+    def submit(srv, j, lat, b, turns):
+        if j["fma"] is None:
+            return srv.submit(lat, b, turns)
+        norm, orbit, tunes = j["fma"]
+        return srv.submit_fma(lat, b, turns, norm, orbit, tunes)
+
+    fma_summary = {}
+
     def run_stream(bunches):
-        srv = lib.Server(ctx)
+        srv = server()
         start = time.perf_counter()
+        ids = []
         for (j, lat, _, _), b in zip(jobs, bunches):
             dt = start + j["arrival"] - time.perf_counter()
             if dt > 0:
                 time.sleep(dt)
-            srv.submit(lat, b, j["turns"])
+            ids.append((j, submit(srv, j, lat, b, j["turns"])))
         srv.wait(-1, timeout=7200)
         st = srv.stats()
+        done = [srv.fma_result(jid)[1] for j, jid in ids if j["fma"] is not None]
+        fma_summary["particles_with_tunes"] = int(sum(int(np.sum(x == 0)) for x in done))
+        fma_summary["particles"] = int(sum(len(x) for x in done))
         srv.close()
         return st
 
     # warm-up: a server with the first few jobs of the stream, shortened to 8 turns each
-    warm = lib.Server(ctx)
+    warm = server()
     warm_b = [lib.PinnedBunch(vec, beta) for (_, _, vec, beta) in jobs[:3]]
     for (j, lat, _, _), b in zip(jobs[:3], warm_b):
-        warm.submit(lat, b, 8)
+        submit(warm, j, lat, b, 8)
     warm.wait(-1, timeout=600)
     warm.close()
     clocks = ClockSampler(0)
@@ -525,8 +547,10 @@ def run_serve(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (Poisson stream, perturbed rings, Gaussian / frequency-map grids)",
         "config": {"workload": "serve: first %d jobs of the 2000-job stream (mean gap 5 ms), %d particles, "
-                               "50/100/200/400-cell rings" % (len(jobs), n_part),
+                               "50/100/200/400-cell rings, %d frequency-map jobs (turn-by-turn record and tunes on "
+                               "the device)" % (len(jobs), n_part, n_fma),
                    "host_prep_s": t_prep},
+        "fma": fma_summary,
         "latency_s": {"p50": st["latency_p50_s"], "p99": st["latency_p99_s"], "max": st["latency_max_s"]},
         "server": {k: st[k] for k in ("jobs_done", "rounds", "particle_turns", "capacity", "peak_resident")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": n_part * (8 * 8 + 4 * 4),
