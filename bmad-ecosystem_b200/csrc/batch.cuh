@@ -67,6 +67,8 @@ struct BatchKernel {
 };
 
 cudaError_t batch_upload_constants();
+cudaError_t batch_rec_upload_constants();            // batch_rec.cu's copy of the tables
+const void* batch_rec_kernel(int block, int minb);  // record-path instantiation of a shape
 cudaError_t batch_resolve(const BatchLaunch& cfg, uint32_t smem_bytes, int sm_count, BatchKernel* out);
 // record: use the instantiation with the frequency-map record path (rounds with an FMA job).
 cudaError_t batch_launch_track(const BatchKernel& k, const BatchArgs& a, cudaStream_t stream, bool record = false);

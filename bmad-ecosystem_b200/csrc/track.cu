@@ -176,6 +176,8 @@ cudaError_t upload_constants() {
   if (e != cudaSuccess) return e;
   e = batch_upload_constants();
   if (e != cudaSuccess) return e;
+  e = batch_rec_upload_constants();
+  if (e != cudaSuccess) return e;
   return adjoint_upload_constants();
 }
 
