@@ -110,8 +110,9 @@ BG_HD void vjp_quad_step(const Particle& p, double b1, double length, double sl,
   double rel = 1 + p.pz;
   double k1 = b1 / (length * rel);
   double ax, bx, cx_, dx, zx0, zx1, zx2, ay, by, cy, dy, zy0, zy1, zy2;
-  quad_mat2(-k1, sl, rel, ax, bx, cx_, dx, zx0, zx1, zx2);
-  quad_mat2(k1, sl, rel, ay, by, cy, dy, zy0, zy1, zy2);
+  const double ef = 1 / rel;
+  quad_mat2(-k1, sl, rel, ef, ax, bx, cx_, dx, zx0, zx1, zx2);
+  quad_mat2(k1, sl, rel, ef, ay, by, cy, dy, zy0, zy1, zy2);
   double x = p.x, px = p.px, y = p.y, py = p.py;
   // low_energy_z on the stepped particle: pz and beta are unchanged by the step
   vjp_lez(p, sl, a, G);

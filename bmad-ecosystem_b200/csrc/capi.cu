@@ -164,6 +164,7 @@ Globals make_globals(const bmadgpu_param& p) {
   g.lez_f = g.lez_b02 * (2 * g.lez_b02 - g.lez_me2 / 2);
   g.lez_thresh = 3e-7 * p.e_tot;
   g.charge = p.charge;
+  g.inv_beta0 = 1 / g.beta0;
   return g;
 }
 

@@ -70,6 +70,7 @@ double h_cfull_raw[22][22];
 // The element code with every `double` counted. table.h (ApRec, Globals, EleHdr) is already
 // included with plain doubles; the maps and particle state become counted.
 #define double bmadgpu::CD
+#define BG_COUNT_OPS
 #define h_cmulti h_cmulti_c
 #define h_cfull h_cfull_c
 #include "elements.cuh"
@@ -114,6 +115,7 @@ int bmadgpu_hostcheck_count_ops(const bmadgpu_element* eles, int32_t n_ele, cons
   double me = param->mass / param->e_tot;
   G.lez_me2 = me * me; G.lez_b02 = G.beta0 * G.beta0; G.lez_f = G.lez_b02 * (2 * G.lez_b02 - G.lez_me2 / 2);
   G.lez_thresh = 3e-7 * param->e_tot; G.charge = param->charge;
+  G.inv_beta0 = 1 / G.beta0;
   g_ops = OpCounts{0, 0, 0, 0, 0};
   double pturns = 0;
   const int64_t n = b->n;

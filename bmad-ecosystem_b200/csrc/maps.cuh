@@ -65,6 +65,33 @@ BG_HD double sqrt_one(double x) {  // sim_utils/special_functions/sqrt_one.f90
   return x / rad;
 }
 
+// a / b, correctly rounded, from y = RN(1/b) shared by several quotients with the divisor b:
+// q = RN(a y), r = a - b q (exact by an FMA), and RN(q + r y) = RN(a / b) (Markstein's correction
+// theorem: P. Markstein, "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34 (1990) 111-119; J.-M. Muller et al., Handbook of Floating-Point
+// Arithmetic, 2nd ed. (2018), sec. 4.8). The theorem needs no underflow or overflow, so quotients
+// outside [2^-900, 2^900] take the plain division; a zero numerator gives q itself (the sign of the
+// zero quotient is that of a y). Every caller's y is itself a rounded division 1 / b (or an exact
+// power-of-two multiple of one), so each quotient is the same bits as a / b.
+#if defined(BG_COUNT_OPS)
+BG_HD double div_rcp(double a, double b, double y) {  // counted as the one division it replaces
+  (void)y;
+  return a / b;
+}
+#else
+BG_HD double div_rcp(double a, double b, double y) {
+  const double q = a * y;
+  const double aq = fabs(q);
+  if (aq >= 0x1p-900 && aq <= 0x1p+900) {
+    const double r = fma(-b, q, a);
+    return fma(r, y, q);
+  }
+  if (a == 0) return q;
+  return a / b;
+}
+#endif
+constexpr real_const kRcp6 = 1.0 / 6.0;  // RN(1/6): the divisor of the Taylor terms x/6
+
 BG_HD void refresh(Particle& p, const Globals& g) {
   double delta = p.pz;
   double rel_pc = 1 + delta;
@@ -81,7 +108,7 @@ BG_HD void refresh(Particle& p, const Globals& g) {
 // low_energy_z_correction, bmad/low_level/low_energy_z_correction.f90:22-57
 BG_HD double low_energy_z(const Particle& p, double ds, const Globals& g) {
   if (p.lez_series) return ds * p.pz * p.lez_a * g.lez_me2;
-  return ds * p.lez_a / g.beta0;
+  return div_rcp(ds * p.lez_a, g.beta0, g.inv_beta0);
 }
 
 // orbit_too_large, bmad/low_level/orbit_too_large.f90:26-120
@@ -138,20 +165,22 @@ BG_HD void aperture(Particle& p, const ApRec& a, bool elliptical) {
 // motion). sqrt(1 + (-pxy2)) equals ps_rel exactly, so sqrt_one(-pxy2) reuses it.
 BG_HD void drift(Particle& p, double length) {
   if (length == 0) return;
+  // quotients by 1 + pz use the particle's cached 1 / (1 + pz), those by ps_rel one reciprocal
   double rel_pc = 1 + p.pz;
-  double px_rel = p.px / rel_pc;
-  double py_rel = p.py / rel_pc;
+  double px_rel = div_rcp(p.px, rel_pc, p.e_factor);
+  double py_rel = div_rcp(p.py, rel_pc, p.e_factor);
   double pxy2 = px_rel * px_rel + py_rel * py_rel;
   if (pxy2 >= 1) { p.state = S_LOST_PZ; return; }
   double ps_rel = sqrt(1 - pxy2);
-  p.x = p.x + length * px_rel / ps_rel;
-  p.y = p.y + length * py_rel / ps_rel;
+  const double inv_ps = 1 / ps_rel;
+  p.x = p.x + div_rcp(length * px_rel, ps_rel, inv_ps);
+  p.y = p.y + div_rcp(length * py_rel, ps_rel, inv_ps);
   double dz;
   if (p.beta > 0) {
     double so = -pxy2 / (ps_rel + 1);  // sqrt_one(-pxy2)
-    dz = length * (p.dzb + so / ps_rel);
+    dz = length * (p.dzb + div_rcp(so, ps_rel, inv_ps));
   } else {
-    dz = length * (1 - 1 / ps_rel);
+    dz = length * (1 - inv_ps);
   }
   p.z = p.z + dz;
 }
@@ -367,7 +396,8 @@ BG_HD void offset_unset(Particle& p, const double* __restrict__ m, bool has_tilt
 }
 
 // quad_mat2_calc, bmad/low_level/quad_mat2_calc.f90:22-61 (mat2 and z_coef)
-BG_HD void quad_mat2(double k1, double length, double rel_p, double& m11, double& m12, double& m21,
+// ef = RN(1 / rel_p), shared by the quotients by rel_p and 2 rel_p.
+BG_HD void quad_mat2(double k1, double length, double rel_p, double ef, double& m11, double& m12, double& m21,
                      double& m22, double& z0, double& z1, double& z2) {
   double sqrt_k = sqrt(fabs(k1));
   double sk_l = sqrt_k * length;
@@ -375,7 +405,7 @@ BG_HD void quad_mat2(double k1, double length, double rel_p, double& m11, double
   if (fabs(sk_l) < 1e-10) {
     double k_l2 = k1 * (length * length);
     cx = 1 + k_l2 / 2;
-    sx = (1 + k_l2 / 6) * length;
+    sx = (1 + div_rcp(k_l2, 6, kRcp6)) * length;
   } else if (k1 < 0) {
     cx = cos(sk_l);
     sx = sin(sk_l) / sqrt_k;
@@ -384,11 +414,11 @@ BG_HD void quad_mat2(double k1, double length, double rel_p, double& m11, double
     sx = sinh(sk_l) / sqrt_k;
   }
   m11 = cx;
-  m12 = sx / rel_p;
+  m12 = div_rcp(sx, rel_p, ef);
   m21 = k1 * sx * rel_p;
   m22 = cx;
   z0 = k1 * (-cx * sx + length) / 4;
-  z1 = -k1 * (sx * sx) / (2 * rel_p);
+  z1 = div_rcp(-k1 * (sx * sx), 2 * rel_p, 0.5 * ef);
   z2 = -(cx * sx + length) / (4 * (rel_p * rel_p));
 }
 
@@ -398,8 +428,8 @@ BG_HD void quad_step(Particle& p, double b1, double length, double step_len, con
   double rel_p = 1 + p.pz;
   double k1 = b1 / (length * rel_p);
   double ax, bx, cx_, dx, zx0, zx1, zx2, ay, by, cy, dy, zy0, zy1, zy2;
-  quad_mat2(-k1, step_len, rel_p, ax, bx, cx_, dx, zx0, zx1, zx2);
-  quad_mat2(k1, step_len, rel_p, ay, by, cy, dy, zy0, zy1, zy2);
+  quad_mat2(-k1, step_len, rel_p, p.e_factor, ax, bx, cx_, dx, zx0, zx1, zx2);
+  quad_mat2(k1, step_len, rel_p, p.e_factor, ay, by, cy, dy, zy0, zy1, zy2);
   double x = p.x, px = p.px, y = p.y, py = p.py;
   p.z = p.z + (zx0 * (x * x) + zx1 * x * px + zx2 * (px * px) + zy0 * (y * y) + zy1 * y * py + zy2 * (py * py));
   p.x = (0 + ax * x) + bx * px;
@@ -423,7 +453,7 @@ BG_HD void hwang_edge(Particle& p, const double* __restrict__ e, bool entering) 
     dy = gt2 * v1 * v3 * ef;
     dpy = (fg * v3 - gt2 * v1 * v4 - (gtot + gt2) * v2 * v3 - 2 * k1t * v1 * v3) * ef;
     dz = (ef * ef) * 0.5 *
-         (v33 * fg + (v11 * v1) * (4.0 * k1t - gt * gt2) / 6.0 + 0.5 * v1 * v33 * (-4.0 * k1t + gt * gs2) +
+         (v33 * fg + div_rcp((v11 * v1) * (4.0 * k1t - gt * gt2), 6.0, kRcp6) + 0.5 * v1 * v33 * (-4.0 * k1t + gt * gs2) +
           (v11 * v2 - 2.0 * v1 * v3 * v4) * gt2 - v2 * v33 * gs2);
   } else {
     dx = (gt2 * v11 - gs2 * v33) * ef / 2;
@@ -431,7 +461,7 @@ BG_HD void hwang_edge(Particle& p, const double* __restrict__ e, bool entering) 
     dy = -gt2 * v1 * v3 * ef;
     dpy = (fg * v3 + gt2 * v1 * v4 + (gtot + gt2) * v2 * v3 + (gt * gs2 - 2 * k1t) * v1 * v3) * ef;
     dz = (ef * ef) * 0.5 *
-         (v33 * fg + (v11 * v1) * (4.0 * k1t - gt * gt2) / 6.0 + 0.5 * v1 * v33 * (-4.0 * k1t + gt * gs2) -
+         (v33 * fg + div_rcp((v11 * v1) * (4.0 * k1t - gt * gt2), 6.0, kRcp6) + 0.5 * v1 * v33 * (-4.0 * k1t + gt * gs2) -
           (v11 * v2 - 2.0 * v1 * v3 * v4) * gt2 + v2 * v33 * gs2);
   }
   p.x = v1 + 1.0 * dx;
@@ -511,8 +541,9 @@ BG_HD bool bend_exact_step(Particle& p, const double* __restrict__ b, const Glob
   }
   double pt = sqrt(rel_p2 - py * py);
   if (fabs(px) > pt) { p.state = S_LOST_PZ; return false; }
-  double g_p = g_tot / pt;
-  double phi_1 = asin(px / pt);
+  const double inv_pt = 1 / pt;  // shared by the four quotients by pt
+  double g_p = div_rcp(g_tot, pt, inv_pt);
+  double phi_1 = asin(div_rcp(px, pt, inv_pt));
   double cos_plus = cos(angle + phi_1);
   double sin_plus = sin(angle + phi_1);
   double gx1 = 1 + g * x;
@@ -542,8 +573,8 @@ BG_HD bool bend_exact_step(Particle& p, const double* __restrict__ b, const Glob
   double hp = angle_p / 2;
   double L_p = 1 * L_c / ((fabs(hp) < 1e-8) ? 1.0 : sin(hp) / hp);
   p.px = pt * sin(phi_1 + angle - angle_p);
-  p.y = y + py * L_p / pt;
-  p.z = z + p.beta * step_len / G.beta0 - rel_p * L_p / pt;
+  p.y = y + div_rcp(py * L_p, pt, inv_pt);
+  p.z = z + div_rcp(p.beta * step_len, G.beta0, G.inv_beta0) - div_rcp(rel_p * L_p, pt, inv_pt);
   return true;
 }
 

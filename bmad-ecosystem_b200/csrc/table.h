@@ -90,6 +90,7 @@ struct Globals {            // branch constants (lat_param_struct / bmad_com) an
   double lez_me2;           // (mass / e_tot)**2
   double lez_thresh;        // 3d-7 * e_tot
   double charge;            // charge_of(species)
+  double inv_beta0;         // 1 / beta0 (rounded), the shared reciprocal of the quotients by beta0
 };
 
 

@@ -993,3 +993,13 @@ def naff(ctx, signals, n_comp, zero_first=False):
     check(lib.bmadgpu_naff(ctx.handle, n, m, _dptr(data), n_comp, 1 if zero_first else 0, _dptr(freqs),
                            amps.view(np.float64).ctypes.data_as(C.POINTER(C.c_double))))
     return freqs, amps
+
+
+def selftest_division(ctx, n=1 << 30, seed=1):
+    """Mismatching pairs of the maps' shared-reciprocal division against a / b on the device
+    (bmadgpu_selftest_division); 0 is the only correct answer."""
+    lib = load()
+    lib.bmadgpu_selftest_division.argtypes = [C.c_void_p, C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]
+    m = C.c_int64()
+    check(lib.bmadgpu_selftest_division(ctx.handle, n, seed, C.byref(m)))
+    return m.value

@@ -233,6 +233,11 @@ int64_t bmadgpu_ctx_launch_count(const bmadgpu_ctx* ctx);
  * (2 flops per FMA), a roofline denominator; *flops_per_s receives FLOP/s. */
 int bmadgpu_measure_fp64_peak(bmadgpu_ctx* ctx, double* flops_per_s);
 
+/* Self-check of the shared-reciprocal division the element maps use (a / b from RN(1/b) and one
+ * FMA correction): *mismatches = how many of n pseudo-random pairs (seeded) differ in any bit from
+ * the device's a / b. 0 is the only correct answer. */
+int bmadgpu_selftest_division(bmadgpu_ctx* ctx, int64_t n, uint64_t seed, int64_t* mismatches);
+
 /* sizeof() of the ABI structs as this library was compiled, for binding checks. */
 int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning, 4 batch tuning,
                                            5 server config, 6 job info, 7 server stats,
