@@ -474,14 +474,22 @@ def run_serve(args):
             vec = rings.matched_gaussian(e, j["n"], seed=j["variant_seed"] % 100000)
             j["fma"] = None
         else:
-            # frequency-map job: grid offsets from the closed orbit, with the reference's set-up
-            orbit, norm, tunes = lib.fma_setup(ctx, lat)
-            vec = rings.fma_grid(j["n"]) + orbit[:, None]
-            j["fma"] = (norm, orbit, tunes)
+            # frequency-map job: grid offsets from the closed orbit, with the reference's set-up.
+            # A perturbed ring whose closed orbit cannot be found (frequency_map itself would stop
+            # there) is tracked as a plain grid job and counted.
+            try:
+                orbit, norm, tunes = lib.fma_setup(ctx, lat)
+                vec = rings.fma_grid(j["n"]) + orbit[:, None]
+                j["fma"] = (norm, orbit, tunes)
+            except lib.BmadGpuError:
+                vec = rings.fma_grid(j["n"])
+                j["fma"] = None
+                j["no_orbit"] = True
         hb = lib.HostBunch.from_vec(vec, p)
         jobs.append((j, lat, vec, hb.beta))
     t_prep = time.time() - t_prep
     n_fma = sum(1 for j, _, _, _ in jobs if j["fma"] is not None)
+    n_no_orbit = sum(1 for j, _, _, _ in jobs if j.get("no_orbit"))
 
     def pinned_inputs():
         return [lib.PinnedBunch(vec, beta) for (_, _, vec, beta) in jobs]
@@ -548,7 +556,8 @@ def run_serve(args):
         "data": "synthetic (Poisson stream, perturbed rings, Gaussian / frequency-map grids)",
         "config": {"workload": "serve: first %d jobs of the 2000-job stream (mean gap 5 ms), %d particles, "
                                "50/100/200/400-cell rings, %d frequency-map jobs (turn-by-turn record and tunes on "
-                               "the device)" % (len(jobs), n_part, n_fma),
+                               "the device; %d more whose ring has no closed orbit tracked as plain grids)"
+                               % (len(jobs), n_part, n_fma, n_no_orbit),
                    "host_prep_s": t_prep},
         "fma": fma_summary,
         "latency_s": {"p50": st["latency_p50_s"], "p99": st["latency_p99_s"], "max": st["latency_max_s"]},

@@ -195,8 +195,7 @@ double init_beta(const bmadgpu_param& p, double pz) {
 }
 
 // One turn of the 25 stencil particles about x: f(x) and the one-turn matrix. *lost is set when
-// the particle on x itself is lost (the caller's cue to step back); a loss of a stencil particle
-// alone is an error.
+// any of them is lost (the caller's cue to step back: the matrix needs all 25).
 int one_turn(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const double* x, double* fx, double* M,
              OrbitParticles& op, bool* lost) {
   const int n = kStencil;
@@ -217,10 +216,9 @@ int one_turn(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const double* x, double
   CUDA_TRY(cudaMemcpyAsync(op.hs.data(), op.b.state, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   if ((r = check_err_flag(c))) return r;
-  *lost = op.hs[0] != BMADGPU_ALIVE;
+  *lost = false;
+  for (int j = 0; j < n; j++) *lost = *lost || op.hs[j] != BMADGPU_ALIVE;
   if (*lost) return BMADGPU_OK;
-  for (int j = 1; j < n; j++)
-    if (op.hs[j] != BMADGPU_ALIVE) return fail(BMADGPU_EINVAL, "a particle next to the trial orbit was lost in one turn");
   for (int i = 0; i < 6; i++) fx[i] = op.hv[i * n];
   for (int i = 0; i < 6; i++)
     for (int k = 0; k < 6; k++) {
@@ -391,7 +389,7 @@ extern "C" int bmadgpu_one_turn_matrix(bmadgpu_ctx* c, const bmadgpu_lattice* la
   double fx[6];
   bool lost = false;
   if ((r = one_turn(c, tmp.lat, orbit, fx, mat, op, &lost))) return r;
-  if (lost) return fail(BMADGPU_EINVAL, "the orbit particle was lost in one turn");
+  if (lost) return fail(BMADGPU_EINVAL, "the orbit particle or one of its stencil neighbours was lost in one turn");
   if (orbit_end) std::memcpy(orbit_end, fx, sizeof(fx));
   return BMADGPU_OK;
 }

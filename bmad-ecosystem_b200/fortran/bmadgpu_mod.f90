@@ -50,6 +50,15 @@ type, bind(c) :: bmadgpu_bunch_t
   type(c_ptr) :: vec, beta, t, state, ix_ele, ix_turn, location
 end type
 
+! bmadgpu_twiss of include/bmadgpu.h (what twiss_from_mat6 fills in ele%a, ele%b, ele%x, ele%y).
+type, bind(c) :: bmadgpu_twiss_t
+  real(c_double) :: beta_a, alpha_a, gamma_a, phi_a, beta_b, alpha_b, gamma_b, phi_b
+  real(c_double) :: eta_a, etap_a, deta_ds_a, eta_b, etap_b, deta_ds_b
+  real(c_double) :: eta_x, etap_x, deta_ds_x, eta_y, etap_y, deta_ds_y
+  real(c_double) :: c_mat(4), gamma_c, growth_rate, symp_error
+  integer(c_int32_t) :: status, reserved
+end type
+
 interface
   integer(c_int) function bmadgpu_ctx_create(device, ctx) bind(c, name='bmadgpu_ctx_create')
     import
@@ -80,6 +89,27 @@ interface
   end function
   type(c_ptr) function bmadgpu_last_error() bind(c, name='bmadgpu_last_error')
     import
+  end function
+  integer(c_int) function bmadgpu_closed_orbit(ctx, lat, dim, orbit, mat, rel_tol, abs_tol, max_iter, iterations) &
+                                                                             bind(c, name='bmadgpu_closed_orbit')
+    import
+    type(c_ptr), value :: ctx, lat
+    integer(c_int32_t), value :: dim, max_iter
+    real(c_double) :: orbit(6), mat(36)
+    real(c_double), value :: rel_tol, abs_tol
+    integer(c_int32_t) :: iterations
+  end function
+  integer(c_int) function bmadgpu_one_turn_matrix(ctx, lat, orbit, rf_on, orbit_end, mat) &
+                                                                             bind(c, name='bmadgpu_one_turn_matrix')
+    import
+    type(c_ptr), value :: ctx, lat
+    real(c_double) :: orbit(6), orbit_end(6), mat(36)
+    integer(c_int32_t), value :: rf_on
+  end function
+  integer(c_int) function bmadgpu_twiss_from_mat6(mat, orb0, tw) bind(c, name='bmadgpu_twiss_from_mat6')
+    import
+    real(c_double) :: mat(36), orb0(6)
+    type(bmadgpu_twiss_t) :: tw
   end function
 end interface
 
@@ -259,5 +289,69 @@ bunch%n_live = count(bunch%particle%state == alive$)
 bunch%charge_live = sum(bunch%particle%charge, mask = (bunch%particle%state == alive$))
 
 end subroutine track_on_gpu
+
+!+
+! Subroutine bmadgpu_closed_orbit_calc (closed_orb, i_dim, err)
+!
+! closed_orbit_calc (bmad/code/closed_orbit_calc.f90:192) for the installed branch, forward: the
+! closed orbit at the branch start, found by Newton's method on the GPU's one-turn map. The guess
+! is closed_orb(0)%vec (its vec(6) the energy for i_dim = 4); the result goes to closed_orb(0)%vec
+! only -- the orbit at the other elements is not filled. i_dim = 0 takes 6 when a cavity is on,
+! else 4. Tolerances are bmad_com%rel_tol_tracking / %abs_tol_tracking.
+!-
+
+subroutine bmadgpu_closed_orbit_calc (closed_orb, i_dim, err)
+
+type (coord_struct) :: closed_orb(0:)
+integer i_dim
+logical err
+real(c_double) orbit(6), mat(36)
+integer(c_int32_t) its
+
+orbit = closed_orb(0)%vec
+err = (bmadgpu_closed_orbit(gpu_ctx, gpu_lat, int(i_dim, c_int32_t), orbit, mat, bmad_com%rel_tol_tracking, &
+                            bmad_com%abs_tol_tracking, 0_c_int32_t, its) /= 0)
+if (err) return
+closed_orb(0)%vec = orbit
+
+end subroutine bmadgpu_closed_orbit_calc
+
+!+
+! Subroutine bmadgpu_twiss_at_start (lat, orbit, status)
+!
+! The periodic Twiss of twiss_at_start (bmad/code/twiss_at_start.f90:29) for the installed
+! branch: the RF-off one-turn matrix about orbit(1:6) from GPU tracking, decoupled as
+! twiss_from_mat6 does, written to branch%ele(0) (a, b, x, y, c_mat, gamma_c) and the tunes to
+! lat%a%tune, lat%b%tune. status is Bmad's matrix status (ok$ = 1).
+!-
+
+subroutine bmadgpu_twiss_at_start (lat, orbit, status)
+
+type (lat_struct), target :: lat
+real(rp) orbit(6)
+integer status
+type (ele_struct), pointer :: ele0
+type (bmadgpu_twiss_t) tw
+real(c_double) orb(6), orb_end(6), mat(36)
+
+status = unstable$
+orb = orbit
+if (bmadgpu_one_turn_matrix(gpu_ctx, gpu_lat, orb, 0_c_int32_t, orb_end, mat) /= 0) return
+if (bmadgpu_twiss_from_mat6(mat, orb, tw) /= 0) return
+status = tw%status
+if (status /= ok$) return
+ele0 => lat%branch(gpu_branch)%ele(0)
+ele0%a%beta = tw%beta_a;  ele0%a%alpha = tw%alpha_a;  ele0%a%gamma = tw%gamma_a
+ele0%a%eta = tw%eta_a;  ele0%a%etap = tw%etap_a;  ele0%a%deta_ds = tw%deta_ds_a
+ele0%b%beta = tw%beta_b;  ele0%b%alpha = tw%alpha_b;  ele0%b%gamma = tw%gamma_b
+ele0%b%eta = tw%eta_b;  ele0%b%etap = tw%etap_b;  ele0%b%deta_ds = tw%deta_ds_b
+ele0%x%eta = tw%eta_x;  ele0%x%etap = tw%etap_x;  ele0%x%deta_ds = tw%deta_ds_x
+ele0%y%eta = tw%eta_y;  ele0%y%etap = tw%etap_y;  ele0%y%deta_ds = tw%deta_ds_y
+ele0%c_mat = reshape(tw%c_mat, [2, 2], order = [2, 1])   ! C row-major -> c_mat(i,j)
+ele0%gamma_c = tw%gamma_c
+ele0%a%phi = 0;  ele0%b%phi = 0
+lat%a%tune = tw%phi_a;  lat%b%tune = tw%phi_b
+
+end subroutine bmadgpu_twiss_at_start
 
 end module bmadgpu_mod
