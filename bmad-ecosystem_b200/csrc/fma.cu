@@ -7,8 +7,9 @@
 // per-turn record kernel writes coalesced rows. The tune kernel gives one CTA to one signal -- a
 // (particle, plane, half) triple, six per particle -- stages its fft_turns Hanning-windowed complex
 // samples and a twiddle table of exp(+2 pi i m / N) in shared memory, evaluates the amplitude
-// spectrum |X_k| = |sum_j s_j exp(+2 pi i j k / N)| (FFTW_BACKWARD's sign; a direct transform with
-// the tabulated twiddle w[(j k) mod N], so any N works, not only powers of two), finds the first
+// spectrum |X_k| = |sum_j s_j exp(+2 pi i j k / N)| (FFTW_BACKWARD's sign; a radix-2 FFT in shared
+// memory for power-of-two N, else a direct transform with the tabulated twiddle w[(j k) mod N], so
+// any N works), finds the first
 // maximum as the reference's loop does, and applies calc_tune's interpolation
 // (frequency_map.f90:364-375). The reference's own turn loop stops a particle when it is lost or,
 // with z_cut, when |z - z_co| exceeds a quarter RF wavelength (frequency_map.f90:290-299); here the
@@ -101,17 +102,55 @@ __global__ void __launch_bounds__(kTuneThreads) k_fma_tunes(const double* __rest
     wim[j] = sn;
   }
   __syncthreads();
+  // A power-of-two N takes an in-place radix-2 transform (bit reversal, then log2 N butterfly
+  // stages with the twiddles exp(+2 pi i pos / len) = w[pos N / len]); any other N the direct sum.
+  const bool pow2 = (N & (N - 1)) == 0;
+  if (pow2) {
+    int lg = 0;
+    while ((1 << lg) < N) lg++;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      const int r = (int)(__brev((unsigned)i) >> (32 - lg));
+      if (i < r) {
+        const double tr = sre[i], ti = sim[i];
+        sre[i] = sre[r];
+        sim[i] = sim[r];
+        sre[r] = tr;
+        sim[r] = ti;
+      }
+    }
+    __syncthreads();
+    for (int len = 2; len <= N; len <<= 1) {
+      const int h = len >> 1, step = N / len;
+      for (int t = threadIdx.x; t < N / 2; t += blockDim.x) {
+        const int g = t / h, pos = t - g * h;
+        const int ia = g * len + pos, ib = ia + h;
+        const double wr = wre[pos * step], wi = wim[pos * step];
+        const double xr = sre[ib] * wr - sim[ib] * wi, xi = sre[ib] * wi + sim[ib] * wr;
+        const double ar = sre[ia], ai = sim[ia];
+        sre[ib] = ar - xr;
+        sim[ib] = ai - xi;
+        sre[ia] = ar + xr;
+        sim[ia] = ai + xi;
+      }
+      __syncthreads();
+    }
+  }
   double bv = -1.0;
   int bi = 0;
   for (int k = threadIdx.x; k < N; k += blockDim.x) {
     double xr = 0, xi = 0;
-    int m = 0;  // (j k) mod N, advanced by k each step
-    for (int j = 0; j < N; j++) {
-      const double a = sre[j], b = sim[j], c = wre[m], d = wim[m];
-      xr += a * c - b * d;
-      xi += a * d + b * c;
-      m += k;
-      if (m >= N) m -= N;
+    if (pow2) {
+      xr = sre[k];
+      xi = sim[k];
+    } else {
+      int m = 0;  // (j k) mod N, advanced by k each step
+      for (int j = 0; j < N; j++) {
+        const double a = sre[j], b = sim[j], c = wre[m], d = wim[m];
+        xr += a * c - b * d;
+        xi += a * d + b * c;
+        m += k;
+        if (m >= N) m -= N;
+      }
     }
     const double amp = sqrt(xr * xr + xi * xi);
     if (better(amp, k, bv, bi)) {
@@ -143,7 +182,9 @@ __global__ void __launch_bounds__(kTuneThreads) k_fma_tunes(const double* __rest
       }
     // b = |X| at the next bin (recomputed; 0 past the last bin)
     double b = 0;
-    if (ix + 1 < N) {
+    if (ix + 1 < N && pow2) {
+      b = sqrt(sre[ix + 1] * sre[ix + 1] + sim[ix + 1] * sim[ix + 1]);
+    } else if (ix + 1 < N) {
       double xr = 0, xi = 0;
       int m = 0;
       for (int j = 0; j < N; j++) {

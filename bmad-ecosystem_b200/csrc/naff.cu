@@ -2,7 +2,8 @@
 // signals at once: one CTA per signal, the signal and its windowed copy in shared memory.
 //
 // Per component, as the reference does: an interpolated-FFT estimate of the spectral peak
-// (interpolated_fft_gsl, naff.f90:230-290: Gaussian window r = 8, backward transform, peak over
+// (interpolated_fft_gsl, naff.f90:230-290: Gaussian window r = 8, backward transform -- radix-2
+// for power-of-two lengths, a direct sum otherwise -- peak over
 // bins 2..N-1, log-parabola interpolation), refined by maximising the Hanning-windowed projection
 // |<w s | exp(-2 pi i f t)>| (maximize_projection, naff.f90:160-205) with Brent's method (R. P.
 // Brent, Algorithms for Minimization without Derivatives, 1973, ch. 5) from a golden-ratio
@@ -88,17 +89,51 @@ __device__ bool interpolated_fft(const Sig& s, double* f_out, Red& r) {
     s.wim[t] = s.im[t] * w;
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < n; k += kThreads) {
-    double xr = 0, xi = 0;
-    int m = 0;  // (j k) mod N
-    for (int j = 0; j < n; j++) {
-      const double2 w = s.tw[m];  // exp(+2 pi i j k / N)
-      xr += s.wre[j] * w.x - s.wim[j] * w.y;
-      xi += s.wre[j] * w.y + s.wim[j] * w.x;
-      m += k;
-      if (m >= n) m -= n;
+  if ((n & (n - 1)) == 0) {
+    // power of two: in-place radix-2 transform of the windowed copy (bit reversal, then log2 N
+    // butterfly stages with the twiddles exp(+2 pi i pos / len) = w[pos N / len])
+    int lg = 0;
+    while ((1 << lg) < n) lg++;
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+      const int rv = (int)(__brev((unsigned)i) >> (32 - lg));
+      if (i < rv) {
+        const double tr = s.wre[i], ti = s.wim[i];
+        s.wre[i] = s.wre[rv];
+        s.wim[i] = s.wim[rv];
+        s.wre[rv] = tr;
+        s.wim[rv] = ti;
+      }
     }
-    s.amp[k] = sqrt(xr * xr + xi * xi);
+    __syncthreads();
+    for (int len = 2; len <= n; len <<= 1) {
+      const int h = len >> 1, step = n / len;
+      for (int t = threadIdx.x; t < n / 2; t += kThreads) {
+        const int g = t / h, pos = t - g * h;
+        const int ia = g * len + pos, ib = ia + h;
+        const double2 w = s.tw[pos * step];
+        const double xr = s.wre[ib] * w.x - s.wim[ib] * w.y, xi = s.wre[ib] * w.y + s.wim[ib] * w.x;
+        const double ar = s.wre[ia], ai = s.wim[ia];
+        s.wre[ib] = ar - xr;
+        s.wim[ib] = ai - xi;
+        s.wre[ia] = ar + xr;
+        s.wim[ia] = ai + xi;
+      }
+      __syncthreads();
+    }
+    for (int k = threadIdx.x; k < n; k += kThreads) s.amp[k] = sqrt(s.wre[k] * s.wre[k] + s.wim[k] * s.wim[k]);
+  } else {
+    for (int k = threadIdx.x; k < n; k += kThreads) {
+      double xr = 0, xi = 0;
+      int m = 0;  // (j k) mod N
+      for (int j = 0; j < n; j++) {
+        const double2 w = s.tw[m];  // exp(+2 pi i j k / N)
+        xr += s.wre[j] * w.x - s.wim[j] * w.y;
+        xi += s.wre[j] * w.y + s.wim[j] * w.x;
+        m += k;
+        if (m >= n) m -= n;
+      }
+      s.amp[k] = sqrt(xr * xr + xi * xi);
+    }
   }
   __syncthreads();
   __shared__ double sh_f;

@@ -31,7 +31,8 @@ def grid(n_x=5, n_y=4, x_max=0.011, y_max=0.005, pz=(0.0, 0.002)):
     return np.array(off)
 
 
-@pytest.mark.parametrize("ring,n_turn,fft_turns", [("ideal", 256, 0), ("misaligned", 300, 128)])
+@pytest.mark.parametrize("ring,n_turn,fft_turns", [("ideal", 256, 0), ("misaligned", 300, 128), ("ideal", 250, 0),
+                                                   ("misaligned", 300, 96)])
 def test_fma_matches_restatement(ctx, ring, n_turn, fft_turns):
     eles, p = rings.ring(20) if ring == "ideal" else rings.perturbed_ring(20, seed=5)
     lat = lib.Lattice(ctx, eles, p)

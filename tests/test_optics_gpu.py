@@ -176,3 +176,20 @@ def test_beam_full_size_exact_moments(ctx):
     # seeded: the same seed gives the same beam bit for bit
     hb2 = lib.beam_init_gaussian(ctx, p, tw, n, seed=2024, orbit=x, **BEAM)
     assert np.array_equal(hb.vec, hb2.vec)
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 7])
+def test_beam_small_counts_match_restatement(ctx, n):
+    """The reference's special cases: one particle (no renormalisation at all), up to six (only
+    the diagonal normalised, no shears), seven (the first count with the shears)."""
+    eles, p = rings.ring(20)
+    lat = lib.Lattice(ctx, eles, p)
+    x, _, _ = lib.closed_orbit(ctx, lat, dim=6)
+    tw = lib.twiss_from_mat6(lib.one_turn_matrix(ctx, lat, x, rf_on=False)[0], x)
+    normals = R.deviates(31 + n, n)
+    hb = lib.beam_init_gaussian(ctx, p, tw, n, normals=normals, orbit=x, **BEAM)
+    want = R.init_random_distribution(normals, n, tw, orbit=x, **BEAM)
+    scale = np.array([1e-4, 1e-5, 1e-5, 1e-6, 1e-3, 1e-3])[:, None]
+    assert np.max(np.abs(hb.vec - want) / scale) < 1e-10, (hb.vec, want)
+    if n == 1:  # a single particle, re-centred: the closed orbit itself
+        assert np.allclose(hb.vec[:, 0], x, rtol=0, atol=1e-18)
