@@ -78,7 +78,13 @@ BG_HD double div_rcp(double a, double b, double y) {  // counted as the one divi
   (void)y;
   return a / b;
 }
+// The shared reciprocal is not an operation of the reference: the operation count leaves it out
+// (div_rcp above does not use its value when counting).
+BG_HD double shared_rcp(double b) { return b; }
+BG_HD double half_rcp(double y) { return y; }
 #else
+BG_HD double shared_rcp(double b) { return 1 / b; }
+BG_HD double half_rcp(double y) { return 0.5 * y; }  // RN(1/(2b)) from y = RN(1/b): exact scaling
 BG_HD double div_rcp(double a, double b, double y) {
   const double q = a * y;
   const double aq = fabs(q);
@@ -172,7 +178,7 @@ BG_HD void drift(Particle& p, double length) {
   double pxy2 = px_rel * px_rel + py_rel * py_rel;
   if (pxy2 >= 1) { p.state = S_LOST_PZ; return; }
   double ps_rel = sqrt(1 - pxy2);
-  const double inv_ps = 1 / ps_rel;
+  const double inv_ps = shared_rcp(ps_rel);
   p.x = p.x + div_rcp(length * px_rel, ps_rel, inv_ps);
   p.y = p.y + div_rcp(length * py_rel, ps_rel, inv_ps);
   double dz;
@@ -180,7 +186,7 @@ BG_HD void drift(Particle& p, double length) {
     double so = -pxy2 / (ps_rel + 1);  // sqrt_one(-pxy2)
     dz = length * (p.dzb + div_rcp(so, ps_rel, inv_ps));
   } else {
-    dz = length * (1 - inv_ps);
+    dz = length * (1 - div_rcp(1.0, ps_rel, inv_ps));  // = RN(1 / ps_rel), the same bits as inv_ps
   }
   p.z = p.z + dz;
 }
@@ -418,7 +424,7 @@ BG_HD void quad_mat2(double k1, double length, double rel_p, double ef, double& 
   m21 = k1 * sx * rel_p;
   m22 = cx;
   z0 = k1 * (-cx * sx + length) / 4;
-  z1 = div_rcp(-k1 * (sx * sx), 2 * rel_p, 0.5 * ef);
+  z1 = div_rcp(-k1 * (sx * sx), 2 * rel_p, half_rcp(ef));
   z2 = -(cx * sx + length) / (4 * (rel_p * rel_p));
 }
 
@@ -541,7 +547,7 @@ BG_HD bool bend_exact_step(Particle& p, const double* __restrict__ b, const Glob
   }
   double pt = sqrt(rel_p2 - py * py);
   if (fabs(px) > pt) { p.state = S_LOST_PZ; return false; }
-  const double inv_pt = 1 / pt;  // shared by the four quotients by pt
+  const double inv_pt = shared_rcp(pt);  // shared by the four quotients by pt
   double g_p = div_rcp(g_tot, pt, inv_pt);
   double phi_1 = asin(div_rcp(px, pt, inv_pt));
   double cos_plus = cos(angle + phi_1);
