@@ -12,10 +12,12 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "capi_internal.h"
@@ -149,7 +151,7 @@ std::string col(int w, const char* s) {
   return x;
 }
 
-bool write_averages_headers(const std::string& base, const std::string& pre) {
+bool write_averages_headers(const std::string& base, const std::string& pre, const double* cuts, int n_cuts) {
   FILE* f = std::fopen((base + ".ave").c_str(), "w");
   if (!f) return false;
   std::string l1 = "##" + col(8, "1") + col(9, "2") + col(14, "3") + col(14, "4");
@@ -205,12 +207,16 @@ bool write_averages_headers(const std::string& base, const std::string& pre) {
   }
   l1 += "  |";
   l2 += "  |";
+  for (int i = 0; i < n_cuts; i++) {  // lt_tracking_mod.f90:832-839
+    l1 += "                   " + std::to_string((int)std::lround(cuts[i] * 100)) + "% Core                |";
+    l2 += "      Emit_a        Emit_b        Emit_c   |";
+  }
   std::fprintf(f, "%s%s\n%s\n", pre.c_str(), l1.c_str(), l2.c_str());
   std::fclose(f);
   return true;
 }
 
-bool append_averages(const std::string& base, int turn, const bmadgpu_bunch_data& bd) {
+bool append_averages(const std::string& base, int turn, const bmadgpu_bunch_data& bd, const double* core, int n_cuts) {
   const std::string t_str = fmt_i(10, turn);
   FILE* f = std::fopen((base + ".ave").c_str(), "a");
   if (!f) return false;
@@ -238,6 +244,10 @@ bool append_averages(const std::string& base, int turn, const bmadgpu_bunch_data
   for (int i = 0; i < 3; i++) l += fmt_es(14, 6, bd.kurt[i]);
   l += "  ";
   for (int i = 0; i < 3; i++) l += fmt_es(14, 6, bd.skew[i]);
+  for (int k = 0; k < n_cuts; k++) {
+    l += "  ";
+    for (int i = 0; i < 3; i++) l += fmt_es(14, 6, core[k * 3 + i]);
+  }
   std::fprintf(f, "%s\n", l.c_str());
   std::fclose(f);
   return true;
@@ -276,6 +286,229 @@ bool write_phase_space(const std::string& base, int turn, int n_turns, const bma
   return true;
 }
 
+// ---- core emittance (ltt_calc_bunch_data, lt_tracking_mod.f90:2432-2560, combined calculation) ----
+//
+// The reference ranks the live particles by their combined normalised amplitude
+// sum_k (j_2k^2 + j_2k+1^2) / emit_k with j = N^-1 (p - centroid), N the normal-form matrix of the
+// bunch's sigma matrix (Sigma = N diag(emit) N^T), keeps the n_cut = int(cutoff n_live) smallest,
+// repeats the ranking with the core's own centroid and sigma, and scales that core's normal-mode
+// emittances by f = cutoff / (1 - (1 + s + s^2/2 + s^3/6) e^-s), where e^-s solves
+// ltt_beam_fraction(e^-s) = cutoff. Since Sigma^-1 = N^-T diag(1/emit) N^-1, the amplitude is the
+// quadratic form (p - c)^T Sigma^-1 (p - c) = |L^-1 (p - c)|^2 with Sigma = L L^T: the device
+// evaluates that per particle, the host picks the core, and the core's sums are the same two-pass
+// device sums as the bunch's, over the core as the live set.
+
+constexpr int kCoreMax = 8;
+
+struct CoreArgs {
+  double li[21];   // L^-1, lower triangle by rows
+  double c[6];
+};
+
+__global__ void k_core_amp(const double* __restrict__ vec, const int32_t* __restrict__ state, int64_t n, CoreArgs A,
+                           double* __restrict__ amp) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    if (state[i] != BMADGPU_ALIVE) {
+      amp[i] = 1e100;  // the reference's "something large" for dead particles
+      continue;
+    }
+    double d[6];
+    for (int k = 0; k < 6; k++) d[k] = vec[k * n + i] - A.c[k];
+    double s = 0;
+    int q = 0;
+    for (int r = 0; r < 6; r++) {
+      double y = 0;
+      for (int k = 0; k <= r; k++) y += A.li[q++] * d[k];
+      s += y * y;
+    }
+    amp[i] = s;
+  }
+}
+
+// L^-1 of sigma = L L^T (6x6), false unless sigma is positive definite.
+bool chol_inverse(const double* sig, double* li) {
+  double L[36] = {0}, Li[36] = {0};
+  for (int j = 0; j < 6; j++) {
+    double s = sig[j * 6 + j];
+    for (int k = 0; k < j; k++) s -= L[j * 6 + k] * L[j * 6 + k];
+    if (!(s > 0)) return false;
+    L[j * 6 + j] = std::sqrt(s);
+    for (int i = j + 1; i < 6; i++) {
+      double t = sig[i * 6 + j];
+      for (int k = 0; k < j; k++) t -= L[i * 6 + k] * L[j * 6 + k];
+      L[i * 6 + j] = t / L[j * 6 + j];
+    }
+  }
+  for (int j = 0; j < 6; j++) {  // forward substitution column by column
+    Li[j * 6 + j] = 1 / L[j * 6 + j];
+    for (int i = j + 1; i < 6; i++) {
+      double t = 0;
+      for (int k = j; k < i; k++) t += L[i * 6 + k] * Li[k * 6 + j];
+      Li[i * 6 + j] = -t / L[i * 6 + i];
+    }
+  }
+  int q = 0;
+  for (int r = 0; r < 6; r++)
+    for (int k = 0; k <= r; k++) li[q++] = Li[r * 6 + k];
+  return true;
+}
+
+// ltt_beam_fraction (lt_tracking_mod.f90:2566-2570): the share of a Gaussian beam inside the
+// combined normalised amplitude -ln(x).
+double beam_fraction(double x) {
+  const double jc = -std::log(x);
+  return 1.0 - x * (1 + jc + 0.5 * jc * jc);
+}
+
+// Brent's root finder (R. P. Brent, Algorithms for Minimization without Derivatives, 1973, ch. 4)
+// for beam_fraction(x) = y on [a, b], run to full precision (the reference's inverse() stops at
+// 1e-8; the root it approaches is this one).
+double fraction_root(double y, double a, double b) {
+  double fa = beam_fraction(a) - y, fb = beam_fraction(b) - y;
+  if (fa * fb > 0) return b;
+  double c = a, fc = fa, d = b - a, e = d;
+  for (int it = 0; it < 200; it++) {
+    if ((fb > 0) == (fc > 0)) {
+      c = a;
+      fc = fa;
+      d = e = b - a;
+    }
+    if (std::fabs(fc) < std::fabs(fb)) {
+      a = b;
+      b = c;
+      c = a;
+      fa = fb;
+      fb = fc;
+      fc = fa;
+    }
+    const double tol = 2 * 2.220446049250313e-16 * std::fabs(b) + 1e-300;
+    const double m = 0.5 * (c - b);
+    if (std::fabs(m) <= tol || fb == 0) return b;
+    if (std::fabs(e) >= tol && std::fabs(fa) > std::fabs(fb)) {
+      double p, q, r;
+      const double sr = fb / fa;
+      if (a == c) {
+        p = 2 * m * sr;
+        q = 1 - sr;
+      } else {
+        q = fa / fc;
+        r = fb / fc;
+        p = sr * (2 * m * q * (q - r) - (b - a) * (r - 1));
+        q = (q - 1) * (r - 1) * (sr - 1);
+      }
+      if (p > 0) q = -q;
+      p = std::fabs(p);
+      if (2 * p < std::fmin(3 * m * q - std::fabs(tol * q), std::fabs(e * q))) {
+        e = d;
+        d = p / q;
+      } else {
+        d = m;
+        e = m;
+      }
+    } else {
+      d = m;
+      e = m;
+    }
+    a = b;
+    fa = fb;
+    b += std::fabs(d) > tol ? d : (m > 0 ? tol : -tol);
+    fb = beam_fraction(b) - y;
+  }
+  return b;
+}
+
+struct CoreScratch {
+  double* d_amp = nullptr;
+  int32_t* d_mask = nullptr;
+  std::vector<double> amp;
+  std::vector<std::pair<double, int64_t>> order;
+  std::vector<int32_t> mask;
+  ~CoreScratch() {
+    cudaFree(d_amp);
+    cudaFree(d_mask);
+  }
+  bool alloc(int64_t n) {
+    if (d_amp) return true;
+    return cudaMalloc(&d_amp, (size_t)n * sizeof(double)) == cudaSuccess &&
+           cudaMalloc(&d_mask, (size_t)n * sizeof(int32_t)) == cudaSuccess;
+  }
+};
+
+// One ranking: the n_cut live particles of smallest amplitude about (centroid, sigma) of `ref`,
+// and the bunch data of that core from the device sums.
+int core_pass(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch& d, double* d_scratch,
+              const bmadgpu_bunch_data& ref, int64_t n_cut, CoreScratch& cs, bmadgpu_bunch_data* core, bool* ok) {
+  *ok = false;
+  CoreArgs A;
+  if (!chol_inverse(ref.sigma, A.li)) return BMADGPU_OK;
+  for (int k = 0; k < 6; k++) A.c[k] = ref.centroid[k];
+  const int64_t n = d.n;
+  cudaStream_t s = c->stream;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)c->sm_count * 8));
+  k_core_amp<<<grid, 256, 0, s>>>(d.vec, d.state, n, A, cs.d_amp);
+  CUDA_TRY(cudaGetLastError());
+  c->launches++;
+  cs.amp.resize(n);
+  CUDA_TRY(cudaMemcpyAsync(cs.amp.data(), cs.d_amp, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  // the n_cut smallest amplitudes, ties in particle order (a sorted index of the amplitudes)
+  cs.order.resize(n);
+  for (int64_t i = 0; i < n; i++) cs.order[i] = {cs.amp[i], i};
+  std::nth_element(cs.order.begin(), cs.order.begin() + (n_cut - 1), cs.order.end());
+  cs.mask.assign(n, 0);
+  for (int64_t k = 0; k < n_cut; k++) {
+    if (cs.order[k].first >= 1e99) return BMADGPU_OK;  // fewer live particles than n_cut
+    cs.mask[cs.order[k].second] = BMADGPU_ALIVE;
+  }
+  CUDA_TRY(cudaMemcpyAsync(cs.d_mask, cs.mask.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  double sums[kStatSums];
+  CUDA_TRY(launch_bunch_sums(d.vec, d.t, cs.d_mask, n, d_scratch, d_scratch + kStatBlocks * kStatPass2, s));
+  c->launches += 4;
+  CUDA_TRY(cudaMemcpyAsync(sums, d_scratch + kStatBlocks * kStatPass2, sizeof(sums), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  int r = bmadgpu_bunch_data_from_sums(sums, lat->param.p0c, lat->param.mass, core);
+  if (r) return r;
+  *ok = core->emit_valid != 0;
+  return BMADGPU_OK;
+}
+
+// core_emit [3] of one cutoff (zeros where the reference leaves them zero).
+int core_emittance(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch& d, double* d_scratch,
+                   const bmadgpu_bunch_data& bd, double cutoff_in, CoreScratch& cs, double* out) {
+  out[0] = out[1] = out[2] = 0;
+  if (!bd.emit_valid || bd.emit[0] == 0 || bd.emit[1] == 0 || bd.emit[2] == 0) return BMADGPU_OK;
+  const int64_t n_cut = (int64_t)(cutoff_in * (double)bd.n_live);
+  if (n_cut <= 0) return BMADGPU_OK;
+  if (!cs.alloc(d.n)) return fail(BMADGPU_ENOMEM, "cannot allocate the core-emittance scratch");
+  const double cutoff = std::fmin(1.0 - 1e-8, cutoff_in);
+  const double sig_cut = -std::log(fraction_root(cutoff, 1e-12, 1.0));
+  const double f =
+      cutoff / (1 - (1 + sig_cut + sig_cut * sig_cut / 2 + sig_cut * sig_cut * sig_cut / 6) * std::exp(-sig_cut));
+  bmadgpu_bunch_data core1, core2;
+  bool ok = false;
+  int r = core_pass(c, lat, d, d_scratch, bd, n_cut, cs, &core1, &ok);
+  if (r || !ok) return r;
+  r = core_pass(c, lat, d, d_scratch, core1, n_cut, cs, &core2, &ok);
+  if (r || !ok) return r;
+  for (int k = 0; k < 3; k++) out[k] = f * core2.emit[k];
+  return BMADGPU_OK;
+}
+
+// The cutoffs in effect: the list up to its first entry <= 0; all zero means the reference's
+// default, one cutoff of 0.5 (lt_tracking_mod.f90:74).
+int core_cutoffs(const bmadgpu_ltt_params* P, double* cut) {
+  bool any = false;
+  for (int i = 0; i < kCoreMax; i++) any = any || P->core_emit_cutoff[i] != 0;
+  if (!any) {
+    cut[0] = 0.5;
+    return 1;
+  }
+  int n = 0;
+  for (int i = 0; i < kCoreMax && P->core_emit_cutoff[i] > 0; i++) cut[n++] = P->core_emit_cutoff[i];
+  return n;
+}
+
 int device_stats(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch& d, double* d_scratch,
                  bmadgpu_bunch_data* bd) {
   double sums[kStatSums];
@@ -298,6 +531,23 @@ extern "C" int bmadgpu_bunch_stats(bmadgpu_ctx* c, const bmadgpu_lattice* lat, c
   if (cudaMalloc(&scratch, sizeof(double) * (kStatBlocks * kStatPass2 + kStatSums)) != cudaSuccess)
     return fail(BMADGPU_ENOMEM, "cannot allocate statistics scratch");
   int r = device_stats(c, lat, *d, scratch, bd);
+  cudaFree(scratch);
+  return r;
+}
+
+extern "C" int bmadgpu_bunch_core_emit(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch* d,
+                                       double cutoff, double* core_emit) {
+  if (!c || !lat || !d || !core_emit) return fail(BMADGPU_EINVAL, "NULL argument");
+  if (d->n < 1 || !d->vec || !d->state) return fail(BMADGPU_EINVAL, "bad bunch");
+  if (!(cutoff > 0 && cutoff <= 1.00000001)) return fail(BMADGPU_EINVAL, "cutoff must be in (0, 1]");
+  CUDA_TRY(cudaSetDevice(c->device));
+  double* scratch = nullptr;
+  if (cudaMalloc(&scratch, sizeof(double) * (kStatBlocks * kStatPass2 + kStatSums)) != cudaSuccess)
+    return fail(BMADGPU_ENOMEM, "cannot allocate statistics scratch");
+  bmadgpu_bunch_data bd;
+  CoreScratch cs;
+  int r = device_stats(c, lat, *d, scratch, &bd);
+  if (!r) r = core_emittance(c, lat, *d, scratch, bd, cutoff, cs, core_emit);
   cudaFree(scratch);
   return r;
 }
@@ -360,7 +610,12 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
   std::vector<double> hbeta, ht;
   std::vector<int32_t> hstate;
   const std::string pre = preheader(lat, P);
-  if (!ave_base.empty() && !write_averages_headers(ave_base, pre))
+  double cuts[kCoreMax];
+  for (int i = 0; i < kCoreMax; i++)
+    if (P->core_emit_cutoff[i] > 1.00000001) return fail(BMADGPU_EINVAL, "core_emit_cutoff must be <= 1");
+  const int n_cuts = core_cutoffs(P, cuts);
+  CoreScratch core_scratch;
+  if (!ave_base.empty() && !write_averages_headers(ave_base, pre, cuts, n_cuts))
     return fail(BMADGPU_EINVAL, "cannot write the averages files " + ave_base + ".*");
 
   auto outputs = [&](int turn) -> int {
@@ -368,7 +623,11 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
       bmadgpu_bunch_data bd;
       int r = device_stats(c, lat, cur.b, d_scratch, &bd);
       if (r) return r;
-      if (!append_averages(ave_base, turn, bd)) return fail(BMADGPU_EINVAL, "cannot append to the averages files");
+      double core[kCoreMax * 3];
+      for (int k = 0; k < n_cuts; k++)
+        if ((r = core_emittance(c, lat, cur.b, d_scratch, bd, cuts[k], core_scratch, core + 3 * k))) return r;
+      if (!append_averages(ave_base, turn, bd, core, n_cuts))
+        return fail(BMADGPU_EINVAL, "cannot append to the averages files");
     }
     if (!ps_base.empty() && wants(P->particle_every_n_turns, P->output_only_last_turns, P->n_turns, turn)) {
       hvec.resize(6 * n);

@@ -617,7 +617,7 @@ class LttParams(C.Structure):
                 ("output_only_last_turns", C.c_int32), ("only_live_particles_out", C.c_int32),
                 ("ix_turn_start", C.c_int32), ("beam_every_n_turns", C.c_int32), ("beam_exact", C.c_int32),
                 ("dead_cutoff", C.c_double), ("averages_file", C.c_char_p), ("phase_space_file", C.c_char_p),
-                ("beam_file", C.c_char_p)]
+                ("beam_file", C.c_char_p), ("core_emit_cutoff", C.c_double * 8)]
 
 
 def _ltt_sigs(lib):
@@ -640,6 +640,17 @@ def bunch_data_from_sums(sums, p0c, mass):
     return bd.as_dict()
 
 
+def bunch_core_emit(ctx, lat, device_view, cutoff=0.5):
+    """Core emittances (a, b, c) of a device-resident bunch (the combined calculation of
+    ltt_calc_bunch_data)."""
+    lib = load()
+    lib.bmadgpu_bunch_core_emit.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(abi.Bunch), C.c_double,
+                                            C.POINTER(C.c_double)]
+    out = (C.c_double * 3)()
+    check(lib.bmadgpu_bunch_core_emit(ctx.handle, lat.handle, C.byref(device_view), cutoff, out))
+    return np.array(out[:])
+
+
 def bunch_stats(ctx, lat, device_view):
     """Bunch data (ltt_calc_bunch_data) of a device-resident bunch."""
     lib = _ltt_sigs(load())
@@ -650,14 +661,19 @@ def bunch_stats(ctx, lat, device_view):
 
 def ltt_run(ctx, lat, bunch, n_turns, averages_file=None, phase_space_file=None, averages_every_n_turns=-1,
             particle_every_n_turns=-1, output_only_last_turns=0, only_live_particles_out=True, dead_cutoff=1.0,
-            beam_file=None, beam_every_n_turns=-1, beam_exact=False, ix_turn_start=0):
-    """long_term_tracking's beam mode for a HostBunch (updated in place); returns the turn reached."""
+            beam_file=None, beam_every_n_turns=-1, beam_exact=False, ix_turn_start=0, core_emit_cutoff=None):
+    """long_term_tracking's beam mode for a HostBunch (updated in place); returns the turn reached.
+    core_emit_cutoff: list of core fractions for the .emit file (None: the reference's [0.5];
+    []: no core columns)."""
     lib = _ltt_sigs(load())
     p = LttParams(n_turns, averages_every_n_turns, particle_every_n_turns, output_only_last_turns,
                   1 if only_live_particles_out else 0, ix_turn_start, beam_every_n_turns, 1 if beam_exact else 0,
                   dead_cutoff, averages_file.encode() if averages_file else None,
                   phase_space_file.encode() if phase_space_file else None,
                   beam_file.encode() if beam_file else None)
+    if core_emit_cutoff is not None:
+        cuts = list(core_emit_cutoff)[:8]
+        p.core_emit_cutoff[:] = cuts + [-1.0] * (8 - len(cuts))
     done = C.c_int32()
     v = bunch.view()
     check(lib.bmadgpu_ltt_run(ctx.handle, lat.handle, C.byref(v), C.byref(p), C.byref(done)))

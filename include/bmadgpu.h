@@ -435,9 +435,17 @@ typedef struct bmadgpu_ltt_params {
   const char* averages_file;        /* NULL or "": no averages output */
   const char* phase_space_file;     /* NULL or "": no phase-space output */
   const char* beam_file;            /* NULL or "": no beam files; "<stem>-<turn><.ext>" as ltt_write_beam_file names them */
+  double core_emit_cutoff[8];       /* ltt%core_emit_cutoff: core fractions whose emittances the .emit file adds
+                                       (combined calculation), up to the first entry <= 0; all zero: the
+                                       reference's default, 0.5; core_emit_cutoff[0] < 0: none */
 } bmadgpu_ltt_params;
 int bmadgpu_ltt_run(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* host_bunch,
                     const bmadgpu_ltt_params* params, int32_t* turns_done);
+/* Core emittances a, b, c of a device-resident bunch for one core fraction cutoff (0, 1]: the
+ * combined calculation of ltt_calc_bunch_data (bsim/modules/lt_tracking_mod.f90:2432-2560), zeros
+ * where the reference leaves them zero (a zero bunch emittance, an empty core). */
+int bmadgpu_bunch_core_emit(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const bmadgpu_bunch* device_bunch,
+                            double cutoff, double* core_emit);
 
 /* ---- Dynamic aperture ------------------------------------------------------------------------
  * dynamic_aperture_point (bmad/modules/dynamic_aperture_mod.f90:284-398) for many rays at once:

@@ -141,3 +141,41 @@ def read_table(path):
             continue
         rows.append(line.split())
     return rows
+
+
+def beam_fraction(x):
+    """ltt_beam_fraction (lt_tracking_mod.f90:2566-2570)."""
+    jc = -np.log(x)
+    return 1.0 - x * (1 + jc + 0.5 * jc ** 2)
+
+
+def core_emit(vec, t, state, p0c, mass, cutoff):
+    """Core emittances of ltt_calc_bunch_data's combined calculation (lt_tracking_mod.f90:
+    2432-2560): rank the live particles by sum_k (j_2k^2 + j_2k+1^2) / emit_k, j = N^-1 (p - c) --
+    the quadratic form (p - c)^T Sigma^-1 (p - c) -- keep the int(cutoff n_live) smallest, rank again
+    about the core, and scale the core's normal-mode emittances by f(cutoff)."""
+    from scipy.optimize import brentq
+    bd = bunch_data(vec, t, state, p0c, mass)
+    if "emit" not in bd or np.any(bd["emit"] == 0):
+        return np.zeros(3)
+    n_cut = int(cutoff * bd["n_live"])
+    if n_cut == 0:
+        return np.zeros(3)
+    cut = min(1.0 - 1e-8, cutoff)
+    x = brentq(lambda u: beam_fraction(u) - cut, 1e-12, 1.0, xtol=1e-300, rtol=1e-15)
+    s = -np.log(x)
+    f = cut / (1 - (1 + s + s ** 2 / 2 + s ** 3 / 6) * np.exp(-s))
+    alive = state == 1
+
+    def core(ref):
+        d = vec - np.asarray(ref["centroid"])[:, None]
+        amp = np.einsum("in,ij,jn->n", d, np.linalg.inv(ref["sigma"]), d)
+        amp[~alive] = 1e100
+        idx = np.argsort(amp, kind="stable")[:n_cut]
+        st = np.zeros_like(state)
+        st[idx] = 1
+        return bunch_data(vec, t, st, p0c, mass)
+
+    c1 = core(bd)
+    c2 = core(c1)
+    return f * np.asarray(c2["emit"])

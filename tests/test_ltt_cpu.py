@@ -58,3 +58,28 @@ def test_host_reduction_matches_reference(case):
         assert got["emit_valid"] == 1
         if case.get("sig_pz", 1e-3) == 0.0:
             assert got["emit"][2] == 0.0     # no energy spread: transverse modes only (dim = 4)
+
+
+def test_combined_amplitude_is_the_sigma_quadratic_form():
+    """The reference ranks particles by sum_k (j_2k^2 + j_2k+1^2) / emit_k with j = N^-1 (p - c)
+    and Sigma = N diag(emit) N^T; that is (p - c)^T Sigma^-1 (p - c), the form the core-emittance
+    code evaluates. Checked on a sigma matrix built from a random symplectic N."""
+    rng = np.random.default_rng(3)
+    S = np.zeros((6, 6))
+    for k in range(3):
+        S[2 * k, 2 * k + 1], S[2 * k + 1, 2 * k] = 1.0, -1.0
+    N = np.eye(6)
+    for _ in range(3):  # products of symplectic maps exp(S H) with H symmetric
+        H = rng.normal(size=(6, 6))
+        H = 0.1 * (H + H.T)
+        import scipy.linalg
+        N = N @ scipy.linalg.expm(S @ H)
+    assert np.max(np.abs(N.T @ S @ N - S)) < 1e-9
+    emit = np.array([2e-9, 3e-10, 4e-9])
+    D = np.diag(np.repeat(emit, 2))
+    Sigma = N @ D @ N.T
+    d = rng.normal(size=(6, 50)) * np.sqrt(np.diag(Sigma))[:, None]
+    j = np.linalg.solve(N, d)
+    amp_modes = sum((j[2 * k] ** 2 + j[2 * k + 1] ** 2) / emit[k] for k in range(3))
+    amp_form = np.einsum("in,ij,jn->n", d, np.linalg.inv(Sigma), d)
+    assert np.allclose(amp_modes, amp_form, rtol=1e-8)

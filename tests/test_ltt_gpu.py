@@ -18,7 +18,7 @@ import torch
 
 from conftest import load_abi
 from helpers import oracle_track
-from ltt_reference import bunch_data, read_table
+from ltt_reference import bunch_data, core_emit, read_table
 
 pytestmark = pytest.mark.gpu
 lib = importlib.import_module("bmad-ecosystem_b200.lib")
@@ -74,6 +74,8 @@ def test_ltt_run_outputs_match_oracle(ctx, tmp_path):
     for line in open(base + ".sigma"):
         if line.startswith("##") and "Turn" in line:
             assert "<x.x>" in line and "<pz.pz>" in line
+    heads = [line for line in open(base + ".emit") if line.startswith("##")]
+    assert "50% Core" in heads[-2] and heads[-1].rstrip().endswith("Emit_c   |")
     for row_a, row_s, row_e in zip(ave, sig, emi):
         T = int(row_a[0])
         o = oracle_track(eles, p, vec, T, t=np.zeros(n)) if T > 0 else dict(
@@ -85,6 +87,9 @@ def test_ltt_run_outputs_match_oracle(ctx, tmp_path):
         close([float(x) for x in row_s[3:24]], w["sigma_vec"], 2e-6, "sigma T=%d" % T)
         close([float(x) for x in row_e[3:6]], w["emit"], 2e-6, "emit T=%d" % T)
         close([float(x) for x in row_e[6:9]], w["kurt"], 2e-5, "kurt T=%d" % T)
+        assert len(row_e) == 15                       # the reference's default: one 50 % core group
+        close([float(x) for x in row_e[12:15]], core_emit(o["vec"], o["t"], o["state"], p.p0c, p.mass, 0.5), 2e-6,
+              "core emit T=%d" % T)
     files = sorted(glob.glob(str(tmp_path / "ps*.dat")))
     assert [os.path.basename(f) for f in files] == ["ps00.dat", "ps10.dat", "ps20.dat"]
     rows = read_table(str(tmp_path / "ps10.dat"))
@@ -148,3 +153,44 @@ def test_checkpoint_and_resume_continue_bit_for_bit(ctx, tmp_path):
     assert np.array_equal(b.ix_turn[late], full.ix_turn[late])
     final = lib.beam_read(str(tmp_path / "beam-24.dat"), p)
     assert np.array_equal(final.vec, full.vec) and np.array_equal(final.state, full.state)
+
+
+@pytest.mark.parametrize("cutoff", [0.5, 0.9, 0.13])
+def test_core_emittance_matches_reference(ctx, cutoff):
+    """bmadgpu_bunch_core_emit against the numpy restatement of the combined core calculation, on a
+    bunch with losses (dead particles excluded from the ranking)."""
+    eles, p = rings.ring(50)
+    vec = rings.matched_gaussian(eles, 20000, seed=21, scale=3.0)
+    hb = lib.HostBunch.from_vec(vec, p, t=np.zeros(20000))
+    lat = lib.Lattice(ctx, eles, p)
+    lib.track_bunch(ctx, lat, hb, n_turns=6)
+    hb.state[::97] = abi.LOST_POS_X  # dead particles stay out of the ranking and the sums
+    dev = torch.device("cuda", 0)
+    t = {k: torch.from_numpy(np.array(getattr(hb, k))).to(dev) for k in ("vec", "beta", "t", "state")}
+    view = abi.Bunch(hb.n, t["vec"].data_ptr(), t["beta"].data_ptr(), t["t"].data_ptr(), t["state"].data_ptr(),
+                     None, None, None)
+    got = lib.bunch_core_emit(ctx, lat, view, cutoff)
+    want = core_emit(hb.vec, hb.t, hb.state, p.p0c, p.mass, cutoff)
+    assert np.all(want > 0)
+    assert np.allclose(got, want, rtol=1e-9, atol=0), (got, want)
+    # the core is smaller than the bunch for cutoffs below 1 (before the f scaling)
+    bd = bunch_data(hb.vec, hb.t, hb.state, p.p0c, p.mass)
+    assert np.all(got < bd["emit"] * 1.5)
+
+
+def test_ltt_core_columns_follow_the_cutoff_list(ctx, tmp_path):
+    eles, p = rings.ring(50)
+    vec = rings.matched_gaussian(eles, 3000, seed=2, scale=2.0)
+    lat = lib.Lattice(ctx, eles, p)
+    for cuts, groups in (([], 0), ([0.5, 0.9], 2)):
+        hb = lib.HostBunch.from_vec(vec, p, t=np.zeros(3000))
+        base = str(tmp_path / ("c%d" % groups))
+        lib.ltt_run(ctx, lat, hb, 4, averages_file=base, averages_every_n_turns=2, core_emit_cutoff=cuts)
+        rows = read_table(base + ".emit")
+        assert all(len(r) == 12 + 3 * groups for r in rows)
+        heads = [line for line in open(base + ".emit") if line.startswith("##")]
+        assert heads[-2].count("% Core") == groups
+        if groups:
+            o = oracle_track(eles, p, vec, 4, t=np.zeros(3000))
+            close([float(x) for x in rows[-1][15:18]], core_emit(o["vec"], o["t"], o["state"], p.p0c, p.mass, 0.9),
+                  2e-6, "90 % core")
