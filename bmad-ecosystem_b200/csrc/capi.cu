@@ -471,7 +471,9 @@ int bmadgpu_autotune(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_b
   int r = check_bunch(b);
   if (r) return r;
   CUDA_TRY(cudaSetDevice(c->device));
-  int64_t m = std::min<int64_t>(b->n, sample_n > 0 ? sample_n : (int64_t)c->sm_count * 2048);
+  // Trials on up to 8192 particles per SM (the whole bunch of a 1M-particle run): shapes that tie on
+  // a few waves of particles can differ by 10 % over many waves.
+  int64_t m = std::min<int64_t>(b->n, sample_n > 0 ? sample_n : (int64_t)c->sm_count * 8192);
   if (m <= 0) return fail(BMADGPU_EINVAL, "empty bunch");
   if (m > c->tune_cap) {
     cudaFree(c->d_tvec);
@@ -517,6 +519,18 @@ int bmadgpu_autotune(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_b
     CUDA_TRY(cudaEventSynchronize(e1));
     float ms = 0;
     CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    // a second turn of the same particles: the shorter of the two timings counts
+    CUDA_TRY(cudaEventRecord(e0, c->stream));
+    r = track_device(c, lat, &t, 0, (int32_t)lat->pk.info.n_ele, 1, 1, nullptr);
+    CUDA_TRY(cudaEventRecord(e1, c->stream));
+    if (r) {
+      c->tuning = saved;
+      return r;
+    }
+    CUDA_TRY(cudaEventSynchronize(e1));
+    float ms2 = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms2, e0, e1));
+    ms = std::min(ms, ms2);
     if (ms < best_ms) {
       best_ms = ms;
       best = c->tuning;

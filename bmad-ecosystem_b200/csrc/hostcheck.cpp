@@ -5,6 +5,8 @@
 // operations. It is built into a separate library (_build/libbmadgpu_hostcheck.so) that the
 // product never loads; libbmadgpu.so has no CPU tracking path.
 
+// The host build of the plain tracking kernel's maps, with its shared-reciprocal quotients.
+#define BG_SHARED_RECIPROCAL
 #include <cstring>
 #include <string>
 

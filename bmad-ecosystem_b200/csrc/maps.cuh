@@ -73,13 +73,16 @@ BG_HD double sqrt_one(double x) {  // sim_utils/special_functions/sqrt_one.f90
 // outside [2^-900, 2^900] take the plain division; a zero numerator gives q itself (the sign of the
 // zero quotient is that of a y). Every caller's y is itself a rounded division 1 / b (or an exact
 // power-of-two multiple of one), so each quotient is the same bits as a / b.
-#if defined(BG_COUNT_OPS)
+// Only a translation unit that defines BG_SHARED_RECIPROCAL before its includes takes the quotients
+// this way (the plain tracking kernel, where it measured faster); every other one -- the batch and
+// adjoint kernels, whose register-tight shapes measured slower with it, and the operation-counting
+// host build -- takes a / b directly, the same bits, and leaves the shared reciprocal out (it is
+// not an operation of the reference, and div_rcp then does not use it).
+#if defined(BG_COUNT_OPS) || !defined(BG_SHARED_RECIPROCAL)
 BG_HD double div_rcp(double a, double b, double y) {  // counted as the one division it replaces
   (void)y;
   return a / b;
 }
-// The shared reciprocal is not an operation of the reference: the operation count leaves it out
-// (div_rcp above does not use its value when counting).
 BG_HD double shared_rcp(double b) { return b; }
 BG_HD double half_rcp(double y) { return y; }
 #else

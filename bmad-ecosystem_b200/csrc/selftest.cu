@@ -5,6 +5,7 @@
 // signs, 52-bit mantissas and exponents in [-60, 60], half of them numerators one ulp either side
 // of an exact product b q (quotients next to a rounding tie), plus zero numerators.
 
+#define BG_SHARED_RECIPROCAL  // the quotient under test
 #include <cuda_runtime.h>
 
 #include "capi_internal.h"

@@ -13,6 +13,9 @@
 //
 // k_compact: warp ballot / popc stream compaction of the live-particle index list.
 
+// The plain tracking kernel takes quotients with a common divisor from one rounded reciprocal
+// (maps.cuh, div_rcp): the same bits as the division, measured faster in this kernel.
+#define BG_SHARED_RECIPROCAL
 #include <cuda_runtime.h>
 
 #include "particle.cuh"

@@ -215,10 +215,11 @@ typedef struct bmadgpu_tuning {
 int bmadgpu_ctx_set_tuning(bmadgpu_ctx* ctx, const bmadgpu_tuning* tuning);
 int bmadgpu_ctx_get_tuning(const bmadgpu_ctx* ctx, bmadgpu_tuning* tuning);
 
-/* Autotuner: times one-turn trial launches of every launch shape (threads per CTA, register
+/* Autotuner: times two one-turn trial launches of every launch shape (threads per CTA, register
  * budget via resident CTAs per SM, element table staged in shared memory or read through L1) on
- * a copy of the first min(n, sample_n) particles of a device-resident bunch, sets the fastest
- * as the context's tuning and returns it in *chosen (nullable). The bunch is not modified. */
+ * a copy of the first min(n, sample_n) particles of a device-resident bunch (sample_n <= 0: 8192
+ * per SM), sets the shape with the shortest trial as the context's tuning and returns it in
+ * *chosen (nullable). The bunch is not modified. */
 int bmadgpu_autotune(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const bmadgpu_bunch* device_bunch,
                      int64_t sample_n, bmadgpu_tuning* chosen);
 
