@@ -13,6 +13,7 @@
 // eigenvectors of sigma.S are L w. The reference uses LAPACK's geev on sigma.S directly.
 
 #include <cmath>
+#include <complex>
 #include <cstring>
 
 #include "../../include/bmadgpu.h"
@@ -58,9 +59,66 @@ void jacobi_sym(int n, double* a, double* d, double* v) {
   for (int i = 0; i < n; i++) d[i] = a[i * n + i];
 }
 
-// Normal-mode emittances of the centred sigma matrix (dim 4 or 6). Returns false if sigma is not
-// positive definite (the reference's eigen-analysis then fails as well).
-bool normal_mode_emittances(const double* sig, int dim, double* emit) {
+// N of calc_emittances_and_twiss_from_sigma_matrix (bmad/multiparticle/beam_utils.f90:1495-1551)
+// from the Jacobi eigenvectors. For the Jacobi pair (x, y) of eigenvalue d, w = x + i y satisfies
+// A w = -i d w, so v = L w is the eigenvector of sigma.S at -i d: the vector geev's pair gives
+// mat_eigen before its flip (mat_eigen.f90:149-150). Then, as there and in normalize_e (:1639-1688):
+// the flip to positive fnorm = sum 2 Im(conj(v_2k) v_2k+1) (:153-164), the phase that makes the
+// mode's own-plane component real and positive (:175-182), e_odd = conj(e_even) with e_even
+// scaled by sqrt(i)/sqrt(wronskian), and N = E Q with Wolski's Q, whose real entries are the
+// single-precision 1.0/sqrt(2.0) and whose imaginary ones are i / (single-precision sqrt(2.0)).
+void normal_form_matrix(const double* L, const double* V, int n2, int dim, int nm, const int* col,
+                        const int* sort, double* nmat) {
+  typedef std::complex<double> cd;
+  const double q_re = (double)(1.0f / std::sqrt(2.0f));
+  const double q_im = 1.0 / (double)std::sqrt(2.0f);
+  for (int i = 0; i < 36; i++) nmat[i] = 0;
+  if (dim == 4) nmat[28] = nmat[35] = 1;
+  for (int m = 0; m < nm; m++) {
+    const int b = col[m], p = sort[m];
+    cd v[6];
+    for (int c = 0; c < dim; c++) {
+      double vr = 0, vi = 0;
+      for (int k = 0; k < dim; k++) {
+        vr += L[c * 6 + k] * V[k * n2 + b];
+        vi += L[c * 6 + k] * V[(dim + k) * n2 + b];
+      }
+      v[c] = cd(vr, vi);
+    }
+    double fnorm = 0;
+    for (int c = 0; c < dim; c += 2) fnorm += 2 * (std::conj(v[c]) * v[c + 1]).imag();
+    if (fnorm < 0) {
+      for (int c = 0; c < dim; c++) v[c] = std::conj(v[c]);
+      fnorm = -fnorm;
+    }
+    const cd vk = v[2 * p];
+    const cd sgn = std::abs(vk) == 0 ? cd(1 / std::sqrt(fnorm), 0) : std::abs(vk) / (std::sqrt(fnorm) * vk);
+    cd e1[6], e2[6];
+    for (int c = 0; c < dim; c++) {
+      e1[c] = sgn * v[c];
+      e2[c] = std::conj(e1[c]);
+    }
+    // normalize_e: wronskian of (conj(e2), S e2), S = blocks [[0, 1], [-1, 0]]
+    cd wr = 0;
+    for (int c = 0; c < dim; c += 2) wr += std::conj(e2[c]) * e2[c + 1] - std::conj(e2[c + 1]) * e2[c];
+    const cd factor = std::sqrt(cd(0, 1)) / std::sqrt(wr);
+    for (int c = 0; c < dim; c++) {
+      e2[c] *= factor;
+      e1[c] = std::conj(e2[c]);
+    }
+    for (int c = 0; c < dim; c++) {
+      nmat[c * 6 + 2 * p] = (e1[c] * q_re + e2[c] * q_re).real();
+      nmat[c * 6 + 2 * p + 1] = (e1[c] * cd(0, q_im) + e2[c] * cd(0, -q_im)).real();
+    }
+  }
+}
+
+// Normal-mode emittances of the centred sigma matrix (dim 4 or 6) and, if nmat is not NULL, the
+// normal-form matrix N of calc_emittances_and_twiss_from_sigma_matrix (6x6 row-major, Wolski
+// Eq. 44; in dim 4 its longitudinal block is the identity, where the reference leaves it unset).
+// Returns false if sigma is not positive definite (the reference's eigen-analysis then fails as
+// well).
+bool normal_mode_emittances(const double* sig, int dim, double* emit, double* nmat) {
   double L[36] = {0};
   for (int j = 0; j < dim; j++) {
     double s = sig[j * 6 + j];
@@ -96,13 +154,14 @@ bool normal_mode_emittances(const double* sig, int dim, double* emit) {
   jacobi_sym(n2, B, d, V);
   // the dim/2 largest eigenvalues (each appears twice) are the emittances; one eigenvector each
   const int nm = dim / 2;
-  int used[12] = {0};
+  int used[12] = {0}, used_first[3] = {0};
   double eps[3] = {0}, amp[3][3] = {{0}};
   for (int m = 0; m < nm; m++) {
     int best = -1;
     for (int i = 0; i < n2; i++)
       if (!used[i] && (best < 0 || d[i] > d[best])) best = i;
     used[best] = 1;
+    used_first[m] = best;
     // mark its twin (the other eigenvector of the same value) as used
     int twin = -1;
     for (int i = 0; i < n2; i++)
@@ -157,6 +216,7 @@ bool normal_mode_emittances(const double* sig, int dim, double* emit) {
   }
   for (int m = 0; m < 3; m++) emit[m] = 0;
   for (int m = 0; m < nm; m++) emit[sort[m]] = eps[m];
+  if (nmat) normal_form_matrix(L, V, n2, dim, nm, used_first, sort, nmat);
   return true;
 }
 
@@ -214,7 +274,7 @@ extern "C" int bmadgpu_bunch_data_from_sums(const double* s, double p0c, double 
     for (int i = 0; i < 36; i++) mx = std::fmax(mx, std::fabs(S[i]));
     const double cut = 1e-20 * mx;
     const int dim = (std::fabs(S[28]) < cut || std::fabs(S[35]) < cut) ? 4 : 6;
-    bd->emit_valid = normal_mode_emittances(S, dim, bd->emit) ? 1 : 0;
+    bd->emit_valid = normal_mode_emittances(S, dim, bd->emit, nullptr) ? 1 : 0;
     for (int m = 0; m < 3; m++) bd->norm_emit[m] = bd->emit[m] * f_emit;
   }
   // ltt_calc_bunch_data (needs at least 10 live particles)
@@ -235,5 +295,18 @@ extern "C" int bmadgpu_bunch_data_from_sums(const double* s, double p0c, double 
       bd->kurt[p] = c4[i] / (n * (sg * sg * sg * sg)) - 3.0;
     }
   }
+  return BMADGPU_OK;
+}
+
+extern "C" int bmadgpu_sigma_normal_form(const double* sigma, double* emit, double* n_mat) {
+  if (!sigma || !n_mat) return BMADGPU_EINVAL;
+  double mx = 0;
+  for (int i = 0; i < 36; i++) mx = std::fmax(mx, std::fabs(sigma[i]));
+  const double cut = 1e-20 * mx;
+  const int dim = (std::fabs(sigma[28]) < cut || std::fabs(sigma[35]) < cut) ? 4 : 6;
+  double e[3];
+  if (!normal_mode_emittances(sigma, dim, e, n_mat)) return BMADGPU_EINVAL;
+  if (emit)
+    for (int m = 0; m < 3; m++) emit[m] = e[m];
   return BMADGPU_OK;
 }

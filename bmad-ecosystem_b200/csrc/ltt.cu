@@ -253,8 +253,9 @@ bool append_averages(const std::string& base, int turn, const bmadgpu_bunch_data
   return true;
 }
 
-bool write_phase_space(const std::string& base, int turn, int n_turns, const bmadgpu_bunch& h, double p0c,
-                       bool only_live, const std::string& pre) {
+// File name of write_this_data (lt_tracking_mod.f90:1972-1986): the turn zero-padded to the digits
+// of n_turns replaces a '#' in the base name, or is appended.
+std::string particle_file_name(const std::string& base, int turn, int n_turns) {
   std::string num;
   if (n_turns > 0) {
     const int width = (int)(std::log10((double)n_turns) + 1 + 1e-10);
@@ -264,9 +265,13 @@ bool write_phase_space(const std::string& base, int turn, int n_turns, const bma
   } else {
     num = "000";
   }
-  std::string name;
   size_t ix = base.find('#');
-  name = ix == std::string::npos ? base + num : base.substr(0, ix) + num + base.substr(ix + 1);
+  return ix == std::string::npos ? base + num : base.substr(0, ix) + num + base.substr(ix + 1);
+}
+
+bool write_phase_space(const std::string& base, int turn, int n_turns, const bmadgpu_bunch& h, double p0c,
+                       bool only_live, const std::string& pre) {
+  const std::string name = particle_file_name(base, turn, n_turns);
   FILE* f = std::fopen(name.c_str(), "w");
   if (!f) return false;
   std::fprintf(f, "%s", pre.c_str());
@@ -286,7 +291,69 @@ bool write_phase_space(const std::string& base, int turn, int n_turns, const bma
   return true;
 }
 
-// ---- core emittance (ltt_calc_bunch_data, lt_tracking_mod.f90:2432-2560, combined calculation) ----
+// Action-angle file of write_this_data (lt_tracking_mod.f90:1995-2049): per particle
+// J_k = (j_2k^2 + j_2k+1^2) / 2 and angle_k = atan2(j_2k+1, j_2k), j = N^-1 (p - centroid), as the
+// device computed them into aa [6][n].
+bool write_action_angle(const std::string& base, int turn, int n_turns, const double* aa, const int32_t* state,
+                        int64_t n, bool only_live, const std::string& pre) {
+  const std::string name = particle_file_name(base, turn, n_turns);
+  FILE* f = std::fopen(name.c_str(), "w");
+  if (!f) return false;
+  std::fprintf(f, "%s", pre.c_str());
+  std::fprintf(f, "##     Ix     Turn |          Ja         Angle_a              Jb         Angle_b              Jc "
+                  "        Angle_c   |     spin_x    spin_y    spin_z    State\n");
+  for (int64_t j = 0; j < n; j++) {
+    if (only_live && state[j] != 1) continue;
+    std::string l = fmt_i(9, j + 1) + fmt_i(9, turn);
+    for (int i = 0; i < 6; i++) l += fmt_es(16, 8, aa[i * n + j]);
+    l += "   " + fmt_f(13, 9, 0.0) + fmt_f(13, 9, 0.0) + fmt_f(13, 9, 0.0) + "    " + state_name(state[j]);
+    std::fprintf(f, "%s\n", l.c_str());
+  }
+  std::fclose(f);
+  return true;
+}
+
+// ltt_per_particle_file_name (lt_tracking_mod.f90:725-752): the particle index zero-padded to
+// int(log10(1.001 n_particle)) + 1 digits (a default-real product) replaces a '#', or follows a '.'.
+std::string per_particle_file_name(const std::string& base, int64_t ip, int64_t n_particle) {
+  const int np = (int)std::log10(1.001f * (float)n_particle) + 1;
+  char b[32];
+  std::snprintf(b, sizeof b, "%0*lld", np, (long long)ip);
+  size_t ih = base.find('#');
+  return ih == std::string::npos ? base + "." + b : base.substr(0, ih) + b + base.substr(ih + 1);
+}
+
+// ltt_write_per_particle_file_header (lt_tracking_mod.f90:690-720): one file per particle.
+bool write_per_particle_headers(const std::string& base, int64_t n, const std::string& pre) {
+  for (int64_t ip = 1; ip <= n; ip++) {
+    FILE* f = std::fopen(per_particle_file_name(base, ip, n).c_str(), "w");
+    if (!f) return false;
+    std::fprintf(f, "%s# ix_bunch        = 1\n# ix_particle     = %lld\n", pre.c_str(), (long long)ip);
+    std::fprintf(f, "##   Turn |           x              px               y              py               z          "
+                    "    pz              pc             p0c            time   |    spin_x      spin_y      spin_z     "
+                    "State\n");
+    std::fclose(f);
+  }
+  return true;
+}
+
+// ltt_per_particle_file_write1 (lt_tracking_mod.f90:2062-2077): one line per particle and output turn.
+bool append_per_particle(const std::string& base, int turn, const bmadgpu_bunch& h, double p0c) {
+  const int64_t n = h.n;
+  for (int64_t j = 0; j < n; j++) {
+    FILE* f = std::fopen(per_particle_file_name(base, j + 1, n).c_str(), "a");
+    if (!f) return false;
+    std::string l = fmt_i(9, turn);
+    for (int i = 0; i < 6; i++) l += fmt_es(16, 8, h.vec[i * n + j]);
+    l += fmt_es(16, 8, (1.0 + h.vec[5 * n + j]) * p0c) + fmt_es(16, 8, p0c) + fmt_es(16, 8, h.t ? h.t[j] : 0.0);
+    l += " " + fmt_f(12, 8, 0.0) + fmt_f(12, 8, 0.0) + fmt_f(12, 8, 0.0) + "    " + state_name(h.state[j]);
+    std::fprintf(f, "%s\n", l.c_str());
+    std::fclose(f);
+  }
+  return true;
+}
+
+// ---- core emittance (ltt_calc_bunch_data, lt_tracking_mod.f90:2432-2560) ----
 //
 // The reference ranks the live particles by their combined normalised amplitude
 // sum_k (j_2k^2 + j_2k+1^2) / emit_k with j = N^-1 (p - centroid), N the normal-form matrix of the
@@ -297,11 +364,16 @@ bool write_phase_space(const std::string& base, int turn, int n_turns, const bma
 // quadratic form (p - c)^T Sigma^-1 (p - c) = |L^-1 (p - c)|^2 with Sigma = L L^T: the device
 // evaluates that per particle, the host picks the core, and the core's sums are the same two-pass
 // device sums as the bunch's, over the core as the live set.
+//
+// With core_emit_combined_calc off (:2496-2516) each mode k has its own core: the particles of
+// smallest action (j_2k^2 + j_2k+1^2) / 2 with N^-1 of the bunch, then of the core, and
+// f = cutoff / (1 - (1 + s) e^-s), s = -ln(1 - cutoff).
 
 constexpr int kCoreMax = 8;
 
 struct CoreArgs {
-  double li[21];   // L^-1, lower triangle by rows
+  double w[36];    // row-major: L^-1 (combined) or N^-1 (one mode)
+  double wgt[6];   // amplitude = sum_r wgt_r (w (p - c))_r^2
   double c[6];
 };
 
@@ -316,14 +388,78 @@ __global__ void k_core_amp(const double* __restrict__ vec, const int32_t* __rest
     double d[6];
     for (int k = 0; k < 6; k++) d[k] = vec[k * n + i] - A.c[k];
     double s = 0;
-    int q = 0;
     for (int r = 0; r < 6; r++) {
+      if (A.wgt[r] == 0) continue;
       double y = 0;
-      for (int k = 0; k <= r; k++) y += A.li[q++] * d[k];
-      s += y * y;
+      for (int k = 0; k < 6; k++) y += A.w[r * 6 + k] * d[k];
+      s += A.wgt[r] * (y * y);
     }
     amp[i] = s;
   }
+}
+
+// Action and angle of every particle (dead ones too, as the reference writes them):
+// aa [6][n] = J_a, angle_a, J_b, angle_b, J_c, angle_c with j = w (p - c).
+__global__ void k_action_angle(const double* __restrict__ vec, int64_t n, CoreArgs A, double* __restrict__ aa) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double d[6], j[6];
+    for (int k = 0; k < 6; k++) d[k] = vec[k * n + i] - A.c[k];
+    for (int r = 0; r < 6; r++) {
+      double y = 0;
+      for (int k = 0; k < 6; k++) y += A.w[r * 6 + k] * d[k];
+      j[r] = y;
+    }
+    for (int m = 0; m < 3; m++) {
+      aa[(2 * m) * n + i] = 0.5 * (j[2 * m] * j[2 * m] + j[2 * m + 1] * j[2 * m + 1]);
+      aa[(2 * m + 1) * n + i] = atan2(j[2 * m + 1], j[2 * m]);
+    }
+  }
+}
+
+// Inverse of a 6x6 matrix by Gauss-Jordan elimination with partial pivoting (mat_inverse,
+// sim_utils/matrix/mat_inverse.f90:19-56, uses LAPACK's getrf/getri); false if singular.
+bool mat_inverse6(const double* a_in, double* inv) {
+  double a[36];
+  for (int i = 0; i < 36; i++) {
+    a[i] = a_in[i];
+    inv[i] = (i % 7 == 0) ? 1.0 : 0.0;
+  }
+  for (int col = 0; col < 6; col++) {
+    int piv = col;
+    for (int r = col + 1; r < 6; r++)
+      if (std::fabs(a[r * 6 + col]) > std::fabs(a[piv * 6 + col])) piv = r;
+    if (a[piv * 6 + col] == 0) return false;
+    if (piv != col)
+      for (int k = 0; k < 6; k++) {
+        std::swap(a[piv * 6 + k], a[col * 6 + k]);
+        std::swap(inv[piv * 6 + k], inv[col * 6 + k]);
+      }
+    const double p = a[col * 6 + col];
+    for (int k = 0; k < 6; k++) {
+      a[col * 6 + k] /= p;
+      inv[col * 6 + k] /= p;
+    }
+    for (int r = 0; r < 6; r++) {
+      if (r == col) continue;
+      const double f = a[r * 6 + col];
+      if (f == 0) continue;
+      for (int k = 0; k < 6; k++) {
+        a[r * 6 + k] -= f * a[col * 6 + k];
+        inv[r * 6 + k] -= f * inv[col * 6 + k];
+      }
+    }
+  }
+  return true;
+}
+
+// N^-1 of a bunch's sigma matrix (calc_bunch_params' n_mat, then mat_inverse); false where the
+// reference's eigen-analysis fails.
+bool normal_form_inverse(const bmadgpu_bunch_data& bd, double* n_inv) {
+  double n_mat[36];
+  if (bd.n_live < 6 || !bd.emit_valid) return false;
+  if (bmadgpu_sigma_normal_form(bd.sigma, nullptr, n_mat) != BMADGPU_OK) return false;
+  return mat_inverse6(n_mat, n_inv);
 }
 
 // L^-1 of sigma = L L^T (6x6), false unless sigma is positive definite.
@@ -435,13 +571,26 @@ struct CoreScratch {
   }
 };
 
-// One ranking: the n_cut live particles of smallest amplitude about (centroid, sigma) of `ref`,
-// and the bunch data of that core from the device sums.
+// One ranking: the n_cut live particles of smallest amplitude about (centroid, sigma) of `ref` --
+// the combined amplitude (mode 0) or the action of mode 1..3 -- and the bunch data of that core
+// from the device sums.
 int core_pass(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch& d, double* d_scratch,
-              const bmadgpu_bunch_data& ref, int64_t n_cut, CoreScratch& cs, bmadgpu_bunch_data* core, bool* ok) {
+              const bmadgpu_bunch_data& ref, int mode, int64_t n_cut, CoreScratch& cs, bmadgpu_bunch_data* core,
+              bool* ok) {
   *ok = false;
   CoreArgs A;
-  if (!chol_inverse(ref.sigma, A.li)) return BMADGPU_OK;
+  for (int k = 0; k < 6; k++) A.wgt[k] = 0;
+  if (mode == 0) {
+    double li[21];
+    if (!chol_inverse(ref.sigma, li)) return BMADGPU_OK;
+    int q = 0;
+    for (int r = 0; r < 6; r++)
+      for (int k = 0; k < 6; k++) A.w[r * 6 + k] = k <= r ? li[q++] : 0.0;
+    for (int k = 0; k < 6; k++) A.wgt[k] = 1;
+  } else {
+    if (!normal_form_inverse(ref, A.w)) return BMADGPU_OK;
+    A.wgt[2 * mode - 2] = A.wgt[2 * mode - 1] = 0.5;
+  }
   for (int k = 0; k < 6; k++) A.c[k] = ref.centroid[k];
   const int64_t n = d.n;
   cudaStream_t s = c->stream;
@@ -473,25 +622,60 @@ int core_pass(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch& d
   return BMADGPU_OK;
 }
 
-// core_emit [3] of one cutoff (zeros where the reference leaves them zero).
+// core_emit [3] of one cutoff (zeros where the reference leaves them zero; with the per-mode
+// calculation the modes before a failed one keep their values, as this_core_calc returns there).
 int core_emittance(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch& d, double* d_scratch,
-                   const bmadgpu_bunch_data& bd, double cutoff_in, CoreScratch& cs, double* out) {
+                   const bmadgpu_bunch_data& bd, double cutoff_in, bool combined, CoreScratch& cs, double* out) {
   out[0] = out[1] = out[2] = 0;
+  if (bd.n_live < 10) return BMADGPU_OK;
   if (!bd.emit_valid || bd.emit[0] == 0 || bd.emit[1] == 0 || bd.emit[2] == 0) return BMADGPU_OK;
   const int64_t n_cut = (int64_t)(cutoff_in * (double)bd.n_live);
   if (n_cut <= 0) return BMADGPU_OK;
   if (!cs.alloc(d.n)) return fail(BMADGPU_ENOMEM, "cannot allocate the core-emittance scratch");
   const double cutoff = std::fmin(1.0 - 1e-8, cutoff_in);
-  const double sig_cut = -std::log(fraction_root(cutoff, 1e-12, 1.0));
-  const double f =
-      cutoff / (1 - (1 + sig_cut + sig_cut * sig_cut / 2 + sig_cut * sig_cut * sig_cut / 6) * std::exp(-sig_cut));
   bmadgpu_bunch_data core1, core2;
   bool ok = false;
-  int r = core_pass(c, lat, d, d_scratch, bd, n_cut, cs, &core1, &ok);
-  if (r || !ok) return r;
-  r = core_pass(c, lat, d, d_scratch, core1, n_cut, cs, &core2, &ok);
-  if (r || !ok) return r;
-  for (int k = 0; k < 3; k++) out[k] = f * core2.emit[k];
+  int r;
+  if (combined) {
+    const double sig_cut = -std::log(fraction_root(cutoff, 1e-12, 1.0));
+    const double f =
+        cutoff / (1 - (1 + sig_cut + sig_cut * sig_cut / 2 + sig_cut * sig_cut * sig_cut / 6) * std::exp(-sig_cut));
+    r = core_pass(c, lat, d, d_scratch, bd, 0, n_cut, cs, &core1, &ok);
+    if (r || !ok) return r;
+    r = core_pass(c, lat, d, d_scratch, core1, 0, n_cut, cs, &core2, &ok);
+    if (r || !ok) return r;
+    for (int k = 0; k < 3; k++) out[k] = f * core2.emit[k];
+    return BMADGPU_OK;
+  }
+  const double sig_cut = -std::log(1 - cutoff);
+  const double f = cutoff / (1 - (1 + sig_cut) * std::exp(-sig_cut));
+  for (int m = 1; m <= 3; m++) {
+    r = core_pass(c, lat, d, d_scratch, bd, m, n_cut, cs, &core1, &ok);
+    if (r || !ok) return r;
+    r = core_pass(c, lat, d, d_scratch, core1, m, n_cut, cs, &core2, &ok);
+    if (r || !ok) return r;
+    out[m - 1] = f * core2.emit[m - 1];
+  }
+  return BMADGPU_OK;
+}
+
+// Action and angle of every particle of a device bunch about its own normal form (zero where the
+// reference's eigen-analysis fails) into the host arrays aa [6][n].
+int action_angle(bmadgpu_ctx* c, const bmadgpu_bunch& d, const bmadgpu_bunch_data& bd, double* d_aa, double* aa) {
+  CoreArgs A;
+  if (!normal_form_inverse(bd, A.w))
+    for (int k = 0; k < 36; k++) A.w[k] = 0;
+  for (int k = 0; k < 6; k++) {
+    A.c[k] = bd.n_live > 0 ? bd.centroid[k] : 0.0;
+    A.wgt[k] = 0;
+  }
+  const int64_t n = d.n;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)c->sm_count * 8));
+  k_action_angle<<<grid, 256, 0, c->stream>>>(d.vec, n, A, d_aa);
+  CUDA_TRY(cudaGetLastError());
+  c->launches++;
+  CUDA_TRY(cudaMemcpyAsync(aa, d_aa, 6 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
   return BMADGPU_OK;
 }
 
@@ -536,7 +720,7 @@ extern "C" int bmadgpu_bunch_stats(bmadgpu_ctx* c, const bmadgpu_lattice* lat, c
 }
 
 extern "C" int bmadgpu_bunch_core_emit(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch* d,
-                                       double cutoff, double* core_emit) {
+                                       double cutoff, int32_t combined_calc, double* core_emit) {
   if (!c || !lat || !d || !core_emit) return fail(BMADGPU_EINVAL, "NULL argument");
   if (d->n < 1 || !d->vec || !d->state) return fail(BMADGPU_EINVAL, "bad bunch");
   if (!(cutoff > 0 && cutoff <= 1.00000001)) return fail(BMADGPU_EINVAL, "cutoff must be in (0, 1]");
@@ -547,7 +731,7 @@ extern "C" int bmadgpu_bunch_core_emit(bmadgpu_ctx* c, const bmadgpu_lattice* la
   bmadgpu_bunch_data bd;
   CoreScratch cs;
   int r = device_stats(c, lat, *d, scratch, &bd);
-  if (!r) r = core_emittance(c, lat, *d, scratch, bd, cutoff, cs, core_emit);
+  if (!r) r = core_emittance(c, lat, *d, scratch, bd, cutoff, combined_calc != 0, cs, core_emit);
   cudaFree(scratch);
   return r;
 }
@@ -564,6 +748,11 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
   const std::string ave_base = P->averages_file ? P->averages_file : "";
   const std::string ps_base = P->phase_space_file ? P->phase_space_file : "";
   const std::string beam_base = P->beam_file ? P->beam_file : "";
+  const std::string aa_base = P->action_angle_file ? P->action_angle_file : "";
+  const std::string pp_base = P->per_particle_file ? P->per_particle_file : "";
+  if (!pp_base.empty() && n > 1000)
+    return fail(BMADGPU_EINVAL, "per-particle output needs at most 1000 particles (the reference stops there)");
+  const bool particle_out = !ps_base.empty() || !aa_base.empty() || !pp_base.empty();
   if (P->ix_turn_start < 0 || P->ix_turn_start > P->n_turns) return fail(BMADGPU_EINVAL, "ix_turn_start out of range");
   // ltt_write_beam_file's schedule: every beam_every_n_turns turns, and always at n_turns
   auto wants_beam = [&](int turn) {
@@ -617,6 +806,16 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
   CoreScratch core_scratch;
   if (!ave_base.empty() && !write_averages_headers(ave_base, pre, cuts, n_cuts))
     return fail(BMADGPU_EINVAL, "cannot write the averages files " + ave_base + ".*");
+  if (!pp_base.empty() && !write_per_particle_headers(pp_base, n, pre))
+    return fail(BMADGPU_EINVAL, "cannot write the per-particle files " + pp_base);
+  double* d_aa = nullptr;
+  std::vector<double> haa;
+  struct AaFreer {
+    double** p;
+    ~AaFreer() { cudaFree(*p); }
+  } aa_freer{&d_aa};
+  if (!aa_base.empty() && cudaMalloc(&d_aa, 6 * (size_t)n * sizeof(double)) != cudaSuccess)
+    return fail(BMADGPU_ENOMEM, "cannot allocate the action-angle buffer");
 
   auto outputs = [&](int turn) -> int {
     if (!ave_base.empty() && wants(P->averages_every_n_turns, P->output_only_last_turns, P->n_turns, turn)) {
@@ -625,11 +824,15 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
       if (r) return r;
       double core[kCoreMax * 3];
       for (int k = 0; k < n_cuts; k++)
-        if ((r = core_emittance(c, lat, cur.b, d_scratch, bd, cuts[k], core_scratch, core + 3 * k))) return r;
+        if ((r = core_emittance(c, lat, cur.b, d_scratch, bd, cuts[k], P->core_emit_per_mode == 0, core_scratch,
+                                core + 3 * k)))
+          return r;
       if (!append_averages(ave_base, turn, bd, core, n_cuts))
         return fail(BMADGPU_EINVAL, "cannot append to the averages files");
     }
-    if (!ps_base.empty() && wants(P->particle_every_n_turns, P->output_only_last_turns, P->n_turns, turn)) {
+    if (!particle_out || !wants(P->particle_every_n_turns, P->output_only_last_turns, P->n_turns, turn))
+      return BMADGPU_OK;
+    if (!ps_base.empty() || !pp_base.empty()) {
       hvec.resize(6 * n);
       ht.resize(n);
       hstate.resize(n);
@@ -641,8 +844,24 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
       CUDA_TRY(cudaMemcpyAsync(h.t, cur.b.t, n * sizeof(double), cudaMemcpyDeviceToHost, s));
       CUDA_TRY(cudaMemcpyAsync(h.state, cur.b.state, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
       CUDA_TRY(cudaStreamSynchronize(s));
-      if (!write_phase_space(ps_base, turn, P->n_turns, h, lat->param.p0c, P->only_live_particles_out != 0, pre))
+      if (!ps_base.empty() &&
+          !write_phase_space(ps_base, turn, P->n_turns, h, lat->param.p0c, P->only_live_particles_out != 0, pre))
         return fail(BMADGPU_EINVAL, "cannot write the phase-space file");
+      if (!pp_base.empty() && !append_per_particle(pp_base, turn, h, lat->param.p0c))
+        return fail(BMADGPU_EINVAL, "cannot append to the per-particle files");
+    }
+    if (!aa_base.empty()) {
+      bmadgpu_bunch_data bd;
+      int r = device_stats(c, lat, cur.b, d_scratch, &bd);
+      if (r) return r;
+      haa.resize(6 * n);
+      hstate.resize(n);
+      if ((r = action_angle(c, cur.b, bd, d_aa, haa.data()))) return r;
+      CUDA_TRY(cudaMemcpyAsync(hstate.data(), cur.b.state, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      CUDA_TRY(cudaStreamSynchronize(s));
+      if (!write_action_angle(aa_base, turn, P->n_turns, haa.data(), hstate.data(), n,
+                              P->only_live_particles_out != 0, pre))
+        return fail(BMADGPU_EINVAL, "cannot write the action-angle file");
     }
     return BMADGPU_OK;
   };
@@ -686,7 +905,7 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
     int next = turn + 1;
     while (next < P->n_turns && next - turn < kChunk &&
            !(wants(P->averages_every_n_turns, P->output_only_last_turns, P->n_turns, next) && !ave_base.empty()) &&
-           !(wants(P->particle_every_n_turns, P->output_only_last_turns, P->n_turns, next) && !ps_base.empty()) &&
+           !(wants(P->particle_every_n_turns, P->output_only_last_turns, P->n_turns, next) && particle_out) &&
            !wants_beam(next))
       ++next;
     const int chunk = next - turn;

@@ -617,7 +617,8 @@ class LttParams(C.Structure):
                 ("output_only_last_turns", C.c_int32), ("only_live_particles_out", C.c_int32),
                 ("ix_turn_start", C.c_int32), ("beam_every_n_turns", C.c_int32), ("beam_exact", C.c_int32),
                 ("dead_cutoff", C.c_double), ("averages_file", C.c_char_p), ("phase_space_file", C.c_char_p),
-                ("beam_file", C.c_char_p), ("core_emit_cutoff", C.c_double * 8)]
+                ("beam_file", C.c_char_p), ("core_emit_cutoff", C.c_double * 8), ("core_emit_per_mode", C.c_int32),
+                ("action_angle_file", C.c_char_p), ("per_particle_file", C.c_char_p)]
 
 
 def _ltt_sigs(lib):
@@ -631,6 +632,18 @@ def _ltt_sigs(lib):
     return lib
 
 
+def sigma_normal_form(sigma):
+    """Host-only: (emit[3], n_mat[6, 6]) of a 6x6 sigma matrix, the normal-form matrix N that
+    calc_emittances_and_twiss_from_sigma_matrix returns (no GPU needed)."""
+    lib = load()
+    lib.bmadgpu_sigma_normal_form.argtypes = [C.POINTER(C.c_double)] * 3
+    sig = np.ascontiguousarray(sigma, dtype=np.float64).reshape(36)
+    emit = np.zeros(3)
+    n_mat = np.zeros(36)
+    check_host(lib.bmadgpu_sigma_normal_form(*(a.ctypes.data_as(C.POINTER(C.c_double)) for a in (sig, emit, n_mat))))
+    return emit, n_mat.reshape(6, 6)
+
+
 def bunch_data_from_sums(sums, p0c, mass):
     """Host-only: the bunch data from the 63 two-pass sums (no GPU needed)."""
     lib = _ltt_sigs(load())
@@ -640,14 +653,15 @@ def bunch_data_from_sums(sums, p0c, mass):
     return bd.as_dict()
 
 
-def bunch_core_emit(ctx, lat, device_view, cutoff=0.5):
-    """Core emittances (a, b, c) of a device-resident bunch (the combined calculation of
-    ltt_calc_bunch_data)."""
+def bunch_core_emit(ctx, lat, device_view, cutoff=0.5, combined_calc=True):
+    """Core emittances (a, b, c) of a device-resident bunch as ltt_calc_bunch_data computes them
+    (combined_calc: ltt%core_emit_combined_calc)."""
     lib = load()
-    lib.bmadgpu_bunch_core_emit.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(abi.Bunch), C.c_double,
+    lib.bmadgpu_bunch_core_emit.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(abi.Bunch), C.c_double, C.c_int32,
                                             C.POINTER(C.c_double)]
     out = (C.c_double * 3)()
-    check(lib.bmadgpu_bunch_core_emit(ctx.handle, lat.handle, C.byref(device_view), cutoff, out))
+    check(lib.bmadgpu_bunch_core_emit(ctx.handle, lat.handle, C.byref(device_view), cutoff,
+                                      1 if combined_calc else 0, out))
     return np.array(out[:])
 
 
@@ -661,10 +675,12 @@ def bunch_stats(ctx, lat, device_view):
 
 def ltt_run(ctx, lat, bunch, n_turns, averages_file=None, phase_space_file=None, averages_every_n_turns=-1,
             particle_every_n_turns=-1, output_only_last_turns=0, only_live_particles_out=True, dead_cutoff=1.0,
-            beam_file=None, beam_every_n_turns=-1, beam_exact=False, ix_turn_start=0, core_emit_cutoff=None):
+            beam_file=None, beam_every_n_turns=-1, beam_exact=False, ix_turn_start=0, core_emit_cutoff=None,
+            core_emit_combined_calc=True, action_angle_file=None, per_particle_file=None):
     """long_term_tracking's beam mode for a HostBunch (updated in place); returns the turn reached.
     core_emit_cutoff: list of core fractions for the .emit file (None: the reference's [0.5];
-    []: no core columns)."""
+    []: no core columns); core_emit_combined_calc False: a core per normal mode.
+    action_angle_file / per_particle_file: the reference's action-angle and per-particle outputs."""
     lib = _ltt_sigs(load())
     p = LttParams(n_turns, averages_every_n_turns, particle_every_n_turns, output_only_last_turns,
                   1 if only_live_particles_out else 0, ix_turn_start, beam_every_n_turns, 1 if beam_exact else 0,
@@ -674,6 +690,9 @@ def ltt_run(ctx, lat, bunch, n_turns, averages_file=None, phase_space_file=None,
     if core_emit_cutoff is not None:
         cuts = list(core_emit_cutoff)[:8]
         p.core_emit_cutoff[:] = cuts + [-1.0] * (8 - len(cuts))
+    p.core_emit_per_mode = 0 if core_emit_combined_calc else 1
+    p.action_angle_file = action_angle_file.encode() if action_angle_file else None
+    p.per_particle_file = per_particle_file.encode() if per_particle_file else None
     done = C.c_int32()
     v = bunch.view()
     check(lib.bmadgpu_ltt_run(ctx.handle, lat.handle, C.byref(v), C.byref(p), C.byref(done)))

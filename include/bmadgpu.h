@@ -415,6 +415,11 @@ int bmadgpu_bunch_stats(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const bmad
 /* Host-only: bunch data from the 63 sums of the two passes (count, sum v, sum t, sum t^2,
  * sum v_i v_j; centred sum d_i d_j, sum d^3, sum d^4), for callers with their own sums. */
 int bmadgpu_bunch_data_from_sums(const double* sums, double p0c, double mass, bmadgpu_bunch_data* data);
+/* Host only: the normal-mode emittances emit [3] (nullable) and the normal-form matrix n_mat [36]
+ * (row-major; sigma = N diag(emit) N^T up to Q's single-precision entries) of a 6x6 sigma matrix, as
+ * calc_emittances_and_twiss_from_sigma_matrix returns them in n_mat
+ * (bmad/multiparticle/beam_utils.f90:1495-1551). BMADGPU_EINVAL if sigma is not positive definite. */
+int bmadgpu_sigma_normal_form(const double* sigma, double* emit, double* n_mat);
 
 /* ltt_run_beam_mode (lt_tracking_mod.f90:1571-1715) for one bunch with bmad_standard tracking:
  * turns ix_turn_start .. n_turns - 1 with the reference's stop conditions (no particle left; lost count reaching
@@ -436,17 +441,26 @@ typedef struct bmadgpu_ltt_params {
   const char* averages_file;        /* NULL or "": no averages output */
   const char* phase_space_file;     /* NULL or "": no phase-space output */
   const char* beam_file;            /* NULL or "": no beam files; "<stem>-<turn><.ext>" as ltt_write_beam_file names them */
-  double core_emit_cutoff[8];       /* ltt%core_emit_cutoff: core fractions whose emittances the .emit file adds
-                                       (combined calculation), up to the first entry <= 0; all zero: the
-                                       reference's default, 0.5; core_emit_cutoff[0] < 0: none */
+  double core_emit_cutoff[8];       /* ltt%core_emit_cutoff: core fractions whose emittances the .emit file adds,
+                                       up to the first entry <= 0; all zero: the reference's default, 0.5;
+                                       core_emit_cutoff[0] < 0: none */
+  int32_t core_emit_per_mode;       /* .not. ltt%core_emit_combined_calc: a core per normal mode, ranked by
+                                       that mode's action (0: the combined calculation, the default) */
+  const char* action_angle_file;    /* ltt%action_angle_output_file: NULL or "": none; written with the
+                                       phase-space schedule, actions and angles about the bunch's own
+                                       normal form (calc_bunch_params' n_mat) */
+  const char* per_particle_file;    /* ltt%per_particle_output_file: NULL or "": none; one file per
+                                       particle (at most 1000 particles, as the reference requires) */
 } bmadgpu_ltt_params;
 int bmadgpu_ltt_run(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* host_bunch,
                     const bmadgpu_ltt_params* params, int32_t* turns_done);
-/* Core emittances a, b, c of a device-resident bunch for one core fraction cutoff (0, 1]: the
- * combined calculation of ltt_calc_bunch_data (bsim/modules/lt_tracking_mod.f90:2432-2560), zeros
- * where the reference leaves them zero (a zero bunch emittance, an empty core). */
+/* Core emittances a, b, c of a device-resident bunch for one core fraction cutoff (0, 1] as
+ * ltt_calc_bunch_data computes them (bsim/modules/lt_tracking_mod.f90:2432-2516): combined_calc != 0
+ * ranks by the combined normalised amplitude (ltt%core_emit_combined_calc, the default), 0 gives
+ * each mode its own core ranked by that mode's action; zeros where the reference leaves them zero
+ * (fewer than 10 live particles, a zero bunch emittance, an empty core). */
 int bmadgpu_bunch_core_emit(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const bmadgpu_bunch* device_bunch,
-                            double cutoff, double* core_emit);
+                            double cutoff, int32_t combined_calc, double* core_emit);
 
 /* ---- Dynamic aperture ------------------------------------------------------------------------
  * dynamic_aperture_point (bmad/modules/dynamic_aperture_mod.f90:284-398) for many rays at once:

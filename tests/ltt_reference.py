@@ -149,23 +149,40 @@ def beam_fraction(x):
     return 1.0 - x * (1 + jc + 0.5 * jc ** 2)
 
 
-def core_emit(vec, t, state, p0c, mass, cutoff):
-    """Core emittances of ltt_calc_bunch_data's combined calculation (lt_tracking_mod.f90:
-    2432-2560): rank the live particles by sum_k (j_2k^2 + j_2k+1^2) / emit_k, j = N^-1 (p - c) --
+def core_emit(vec, t, state, p0c, mass, cutoff, combined=True):
+    """Core emittances of ltt_calc_bunch_data (lt_tracking_mod.f90:2432-2560). Combined
+    calculation: rank the live particles by sum_k (j_2k^2 + j_2k+1^2) / emit_k, j = N^-1 (p - c) --
     the quadratic form (p - c)^T Sigma^-1 (p - c) -- keep the int(cutoff n_live) smallest, rank again
-    about the core, and scale the core's normal-mode emittances by f(cutoff)."""
+    about the core, and scale the core's normal-mode emittances by f(cutoff). Per mode
+    (combined=False): the same with each mode's action (j_2k^2 + j_2k+1^2) / 2 and N^-1 from
+    normal_form_n, f = cutoff / (1 - (1 + s) e^-s), s = -ln(1 - cutoff)."""
     from scipy.optimize import brentq
     bd = bunch_data(vec, t, state, p0c, mass)
-    if "emit" not in bd or np.any(bd["emit"] == 0):
+    if bd["n_live"] < 10 or "emit" not in bd or np.any(bd["emit"] == 0):
         return np.zeros(3)
     n_cut = int(cutoff * bd["n_live"])
     if n_cut == 0:
         return np.zeros(3)
     cut = min(1.0 - 1e-8, cutoff)
+    alive = state == 1
+    if not combined:
+        s = -np.log(1 - cut)
+        f = cut / (1 - (1 + s) * np.exp(-s))
+        out = np.zeros(3)
+        for m in range(3):
+            def core_m(ref):
+                n_inv = np.linalg.inv(normal_form_n(ref["sigma"])[1])
+                j = n_inv @ (vec - np.asarray(ref["centroid"])[:, None])
+                amp = 0.5 * (j[2 * m] ** 2 + j[2 * m + 1] ** 2)
+                amp[~alive] = 1e100
+                st = np.zeros_like(state)
+                st[np.argsort(amp, kind="stable")[:n_cut]] = 1
+                return bunch_data(vec, t, st, p0c, mass)
+            out[m] = f * core_m(core_m(bd))["emit"][m]
+        return out
     x = brentq(lambda u: beam_fraction(u) - cut, 1e-12, 1.0, xtol=1e-300, rtol=1e-15)
     s = -np.log(x)
     f = cut / (1 - (1 + s + s ** 2 / 2 + s ** 3 / 6) * np.exp(-s))
-    alive = state == 1
 
     def core(ref):
         d = vec - np.asarray(ref["centroid"])[:, None]
@@ -179,3 +196,116 @@ def core_emit(vec, t, state, p0c, mass, cutoff):
     c1 = core(bd)
     c2 = core(c1)
     return f * np.asarray(c2["emit"])
+
+
+def mat_eigen(mat):
+    """mat_eigen (sim_utils/matrix/mat_eigen.f90:37-187) for a stable matrix: LAPACK geev (through
+    numpy.linalg.eig), the greedy plane sort, the complex-conjugate pair layout, the flip that makes
+    fnorm positive and the phase that makes each eigenvector's own-plane component real and
+    positive. Returns (eigen_val[n], eigen_vec[n, n]) with eigenvectors as rows, 0-based."""
+    n = mat.shape[0]
+    nn = n // 2
+    w, v = np.linalg.eig(mat)
+    # geev's real layout: a pair (p, p+1) keeps Re and Im of the first (positive imaginary) vector
+    vec = np.zeros((n, n))
+    eval_r, eval_i = w.real.copy(), w.imag.copy()
+    p = 0
+    while p < n:
+        if w[p].imag != 0:
+            vec[:, p], vec[:, p + 1] = v[:, p].real, v[:, p].imag
+            p += 2
+        else:
+            vec[:, p] = v[:, p].real
+            p += 1
+    amp = np.zeros((nn, nn))
+    for ii in range(nn):
+        for kk in range(nn):
+            amp[kk, ii] = np.sum(vec[2 * kk:2 * kk + 2, 2 * ii:2 * ii + 2] ** 2)
+        amp[:, ii] /= np.sum(amp[:, ii])
+    sort = np.zeros(nn, int)
+    for _ in range(nn):
+        amp2 = amp.copy()
+        dmax = np.zeros(nn)
+        for j in range(nn):
+            m = int(np.argmax(amp2[j]))
+            amp2[j, m] = -1
+            m2 = int(np.argmax(amp2[j]))
+            dmax[j] = amp[j, m] - amp[j, m2]
+        k = int(np.argmax(dmax))
+        m = int(np.argmax(amp[k]))
+        sort[m] = k
+        amp[k, :] = 0
+        amp[:, m] = 0
+    eigen_val = np.zeros(n, complex)
+    eigen_vec = np.zeros((n, n), complex)
+    for ii in range(nn):
+        i = 2 * ii + 1          # 0-based index of the Fortran i = 2 ii
+        k = 2 * sort[ii]        # 0-based index of the Fortran j - 1
+        if eval_i[i - 1] == 0:
+            raise ValueError("unstable mode")
+        eigen_val[k] = complex(eval_r[i], eval_i[i])
+        eigen_val[k + 1] = complex(eval_r[i - 1], eval_i[i - 1])
+        eigen_vec[k] = vec[:, i - 1] - 1j * vec[:, i]
+        eigen_vec[k + 1] = vec[:, i - 1] + 1j * vec[:, i]
+        fnorm = sum(2 * (np.conj(eigen_vec[k, jj]) * eigen_vec[k, jj + 1]).imag for jj in range(0, n, 2))
+        if fnorm < 0:
+            eigen_vec[[k, k + 1]] = eigen_vec[[k + 1, k]]
+            eigen_val[[k, k + 1]] = eigen_val[[k + 1, k]]
+            fnorm = -fnorm
+        if abs(eigen_vec[k, k]) == 0:
+            sgn = 1.0 / np.sqrt(fnorm)
+        else:
+            sgn = abs(eigen_vec[k, k]) / (np.sqrt(fnorm) * eigen_vec[k, k])
+        eigen_vec[k] = sgn * eigen_vec[k]
+        eigen_vec[k + 1] = np.conj(sgn) * eigen_vec[k + 1]
+    return eigen_val, eigen_vec
+
+
+# Wolski's Q of calc_emittances_and_twiss_from_sigma_matrix (beam_utils.f90:1533-1545): the real
+# entries are the default-real (single precision) expression 1.0/sqrt(2.0), the imaginary ones
+# i_imag / sqrt(2.0) with the single-precision square root widened.
+Q_RE = float(np.float32(1.0) / np.sqrt(np.float32(2.0)))
+Q_IM = 1.0 / float(np.sqrt(np.float32(2.0)))
+
+
+def normal_form_n(sigma):
+    """(emit[3], n_mat[6, 6]) of calc_emittances_and_twiss_from_sigma_matrix (beam_utils.f90:
+    1495-1551): eigen-decomposition of sigma.S by mat_eigen, normalize_e (:1639-1688), N = E Q
+    (Wolski Eq. 44). Only the 6-dimensional case (non-zero longitudinal spread)."""
+    S = np.zeros((6, 6))
+    for k in range(3):
+        S[2 * k, 2 * k + 1], S[2 * k + 1, 2 * k] = 1, -1
+    ev, e = mat_eigen(sigma @ S)
+    for i2 in range(3):
+        i = 2 * i2
+        e[i] = np.conj(e[i + 1])
+        temp = S @ e[i + 1]
+        wronsk = np.sum(e[i] * temp)
+        factor = np.sqrt(1j) / np.sqrt(wronsk)
+        e[i + 1] = e[i + 1] * factor
+        e[i] = np.conj(e[i + 1])
+    emit = np.array([ev[0].imag, ev[2].imag, ev[4].imag])
+    E = e.T
+    q = np.zeros((6, 6), complex)
+    for k in range(3):
+        q[2 * k, 2 * k] = q[2 * k + 1, 2 * k] = Q_RE
+        q[2 * k, 2 * k + 1] = 1j * Q_IM
+        q[2 * k + 1, 2 * k + 1] = -1j * Q_IM
+    return emit, (E @ q).real
+
+
+def action_angle(vec, t, state, p0c, mass):
+    """[6, n] = J_a, angle_a, J_b, angle_b, J_c, angle_c of write_this_data's action-angle file
+    (lt_tracking_mod.f90:2024-2045): j = N^-1 (p - centroid) with N of the bunch (zero where
+    calc_bunch_params fails), J = (j_2k^2 + j_2k+1^2) / 2, angle = atan2(j_2k+1, j_2k)."""
+    bd = bunch_data(vec, t, state, p0c, mass)
+    n_inv = np.zeros((6, 6))
+    if bd["n_live"] >= 6 and "emit" in bd:
+        n_inv = np.linalg.inv(normal_form_n(bd["sigma"])[1])
+    c = np.asarray(bd.get("centroid", np.zeros(6)))
+    j = n_inv @ (vec - c[:, None])
+    out = np.zeros((6, vec.shape[1]))
+    for m in range(3):
+        out[2 * m] = 0.5 * (j[2 * m] ** 2 + j[2 * m + 1] ** 2)
+        out[2 * m + 1] = np.arctan2(j[2 * m + 1], j[2 * m])
+    return out

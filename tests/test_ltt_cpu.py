@@ -83,3 +83,57 @@ def test_combined_amplitude_is_the_sigma_quadratic_form():
     amp_modes = sum((j[2 * k] ** 2 + j[2 * k + 1] ** 2) / emit[k] for k in range(3))
     amp_form = np.einsum("in,ij,jn->n", d, np.linalg.inv(Sigma), d)
     assert np.allclose(amp_modes, amp_form, rtol=1e-8)
+
+
+def _coupled_sigma(seed):
+    import scipy.linalg
+    rng = np.random.default_rng(seed)
+    S = np.zeros((6, 6))
+    for k in range(3):
+        S[2 * k, 2 * k + 1], S[2 * k + 1, 2 * k] = 1.0, -1.0
+    H = rng.normal(size=(6, 6))
+    M = scipy.linalg.expm(S @ (0.2 * (H + H.T)))
+    e = np.repeat([2e-9 * (1 + rng.random()), 3e-10 * (1 + rng.random()), 4e-6 * (1 + rng.random())], 2)
+    return M @ np.diag(e) @ M.T
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_sigma_normal_form_matches_restatement(seed):
+    """bmadgpu_sigma_normal_form (Jacobi eigenvectors, then mat_eigen's flip and phase, normalize_e
+    and Wolski's Q) against the numpy restatement that follows the reference step by step from
+    LAPACK's geev: coupled sigma matrices, and the sample sigma of a synthetic bunch."""
+    from ltt_reference import normal_form_n
+    if seed < 8:
+        sig = _coupled_sigma(seed)
+    else:
+        v, t, st = bunch(4000, seed, couple=0.05 * (seed - 7))
+        sig = np.cov(v, bias=True)
+    emit, N = lib.sigma_normal_form(sig)
+    e_ref, N_ref = normal_form_n(sig)
+    assert np.allclose(emit, e_ref, rtol=1e-10, atol=0)
+    assert np.max(np.abs(N - N_ref)) <= 1e-10 * np.max(np.abs(N_ref))
+
+
+def test_sigma_normal_form_structure():
+    """N diagonalises sigma (N^-1 sigma N^-T = diag(emit), up to the 7e-8 of Q's single-precision
+    entries), is symplectic to the same level, and carries mat_eigen's phase: each mode's own-plane
+    row has N(2p, 2p) = 0 and N(2p, 2p+1) > 0. A sigma that is not positive definite is refused."""
+    S = np.zeros((6, 6))
+    for k in range(3):
+        S[2 * k, 2 * k + 1], S[2 * k + 1, 2 * k] = 1.0, -1.0
+    for seed in range(5):
+        sig = _coupled_sigma(100 + seed)
+        emit, N = lib.sigma_normal_form(sig)
+        n_inv = np.linalg.inv(N)
+        D = n_inv @ sig @ n_inv.T
+        assert np.allclose(np.diag(D), np.repeat(emit, 2), rtol=2e-7, atol=0)
+        off = D - np.diag(np.diag(D))
+        assert np.max(np.abs(off)) < 1e-9 * np.max(emit)
+        assert np.max(np.abs(N.T @ S @ N + S)) < 2e-7       # N^T S N = -S in this convention
+        for pl in range(3):
+            assert abs(N[2 * pl, 2 * pl]) < 1e-12 * np.max(np.abs(N))
+            assert N[2 * pl, 2 * pl + 1] > 0
+    bad = np.eye(6)
+    bad[0, 0] = -1.0
+    with pytest.raises(lib.BmadGpuError):
+        lib.sigma_normal_form(bad)

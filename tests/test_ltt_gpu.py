@@ -7,7 +7,9 @@
     printed precision (es14.6 / es16.8), and the reference's column layout;
   - the stop conditions: with dead_cutoff, tracking ends at the first turn where the lost count
     reaches nint(dead_cutoff * n), as the reference's turn loop does, and no output is written for
-    that turn."""
+    that turn;
+  - core emittances (combined and per mode), the action-angle files and the per-particle files
+    against the restatement on the oracle's tracking."""
 import glob
 import importlib
 import os
@@ -18,7 +20,7 @@ import torch
 
 from conftest import load_abi
 from helpers import oracle_track
-from ltt_reference import bunch_data, core_emit, read_table
+from ltt_reference import action_angle, bunch_data, core_emit, read_table
 
 pytestmark = pytest.mark.gpu
 lib = importlib.import_module("bmad-ecosystem_b200.lib")
@@ -194,3 +196,89 @@ def test_ltt_core_columns_follow_the_cutoff_list(ctx, tmp_path):
             o = oracle_track(eles, p, vec, 4, t=np.zeros(3000))
             close([float(x) for x in rows[-1][15:18]], core_emit(o["vec"], o["t"], o["state"], p.p0c, p.mass, 0.9),
                   2e-6, "90 % core")
+
+
+@pytest.mark.parametrize("cutoff", [0.5, 0.9])
+def test_core_emittance_per_mode_matches_reference(ctx, cutoff):
+    """The per-mode core calculation (core_emit_combined_calc = F): each mode's core ranked by that
+    mode's action with N^-1 of the bunch and then of the core, against the numpy restatement."""
+    eles, p = rings.ring(50)
+    vec = rings.matched_gaussian(eles, 20000, seed=23, scale=3.0)
+    hb = lib.HostBunch.from_vec(vec, p, t=np.zeros(20000))
+    lat = lib.Lattice(ctx, eles, p)
+    lib.track_bunch(ctx, lat, hb, n_turns=5)
+    hb.state[::89] = abi.LOST_NEG_Y
+    dev = torch.device("cuda", 0)
+    t = {k: torch.from_numpy(np.array(getattr(hb, k))).to(dev) for k in ("vec", "beta", "t", "state")}
+    view = abi.Bunch(hb.n, t["vec"].data_ptr(), t["beta"].data_ptr(), t["t"].data_ptr(), t["state"].data_ptr(),
+                     None, None, None)
+    got = lib.bunch_core_emit(ctx, lat, view, cutoff, combined_calc=False)
+    want = core_emit(hb.vec, hb.t, hb.state, p.p0c, p.mass, cutoff, combined=False)
+    assert np.all(want > 0)
+    assert np.allclose(got, want, rtol=1e-9, atol=0), (got, want)
+    combined = lib.bunch_core_emit(ctx, lat, view, cutoff, combined_calc=True)
+    assert not np.allclose(got, combined, rtol=1e-6, atol=0)       # a different calculation
+
+
+def test_ltt_action_angle_and_per_particle_files(ctx, tmp_path):
+    eles, p = rings.ring(50)
+    n, n_turns = 600, 10
+    vec = rings.matched_gaussian(eles, n, seed=8, scale=5.0)
+    hb = lib.HostBunch.from_vec(vec, p, t=np.zeros(n))
+    lat = lib.Lattice(ctx, eles, p)
+    base = str(tmp_path / "run")
+    done = lib.ltt_run(ctx, lat, hb, n_turns, averages_file=base, averages_every_n_turns=5,
+                       particle_every_n_turns=5, only_live_particles_out=False,
+                       action_angle_file=str(tmp_path / "aa#.dat"), per_particle_file=str(tmp_path / "pp"),
+                       core_emit_combined_calc=False)
+    assert done == n_turns
+    files = sorted(os.path.basename(f) for f in glob.glob(str(tmp_path / "aa*.dat")))
+    assert files == ["aa00.dat", "aa05.dat", "aa10.dat"]
+    head = [line for line in open(str(tmp_path / "aa05.dat")) if line.startswith("##")][-1]
+    assert head.split()[4:10] == ["Ja", "Angle_a", "Jb", "Angle_b", "Jc", "Angle_c"]
+    states = {}
+    for T in (0, 5, 10):
+        o = oracle_track(eles, p, vec, T, t=np.zeros(n)) if T > 0 else dict(
+            vec=vec, t=np.zeros(n), state=np.ones(n, np.int32))
+        states[T] = o
+        rows = read_table(str(tmp_path / ("aa%02d.dat" % T)))
+        assert [int(r[0]) for r in rows] == list(range(1, n + 1))   # dead particles too
+        got = np.array([[float(x) for x in r[2:8]] for r in rows]).T
+        want = action_angle(o["vec"], o["t"], o["state"], p.p0c, p.mass)
+        for m in range(3):
+            # printed to 9 digits; a particle with a tiny action in one mode sees the rounding of
+            # N^-1 leak in from the larger modes, hence the absolute floor and the scaled angle bound
+            J, Jw = got[2 * m], want[2 * m]
+            assert np.all(np.abs(J - Jw) <= 1e-7 * np.abs(Jw) + 1e-9 * np.max(Jw)), ("J", m, T)
+            dphi = np.abs(got[2 * m + 1] - want[2 * m + 1])
+            tol = 1e-7 * np.maximum(1.0, np.sqrt(np.median(Jw) / np.maximum(Jw, 1e-300)))
+            assert np.all(np.minimum(dphi, 2 * np.pi - dphi) <= tol), ("angle", m, T)
+        names = [r[-1] for r in rows]
+        assert names.count("Alive") == int(np.sum(o["state"] == abi.ALIVE))
+    # the per-mode core emittances reached the .emit file
+    emi = read_table(base + ".emit")
+    o = states[10]
+    close([float(x) for x in emi[-1][12:15]],
+          core_emit(o["vec"], o["t"], o["state"], p.p0c, p.mass, 0.5, combined=False), 2e-6, "per-mode core")
+    # per-particle files: pp.001 .. pp.600, a header and one line per output turn
+    pp = sorted(glob.glob(str(tmp_path / "pp.*")))
+    assert len(pp) == n and os.path.basename(pp[0]) == "pp.001" and os.path.basename(pp[-1]) == "pp.600"
+    for ip in (1, 77, 600):
+        lines = open(str(tmp_path / ("pp.%03d" % ip))).read().splitlines()
+        assert "# ix_particle     = %d" % ip in lines
+        rows = [ln.split() for ln in lines if not ln.startswith("#")]
+        assert [int(r[0]) for r in rows] == [0, 5, 10]
+        for r, T in zip(rows, (0, 5, 10)):
+            want = states[T]["vec"][:, ip - 1]
+            got = np.array([float(x) for x in r[1:7]])
+            assert np.all(np.abs(got - want) <= 1e-8 * np.abs(want) + 1e-300), (ip, T, got, want)
+            assert float(r[8]) == pytest.approx(p.p0c, rel=1e-8)
+
+
+def test_per_particle_output_refuses_large_bunches(ctx, tmp_path):
+    eles, p = rings.ring(50)
+    vec = rings.matched_gaussian(eles, 1001, seed=1)
+    hb = lib.HostBunch.from_vec(vec, p)
+    lat = lib.Lattice(ctx, eles, p)
+    with pytest.raises(lib.BmadGpuError):
+        lib.ltt_run(ctx, lat, hb, 2, per_particle_file=str(tmp_path / "pp"))
