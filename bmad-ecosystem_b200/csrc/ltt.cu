@@ -659,14 +659,19 @@ int core_emittance(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bun
   return BMADGPU_OK;
 }
 
-// Action and angle of every particle of a device bunch about its own normal form (zero where the
-// reference's eigen-analysis fails) into the host arrays aa [6][n].
-int action_angle(bmadgpu_ctx* c, const bmadgpu_bunch& d, const bmadgpu_bunch_data& bd, double* d_aa, double* aa) {
+// Action and angle of every particle of a device bunch into the host arrays aa [6][n]: about the
+// bunch's own normal form and centroid (zero where the reference's eigen-analysis fails), or, with
+// n_inv given (the one-turn matrix's N^-1), about zero.
+int action_angle(bmadgpu_ctx* c, const bmadgpu_bunch& d, const bmadgpu_bunch_data& bd, const double* n_inv,
+                 double* d_aa, double* aa) {
   CoreArgs A;
-  if (!normal_form_inverse(bd, A.w))
+  if (n_inv) {
+    for (int k = 0; k < 36; k++) A.w[k] = n_inv[k];
+  } else if (!normal_form_inverse(bd, A.w)) {
     for (int k = 0; k < 36; k++) A.w[k] = 0;
+  }
   for (int k = 0; k < 6; k++) {
-    A.c[k] = bd.n_live > 0 ? bd.centroid[k] : 0.0;
+    A.c[k] = (!n_inv && bd.n_live > 0) ? bd.centroid[k] : 0.0;
     A.wgt[k] = 0;
   }
   const int64_t n = d.n;
@@ -852,11 +857,12 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
     }
     if (!aa_base.empty()) {
       bmadgpu_bunch_data bd;
-      int r = device_stats(c, lat, cur.b, d_scratch, &bd);
+      std::memset(&bd, 0, sizeof bd);
+      int r = P->action_angle_n_inv ? BMADGPU_OK : device_stats(c, lat, cur.b, d_scratch, &bd);
       if (r) return r;
       haa.resize(6 * n);
       hstate.resize(n);
-      if ((r = action_angle(c, cur.b, bd, d_aa, haa.data()))) return r;
+      if ((r = action_angle(c, cur.b, bd, P->action_angle_n_inv, d_aa, haa.data()))) return r;
       CUDA_TRY(cudaMemcpyAsync(hstate.data(), cur.b.state, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
       CUDA_TRY(cudaStreamSynchronize(s));
       if (!write_action_angle(aa_base, turn, P->n_turns, haa.data(), hstate.data(), n,

@@ -618,7 +618,8 @@ class LttParams(C.Structure):
                 ("ix_turn_start", C.c_int32), ("beam_every_n_turns", C.c_int32), ("beam_exact", C.c_int32),
                 ("dead_cutoff", C.c_double), ("averages_file", C.c_char_p), ("phase_space_file", C.c_char_p),
                 ("beam_file", C.c_char_p), ("core_emit_cutoff", C.c_double * 8), ("core_emit_per_mode", C.c_int32),
-                ("action_angle_file", C.c_char_p), ("per_particle_file", C.c_char_p)]
+                ("action_angle_file", C.c_char_p), ("per_particle_file", C.c_char_p),
+                ("action_angle_n_inv", C.POINTER(C.c_double))]
 
 
 def _ltt_sigs(lib):
@@ -676,11 +677,14 @@ def bunch_stats(ctx, lat, device_view):
 def ltt_run(ctx, lat, bunch, n_turns, averages_file=None, phase_space_file=None, averages_every_n_turns=-1,
             particle_every_n_turns=-1, output_only_last_turns=0, only_live_particles_out=True, dead_cutoff=1.0,
             beam_file=None, beam_every_n_turns=-1, beam_exact=False, ix_turn_start=0, core_emit_cutoff=None,
-            core_emit_combined_calc=True, action_angle_file=None, per_particle_file=None):
+            core_emit_combined_calc=True, action_angle_file=None, per_particle_file=None,
+            action_angle_calc_uses_1turn_matrix=False):
     """long_term_tracking's beam mode for a HostBunch (updated in place); returns the turn reached.
     core_emit_cutoff: list of core fractions for the .emit file (None: the reference's [0.5];
     []: no core columns); core_emit_combined_calc False: a core per normal mode.
-    action_angle_file / per_particle_file: the reference's action-angle and per-particle outputs."""
+    action_angle_file / per_particle_file: the reference's action-angle and per-particle outputs;
+    action_angle_calc_uses_1turn_matrix: actions from make_N of the one-turn matrix about the
+    closed orbit (RF on), as the reference's option does, instead of the bunch's normal form."""
     lib = _ltt_sigs(load())
     p = LttParams(n_turns, averages_every_n_turns, particle_every_n_turns, output_only_last_turns,
                   1 if only_live_particles_out else 0, ix_turn_start, beam_every_n_turns, 1 if beam_exact else 0,
@@ -693,6 +697,14 @@ def ltt_run(ctx, lat, bunch, n_turns, averages_file=None, phase_space_file=None,
     p.core_emit_per_mode = 0 if core_emit_combined_calc else 1
     p.action_angle_file = action_angle_file.encode() if action_angle_file else None
     p.per_particle_file = per_particle_file.encode() if per_particle_file else None
+    n_inv = None
+    if action_angle_file and action_angle_calc_uses_1turn_matrix:
+        orbit = closed_orbit(ctx, lat)[0]
+        t6 = one_turn_matrix(ctx, lat, orbit, rf_on=True)[0]
+        if np.all(t6[0:5, 5] == 0):
+            raise BmadGpuError(abi.EINVAL, "action_angle_calc_uses_1turn_matrix needs the RF on")
+        n_inv = np.ascontiguousarray(np.linalg.inv(make_n(t6)).ravel())
+        p.action_angle_n_inv = n_inv.ctypes.data_as(C.POINTER(C.c_double))
     done = C.c_int32()
     v = bunch.view()
     check(lib.bmadgpu_ltt_run(ctx.handle, lat.handle, C.byref(v), C.byref(p), C.byref(done)))
@@ -942,6 +954,62 @@ def mat_eigen(mat):
         vals[j], vals[j + 1] = l1, l2
         vecs[j], vecs[j + 1] = sgn * e1, np.conj(sgn) * e2
     return vals, vecs
+
+
+def make_n(t6):
+    """N of make_N (bmad/modules/mode3_mod.f90:825-912) for a one-turn matrix with three stable
+    modes, ordered by plane dominance: eigen_decomp_6mat (:449-529; LAPACK geev through
+    numpy.linalg.eig, evec(:, 2k-1) = VR(2k-1) + i VR(2k) and its conjugate, each pair conjugated
+    if Im(evec^T S evec)(2k-1, 2k) < 0), order_evecs_by_plane_dominance (:661-687),
+    normalize_evecs (:1129-1154), N = Re(evec) Qr - Im(evec) Qi with m = 1/sqrt(2), and the
+    rotations that make N(1,2), N(3,4), N(5,6) zero (MyTan, :533-544)."""
+    m6 = np.asarray(t6, float)
+    w, v = np.linalg.eig(m6)
+    S = np.zeros((6, 6))
+    for k in range(3):
+        S[2 * k, 2 * k + 1], S[2 * k + 1, 2 * k] = 1.0, -1.0
+    evec = np.zeros((6, 6), complex)
+    ev = np.zeros(6, complex)
+    for k in (0, 2, 4):
+        if w[k].imag <= 0:
+            raise BmadGpuError(abi.EINVAL, "make_N: the one-turn matrix has an unstable mode")
+        evec[:, k], evec[:, k + 1] = v[:, k], np.conj(v[:, k])
+        ev[k], ev[k + 1] = w[k], np.conj(w[k])
+    check_mat = evec.T @ S @ evec
+    for k in (0, 2, 4):
+        if check_mat[k, k + 1].imag < 0:
+            evec[:, k:k + 2] = np.conj(evec[:, k:k + 2])
+            ev[k:k + 2] = np.conj(ev[k:k + 2])
+    pair1 = int(np.argmax(np.abs(evec[0, [0, 2, 4]].real)))
+    vec = np.abs(evec[2, [0, 2, 4]].real)
+    vec[pair1] = -1
+    pair2 = int(np.argmax(vec))
+    pair3 = 3 - pair1 - pair2
+    idx = [2 * pair1, 2 * pair1 + 1, 2 * pair2, 2 * pair2 + 1, 2 * pair3, 2 * pair3 + 1]
+    evec = evec[:, idx]
+    mat = np.conj(evec).T @ S @ evec
+    norms = [math.sqrt(abs(mat[k, k])) for k in (0, 2, 4)]
+    if min(norms) == 0:
+        raise BmadGpuError(abi.EINVAL, "make_N: cannot normalise the eigenvectors (is the RF off?)")
+    for j, k in enumerate((0, 2, 4)):
+        evec[:, k:k + 2] = evec[:, k:k + 2] / norms[j]
+    mq = 1.0 / math.sqrt(2.0)
+    Qr, Qi = np.zeros((6, 6)), np.zeros((6, 6))
+    for k in (0, 2, 4):
+        Qr[k, k] = Qr[k + 1, k] = mq
+        Qi[k, k + 1], Qi[k + 1, k + 1] = mq, -mq
+    N = evec.real @ Qr - evec.imag @ Qi
+
+    def my_tan(y, x):
+        a = math.atan2(y, x)
+        return a if y >= 0 else a + 2.0 * math.pi
+
+    R = np.zeros((6, 6))
+    for k in (0, 2, 4):
+        th = my_tan(N[k, k + 1], N[k, k])
+        c, s_ = math.cos(th), math.sin(th)
+        R[k:k + 2, k:k + 2] = [[c, -s_], [s_, c]]
+    return N @ R
 
 
 def fma_normalization(mat6):

@@ -451,6 +451,11 @@ typedef struct bmadgpu_ltt_params {
                                        normal form (calc_bunch_params' n_mat) */
   const char* per_particle_file;    /* ltt%per_particle_output_file: NULL or "": none; one file per
                                        particle (at most 1000 particles, as the reference requires) */
+  const double* action_angle_n_inv; /* [36] row-major or NULL: with ltt%action_angle_calc_uses_1turn_matrix
+                                       the caller's N^-1 of the one-turn matrix (make_N,
+                                       bmad/modules/mode3_mod.f90:825-912, then mat_inverse); the
+                                       actions are then taken about zero, as the reference's
+                                       write_this_data does (lt_tracking_mod.f90:2007-2022) */
 } bmadgpu_ltt_params;
 int bmadgpu_ltt_run(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* host_bunch,
                     const bmadgpu_ltt_params* params, int32_t* turns_done);

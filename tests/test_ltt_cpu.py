@@ -137,3 +137,36 @@ def test_sigma_normal_form_structure():
     bad[0, 0] = -1.0
     with pytest.raises(lib.BmadGpuError):
         lib.sigma_normal_form(bad)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_make_n_normal_form_of_a_one_turn_matrix(seed):
+    """lib.make_n (make_N of mode3_mod) on a stable coupled one-turn matrix t6 = A B R B^-1 A^-1
+    with planted tunes: N^-1 t6 N is three rotation blocks with those tunes, N is symplectic, and
+    its phase convention holds (N(1,2) = N(3,4) = N(5,6) = 0 with positive diagonal partners)."""
+    import scipy.linalg
+    rng = np.random.default_rng(seed)
+    S = np.zeros((6, 6))
+    for k in range(3):
+        S[2 * k, 2 * k + 1], S[2 * k + 1, 2 * k] = 1.0, -1.0
+    H = rng.normal(size=(6, 6))
+    A = scipy.linalg.expm(S @ (0.15 * (H + H.T)))
+    tunes = np.array([0.22, 0.31, 0.013]) + 0.02 * rng.random(3)
+    R = np.zeros((6, 6))
+    for k in range(3):
+        c, s = np.cos(2 * np.pi * tunes[k]), np.sin(2 * np.pi * tunes[k])
+        R[2 * k:2 * k + 2, 2 * k:2 * k + 2] = [[c, s], [-s, c]]
+    B = np.diag([3.0, 1 / 3.0, 2.0, 0.5, 10.0, 0.1])
+    t6 = A @ B @ R @ np.linalg.inv(B) @ np.linalg.inv(A)
+    N = lib.make_n(t6)
+    U = np.linalg.inv(N) @ t6 @ N
+    for k in range(3):
+        blk = U[2 * k:2 * k + 2, 2 * k:2 * k + 2]
+        assert np.allclose(blk, R[2 * k:2 * k + 2, 2 * k:2 * k + 2], atol=1e-10)
+    off = U.copy()
+    for k in range(3):
+        off[2 * k:2 * k + 2, 2 * k:2 * k + 2] = 0
+    assert np.max(np.abs(off)) < 1e-10
+    assert np.allclose(N.T @ S @ N, S, atol=1e-10)
+    for k in range(3):
+        assert abs(N[2 * k, 2 * k + 1]) < 1e-12 * np.max(np.abs(N)) and N[2 * k, 2 * k] > 0

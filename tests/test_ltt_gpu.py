@@ -282,3 +282,34 @@ def test_per_particle_output_refuses_large_bunches(ctx, tmp_path):
     lat = lib.Lattice(ctx, eles, p)
     with pytest.raises(lib.BmadGpuError):
         lib.ltt_run(ctx, lat, hb, 2, per_particle_file=str(tmp_path / "pp"))
+
+
+def test_ltt_action_angle_from_the_one_turn_matrix(ctx, tmp_path):
+    """action_angle_calc_uses_1turn_matrix: actions about zero with N^-1 of make_N on the one-turn
+    matrix at the closed orbit. The file holds N^-1 p of the oracle's particles, and for small
+    amplitudes the actions are turn-by-turn invariants (the normal form is right)."""
+    eles, p = rings.ring(50)
+    n, n_turns = 400, 10
+    lat = lib.Lattice(ctx, eles, p)
+    orbit = lib.closed_orbit(ctx, lat)[0]
+    vec = rings.matched_gaussian(eles, n, seed=12, scale=0.5) + orbit[:, None]
+    hb = lib.HostBunch.from_vec(vec, p, t=np.zeros(n))
+    done = lib.ltt_run(ctx, lat, hb, n_turns, particle_every_n_turns=10, action_angle_file=str(tmp_path / "aa#"),
+                       action_angle_calc_uses_1turn_matrix=True)
+    assert done == n_turns
+    n_inv = np.linalg.inv(lib.make_n(lib.one_turn_matrix(ctx, lat, orbit, rf_on=True)[0]))
+    J = {}
+    for T in (0, 10):
+        o = oracle_track(eles, p, vec, T, t=np.zeros(n)) if T > 0 else dict(vec=vec, state=np.ones(n, np.int32))
+        rows = read_table(str(tmp_path / ("aa%02d" % T)))
+        got = np.array([[float(x) for x in r[2:8]] for r in rows]).T
+        j = n_inv @ o["vec"]
+        for m in range(3):
+            want = 0.5 * (j[2 * m] ** 2 + j[2 * m + 1] ** 2)
+            assert np.all(np.abs(got[2 * m] - want) <= 1e-7 * want + 1e-9 * np.max(want)), ("J", m, T)
+        J[T] = got[0::2]
+    # about zero, the closed orbit itself shows as a constant offset: compare the changes of J of
+    # the transverse modes over 10 turns with their spread; they are a small fraction of it
+    for m in range(2):
+        dJ = np.abs(J[10][m] - J[0][m])
+        assert np.median(dJ) < 0.05 * np.median(J[0][m]), m
