@@ -264,7 +264,7 @@ int bmadgpu_ctx_create(int32_t device, bmadgpu_ctx** out) {
   if (!c) return fail(BMADGPU_ENOMEM, "host allocation failed");
   c->device = device;
   c->sm_count = prop.multiProcessorCount;
-  c->tuning = bmadgpu_tuning{128, 0, 1, 0, 0, {0, 0, 0}};
+  c->tuning = bmadgpu_tuning{256, 2, 1, 0, 0, {0, 0, 0}};
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&c->d_err, sizeof(int32_t)) != cudaSuccess ||
       cudaMalloc(&c->d_nwork, 2 * sizeof(int64_t)) != cudaSuccess) {

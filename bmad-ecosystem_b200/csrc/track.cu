@@ -201,7 +201,6 @@ static const Variant kVariants[] = {
 
 cudaError_t launch_track(const TrackArgs& a, const LaunchCfg& cfg, int sm_count, cudaStream_t stream) {
   int stage = (cfg.stage_smem && table_fits_smem(a.table_bytes)) ? 1 : 0;
-  size_t smem = stage ? a.table_bytes : 0;
   // ctas_per_sm selects the register budget: the variant with the largest minimum CTA count
   // not above it (0: the most registers per thread)
   const Variant* v = nullptr;
@@ -212,9 +211,26 @@ cudaError_t launch_track(const TrackArgs& a, const LaunchCfg& cfg, int sm_count,
   }
   if (!v) return cudaErrorInvalidValue;
   const void* fn = v->fn;
-  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (err != cudaSuccess) return err;
   int per_sm = 0;
+  cudaError_t err;
+  if (stage) {
+    // Staging is taken only where it costs no residency: a table whose copy would leave room
+    // for fewer CTAs per SM than the registers allow (the multipole pool of a large ring can
+    // take most of the shared memory) is read through L1 instead, which measured ~2.8x faster
+    // on a 176 KB table than one staged CTA per SM.
+    int plain_sm = 0;
+    if ((err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 0)) != cudaSuccess) return err;
+    if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&plain_sm, fn, cfg.block, 0)) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.table_bytes)) !=
+        cudaSuccess)
+      return err;
+    if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, cfg.block, a.table_bytes)) != cudaSuccess)
+      return err;
+    if (per_sm < plain_sm) stage = 0;
+  }
+  const size_t smem = stage ? a.table_bytes : 0;
+  err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
   err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, cfg.block, smem);
   if (err != cudaSuccess) return err;
   if (per_sm < 1) per_sm = 1;
