@@ -27,6 +27,10 @@ Further workloads (one JSON line each, same keys):
             host memory; p50/p99 latency; beside it the plain kernel on a sample of the same jobs.
   adjoint   d(loss)/d(100 quadrupole k1, 100 sextupole k2) on the 50-cell ring, 4096 particles,
             256 turns, checkpoints every 16 turns; a step is one gradient.
+  kinds     the plain kernel's cost per element kind: lattices of 1800 copies of each kind of
+            ring200 (drift, quadrupole, exact bend with and without Hwang edges, sextupole with and
+            without b3..b10) and ring200 itself, 1,048,576 small-amplitude particles, one turn per
+            step at the context's default launch shape; ns per particle-element.
 
 Multi-GPU: one process per GPU (torchrun); each rank tracks its own bunch (particles never
 interact: weak scaling, no collective on the data path); the timing is the max over ranks.
@@ -614,6 +618,71 @@ def run_adjoint(args):
     print(json.dumps(out), flush=True)
 
 
+def run_kinds(args):
+    """ns per particle-element of the plain kernel for each element kind of ring200."""
+    import copy
+    import torch
+    lib = importlib.import_module(PKG + ".lib")
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    ctx = lib.Context(0)
+    n = args.particles or 1 << 20
+    eles200, p = rings.ring(200, fringe=True, multipole_sigma=1e-4)
+    plain, _ = rings.ring(200)
+    nofringe, _ = rings.ring(200, fringe=False)
+    cell = eles200[:9]
+    kinds = {"drift": [cell[0], cell[2]], "quadrupole": [cell[1], cell[6]], "sbend": [nofringe[3]],
+             "sbend_hwang_edges": [cell[3]], "sextupole": [plain[5], plain[7]],
+             "sextupole_b3_b10": [cell[5], cell[7]], "ring200": None}
+    # small amplitudes, so that few particles are lost in one pass through 1800 copies without
+    # focusing; still far above the 1e-9 bounds of the exact bend's near-zero-orbit branch
+    vec0 = rings.matched_gaussian(eles200, n, seed=1, scale=0.003)
+    pc = p.p0c * (1 + vec0[5])
+    beta0 = torch.from_numpy(pc / np.sqrt(pc * pc + p.mass * p.mass)).to(dev)
+    out, alive_end = {}, {}
+    clocks = ClockSampler(0)
+    for name, proto in kinds.items():
+        if proto is None:
+            eles = eles200
+        else:
+            eles = [copy.deepcopy(proto[i % len(proto)]) for i in range(1800)]
+            rings.set_ref_time(eles, p)
+        lat = lib.Lattice(ctx, eles, p)
+        init = {"vec": torch.from_numpy(np.ascontiguousarray(vec0)).to(dev), "beta": beta0,
+                "state": torch.ones(n, dtype=torch.int32, device=dev)}
+        t = {k: x.clone() for k, x in init.items()}
+        v = abi.Bunch(n, t["vec"].data_ptr(), t["beta"].data_ptr(), None, t["state"].data_ptr(), None, None, None)
+        run = lambda: lib.check(lib.load().bmadgpu_track_bunch_device(ctx.handle, lat.handle, ctypes.byref(v), 0,
+                                                                      lat.n_ele, 0, 1, None))
+
+        def reset():
+            # every pass starts from the initial bunch: a lattice of one kind has no focusing, and
+            # the sextupole kicks grow without bound over repeated passes
+            for k in t:
+                t[k].copy_(init[k])
+            torch.cuda.synchronize()
+        secs = []
+        for i in range(args.warmup + args.steps):
+            reset()
+            _flush_l2(dev)
+            sec = _timed(ctx, run)
+            if i >= args.warmup:
+                secs.append(sec)
+        s_min = min(secs)
+        out[name] = s_min / (n * len(eles)) * 1e9
+        alive_end[name] = int((t["state"] == abi.ALIVE).sum())
+    clk = clocks.stop()
+    line = {
+        "metric": "ns per particle-element (FP64 plain kernel, by element kind)", "value": out["ring200"],
+        "unit": "ns/particle-element", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": False, "dtype": "f64", "data": "synthetic (seeded matched Gaussian, 0.003 sigma)",
+        "config": {"workload": "kinds: 1800 copies of each element kind of ring200, %d particles, 1 turn per step, "
+                               "best of the steps, L2 flushed between steps" % n, "tuning": ctx.get_tuning()},
+        "kinds": out, "alive_end": alive_end, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -647,7 +716,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["ring200", "ring50", "batch256", "serve", "adjoint"], default="ring200")
+    ap.add_argument("--workload", choices=["ring200", "ring50", "batch256", "serve", "adjoint", "kinds"],
+                    default="ring200")
     ap.add_argument("--jobs", type=int, default=200, help="serve: number of jobs of the stream")
     ap.add_argument("--variants", type=int, default=256, help="batch256: number of lattice variants")
     ap.add_argument("--plain-sample", type=int, default=12, help="batch256/serve: variants/jobs timed on the plain path")
@@ -664,6 +734,8 @@ def main():
         run_serve(args)
     elif args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "kinds":
+        run_kinds(args)
     else:
         run_ours(args)
 

@@ -115,6 +115,10 @@ cudaError_t batch_resolve(const BatchLaunch& cfg, uint32_t smem_bytes, int sm_co
     if (cfg.ctas_per_sm > 0 && k.minb > cfg.ctas_per_sm) continue;
     if (!v || (cfg.ctas_per_sm > 0 ? k.minb > v->minb : k.minb < v->minb)) v = &k;
   }
+  // no variant compiled for so few CTAs per SM: the one with the most registers per thread
+  if (!v)
+    for (const Variant& k : kVariants)
+      if (k.block == cfg.block && (!v || k.minb < v->minb)) v = &k;
   if (!v || cfg.particles_per_thread < 1) return cudaErrorInvalidValue;
   cudaError_t err = cudaFuncSetAttribute(v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
   if (err != cudaSuccess) return err;

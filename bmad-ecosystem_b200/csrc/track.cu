@@ -209,6 +209,10 @@ cudaError_t launch_track(const TrackArgs& a, const LaunchCfg& cfg, int sm_count,
     if (cfg.ctas_per_sm > 0 && k.minb > cfg.ctas_per_sm) continue;
     if (!v || (cfg.ctas_per_sm > 0 ? k.minb > v->minb : k.minb < v->minb)) v = &k;
   }
+  // no variant compiled for so few CTAs per SM: the one with the most registers per thread
+  if (!v)
+    for (const Variant& k : kVariants)
+      if (k.block == cfg.block && (!v || k.minb < v->minb)) v = &k;
   if (!v) return cudaErrorInvalidValue;
   const void* fn = v->fn;
   int per_sm = 0;

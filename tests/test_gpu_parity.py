@@ -38,13 +38,14 @@ def ctx():
 
 
 def gpu_track(ctx, elements, param, vec, n_turns, moments=False, t=None, **tuning):
+    saved = ctx.get_tuning()
     if tuning:
         ctx.set_tuning(**tuning)
     lat = lib.Lattice(ctx, elements, param)
     b = lib.HostBunch.from_vec(vec, param, t=t)
     mom = lib.track_bunch(ctx, lat, b, n_turns=n_turns, moments=moments)
     if tuning:
-        ctx.set_tuning(block=128, ctas_per_sm=0, stage_smem=1, turns_per_launch=0, compact=0)
+        ctx.set_tuning(**saved)
     return dict(vec=b.vec, beta=b.beta, state=b.state, ix_ele=b.ix_ele, ix_turn=b.ix_turn, location=b.location,
                 t=b.t, moments=mom)
 
