@@ -18,9 +18,10 @@ BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b,
   if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
   const double b1 = b[0], length = b[1], step_len = b[2];
   const int n_step = h.n_step;
+  const bool b_from2 = h.flags & F_KICK_B_FROM2;
   for (int i = 0; i <= n_step; i++) {
     if (i > 0) quad_step(p, b1, length, step_len, G);
-    if (np) ab_kicks(p, (i == 0 || i == n_step) ? kh : kf, np);
+    if (np) ab_kicks(p, (i == 0 || i == n_step) ? kh : kf, np, b_from2);
   }
   if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
 }
@@ -35,9 +36,10 @@ BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b
   if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
   const double step_len = b[0];
   const int n_step = h.n_step;
+  const bool b_from2 = h.flags & F_KICK_B_FROM2;
   for (int i = 0; i <= n_step; i++) {
     if (i > 0) drift(p, step_len);
-    if (np) ab_kicks(p, (i == 0 || i == n_step) ? kh : kf, np);
+    if (np) ab_kicks(p, (i == 0 || i == n_step) ? kh : kf, np, b_from2);
   }
   if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
 }

@@ -296,6 +296,18 @@ void push_kicks(std::vector<double>& blk, const double* a, const double* b, int 
   }
 }
 
+// True if the two kick arrays starting at blk[off] (n_pole (b_n, a_n) pairs each, as the device
+// reads them) hold only normal multipoles from order 2 up: every a_n zero and b_0 = b_1 = 0.
+bool kicks_b_from2(const std::vector<double>& blk, size_t off, int n_pole) {
+  if (n_pole < 3) return false;
+  for (int arr = 0; arr < 2; arr++)
+    for (int n = 0; n < n_pole; n++) {
+      const double bn = blk[off + 2 * (arr * n_pole + n)], an = blk[off + 2 * (arr * n_pole + n) + 1];
+      if (an != 0 || (n < 2 && bn != 0)) return false;
+    }
+  return true;
+}
+
 }  // namespace
 
 void build_cmulti_tables(double cm[22][22], double cf[22][22]) {
@@ -432,6 +444,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
             h.n_pole = (uint8_t)(ix_mag_max + 1);
             push_kicks(blk, a, b, ix_mag_max + 1, r_step / 2);
             push_kicks(blk, a, b, ix_mag_max + 1, r_step);
+            if (kicks_b_from2(blk, 3, ix_mag_max + 1)) flags |= F_KICK_B_FROM2;
           }
           h.n_step = (uint16_t)(e.l == 0 ? 0 : n_step);
           if (has_misalign) misalign_block(tilt_tot);
@@ -450,6 +463,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
             h.n_pole = (uint8_t)(ix_mag_max + 1);
             push_kicks(blk, a, b, ix_mag_max + 1, r_step / 2);
             push_kicks(blk, a, b, ix_mag_max + 1, r_step);
+            if (kicks_b_from2(blk, 1, ix_mag_max + 1)) flags |= F_KICK_B_FROM2;
           }
           h.n_step = (uint16_t)n_step;
           if (has_misalign) misalign_block(tilt_tot);

@@ -290,6 +290,51 @@ BG_HD void ab_kick_sum_any(double x, double y, const double* __restrict__ c, int
   }
 }
 
+// The same sum when every a_n is zero and b_0 = b_1 = 0 (sextupole-like kicks): orders 2 .. NP-1
+// as one branch-free block, so the independent products of all orders can be interleaved. A zero
+// b_n here adds b_n f = +0 to a sum that is never -0, which is what the reference adds, so the
+// bits are those of ab_kick_sum.
+template <int NP>
+BG_HD void ab_kick_sum_b(double x, double y, const double* __restrict__ c, double& kx_tot, double& ky_tot) {
+  double xp[NP], yp[NP];
+  mexp_table<NP - 1>(x, xp);
+  mexp_table<NP - 1>(y, yp);
+  kx_tot = 0;
+  ky_tot = 0;
+#pragma unroll
+  for (int n = 2; n < NP; n++) {
+    const double b2 = c[2 * n];
+    double kx = 0, ky = 0;
+#pragma unroll
+    for (int m = 0; m <= n; m += 2) {
+      const double f = BG_CMULTI(n, m) * xp[n - m] * yp[m];
+      kx = kx + b2 * f;
+    }
+#pragma unroll
+    for (int m = 1; m <= n; m += 2) {
+      const double f = BG_CMULTI(n, m) * xp[n - m] * yp[m];
+      ky = ky + b2 * f;
+    }
+    kx_tot = kx_tot + kx;
+    ky_tot = ky_tot + ky;
+  }
+}
+
+BG_HD void ab_kick_dispatch_b(double x, double y, const double* __restrict__ c, int n_pole, double& kx, double& ky) {
+  switch (n_pole) {
+    case 3: ab_kick_sum_b<3>(x, y, c, kx, ky); break;
+    case 4: ab_kick_sum_b<4>(x, y, c, kx, ky); break;
+    case 5: ab_kick_sum_b<5>(x, y, c, kx, ky); break;
+    case 6: ab_kick_sum_b<6>(x, y, c, kx, ky); break;
+    case 7: ab_kick_sum_b<7>(x, y, c, kx, ky); break;
+    case 8: ab_kick_sum_b<8>(x, y, c, kx, ky); break;
+    case 9: ab_kick_sum_b<9>(x, y, c, kx, ky); break;
+    case 10: ab_kick_sum_b<10>(x, y, c, kx, ky); break;
+    case 11: ab_kick_sum_b<11>(x, y, c, kx, ky); break;
+    default: ab_kick_sum_any(x, y, c, n_pole, kx, ky); break;
+  }
+}
+
 BG_HD void ab_kick_dispatch(double x, double y, const double* __restrict__ c, int n_pole, double& kx, double& ky) {
   switch (n_pole) {
     case 1: ab_kick_sum<1>(x, y, c, kx, ky); break;
@@ -307,10 +352,14 @@ BG_HD void ab_kick_dispatch(double x, double y, const double* __restrict__ c, in
   }
 }
 
-// ab_multipole_kicks (multipole_mod.f90:82-121), magnetic, coefficients pre-scaled.
-BG_HD void ab_kicks(Particle& p, const double* __restrict__ c, int n_pole) {
+// ab_multipole_kicks (multipole_mod.f90:82-121), magnetic, coefficients pre-scaled; b_from2: the
+// element's kicks carry F_KICK_B_FROM2.
+BG_HD void ab_kicks(Particle& p, const double* __restrict__ c, int n_pole, bool b_from2 = false) {
   double kx_tot, ky_tot;
-  ab_kick_dispatch(p.x, p.y, c, n_pole, kx_tot, ky_tot);
+  if (b_from2)
+    ab_kick_dispatch_b(p.x, p.y, c, n_pole, kx_tot, ky_tot);
+  else
+    ab_kick_dispatch(p.x, p.y, c, n_pole, kx_tot, ky_tot);
   p.px = p.px + kx_tot;
   p.py = p.py + ky_tot;
 }

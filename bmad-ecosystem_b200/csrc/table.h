@@ -37,7 +37,8 @@ enum Flag : uint16_t {
   F_REF_ORB_N0 = 1 << 8,   // thin multipole: n = 0 as a zero-length bend (MAD convention)
   F_BEND_DRIFT = 1 << 9,   // sbend with g == 0 and dg == 0 or zero step: drift body
   F_ZERO_LEN = 1 << 10,    // element length is zero
-  F_TILT = 1 << 11         // misalign block carries a non-zero tilt rotation
+  F_TILT = 1 << 11,        // misalign block carries a non-zero tilt rotation
+  F_KICK_B_FROM2 = 1 << 12 // both kick arrays: every a_n zero and b_0 = b_1 = 0, at least 3 orders
 };
 
 struct EleHdr {            // 16 bytes
