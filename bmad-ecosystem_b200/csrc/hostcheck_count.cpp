@@ -62,6 +62,7 @@ inline CD atan2(CD a, CD b) { g_ops.trans++; return CD(std::atan2(a.v, b.v)); }
 inline CD sinh(CD a) { g_ops.trans++; return CD(std::sinh(a.v)); }
 inline CD cosh(CD a) { g_ops.trans++; return CD(std::cosh(a.v)); }
 inline CD fmod(CD a, CD b) { g_ops.trans++; return CD(std::fmod(a.v, b.v)); }
+inline CD floor(CD a) { g_ops.trans++; return CD(std::floor(a.v)); }
 inline CD fma(CD a, CD b, CD c) { g_ops.trans++; return CD(std::fma(a.v, b.v, c.v)); }
 double h_cmulti_raw[22][22];
 double h_cfull_raw[22][22];

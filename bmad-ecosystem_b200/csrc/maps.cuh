@@ -672,9 +672,24 @@ BG_HD double modulo2(double x, double amp) {
 BG_HD double rf_phase(const Particle& p, double phi0, double f, double twopi_mp) {
   double time = -p.z / (p.beta * kCLight);
   double amp = 0.5 / f;
-  if (!(fabs(time) < amp)) time = modulo2(time, amp);   // qp fold; identity for |t| < 1/(2f)
+  double t_lo = 0;
+  if (!(fabs(time) < amp)) {
+    // Outside half an RF period the reference folds t into [-amp, amp) with amp = 0.5_qp/f in
+    // real(qp), where t - k 2 amp is exact. Kept here as t + t_lo, with amp carried as
+    // amp + amp_lo (the residual 0.5 - amp f is exact by fma).
+    const double amp_lo = fma(-amp, f, 0.5) / f;
+    const double k = floor((time + amp) / (2 * amp));
+    const double ph = k * (2 * amp);
+    const double pl = fma(k, 2 * amp, -ph);          // k 2 amp = ph + pl exactly
+    const double s = time - ph;                      // two-sum of time and -ph
+    const double sb = s - time;
+    const double e = (time - (s - sb)) + (-ph - sb);
+    const double lo = e - pl - k * (2 * amp_lo);
+    time = s + lo;
+    t_lo = lo - (time - s);
+  }
   double pr = time * f;
-  double pe = fma(time, f, -pr);
+  double pe = fma(time, f, -pr) + t_lo * f;
   double s = phi0 - pr;
   double bb = s - phi0;
   double err = (phi0 - (s - bb)) + (-pr - bb);

@@ -99,3 +99,55 @@ def test_noise_envelope_is_ulp_scale_after_one_turn():
     z = noise_track(eles, p, vec, 1)
     e = per_particle_err(z["vec"], o["vec"])
     assert 0 < e.max() < 2e-11
+
+
+@pytest.mark.parametrize("case", ["zero_middle_orders", "skew_order", "octupole_b6"])
+def test_multipole_kick_forms_bit_exact_on_host(hc, case):
+    """Sextupoles and octupoles whose kicks take the branch-free normal-multipole form (every a_n
+    zero, b_0 = b_1 = 0), with exactly zero orders in the middle of the range, and one with a skew
+    order (the general form) stay bit-identical to the oracle over several turns."""
+    eles, p = rings.ring(30)
+    rng = np.random.default_rng(7)
+    for e in eles:
+        if e.key != abi.SEXTUPOLE:
+            continue
+        if case == "zero_middle_orders":
+            poles = {n: float(rng.normal(0, 1e-3)) for n in (3, 4, 6, 9)}   # b5, b7, b8 exactly zero
+            for n, v in poles.items():
+                e.b_pole[n] = v
+        elif case == "skew_order":
+            e.b_pole[4] = 2e-4
+            e.a_pole[5] = -3e-4
+        else:
+            e.key = abi.OCTUPOLE
+            e.k3 = 50.0
+            e.k2 = 0.0
+            e.b_pole[6] = 1e-3
+    vec = rings.matched_gaussian(eles, 300, seed=2, scale=6.0)
+    o = oracle_track(eles, p, vec, 4)
+    h = host_track(hc, eles, p, vec, 4)
+    alive = o["state"] == abi.ALIVE
+    assert 0 < alive.sum() < 300           # some losses, some survivors
+    assert np.array_equal(h["vec"][:, alive], o["vec"][:, alive])
+    for k in ("state", "ix_ele", "ix_turn"):
+        assert np.array_equal(h[k], o[k]), k
+
+
+def test_rf_phase_fold_outside_the_bucket_bit_exact_on_host(hc):
+    """Particles beyond half an RF wavelength: the reference folds the RF time with modulo2 in
+    real(qp) (particle_rf_time.f90:115), where t - k 2 amp is exact; the device carries the folded
+    time in double-double and must give the same pz bits as the oracle's __float128 path."""
+    cav = rings.rf_cavity()
+    drift = abi.default_element(abi.DRIFT, l=0.5)
+    eles = rings.set_ref_time([cav, drift, cav], rings.ring(1)[1])
+    p = rings.ring(1)[1]
+    rng = np.random.default_rng(3)
+    n = 4000
+    vec = np.zeros((6, n))
+    vec[4] = rng.uniform(-0.9, 0.9, n)          # half wavelength at 500 MHz: 0.30 m
+    vec[5] = rng.normal(0, 1e-3, n)
+    o = oracle_track(eles, p, vec, 2)
+    h = host_track(hc, eles, p, vec, 2)
+    assert np.sum(np.abs(vec[4]) > 0.3) > n // 2
+    for k in ("vec", "beta", "state"):
+        assert np.array_equal(h[k], o[k]), k
