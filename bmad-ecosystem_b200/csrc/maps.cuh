@@ -455,6 +455,18 @@ BG_HD void offset_unset(Particle& p, const double* __restrict__ m, bool has_tilt
 
 // quad_mat2_calc, bmad/low_level/quad_mat2_calc.f90:22-61 (mat2 and z_coef)
 // ef = RN(1 / rel_p), shared by the quotients by rel_p and 2 rel_p.
+// The part of quad_mat2_calc after cx, sx (quad_mat2_calc.f90:49-61).
+BG_HD void quad_mat2_tail(double k1, double length, double rel_p, double ef, double cx, double sx, double& m11,
+                          double& m12, double& m21, double& m22, double& z0, double& z1, double& z2) {
+  m11 = cx;
+  m12 = div_rcp(sx, rel_p, ef);
+  m21 = k1 * sx * rel_p;
+  m22 = cx;
+  z0 = k1 * (-cx * sx + length) / 4;
+  z1 = div_rcp(-k1 * (sx * sx), 2 * rel_p, half_rcp(ef));
+  z2 = -(cx * sx + length) / (4 * (rel_p * rel_p));
+}
+
 BG_HD void quad_mat2(double k1, double length, double rel_p, double ef, double& m11, double& m12, double& m21,
                      double& m22, double& z0, double& z1, double& z2) {
   double sqrt_k = sqrt(fabs(k1));
@@ -471,13 +483,34 @@ BG_HD void quad_mat2(double k1, double length, double rel_p, double ef, double& 
     cx = cosh(sk_l);
     sx = sinh(sk_l) / sqrt_k;
   }
-  m11 = cx;
-  m12 = div_rcp(sx, rel_p, ef);
-  m21 = k1 * sx * rel_p;
-  m22 = cx;
-  z0 = k1 * (-cx * sx + length) / 4;
-  z1 = div_rcp(-k1 * (sx * sx), 2 * rel_p, half_rcp(ef));
-  z2 = -(cx * sx + length) / (4 * (rel_p * rel_p));
+  quad_mat2_tail(k1, length, rel_p, ef, cx, sx, m11, m12, m21, m22, z0, z1, z2);
+}
+
+// Both planes of a quadrupole step, x with -k1 and y with k1, as two quad_mat2 calls give them.
+// One plane takes cos/sin and the other cosh/sinh of the same sqrt(|k1|) L; evaluating the four
+// in one block, with the planes picked by the reference's sign tests, lets the two independent
+// chains interleave. The calls and their arguments are those of quad_mat2, so are the bits.
+BG_HD void quad_mat2_xy(double k1, double length, double rel_p, double ef, double* mx, double* my) {
+  const double sqrt_k = sqrt(fabs(k1));
+  const double sk_l = sqrt_k * length;
+  double cxx, sxx, cxy, sxy;
+  if (fabs(sk_l) < 1e-10) {
+    const double kl2x = -k1 * (length * length), kl2y = k1 * (length * length);
+    cxx = 1 + kl2x / 2;
+    sxx = (1 + div_rcp(kl2x, 6, kRcp6)) * length;
+    cxy = 1 + kl2y / 2;
+    sxy = (1 + div_rcp(kl2y, 6, kRcp6)) * length;
+  } else {
+    const double c_t = cos(sk_l), s_t = sin(sk_l) / sqrt_k;
+    const double c_h = cosh(sk_l), s_h = sinh(sk_l) / sqrt_k;
+    const bool x_trig = -k1 < 0, y_trig = k1 < 0;
+    cxx = x_trig ? c_t : c_h;
+    sxx = x_trig ? s_t : s_h;
+    cxy = y_trig ? c_t : c_h;
+    sxy = y_trig ? s_t : s_h;
+  }
+  quad_mat2_tail(-k1, length, rel_p, ef, cxx, sxx, mx[0], mx[1], mx[2], mx[3], mx[4], mx[5], mx[6]);
+  quad_mat2_tail(k1, length, rel_p, ef, cxy, sxy, my[0], my[1], my[2], my[3], my[4], my[5], my[6]);
 }
 
 // One body step of track_a_quadrupole (track_a_quadrupole.f90:95-120); b1 and length are the
@@ -485,9 +518,10 @@ BG_HD void quad_mat2(double k1, double length, double rel_p, double ef, double& 
 BG_HD void quad_step(Particle& p, double b1, double length, double step_len, const Globals& G) {
   double rel_p = 1 + p.pz;
   double k1 = b1 / (length * rel_p);
-  double ax, bx, cx_, dx, zx0, zx1, zx2, ay, by, cy, dy, zy0, zy1, zy2;
-  quad_mat2(-k1, step_len, rel_p, p.e_factor, ax, bx, cx_, dx, zx0, zx1, zx2);
-  quad_mat2(k1, step_len, rel_p, p.e_factor, ay, by, cy, dy, zy0, zy1, zy2);
+  double mx[7], my[7];
+  quad_mat2_xy(k1, step_len, rel_p, p.e_factor, mx, my);
+  const double ax = mx[0], bx = mx[1], cx_ = mx[2], dx = mx[3], zx0 = mx[4], zx1 = mx[5], zx2 = mx[6];
+  const double ay = my[0], by = my[1], cy = my[2], dy = my[3], zy0 = my[4], zy1 = my[5], zy2 = my[6];
   double x = p.x, px = p.px, y = p.y, py = p.py;
   p.z = p.z + (zx0 * (x * x) + zx1 * x * px + zx2 * (px * px) + zy0 * (y * y) + zy1 * y * py + zy2 * (py * py));
   p.x = (0 + ax * x) + bx * px;
