@@ -170,3 +170,20 @@ def test_make_n_normal_form_of_a_one_turn_matrix(seed):
     assert np.allclose(N.T @ S @ N, S, atol=1e-10)
     for k in range(3):
         assert abs(N[2 * k, 2 * k + 1]) < 1e-12 * np.max(np.abs(N)) and N[2 * k, 2 * k] > 0
+
+
+def test_sigma_normal_form_without_longitudinal_spread():
+    """dim 4 (zero z and pz spread, as calc_emittances_and_twiss_from_sigma_matrix decides it): the
+    transverse modes as in 6D, the c emittance zero, and N's longitudinal block the identity (the
+    reference leaves it unset)."""
+    from ltt_reference import normal_form_n
+    sig6 = _coupled_sigma(3)
+    sig = sig6.copy()
+    sig[4:, :] = 0
+    sig[:, 4:] = 0
+    emit, N = lib.sigma_normal_form(sig)
+    assert emit[2] == 0 and emit[0] > 0 and emit[1] > 0
+    assert np.array_equal(N[4:, 4:], np.eye(2)) and not np.any(N[4:, :4]) and not np.any(N[:4, 4:])
+    n_inv = np.linalg.inv(N[:4, :4])
+    D = n_inv @ sig[:4, :4] @ n_inv.T
+    assert np.allclose(np.diag(D), np.repeat(emit[:2], 2), rtol=2e-7, atol=0)
