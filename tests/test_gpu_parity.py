@@ -238,3 +238,35 @@ def test_autotuner_leaves_bunch_untouched(ctx):
     assert np.array_equal(d["vec"].cpu().numpy(), hb.vec)
     assert np.array_equal(d["state"].cpu().numpy(), hb.state)
     ctx.set_tuning(block=128, ctas_per_sm=0, stage_smem=1, turns_per_launch=0, compact=0)
+
+
+@pytest.mark.parametrize("case", ["orders_3_4_6_9", "skew_order", "octupole_b6", "orders_to_5"])
+def test_multipole_kick_forms_match_oracle(ctx, case):
+    """The device's kick forms on orders the benchmark rings do not reach: the branch-free normal
+    form for 4 to 10 orders (with exactly zero orders inside the range), an octupole, and a skew
+    order (the general form), each against the oracle after one and five turns."""
+    eles, p = rings.ring(30)
+    rng = np.random.default_rng(11)
+    for e in eles:
+        if e.key != abi.SEXTUPOLE:
+            continue
+        if case == "orders_3_4_6_9":
+            for n in (3, 4, 6, 9):
+                e.b_pole[n] = float(rng.normal(0, 1e-3))
+        elif case == "orders_to_5":
+            for n in (3, 5):
+                e.b_pole[n] = float(rng.normal(0, 1e-3))
+        elif case == "skew_order":
+            e.b_pole[4] = 2e-4
+            e.a_pole[5] = -3e-4
+        else:
+            e.key = abi.OCTUPOLE
+            e.k3 = 50.0
+            e.k2 = 0.0
+            e.b_pole[6] = 1e-3
+    vec = rings.matched_gaussian(eles, 400, seed=5, scale=4.0)
+    for nt in (1, 5):
+        o = oracle_track(eles, p, vec, nt)
+        g = gpu_track(ctx, eles, p, vec, nt)
+        assert np.array_equal(g["state"], o["state"])
+        assert_close(g, o, 1e-11 if nt == 1 else 1e-9)
