@@ -270,3 +270,23 @@ def test_multipole_kick_forms_match_oracle(ctx, case):
         g = gpu_track(ctx, eles, p, vec, nt)
         assert np.array_equal(g["state"], o["state"])
         assert_close(g, o, 1e-11 if nt == 1 else 1e-9)
+
+
+def test_edge_inputs_match_oracle(ctx):
+    """Particles at the edges of orbit_too_large and the apertures, and NaN or infinite coordinates
+    (alive in the reference, whose comparisons let NaN through): states, loss elements, turns and
+    locations equal the oracle's; coordinates agree, NaN where the oracle has NaN."""
+    from test_hostcheck_cpu import _edge_bunch
+    eles, p = rings.ring(20)
+    vec = _edge_bunch()
+    with np.errstate(invalid="ignore"):
+        o = oracle_track(eles, p, vec, 2)
+        g = gpu_track(ctx, eles, p, vec, 2)
+    for k in ("state", "ix_ele", "ix_turn", "location"):
+        assert np.array_equal(g[k], o[k]), (k, g[k], o[k])
+    assert np.array_equal(np.isnan(g["vec"]), np.isnan(o["vec"]))
+    fin = np.isfinite(o["vec"]) & np.isfinite(g["vec"])
+    scale = np.maximum(np.abs(o["vec"]), 1e-12)
+    with np.errstate(invalid="ignore"):
+        diff = np.abs(g["vec"] - o["vec"])
+    assert np.all(diff[fin] <= 1e-11 * scale[fin])

@@ -151,3 +151,34 @@ def test_rf_phase_fold_outside_the_bucket_bit_exact_on_host(hc):
     assert np.sum(np.abs(vec[4]) > 0.3) > n // 2
     for k in ("vec", "beta", "state"):
         assert np.array_equal(h[k], o[k]), k
+
+
+def _edge_bunch():
+    """Particles at the edges of orbit_too_large and the apertures: beyond max_aperture_limit in
+    either plane, 1 + pz < 0, px^2 + py^2 > (1 + pz)^2, just inside and just outside the 20 mm /
+    10 mm apertures, and NaN or infinite coordinates (which every comparison lets through, as in
+    the reference)."""
+    rows = [
+        [2e3, 0, 0, 0, 0, 0], [-2e3, 0, 0, 0, 0, 0], [0, 0, 2e3, 0, 0, 0], [0, 0, -2e3, 0, 0, 0],
+        [0, 0, 0, 0, 0, -1.5], [0, 1.2, 0, 0, 0, 0], [0, 0.1, 0, -1.3, 0, 0.0],
+        [0.0199999, 0, 0, 0, 0, 0], [0.0200001, 0, 0, 0, 0, 0], [0, 0, -0.0100001, 0, 0, 0],
+        [np.nan, 0, 0, 0, 0, 0], [0, np.nan, 0, 0, 0, 0], [0, 0, 0, 0, np.nan, 0], [0, 0, 0, 0, 0, np.nan],
+        [np.inf, 0, 0, 0, 0, 0], [0, 0, 0, 0, 0, 0], [1e-3, 1e-4, -1e-3, 2e-5, 1e-3, 1e-3],
+    ]
+    return np.ascontiguousarray(np.array(rows, dtype=np.float64).T)
+
+
+def test_edge_inputs_on_host_match_oracle(hc):
+    eles, p = rings.ring(20)
+    vec = _edge_bunch()
+    with np.errstate(invalid="ignore"):
+        o = oracle_track(eles, p, vec, 2)
+        h = host_track(hc, eles, p, vec, 2)
+    for k in ("state", "ix_ele", "ix_turn", "location"):
+        assert np.array_equal(h[k], o[k]), (k, h[k], o[k])
+    assert np.array_equal(h["vec"], o["vec"], equal_nan=True)
+    lost = o["state"] != abi.ALIVE
+    assert lost[[0, 1, 2, 3, 4, 5, 6, 8, 9]].all()
+    assert o["state"][0] == abi.LOST_POS_X and o["state"][1] == abi.LOST_NEG_X
+    assert o["state"][2] == abi.LOST_POS_Y and o["state"][3] == abi.LOST_NEG_Y
+    assert o["state"][4] == abi.LOST_PZ
