@@ -59,6 +59,19 @@ type, bind(c) :: bmadgpu_twiss_t
   integer(c_int32_t) :: status, reserved
 end type
 
+! bmadgpu_ltt_params of include/bmadgpu.h: the ltt_params_struct settings that ltt_run_beam_mode
+! (bsim/modules/lt_tracking_mod.f90:46-110) reads. File names are NUL-terminated C strings
+! (c_loc of a character(kind=c_char) array), c_null_ptr for none.
+type, bind(c) :: bmadgpu_ltt_params_t
+  integer(c_int32_t) :: n_turns, averages_every_n_turns, particle_every_n_turns, output_only_last_turns
+  integer(c_int32_t) :: only_live_particles_out, ix_turn_start, beam_every_n_turns, beam_exact
+  real(c_double) :: dead_cutoff
+  type(c_ptr) :: averages_file, phase_space_file, beam_file
+  real(c_double) :: core_emit_cutoff(8)
+  integer(c_int32_t) :: core_emit_per_mode
+  type(c_ptr) :: action_angle_file, per_particle_file, action_angle_n_inv
+end type
+
 interface
   integer(c_int) function bmadgpu_ctx_create(device, ctx) bind(c, name='bmadgpu_ctx_create')
     import
@@ -110,6 +123,13 @@ interface
     import
     real(c_double) :: mat(36), orb0(6)
     type(bmadgpu_twiss_t) :: tw
+  end function
+  integer(c_int) function bmadgpu_ltt_run(ctx, lat, bunch, params, turns_done) bind(c, name='bmadgpu_ltt_run')
+    import
+    type(c_ptr), value :: ctx, lat
+    type(bmadgpu_bunch_t) :: bunch
+    type(bmadgpu_ltt_params_t) :: params
+    integer(c_int32_t) :: turns_done
   end function
 end interface
 
@@ -353,5 +373,119 @@ ele0%a%phi = 0;  ele0%b%phi = 0
 lat%a%tune = tw%phi_a;  lat%b%tune = tw%phi_b
 
 end subroutine bmadgpu_twiss_at_start
+
+!+
+! Subroutine bmadgpu_ltt_beam (bunch, n_turns, averages_file, phase_space_file, beam_file,
+!     averages_every, particle_every, beam_every, dead_cutoff, core_emit_cutoff,
+!     core_emit_combined_calc, action_angle_file, per_particle_file, only_live_out,
+!     output_only_last_turns, ix_turn_start, turns_done, err)
+!
+! ltt_run_beam_mode (bsim/modules/lt_tracking_mod.f90:1571-1715) for one bunch on the installed
+! branch, outputs included. The arguments are the ltt%... settings of the same meaning
+! (ltt%averages_output_file, ltt%phase_space_output_file, ltt%beam_output_file,
+! ltt%averages_output_every_n_turns, ltt%particle_output_every_n_turns,
+! ltt%beam_output_every_n_turns, ltt%dead_cutoff, ltt%core_emit_cutoff,
+! ltt%core_emit_combined_calc, ltt%action_angle_output_file, ltt%per_particle_output_file,
+! ltt%only_live_particles_out, ltt%output_only_last_turns, ltt%ix_turn_start); '' means no
+! file. The bunch is updated in place as bmadgpu_track_turns updates it; turns_done is the turn
+! reached (n_turns, or the turn the stop conditions ended the run).
+!-
+
+subroutine bmadgpu_ltt_beam (bunch, n_turns, averages_file, phase_space_file, beam_file, averages_every, &
+                             particle_every, beam_every, dead_cutoff, core_emit_cutoff, core_emit_combined_calc, &
+                             action_angle_file, per_particle_file, only_live_out, output_only_last_turns, &
+                             ix_turn_start, turns_done, err)
+
+type (bunch_struct), target :: bunch
+integer n_turns, averages_every, particle_every, beam_every, output_only_last_turns, ix_turn_start, turns_done
+character(*) averages_file, phase_space_file, beam_file, action_angle_file, per_particle_file
+real(rp) dead_cutoff, core_emit_cutoff(:)
+logical core_emit_combined_calc, only_live_out, err
+character(kind=c_char), allocatable, target :: f_ave(:), f_ps(:), f_beam(:), f_aa(:), f_pp(:)
+real(c_double), allocatable, target :: vec(:,:), beta(:), t(:)
+integer(c_int32_t), allocatable, target :: state(:), ix_ele(:), ix_turn(:), location(:)
+type (bmadgpu_bunch_t) b
+type (bmadgpu_ltt_params_t) p
+integer(c_int32_t) done
+integer i, j, n
+
+n = size(bunch%particle)
+allocate (vec(n, 6), beta(n), t(n), state(n), ix_ele(n), ix_turn(n), location(n))
+do j = 1, n
+  do i = 1, 6
+    vec(j, i) = bunch%particle(j)%vec(i)
+  enddo
+  beta(j) = bunch%particle(j)%beta
+  t(j) = real(bunch%particle(j)%t, c_double)
+  state(j) = bunch%particle(j)%state
+enddo
+ix_ele = -1;  ix_turn = -1;  location = 0
+b%n = n
+b%vec = c_loc(vec);  b%beta = c_loc(beta);  b%t = c_loc(t);  b%state = c_loc(state)
+b%ix_ele = c_loc(ix_ele);  b%ix_turn = c_loc(ix_turn);  b%location = c_loc(location)
+
+p%n_turns = n_turns
+p%averages_every_n_turns = averages_every
+p%particle_every_n_turns = particle_every
+p%output_only_last_turns = output_only_last_turns
+p%only_live_particles_out = merge(1, 0, only_live_out)
+p%ix_turn_start = ix_turn_start
+p%beam_every_n_turns = beam_every
+p%beam_exact = 0
+p%dead_cutoff = dead_cutoff
+p%core_emit_cutoff = -1
+do i = 1, min(8, size(core_emit_cutoff))
+  p%core_emit_cutoff(i) = core_emit_cutoff(i)
+enddo
+p%core_emit_per_mode = merge(0, 1, core_emit_combined_calc)
+call c_string (averages_file, f_ave, p%averages_file)
+call c_string (phase_space_file, f_ps, p%phase_space_file)
+call c_string (beam_file, f_beam, p%beam_file)
+call c_string (action_angle_file, f_aa, p%action_angle_file)
+call c_string (per_particle_file, f_pp, p%per_particle_file)
+p%action_angle_n_inv = c_null_ptr
+
+err = (bmadgpu_ltt_run(gpu_ctx, gpu_lat, b, p, done) /= 0)
+if (err) return
+turns_done = done
+do j = 1, n
+  do i = 1, 6
+    bunch%particle(j)%vec(i) = vec(j, i)
+  enddo
+  bunch%particle(j)%beta = beta(j)
+  bunch%particle(j)%t = t(j)
+  bunch%particle(j)%state = state(j)
+  if (ix_ele(j) >= 0) then        ! lost in this run
+    bunch%particle(j)%ix_ele = ix_ele(j) + 1
+    bunch%particle(j)%location = location(j)
+  else
+    bunch%particle(j)%location = downstream_end$
+  endif
+enddo
+bunch%n_live = count(bunch%particle%state == alive$)
+bunch%charge_live = sum(bunch%particle%charge, mask = (bunch%particle%state == alive$))
+
+contains
+
+! A NUL-terminated copy of trim(str) in buf and its address, or c_null_ptr for an empty name.
+subroutine c_string (str, buf, ptr)
+character(*) str
+character(kind=c_char), allocatable, target :: buf(:)
+type(c_ptr) ptr
+integer k, m
+m = len_trim(str)
+if (m == 0) then
+  ptr = c_null_ptr
+  return
+endif
+allocate (buf(m + 1))
+do k = 1, m
+  buf(k) = str(k:k)
+enddo
+buf(m + 1) = c_null_char
+ptr = c_loc(buf)
+end subroutine c_string
+
+end subroutine bmadgpu_ltt_beam
 
 end module bmadgpu_mod
