@@ -557,19 +557,119 @@ double fraction_root(double y, double a, double b) {
 struct CoreScratch {
   double* d_amp = nullptr;
   int32_t* d_mask = nullptr;
-  std::vector<double> amp;
-  std::vector<std::pair<double, int64_t>> order;
-  std::vector<int32_t> mask;
+  int32_t* d_eq = nullptr;            // indices of the particles whose amplitude ties the threshold
+  unsigned int* d_count = nullptr;    // [256] histogram, then [1] count of ties
+  std::vector<int32_t> eq;
   ~CoreScratch() {
     cudaFree(d_amp);
     cudaFree(d_mask);
+    cudaFree(d_eq);
+    cudaFree(d_count);
   }
   bool alloc(int64_t n) {
     if (d_amp) return true;
     return cudaMalloc(&d_amp, (size_t)n * sizeof(double)) == cudaSuccess &&
-           cudaMalloc(&d_mask, (size_t)n * sizeof(int32_t)) == cudaSuccess;
+           cudaMalloc(&d_mask, (size_t)n * sizeof(int32_t)) == cudaSuccess &&
+           cudaMalloc(&d_eq, (size_t)n * sizeof(int32_t)) == cudaSuccess &&
+           cudaMalloc(&d_count, 256 * sizeof(unsigned int)) == cudaSuccess;
   }
 };
+
+// Selection of the n_cut smallest amplitudes on the device, ties going to the lower particle
+// index (the order of a stable sort of the amplitudes). Amplitudes are non-negative, so their
+// IEEE bit patterns order as unsigned integers: eight 8-bit radix passes find the n_cut-th key T
+// exactly (a histogram of the keys that share the prefix found so far, per pass).
+__global__ void k_select_hist(const double* __restrict__ amp, int64_t n, unsigned long long prefix,
+                              unsigned long long prefix_mask, int shift, unsigned int* __restrict__ hist) {
+  __shared__ unsigned int h[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const unsigned long long k = (unsigned long long)__double_as_longlong(amp[i]);
+    if ((k & prefix_mask) == prefix) atomicAdd(&h[(k >> shift) & 255ull], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 256; i += blockDim.x)
+    if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+// mask = keys below T, plus every key equal to T when all ties are taken; otherwise the tied
+// indices are listed in eq for the host to take the lowest.
+__global__ void k_select_mask(const double* __restrict__ amp, int64_t n, unsigned long long t, int take_all_ties,
+                              int32_t* __restrict__ mask, int32_t* __restrict__ eq, unsigned int* __restrict__ n_eq) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const unsigned long long k = (unsigned long long)__double_as_longlong(amp[i]);
+    int32_t m = k < t ? BMADGPU_ALIVE : 0;
+    if (k == t) {
+      if (take_all_ties) m = BMADGPU_ALIVE;
+      else eq[atomicAdd(n_eq, 1u)] = (int32_t)i;
+    }
+    mask[i] = m;
+  }
+}
+
+__global__ void k_select_ties(const int32_t* __restrict__ idx, int64_t count, int32_t* __restrict__ mask) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < count; k += stride) mask[idx[k]] = BMADGPU_ALIVE;
+}
+
+// The core mask in cs.d_mask; *ok false if the core would need a dead particle.
+int select_core(bmadgpu_ctx* c, int64_t n, int64_t n_cut, CoreScratch& cs, bool* ok) {
+  *ok = false;
+  cudaStream_t s = c->stream;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)c->sm_count * 4));
+  unsigned long long prefix = 0, pmask = 0;
+  int64_t rank = n_cut;       // 1-based rank of the wanted key among those sharing the prefix
+  unsigned int hist[256];
+  unsigned int ties = 0;
+  for (int pass = 0; pass < 8; pass++) {
+    const int shift = 56 - 8 * pass;
+    CUDA_TRY(cudaMemsetAsync(cs.d_count, 0, 256 * sizeof(unsigned int), s));
+    k_select_hist<<<grid, 256, 0, s>>>(cs.d_amp, n, prefix, pmask, shift, cs.d_count);
+    CUDA_TRY(cudaGetLastError());
+    c->launches++;
+    CUDA_TRY(cudaMemcpyAsync(hist, cs.d_count, sizeof(hist), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    int64_t cum = 0;
+    int b = 0;
+    for (; b < 255; b++) {
+      if (cum + (int64_t)hist[b] >= rank) break;
+      cum += hist[b];
+    }
+    rank -= cum;
+    ties = hist[b];
+    prefix |= (unsigned long long)b << shift;
+    pmask |= 255ull << shift;
+  }
+  // the n_cut-th smallest is a dead particle's 1e100: fewer live particles than n_cut
+  if ((double)__builtin_bit_cast(double, prefix) >= 1e99) return BMADGPU_OK;
+  const int take_all = (int64_t)ties == rank;
+  CUDA_TRY(cudaMemsetAsync(cs.d_count, 0, sizeof(unsigned int), s));
+  k_select_mask<<<grid, 256, 0, s>>>(cs.d_amp, n, prefix, take_all, cs.d_mask, cs.d_eq, cs.d_count);
+  CUDA_TRY(cudaGetLastError());
+  c->launches++;
+  if (!take_all) {
+    // a tie split by the cut: the lowest indices of the tied particles
+    unsigned int n_eq = 0;
+    CUDA_TRY(cudaMemcpyAsync(&n_eq, cs.d_count, sizeof(n_eq), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    cs.eq.resize(n_eq);
+    CUDA_TRY(cudaMemcpyAsync(cs.eq.data(), cs.d_eq, n_eq * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    std::sort(cs.eq.begin(), cs.eq.end());
+    const int64_t take = std::min<int64_t>(rank, (int64_t)n_eq);
+    CUDA_TRY(cudaMemcpyAsync(cs.d_eq, cs.eq.data(), take * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>((take + 255) / 256, (int64_t)c->sm_count * 4));
+    k_select_ties<<<g2, 256, 0, s>>>(cs.d_eq, take, cs.d_mask);
+    CUDA_TRY(cudaGetLastError());
+    c->launches++;
+    CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  *ok = true;
+  return BMADGPU_OK;
+}
 
 // One ranking: the n_cut live particles of smallest amplitude about (centroid, sigma) of `ref` --
 // the combined amplitude (mode 0) or the action of mode 1..3 -- and the bunch data of that core
@@ -598,19 +698,10 @@ int core_pass(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch& d
   k_core_amp<<<grid, 256, 0, s>>>(d.vec, d.state, n, A, cs.d_amp);
   CUDA_TRY(cudaGetLastError());
   c->launches++;
-  cs.amp.resize(n);
-  CUDA_TRY(cudaMemcpyAsync(cs.amp.data(), cs.d_amp, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaStreamSynchronize(s));
-  // the n_cut smallest amplitudes, ties in particle order (a sorted index of the amplitudes)
-  cs.order.resize(n);
-  for (int64_t i = 0; i < n; i++) cs.order[i] = {cs.amp[i], i};
-  std::nth_element(cs.order.begin(), cs.order.begin() + (n_cut - 1), cs.order.end());
-  cs.mask.assign(n, 0);
-  for (int64_t k = 0; k < n_cut; k++) {
-    if (cs.order[k].first >= 1e99) return BMADGPU_OK;  // fewer live particles than n_cut
-    cs.mask[cs.order[k].second] = BMADGPU_ALIVE;
-  }
-  CUDA_TRY(cudaMemcpyAsync(cs.d_mask, cs.mask.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  // the n_cut smallest amplitudes, ties in particle order, selected on the device
+  bool selected = false;
+  int rs = select_core(c, n, n_cut, cs, &selected);
+  if (rs || !selected) return rs;
   double sums[kStatSums];
   CUDA_TRY(launch_bunch_sums(d.vec, d.t, cs.d_mask, n, d_scratch, d_scratch + kStatBlocks * kStatPass2, s));
   c->launches += 4;

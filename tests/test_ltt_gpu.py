@@ -313,3 +313,24 @@ def test_ltt_action_angle_from_the_one_turn_matrix(ctx, tmp_path):
     for m in range(2):
         dJ = np.abs(J[10][m] - J[0][m])
         assert np.median(dJ) < 0.05 * np.median(J[0][m]), m
+
+
+@pytest.mark.parametrize("combined", [True, False])
+def test_core_emittance_with_tied_amplitudes(ctx, combined):
+    """Every particle three times: the amplitudes tie in threes and the cut splits a tie, which the
+    device selection must resolve to the lower particle indices as a stable sort does."""
+    eles, p = rings.ring(50)
+    base = rings.matched_gaussian(eles, 6001, seed=31, scale=2.0)
+    vec = np.ascontiguousarray(np.repeat(base, 3, axis=1))
+    n = vec.shape[1]
+    hb = lib.HostBunch.from_vec(vec, p, t=np.zeros(n))
+    dev = torch.device("cuda", 0)
+    t = {k: torch.from_numpy(np.array(getattr(hb, k))).to(dev) for k in ("vec", "beta", "t", "state")}
+    view = abi.Bunch(hb.n, t["vec"].data_ptr(), t["beta"].data_ptr(), t["t"].data_ptr(), t["state"].data_ptr(),
+                     None, None, None)
+    lat = lib.Lattice(ctx, eles, p)
+    for cutoff in (0.5, 0.37):
+        assert int(cutoff * n) % 3 != 0          # the cut falls inside a group of three
+        got = lib.bunch_core_emit(ctx, lat, view, cutoff, combined_calc=combined)
+        want = core_emit(hb.vec, hb.t, hb.state, p.p0c, p.mass, cutoff, combined=combined)
+        assert np.allclose(got, want, rtol=1e-9, atol=0), (cutoff, got, want)
