@@ -362,8 +362,8 @@ bool append_per_particle(const std::string& base, int turn, const bmadgpu_bunch&
 // emittances by f = cutoff / (1 - (1 + s + s^2/2 + s^3/6) e^-s), where e^-s solves
 // ltt_beam_fraction(e^-s) = cutoff. Since Sigma^-1 = N^-T diag(1/emit) N^-1, the amplitude is the
 // quadratic form (p - c)^T Sigma^-1 (p - c) = |L^-1 (p - c)|^2 with Sigma = L L^T: the device
-// evaluates that per particle, the host picks the core, and the core's sums are the same two-pass
-// device sums as the bunch's, over the core as the live set.
+// evaluates that per particle and selects the core (select_core), and the core's sums are the same
+// two-pass device sums as the bunch's, over the core as the live set.
 //
 // With core_emit_combined_calc off (:2496-2516) each mode k has its own core: the particles of
 // smallest action (j_2k^2 + j_2k+1^2) / 2 with N^-1 of the bunch, then of the core, and
