@@ -15,6 +15,12 @@ the whole bunch included every step.
 --impl reference: the reference algorithm's CPU implementation (the C++ oracle restating the
 Fortran track1_bunch path, OpenMP over particles) on the host cores, bounded samples.
 
+The default line (ring200 on one GPU) also carries the benchmark's other headline figures as
+sub-records, each timed in its own region: "batched" (the batch256 job, one step, against the
+plain kernel on 8 sampled variants), "served" (the first 200 jobs of the request stream, p50/p99
+latency, against the plain kernel on 8 sampled jobs) and "adjoint" (gradients/s); --no-extras
+leaves them out.
+
 Further workloads (one JSON line each, same keys):
   batch256  256 perturbed 50-cell rings (strengths, offsets, tilts per variant seed), each with a
             dynamic-aperture grid of log-uniform [1024, 65536] particles, 2048 turns; a step is the
@@ -336,12 +342,37 @@ def run_ours(args):
         }
         if world == 1:
             out["cpu_baseline"] = cpu_baseline(eles, p, scale)
-        print(json.dumps(out), flush=True)
     lat.close()
     ctx.close()
+    if rank == 0 and world == 1 and args.workload == "ring200" and not args.no_extras:
+        # the benchmark's other headline figures, each from its own timed region on this GPU
+        out.update(headline_extras(args, peak))
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def headline_extras(args, peak):
+    """Sub-records of the default line: the batched 256-variant job, a 200-job served stream and
+    the adjoint gradient, each with its comparison against the plain kernel and its FP64 roofline."""
+    ns = lambda **kw: argparse.Namespace(**dict(vars(args), **kw))
+    b = run_batch(ns(steps=1, warmup=1, variants=256, plain_sample=8, turns_per_step=10), peak)
+    sv = run_serve(ns(jobs=200, plain_sample=8), peak)
+    ad = run_adjoint(ns(steps=3, warmup=1), peak)
+    keep = lambda d, *ks: {k: d[k] for k in ks if k in d}
+    return {
+        "batched": dict(keep(b, "value", "unit", "ms_per_step", "e2e", "clocks", "gpu_launches"),
+                        workload=b["config"]["workload"], tuning=b["config"]["tuning"],
+                        vs_plain=b["plain_kernel"]["ratio"], plain_kernel=b["plain_kernel"],
+                        roofline=b.get("roofline")),
+        "served": dict(keep(sv, "value", "unit", "ms_per_step", "latency_s", "fma", "server", "clocks", "gpu_launches"),
+                       workload=sv["config"]["workload"], vs_plain=sv["plain_kernel"]["ratio"],
+                       plain_kernel=sv["plain_kernel"], roofline=sv.get("roofline")),
+        "adjoint": dict(keep(ad, "value", "unit", "ms_per_step", "forward_equivalent", "fd_check", "clocks",
+                             "gpu_launches"), workload=ad["config"]["workload"], roofline=ad.get("roofline")),
+    }
 
 
 def _timed(ctx, fn):
@@ -370,8 +401,9 @@ def _flush_l2(dev):
     torch.cuda.synchronize()
 
 
-def run_batch(args):
-    """256 lattice variants, dynamic-aperture grids, 2048 turns, batched path vs plain kernel."""
+def run_batch(args, peak=None):
+    """256 lattice variants, dynamic-aperture grids, 2048 turns, batched path vs plain kernel.
+    Returns the JSON line; peak (FP64 flop/s), if given, adds its roofline."""
     import torch
     lib = importlib.import_module(PKG + ".lib")
     torch.cuda.set_device(0)
@@ -458,11 +490,24 @@ def run_batch(args):
                                                                           tuning["turns_per_launch"], p_s)},
         "gpu_launches": launches, "clocks": clk,
     }
-    print(json.dumps(out), flush=True)
+    if peak:
+        ops, _ = op_count(*rings.perturbed_ring(50, seed=1000), 1.0)
+        out["roofline"] = _fp64_roofline(ops * value, peak, "%.0f ops per particle-turn (perturbed 50-cell ring)" % ops)
+    batch.close()
+    for lat in lats:
+        lat.close()
+    ctx.close()
+    return out
 
 
-def run_serve(args):
-    """The Poisson stream of tracking jobs through the continuous-batching server."""
+def _fp64_roofline(ops_per_s, peak, what):
+    return {"bound": "fp64", "achieved": ops_per_s / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+            "frac": ops_per_s / peak, "ops": what}
+
+
+def run_serve(args, peak=None):
+    """The Poisson stream of tracking jobs through the continuous-batching server. Returns the
+    JSON line; peak (FP64 flop/s), if given, adds its roofline."""
     import threading
     import torch
     lib = importlib.import_module(PKG + ".lib")
@@ -522,6 +567,7 @@ def run_serve(args):
             ids.append((j, submit(srv, j, lat, b, j["turns"])))
         srv.wait(-1, timeout=7200)
         st = srv.stats()
+        st["job_pt"] = [(j["cells"], srv.job(jid)["particle_turns"]) for j, jid in ids]
         done = [srv.fma_result(jid)[1] for j, jid in ids if j["fma"] is not None]
         fma_summary["particles_with_tunes"] = int(sum(int(np.sum(x == 0)) for x in done))
         fma_summary["particles"] = int(sum(len(x) for x in done))
@@ -573,11 +619,22 @@ def run_serve(args):
                                    "%.1f s" % (len(sample), len(jobs), p_s)},
         "gpu_launches": ctx.launch_count - l0, "clocks": clk,
     }
-    print(json.dumps(out), flush=True)
+    if peak:
+        ops = {c: op_count(*rings.perturbed_ring(c, seed=7), 1.0)[0] for c in sorted({c for c, _ in st["job_pt"]})}
+        work = sum(ops[c] * pt for c, pt in st["job_pt"])
+        out["roofline"] = _fp64_roofline(work / st["elapsed_s"], peak, "per job: ops per particle-turn of its ring "
+                                         "(%s) x its particle-turns" % ", ".join("%d cells %.0f" % kv for kv in ops.items()))
+    for _, lat, _, _ in jobs:
+        lat.close()
+    ctx.close()
+    return out
 
 
-def run_adjoint(args):
-    """Gradient of the tracking loss with respect to 200 strengths by the adjoint kernel."""
+def run_adjoint(args, peak=None):
+    """Gradient of the tracking loss with respect to 200 strengths by the adjoint kernel. Returns
+    the JSON line; peak (FP64 flop/s), if given, adds its roofline, counting only the three
+    forward passes of the sweep (tracking, segment and turn recomputation), not the adjoint's own
+    operations."""
     import torch
     lib = importlib.import_module(PKG + ".lib")
     torch.cuda.set_device(0)
@@ -615,7 +672,13 @@ def run_adjoint(args):
                 "d2h_bytes_per_step": 8 * 201},
         "loss": loss, "fd_check": fd_check, "gpu_launches": ctx.launch_count - l0, "clocks": clk,
     }
-    print(json.dumps(out), flush=True)
+    if peak:
+        ops, _ = op_count(eles, p, 1.0)
+        out["roofline"] = _fp64_roofline(3 * ops * 4096 * 256 / s, peak, "3 forward passes x %.0f ops per particle-"
+                                         "turn (the adjoint's own operations not counted)" % ops)
+    lat.close()
+    ctx.close()
+    return out
 
 
 def run_kinds(args):
@@ -723,17 +786,22 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=12, help="batch256/serve: variants/jobs timed on the plain path")
     ap.add_argument("--turns-per-step", type=int, default=10)
     ap.add_argument("--particles", type=int, default=0)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="ring200: leave out the batched, served and adjoint sub-records of the default line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "batch256":
-        run_batch(args)
-    elif args.workload == "serve":
-        run_serve(args)
-    elif args.workload == "adjoint":
-        run_adjoint(args)
+    elif args.workload in ("batch256", "serve", "adjoint"):
+        import torch
+        lib = importlib.import_module(PKG + ".lib")
+        torch.cuda.set_device(0)
+        c = lib.Context(0)
+        peak = c.measure_fp64_peak()
+        c.close()
+        fn = {"batch256": run_batch, "serve": run_serve, "adjoint": run_adjoint}[args.workload]
+        print(json.dumps(fn(args, peak)), flush=True)
     elif args.workload == "kinds":
         run_kinds(args)
     else:

@@ -643,8 +643,9 @@ int select_core(bmadgpu_ctx* c, int64_t n, int64_t n_cut, CoreScratch& cs, bool*
     prefix |= (unsigned long long)b << shift;
     pmask |= 255ull << shift;
   }
-  // the n_cut-th smallest is a dead particle's 1e100: fewer live particles than n_cut
-  if ((double)__builtin_bit_cast(double, prefix) >= 1e99) return BMADGPU_OK;
+  // the n_cut-th smallest is a dead particle's 1e100 (or an infinite or NaN amplitude, whose bits
+  // order above it): fewer live particles of finite amplitude than n_cut
+  if (prefix >= (unsigned long long)__builtin_bit_cast(unsigned long long, 1e99)) return BMADGPU_OK;
   const int take_all = (int64_t)ties == rank;
   CUDA_TRY(cudaMemsetAsync(cs.d_count, 0, sizeof(unsigned int), s));
   k_select_mask<<<grid, 256, 0, s>>>(cs.d_amp, n, prefix, take_all, cs.d_mask, cs.d_eq, cs.d_count);
@@ -813,6 +814,24 @@ extern "C" int bmadgpu_bunch_stats(bmadgpu_ctx* c, const bmadgpu_lattice* lat, c
   int r = device_stats(c, lat, *d, scratch, bd);
   cudaFree(scratch);
   return r;
+}
+
+extern "C" int bmadgpu_select_smallest(bmadgpu_ctx* c, const double* keys, int64_t n, int64_t n_cut,
+                                       int32_t* mask, int32_t* selected) {
+  if (!c || !keys || !mask || !selected) return fail(BMADGPU_EINVAL, "NULL argument");
+  if (n < 1 || n_cut < 1 || n_cut > n) return fail(BMADGPU_EINVAL, "need 1 <= n_cut <= n");
+  CUDA_TRY(cudaSetDevice(c->device));
+  CoreScratch cs;
+  if (!cs.alloc(n)) return fail(BMADGPU_ENOMEM, "cannot allocate the selection scratch");
+  CUDA_TRY(cudaMemcpyAsync(cs.d_amp, keys, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  bool ok = false;
+  int r = select_core(c, n, n_cut, cs, &ok);
+  if (r) return r;
+  if (ok)
+    CUDA_TRY(cudaMemcpyAsync(mask, cs.d_mask, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  *selected = ok ? 1 : 0;
+  return BMADGPU_OK;
 }
 
 extern "C" int bmadgpu_bunch_core_emit(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch* d,

@@ -1,8 +1,8 @@
 // noalloc.cu -- multi-turn tracking with loss compaction that allocates no memory.
 //
-// Some callers cannot call cudaMalloc while they track: code that runs inside CUDA stream
-// capture, or a host program that gives the GPU's memory to its own pool allocator and forbids
-// other allocations during a run. bmadgpu_track_bunch_device_noalloc serves them. It runs the
+// Some callers cannot call cudaMalloc while they track: a host program that gives the GPU's
+// memory to its own pool allocator and forbids other allocations during a run, or a loop that
+// may not stall on an allocation (cudaMalloc can synchronise the device). bmadgpu_track_bunch_device_noalloc serves them. It runs the
 // same tracking and compaction kernels as bmadgpu_track_bunch_device with compaction on, but its
 // scratch memory -- the two live-particle index lists and their lengths -- lives in the fixed
 // file-scope device array below instead of context buffers grown with cudaMalloc.

@@ -666,6 +666,21 @@ def bunch_core_emit(ctx, lat, device_view, cutoff=0.5, combined_calc=True):
     return np.array(out[:])
 
 
+def select_smallest(ctx, keys, n_cut):
+    """Device core selection (bmadgpu_select_smallest) of the n_cut smallest of the amplitudes
+    `keys` (a CUDA torch tensor of float64), ties to the lower index. Returns the mask as a numpy
+    int32 array, or None where the n_cut-th smallest marks a particle that cannot be in a core."""
+    import torch
+    lib = load()
+    lib.bmadgpu_select_smallest.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
+                                            C.POINTER(C.c_int32)]
+    n = keys.numel()
+    mask = torch.full((n,), -7, dtype=torch.int32, device=keys.device)
+    sel = C.c_int32(0)
+    check(lib.bmadgpu_select_smallest(ctx.handle, keys.data_ptr(), n, n_cut, mask.data_ptr(), C.byref(sel)))
+    return mask.cpu().numpy() if sel.value else None
+
+
 def bunch_stats(ctx, lat, device_view):
     """Bunch data (ltt_calc_bunch_data) of a device-resident bunch."""
     lib = _ltt_sigs(load())

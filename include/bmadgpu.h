@@ -185,13 +185,16 @@ int bmadgpu_track_bunch_device(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bma
  * ix_end = n_ele, no moments), with the live-particle list compacted every turns_per_launch
  * turns (0 = one launch), but allocating nothing: its scratch (two index lists and their
  * lengths, 2 MiB) is a fixed device array inside the library, for callers that cannot call
- * cudaMalloc mid-run -- code inside CUDA stream capture, or programs whose memory pool owns the
- * GPU's memory. Every bunch pointer is device memory; the context and lattice already exist.
+ * cudaMalloc mid-run: programs whose own pool allocator has taken the GPU's memory, and loops
+ * that may not stall on an allocation (cudaMalloc can synchronise the device). Every bunch
+ * pointer is device memory; the context and lattice already exist.
  * Limits: at most BMADGPU_NOALLOC_MAX_PARTICLES particles (BMADGPU_EINVAL otherwise). The
  * array is shared by all calls on a device and keeps the last call's contents (the lengths are
  * reset by each call); calls that overlap on the GPU race and must be serialised. The first
  * call on each device looks up the array's device address (cudaGetSymbolAddress) with that
- * device current: make that first call before any stream capture. */
+ * device current: make that first call before any stream capture. The call only enqueues work on
+ * the context's stream; a timed-out element-table staging wait inside it is reported by the next
+ * bmadgpu_ctx_synchronize on the context (BMADGPU_ETIMEDOUT; the results are still correct). */
 int bmadgpu_track_bunch_device_noalloc(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch* bunch,
                                        int32_t turn0, int32_t n_turns, int32_t turns_per_launch);
 
@@ -471,6 +474,15 @@ int bmadgpu_ltt_run(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, bmadgpu_bunch*
  * (fewer than 10 live particles, a zero bunch emittance, an empty core). */
 int bmadgpu_bunch_core_emit(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const bmadgpu_bunch* device_bunch,
                             double cutoff, int32_t combined_calc, double* core_emit);
+
+/* The core selection used by bmadgpu_bunch_core_emit and the LTT core emittances: of n
+ * non-negative amplitudes (device memory), the n_cut smallest, ties going to the lower index as
+ * the reference's stable sort ranks them (bsim/modules/lt_tracking_mod.f90:2550). mask (device, [n])
+ * gets BMADGPU_ALIVE for the selected and 0 for the others. Amplitudes of 1e99 and above,
+ * infinite and NaN amplitudes mark particles that cannot be in a core: if the n_cut-th smallest
+ * is one of them, *selected = 0 and mask is left as it was; otherwise *selected = 1. */
+int bmadgpu_select_smallest(bmadgpu_ctx* ctx, const double* keys, int64_t n, int64_t n_cut, int32_t* mask,
+                            int32_t* selected);
 
 /* ---- Dynamic aperture ------------------------------------------------------------------------
  * dynamic_aperture_point (bmad/modules/dynamic_aperture_mod.f90:284-398) for many rays at once:

@@ -2,7 +2,7 @@
 round trips in the reference's es23.15 layout (16 significant digits) and the exact layout (17
 digits plus beta), lost particles with their state, element and location, alive-only output,
 Fortran's three-digit exponent, and the reference's own ASCII::3 test beam
-(regression_tests/hdf5_test/beam_1.dat) where the reference tree is present."""
+(regression_tests/hdf5_test/beam_1.dat, committed as tests/golden/hdf5_test_beam_1.dat)."""
 import importlib
 import os
 
@@ -13,7 +13,7 @@ lib = importlib.import_module("bmad-ecosystem_b200.lib")
 abi = importlib.import_module("bmad-ecosystem_b200.abi")
 rings = importlib.import_module("bmad-ecosystem_b200.rings")
 
-REF_BEAM = "/root/reference/regression_tests/hdf5_test/beam_1.dat"
+REF_BEAM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "hdf5_test_beam_1.dat")
 
 
 def sample(n=300, seed=3):
@@ -63,7 +63,6 @@ def test_alive_only(tmp_path):
     assert np.all(r.state == abi.ALIVE)
 
 
-@pytest.mark.skipif(not os.path.exists(REF_BEAM), reason="reference tree not present")
 def test_reads_reference_ascii3_beam():
     p = abi.electron_param(3e9)
     r = lib.beam_read(REF_BEAM, p)

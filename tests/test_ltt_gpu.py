@@ -334,3 +334,29 @@ def test_core_emittance_with_tied_amplitudes(ctx, combined):
         got = lib.bunch_core_emit(ctx, lat, view, cutoff, combined_calc=combined)
         want = core_emit(hb.vec, hb.t, hb.state, p.p0c, p.mass, cutoff, combined=combined)
         assert np.allclose(got, want, rtol=1e-9, atol=0), (cutoff, got, want)
+
+
+def test_core_selection_mask_ties_to_lower_index(ctx):
+    """The selection itself: ties at scattered indices, split by the cut, go to the lower indices
+    (a stable sort's order); dead (1e100), infinite and NaN amplitudes are never taken, and a cut
+    that would need one of them reports no core."""
+    rng = np.random.default_rng(5)
+    n = 50000
+    keys = rng.choice(rng.uniform(0.0, 3.0, 700), n)        # about 70 copies of each value
+    keys[rng.choice(n, 900, replace=False)] = 1e100
+    keys[rng.choice(n, 30, replace=False)] = np.inf
+    keys[rng.choice(n, 30, replace=False)] = np.nan
+    keys[17] = 0.0
+    dev = torch.from_numpy(keys).to("cuda:0")
+    finite = np.count_nonzero(keys < 1e99)
+    order = np.argsort(np.where(np.isnan(keys), np.inf, keys), kind="stable")
+    for n_cut in (1, 2, 12345, n // 2, finite - 1, finite):
+        got = lib.select_smallest(ctx, dev, n_cut)
+        want = np.zeros(n, np.int32)
+        want[order[:n_cut]] = abi.ALIVE
+        assert got is not None, n_cut
+        assert np.array_equal(got, want), n_cut
+        t = keys[order[n_cut - 1]]
+        assert n_cut < 3 or np.count_nonzero(keys == t) > 1      # the cut falls inside a tie
+    for n_cut in (finite + 1, n):
+        assert lib.select_smallest(ctx, dev, n_cut) is None

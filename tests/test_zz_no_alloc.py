@@ -1,7 +1,7 @@
 """The allocation-free tracking entry point, bmadgpu_track_bunch_device_noalloc.
 
-Callers that cannot call cudaMalloc while tracking -- code inside CUDA stream capture, or
-programs whose own pool allocator owns the GPU's memory -- use this entry point; its scratch (the
+Callers that cannot call cudaMalloc while tracking -- programs whose own pool allocator holds
+the GPU's memory, or loops that may not stall on an allocation -- use this entry point; its scratch (the
 live-particle lists of loss compaction) is a fixed array inside the library. This file checks,
 through the C-ABI, that it gives the same result as bmadgpu_track_bunch_device with the same
 compaction schedule, on two calls in a row (the second call finds the first call's leftovers in
@@ -54,10 +54,10 @@ def test_noalloc_matches_allocating_entry_point_twice_in_a_row():
         assert np.array_equal(st_new, st_ref)
         for k in ("ix_ele", "ix_turn", "location"):
             assert np.array_equal(new[k].cpu().numpy(), ref[k].cpu().numpy()), k
-        vr, vn = ref["vec"].cpu().numpy(), new["vec"].cpu().numpy()
-        scale = np.sqrt(np.mean(vr * vr, axis=1))[:, None]
-        assert np.max(np.abs(vn - vr) / scale) <= 1e-12
-        assert np.max(np.abs(new["beta"].cpu().numpy() - ref["beta"].cpu().numpy())) <= 1e-15
+        # the same kernels on the same inputs: the same bits
+        assert np.array_equal(new["vec"].cpu().numpy(), ref["vec"].cpu().numpy())
+        assert np.array_equal(new["beta"].cpu().numpy(), ref["beta"].cpu().numpy())
+    lib.check(so.bmadgpu_ctx_synchronize(ctx.handle))      # no staging time-out was left pending
     ctx.set_tuning(turns_per_launch=0, compact=0)
 
 
