@@ -16,7 +16,9 @@ the whole bunch included every step.
 Fortran track1_bunch path, OpenMP over particles) on the host cores, bounded samples.
 
 The default line (ring200 on one GPU) also carries the benchmark's other headline figures as
-sub-records, each timed in its own region: "batched" (the batch256 job, one step, against the
+sub-records, each timed in its own region: "correctly_rounded" (the same ring200 workload with
+libbmadgpu_cr.so, the build whose transcendentals are correctly rounded and whose results are
+bit-identical to the oracle run with a correctly rounded libm), "batched" (the batch256 job, one step, against the
 plain kernel on 8 sampled variants), "served" (the first 200 jobs of the request stream, p50/p99
 latency, against the plain kernel on 8 sampled jobs) and "adjoint" (gradients/s); --no-extras
 leaves them out.
@@ -354,6 +356,56 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_cr_ring(args, peak, steps=3, warmup=3):
+    """ring200 with libbmadgpu_cr.so (correctly rounded transcendentals; bit-identical to the
+    oracle run with a correctly rounded libm): device-resident particle-turns/s, L2 flushed between
+    steps, the library's autotuned shape."""
+    import torch
+    lib = importlib.import_module(PKG + ".lib")
+    previous = lib.get_math()
+    lib.set_math("cr")
+    try:
+        eles, p, n, scale = workload("ring200", 0)
+        T = args.turns_per_step
+        ctx = lib.Context(0)
+        lat = lib.Lattice(ctx, eles, p)
+        dev = torch.device("cuda", 0)
+        hb = lib.HostBunch.from_vec(rings.matched_gaussian(eles, n, seed=0, scale=scale), p)
+        t = {k: torch.from_numpy(getattr(hb, k)).to(dev) for k in ("vec", "beta", "state", "ix_ele", "ix_turn", "location")}
+        torch.cuda.synchronize()
+        v = abi.Bunch(n, t["vec"].data_ptr(), t["beta"].data_ptr(), None, t["state"].data_ptr(),
+                      t["ix_ele"].data_ptr(), t["ix_turn"].data_ptr(), t["location"].data_ptr())
+        best = lib.autotune(ctx, lat, v)
+        turn, tot_s, tot_pt = 0, 0.0, 0
+        clocks = None
+        for i in range(warmup + steps):
+            if i == warmup:
+                clocks = ClockSampler(0)
+            state0 = t["state"].cpu().numpy()
+            _flush_l2(dev)
+            sec = _timed(ctx, lambda: lib.check(lib.load().bmadgpu_track_bunch_device(
+                ctx.handle, lat.handle, ctypes.byref(v), 0, lat.n_ele, turn, T, None)))
+            st, it = t["state"].cpu().numpy(), t["ix_turn"].cpu().numpy()
+            pt = int((st == abi.ALIVE).sum()) * T + int((it[(state0 == abi.ALIVE) & (st != abi.ALIVE)] - turn + 1).sum())
+            turn += T
+            if i >= warmup:
+                tot_s += sec
+                tot_pt += pt
+        clk = clocks.stop()
+        value = tot_pt / tot_s
+        ops, _ = op_count(eles, p, scale)
+        out = {"value": value, "unit": UNIT, "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * tot_s / steps,
+               "library": "libbmadgpu_cr.so", "tuning": best, "clocks": clk,
+               "workload": "ring200 as the main line (%d particles, %d turns per step)" % (n, T),
+               "parity": "bit-identical to the oracle run with a correctly rounded libm (tests/test_gpu_bitexact.py)",
+               "roofline": _fp64_roofline(ops * value, peak, "%.0f ops per particle-turn" % ops) if peak else None}
+        lat.close()
+        ctx.close()
+        return out
+    finally:
+        lib.set_math(previous)
+
+
 def headline_extras(args, peak):
     """Sub-records of the default line: the batched 256-variant job, a 200-job served stream and
     the adjoint gradient, each with its comparison against the plain kernel and its FP64 roofline."""
@@ -362,7 +414,9 @@ def headline_extras(args, peak):
     sv = run_serve(ns(jobs=200, plain_sample=8), peak)
     ad = run_adjoint(ns(steps=3, warmup=1), peak)
     keep = lambda d, *ks: {k: d[k] for k in ks if k in d}
+    cr = run_cr_ring(args, peak)
     return {
+        "correctly_rounded": cr,
         "batched": dict(keep(b, "value", "unit", "ms_per_step", "e2e", "clocks", "gpu_launches"),
                         workload=b["config"]["workload"], tuning=b["config"]["tuning"],
                         vs_plain=b["plain_kernel"]["ratio"], plain_kernel=b["plain_kernel"],

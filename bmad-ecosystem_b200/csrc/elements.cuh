@@ -112,7 +112,7 @@ BG_HD void body_rf(Particle& p, const EleHdr& h, const double* __restrict__ b, c
   const int n_slice = h.n_step;
   double phase = rf_phase(p, b[2], f, b[3]);
   for (int i = 0; i <= n_slice; i++) {
-    double dE = 1.0 * voltage * sin(phase) / n_slice;
+    double dE = 1.0 * voltage * m_sin(phase) / n_slice;
     if (i == 0 || i == n_slice) dE = dE / 2;
     energy_kick(p, dE, G);
     if (p.pz == -1) {

@@ -20,8 +20,25 @@
 #include <string>
 #include <vector>
 
+#if defined(BG_CR_MATH)
+#include "crmath.cuh"
+#endif
+
 namespace bmadgpu {
 namespace {
+
+// The libm of the element invariants: correctly rounded in the product library (whose device
+// maps are correctly rounded) and in the test-only host builds made with BG_CR_MATH; the host's
+// libm in the other test-only host builds, which the oracle's default mode matches.
+#if defined(BG_CR_MATH)
+double l_sin(double x) { return cr::sin(x); }
+double l_cos(double x) { return cr::cos(x); }
+double l_atan2(double y, double x) { return cr::atan2(y, x); }
+#else
+double l_sin(double x) { return std::sin(x); }
+double l_cos(double x) { return std::cos(x); }
+double l_atan2(double y, double x) { return std::atan2(y, x); }
+#endif
 
 const double kPi = 3.141592653589793238462643383279;
 const int kNPole = BMADGPU_N_POLE;
@@ -46,7 +63,7 @@ double factorial(int n) {
   return f;
 }
 
-double sinc0(double x) { return std::fabs(x) < 1e-8 ? 1.0 : std::sin(x) / x; }
+double sinc0(double x) { return std::fabs(x) < 1e-8 ? 1.0 : l_sin(x) / x; }
 double cosc0(double x) {
   if (std::fabs(x) < 1e-8) return 0.5;
   double s = sinc0(x / 2);
@@ -56,7 +73,7 @@ double sincc0(double x) {
   double x2 = x * x;
   if (std::fabs(x) < 0.1)
     return 1.0 / 6.0 + x2 * (-1.0 / 120.0 + x2 * (1.0 / 5040.0 + x2 * (-1.0 / 362880.0)));
-  return (x - std::sin(x)) / (x * x2);
+  return (x - l_sin(x)) / (x * x2);
 }
 
 struct Fail {
@@ -96,8 +113,8 @@ void mag_ab(const bmadgpu_element& e, double tilt_tot, double ref_tilt_tot, doub
       double knl = e.a_pole[n], tn = e.b_pole[n];
       if (knl == 0) continue;
       double angle = -tn * (n + 1);
-      b[n] = (knl * std::cos(angle) - 0.0 * std::sin(angle)) / factorial(n);
-      a[n] = (knl * std::sin(angle) + 0.0 * std::cos(angle)) / factorial(n);
+      b[n] = (knl * l_cos(angle) - 0.0 * l_sin(angle)) / factorial(n);
+      a[n] = (knl * l_sin(angle) + 0.0 * l_cos(angle)) / factorial(n);
     }
     *ix_pole_max = max_nonzero(a, b, kNPole - 1);
     return;
@@ -135,7 +152,7 @@ void mag_ab(const bmadgpu_element& e, double tilt_tot, double ref_tilt_tot, doub
   if (key_has_hkick(e.key) && (e.hkick != 0 || e.vkick != 0)) {
     double tilt = (e.key == BMADGPU_SBEND) ? ref_tilt_tot : tilt_tot;
     if (tilt != 0) {
-      double c = std::cos(tilt), s = std::sin(tilt);
+      double c = l_cos(tilt), s = l_sin(tilt);
       bk[0] = -e.hkick * c - e.vkick * s;
       ak[0] = -e.hkick * s + e.vkick * c;
     } else {
@@ -163,7 +180,7 @@ void tilt_ab(double tilt, double* a, double* b, int ix_pole_max) {
   for (int n = 0; n <= ix_pole_max; n++) {
     if (a[n] == 0 && b[n] == 0) continue;
     double an = a[n], bn = b[n];
-    double c = std::cos((n + 1) * tilt), s = std::sin((n + 1) * tilt);
+    double c = l_cos((n + 1) * tilt), s = l_sin((n + 1) * tilt);
     b[n] = bn * c + an * s;
     a[n] = -bn * s + an * c;
   }
@@ -173,7 +190,7 @@ void tilt_ab(double tilt, double* a, double* b, int ix_pole_max) {
 void ab_to_kt(double an, double bn, int n, double* knl, double* tn) {
   if (an == 0 && bn == 0) { *knl = 0; *tn = 0; return; }
   *knl = factorial(n) * std::sqrt(an * an + bn * bn);
-  *tn = -std::atan2(an, bn) / (n + 1);
+  *tn = -l_atan2(an, bn) / (n + 1);
   if (2 * (n + 1) * std::fabs(*tn) > kPi) {
     *knl = -*knl;
     double sgn = (*tn < 0) ? -1.0 : 1.0;
@@ -418,7 +435,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
       int ix_mag_max;
       std::vector<double> mis;
       auto misalign_block = [&](double tilt) {
-        mis = {e.x_offset, e.y_offset, std::cos(tilt), std::sin(tilt)};
+        mis = {e.x_offset, e.y_offset, l_cos(tilt), l_sin(tilt)};
         flags |= F_MISALIGN;
       };
 
@@ -496,7 +513,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           double step_len = e.l / n_step;
           double angle = g * step_len;
           double gl = g * step_len;
-          blk = {step_len, g, g_tot, dg, angle, std::cos(angle), std::sin(angle), sinc0(angle), cosc0(angle),
+          blk = {step_len, g, g_tot, dg, angle, l_cos(angle), l_sin(angle), sinc0(angle), cosc0(angle),
                  (gl * gl) * sincc0(angle), (b1 != 0 && e.l != 0) ? b1 / e.l : 0.0,
                  r_step * p.p0c / (2.99792458e8 * p.charge)};
           if (b1 != 0) flags |= F_BEND_K1;
@@ -509,7 +526,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
             double ee = end == 0 ? e.e1 : e.e2;
             double fint_gap = end == 0 ? e.fint * e.hgap : e.fintx * e.hgapx;
             if (e.fringe_type == BMADGPU_FRINGE_HARD_EDGE_ONLY || e.fringe_type == BMADGPU_FRINGE_SAD_FULL) fint_gap = 0;
-            double cos_e = std::cos(ee), sin_e = std::sin(ee);
+            double cos_e = l_cos(ee), sin_e = l_sin(ee);
             double tan_e = sin_e / cos_e, sec_e = 1 / cos_e;
             double gt = ge * tan_e;
             double gt2 = ge * (tan_e * tan_e);
@@ -532,7 +549,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           }
           h.n_step = (uint16_t)n_step;
           if (has_misalign) {  // ref_tilt only (offsets/roll rejected above)
-            mis = {0.0, 0.0, std::cos(e.ref_tilt), std::sin(e.ref_tilt)};
+            mis = {0.0, 0.0, l_cos(e.ref_tilt), l_sin(e.ref_tilt)};
             flags |= F_MISALIGN;
           }
           break;
@@ -558,7 +575,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           blk.clear();
           for (int n = 0; n <= top; n++) {
             bool tz = (tn[n] == 0);
-            blk.insert(blk.end(), {knl[n], tz ? 1.0 : std::cos(tn[n]), tz ? 0.0 : std::sin(tn[n]), tz ? 1.0 : 0.0});
+            blk.insert(blk.end(), {knl[n], tz ? 1.0 : l_cos(tn[n]), tz ? 0.0 : l_sin(tn[n]), tz ? 1.0 : 0.0});
           }
           if (top >= 0) flags |= F_KICKS;
           h.n_pole = (uint8_t)(top + 1);

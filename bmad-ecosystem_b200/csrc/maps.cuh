@@ -7,13 +7,24 @@
 // that the reference recomputes from element attributes alone come precomputed from the packed
 // table with the same expressions, hence bit-identical. Functions of pz alone that the reference
 // recomputes per element with the same expression are cached in the particle (refresh()).
-// The kernels are compiled without FMA contraction, so on the device the results differ from the
-// reference only through the device libm (sin, cos, asin, atan2, sinh, cosh).
+// The kernels are compiled without FMA contraction, so the device results differ from the
+// reference's only through the six transcendentals the maps call (sin, cos, asin, atan2, sinh,
+// cosh). The library is built twice from this source: with the device libm (libbmadgpu.so, the
+// fast build), and with BG_CR_MATH, where those six are correctly rounded (crmath.cuh) and the
+// results are bit for bit those of the reference's algorithm run with a correctly rounded libm
+// (libbmadgpu_cr.so).
 #pragma once
 #include <math.h>
 #include <stdint.h>
 
 #include "table.h"
+
+// The maps' transcendentals: correctly rounded with BG_CR_MATH (device, or the test-only host
+// build made with it), otherwise the device's or host's libm.
+#if defined(BG_CR_MATH)
+#include "crmath.cuh"
+#define BG_CR_TRANSCENDENTALS 1
+#endif
 
 // The maps compile for the device (the product) and, for the test-only host check build
 // (hostcheck.cpp: op counting and algorithm checks on CPU), for the host.
@@ -46,6 +57,28 @@ extern double h_cmulti[kNPole][kNPole];
 extern double h_cfull[kNPole][kNPole];
 #define BG_CMULTI(n, m) h_cmulti[n][m]
 #define BG_CFULL(n, m) h_cfull[n][m]
+#endif
+
+#if defined(BG_CR_TRANSCENDENTALS)
+BG_HD double m_sin(double x) { return cr::sin(x); }
+BG_HD double m_cos(double x) { return cr::cos(x); }
+BG_HD double m_asin(double x) { return cr::asin(x); }
+BG_HD double m_atan2(double y, double x) { return cr::atan2(y, x); }
+BG_HD void m_sincos(double x, double& s, double& c) { cr::sincos(x, &s, &c); }
+BG_HD void m_sinhcosh(double x, double& s, double& c) { cr::sinhcosh(x, &s, &c); }
+#else
+BG_HD double m_sin(double x) { return sin(x); }
+BG_HD double m_cos(double x) { return cos(x); }
+BG_HD double m_asin(double x) { return asin(x); }
+BG_HD double m_atan2(double y, double x) { return atan2(y, x); }
+BG_HD void m_sincos(double x, double& s, double& c) {
+  s = sin(x);
+  c = cos(x);
+}
+BG_HD void m_sinhcosh(double x, double& s, double& c) {
+  s = sinh(x);
+  c = cosh(x);
+}
 #endif
 
 struct Particle {
@@ -477,11 +510,13 @@ BG_HD void quad_mat2(double k1, double length, double rel_p, double ef, double& 
     cx = 1 + k_l2 / 2;
     sx = (1 + div_rcp(k_l2, 6, kRcp6)) * length;
   } else if (k1 < 0) {
-    cx = cos(sk_l);
-    sx = sin(sk_l) / sqrt_k;
+    double s;
+    m_sincos(sk_l, s, cx);
+    sx = s / sqrt_k;
   } else {
-    cx = cosh(sk_l);
-    sx = sinh(sk_l) / sqrt_k;
+    double s;
+    m_sinhcosh(sk_l, s, cx);
+    sx = s / sqrt_k;
   }
   quad_mat2_tail(k1, length, rel_p, ef, cx, sx, m11, m12, m21, m22, z0, z1, z2);
 }
@@ -501,8 +536,11 @@ BG_HD void quad_mat2_xy(double k1, double length, double rel_p, double ef, doubl
     cxy = 1 + kl2y / 2;
     sxy = (1 + div_rcp(kl2y, 6, kRcp6)) * length;
   } else {
-    const double c_t = cos(sk_l), s_t = sin(sk_l) / sqrt_k;
-    const double c_h = cosh(sk_l), s_h = sinh(sk_l) / sqrt_k;
+    double c_t, s_t, c_h, s_h;
+    m_sincos(sk_l, s_t, c_t);
+    m_sinhcosh(sk_l, s_h, c_h);
+    s_t = s_t / sqrt_k;
+    s_h = s_h / sqrt_k;
     const bool x_trig = -k1 < 0, y_trig = k1 < 0;
     cxx = x_trig ? c_t : c_h;
     sxx = x_trig ? s_t : s_h;
@@ -578,12 +616,12 @@ BG_HD void bend_k1_step(Particle& p, const double* __restrict__ b) {
     c_x = 1 + tau_x * (arg * arg) / 2;
     z2 = g * (length * length) / (2 * rel_p);
   } else if (k_x > 0) {
-    s_x = sin(arg) / om_x;
-    c_x = cos(arg);
+    m_sincos(arg, s_x, c_x);
+    s_x = s_x / om_x;
     z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
   } else {
-    s_x = sinh(arg) / om_x;
-    c_x = cosh(arg);
+    m_sinhcosh(arg, s_x, c_x);
+    s_x = s_x / om_x;
     z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
   }
   arg = om_y * length;
@@ -591,11 +629,11 @@ BG_HD void bend_k1_step(Particle& p, const double* __restrict__ b) {
     s_y = (1 + tau_y * (arg * arg) / 6) * length;
     c_y = 1 + tau_y * (arg * arg) / 2;
   } else if (k1 < 0) {
-    s_y = sin(om_y * length) / om_y;
-    c_y = cos(om_y * length);
+    m_sincos(om_y * length, s_y, c_y);
+    s_y = s_y / om_y;
   } else {
-    s_y = sinh(om_y * length) / om_y;
-    c_y = cosh(om_y * length);
+    m_sinhcosh(om_y * length, s_y, c_y);
+    s_y = s_y / om_y;
   }
   double r1 = p.x - x_c, r2 = p.px, r3 = p.y, r4 = p.py, r5 = p.z;
   double z0 = -g * x_c * length, z1 = -g * s_x;
@@ -635,9 +673,9 @@ BG_HD bool bend_exact_step(Particle& p, const double* __restrict__ b, const Glob
   if (fabs(px) > pt) { p.state = S_LOST_PZ; return false; }
   const double inv_pt = shared_rcp(pt);  // shared by the four quotients by pt
   double g_p = div_rcp(g_tot, pt, inv_pt);
-  double phi_1 = asin(div_rcp(px, pt, inv_pt));
-  double cos_plus = cos(angle + phi_1);
-  double sin_plus = sin(angle + phi_1);
+  double phi_1 = m_asin(div_rcp(px, pt, inv_pt));
+  double cos_plus, sin_plus;
+  m_sincos(angle + phi_1, sin_plus, cos_plus);
   double gx1 = 1 + g * x;
   double ls = gx1 * step_len * sinc_a;
   double alpha = 2 * gx1 * sin_plus * step_len * sinc_a - g_p * (ls * ls);
@@ -661,10 +699,10 @@ BG_HD bool bend_exact_step(Particle& p, const double* __restrict__ b, const Glob
   double L_u = xi;
   double L_v = -1 * (step_len * sinc_a + x * sin_a);
   double L_c = sqrt(L_v * L_v + L_u * L_u);
-  double angle_p = 2 * (angle + phi_1 - 1 * atan2(L_u, -L_v));
+  double angle_p = 2 * (angle + phi_1 - 1 * m_atan2(L_u, -L_v));
   double hp = angle_p / 2;
-  double L_p = 1 * L_c / ((fabs(hp) < 1e-8) ? 1.0 : sin(hp) / hp);
-  p.px = pt * sin(phi_1 + angle - angle_p);
+  double L_p = 1 * L_c / ((fabs(hp) < 1e-8) ? 1.0 : m_sin(hp) / hp);
+  p.px = pt * m_sin(phi_1 + angle - angle_p);
   p.y = y + div_rcp(py * L_p, pt, inv_pt);
   p.z = z + div_rcp(p.beta * step_len, G.beta0, G.inv_beta0) - div_rcp(rel_p * L_p, pt, inv_pt);
   return true;

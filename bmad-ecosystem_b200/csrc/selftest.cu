@@ -4,11 +4,16 @@
 // device's own division a / b, bit for bit, on n pseudo-random pairs (splitmix64 stream): random
 // signs, 52-bit mantissas and exponents in [-60, 60], half of them numerators one ulp either side
 // of an exact product b q (quotients next to a rounding tie), plus zero numerators.
+// k_cr_eval: the correctly rounded transcendentals of the maps (crmath.cuh) on given arguments,
+// for comparison with their host build and with mpmath in the tests.
 
 #define BG_SHARED_RECIPROCAL  // the quotient under test
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "capi_internal.h"
+#include "crmath.cuh"
 #include "maps.cuh"
 
 using namespace bmadgpu;
@@ -55,7 +60,49 @@ __global__ void k_check_div(int64_t n, uint64_t seed, unsigned long long* mismat
   if (bad) atomicAdd(mismatches, bad);
 }
 
+__global__ void k_cr_eval(int fn, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out,
+                          int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double x = a[i];
+    double r;
+    switch (fn) {
+      case 0: r = cr::sin(x); break;
+      case 1: r = cr::cos(x); break;
+      case 2: r = cr::asin(x); break;
+      case 3: r = cr::atan2(x, b[i]); break;
+      case 4: r = cr::sinh(x); break;
+      case 5: r = cr::cosh(x); break;
+      case 6: {  // sincos: sin in out[i], cos in out[n + i]
+        double c;
+        cr::sincos(x, &r, &c);
+        out[n + i] = c;
+        break;
+      }
+      default: {  // sinhcosh
+        double c;
+        cr::sinhcosh(x, &r, &c);
+        out[n + i] = c;
+        break;
+      }
+    }
+    out[i] = r;
+  }
+}
+
 }  // namespace
+
+extern "C" int bmadgpu_cr_eval(bmadgpu_ctx* c, int32_t fn, const double* a, const double* b, double* out, int64_t n) {
+  if (!c || !a || !out || n < 0 || fn < 0 || fn > 7 || (fn == 3 && !b)) return fail(BMADGPU_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(c->device));
+  if (n == 0) return BMADGPU_OK;
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)c->sm_count * 8);
+  k_cr_eval<<<(int)blocks, 256, 0, c->stream>>>(fn, a, b, out, n);
+  CUDA_TRY(cudaGetLastError());
+  c->launches++;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return BMADGPU_OK;
+}
 
 extern "C" int bmadgpu_selftest_division(bmadgpu_ctx* c, int64_t n, uint64_t seed, int64_t* mismatches) {
   if (!c || !mismatches || n < 0) return fail(BMADGPU_EINVAL, "bad argument");

@@ -3,6 +3,13 @@
 Names follow the reference: ``track_bunch`` is track_bunch (bmad/multiparticle/beam_mod.f90:103)
 over turns, ``track1_bunch`` the per-element hook (beam_mod.f90:238). Errors raise
 ``BmadGpuError`` with the library's last-error message; nothing here falls back to a CPU path.
+
+Two builds of the library share this binding: libbmadgpu.so (the device libm in the element
+maps, the default) and libbmadgpu_cr.so (correctly rounded transcendentals: bit-identical to the
+reference's algorithm run with a correctly rounded libm). ``set_math("cr")`` (or the environment
+variable BMADGPU_MATH=cr) selects the second for everything created afterwards; an object keeps
+calling the build that was current when it was made only if the selection is not changed while
+it lives.
 """
 import ctypes as C
 import math
@@ -15,6 +22,8 @@ from . import abi
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libbmadgpu.so")
+LIB_CR_PATH = os.path.join(_HERE, "lib", "libbmadgpu_cr.so")
+MATH = ("fast", "cr")
 HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "bmadgpu.h")
 
 
@@ -37,18 +46,35 @@ class BatchTuning(C.Structure):
 
 _BATCH_FIELDS = ("block", "ctas_per_sm", "particles_per_thread", "turns_per_launch", "stage_smem", "use_graph")
 
-_lib = None
+_libs = {}
+_math = os.environ.get("BMADGPU_MATH", "fast")
+
+
+def set_math(math):
+    """Select the library build for what is created from now on: "fast" (libbmadgpu.so) or "cr"
+    (libbmadgpu_cr.so, correctly rounded transcendentals)."""
+    global _math
+    if math not in MATH:
+        raise BmadGpuError(abi.EINVAL, "math must be one of %s" % (MATH,))
+    _math = math
+
+
+def get_math():
+    return _math
 
 
 def load(path=None):
-    """Load the shared library (built by csrc/Makefile; BMADGPU_LIBRARY overrides the path).
-    Raises if it is missing."""
-    global _lib
-    if _lib is not None:
-        return _lib
-    path = path or os.environ.get("BMADGPU_LIBRARY") or LIB_PATH
+    """Load the shared library of the selected build (built by csrc/Makefile; BMADGPU_LIBRARY and
+    BMADGPU_LIBRARY_CR override the paths). Raises if it is missing."""
+    if path is None:
+        if _math == "cr":
+            path = os.environ.get("BMADGPU_LIBRARY_CR") or LIB_CR_PATH
+        else:
+            path = os.environ.get("BMADGPU_LIBRARY") or LIB_PATH
+    if path in _libs:
+        return _libs[path]
     if not os.path.exists(path):
-        raise BmadGpuError(abi.EINVAL, "libbmadgpu.so not built: run make -C bmad-ecosystem_b200/csrc")
+        raise BmadGpuError(abi.EINVAL, "%s not built: run make -C bmad-ecosystem_b200/csrc" % os.path.basename(path))
     lib = C.CDLL(path)
     P, V = C.POINTER, C.c_void_p
     sig = {
@@ -89,7 +115,7 @@ def load(path=None):
             continue
         f.argtypes = args
         f.restype = res
-    _lib = lib
+    _libs[path] = lib
     return lib
 
 

@@ -247,6 +247,14 @@ int bmadgpu_measure_fp64_peak(bmadgpu_ctx* ctx, double* flops_per_s);
  * the device's a / b. 0 is the only correct answer. */
 int bmadgpu_selftest_division(bmadgpu_ctx* ctx, int64_t n, uint64_t seed, int64_t* mismatches);
 
+/* The correctly rounded transcendentals the element maps use, evaluated on the device for n
+ * arguments (device memory): fn 0 sin(a), 1 cos(a), 2 asin(a), 3 atan2(a, b), 4 sinh(a),
+ * 5 cosh(a), 6 sincos(a) (sin in out[0, n), cos in out[n, 2n)), 7 sinhcosh(a) (likewise). The
+ * reference calls its libm here (sin, cos, asin, atan2, sinh, cosh in track_a_bend.f90:163-209,
+ * quad_mat2_calc.f90:34-47, track_a_rfcavity.f90:117); the device's are correctly rounded so that
+ * its results equal the reference algorithm's with a correctly rounded libm, bit for bit. */
+int bmadgpu_cr_eval(bmadgpu_ctx* ctx, int32_t fn, const double* a, const double* b, double* out, int64_t n);
+
 /* sizeof() of the ABI structs as this library was compiled, for binding checks. */
 int64_t bmadgpu_sizeof(int32_t which); /* 0 element, 1 param, 2 bunch, 3 tuning, 4 batch tuning,
                                            5 server config, 6 job info, 7 server stats,

@@ -28,6 +28,25 @@ namespace {
 
 typedef __float128 qp;
 
+// The libm of the restated routines: the host's (default: glibc, as a gfortran build of the
+// reference on Linux uses), or six functions the caller installs with oracle_set_libm (the tests
+// install correctly rounded ones to compare with the device, whose maps are correctly rounded).
+double h_sin(double x) { return std::sin(x); }
+double h_cos(double x) { return std::cos(x); }
+double h_asin(double x) { return std::asin(x); }
+double h_atan2(double y, double x) { return std::atan2(y, x); }
+double h_sinh(double x) { return std::sinh(x); }
+double h_cosh(double x) { return std::cosh(x); }
+struct Libm {
+  double (*sin)(double);
+  double (*cos)(double);
+  double (*asin)(double);
+  double (*atan2)(double, double);
+  double (*sinh)(double);
+  double (*cosh)(double);
+};
+Libm lm = {h_sin, h_cos, h_asin, h_atan2, h_sinh, h_cosh};
+
 // sim_utils/interfaces/physical_constants.f90:12-13, 34
 const double pi = 3.141592653589793238462643383279;
 const double twopi = 2 * pi;
@@ -47,10 +66,10 @@ double sinc(double x, int nd = 0) {
   double x2 = x * x;
   if (nd == 0) {
     if (std::fabs(x) < 1e-8) return 1.0;
-    return std::sin(x) / x;
+    return lm.sin(x) / x;
   }
   if (std::fabs(x) < 0.1) return x * (c1 + x2 * (c2 + x2 * (c3 + x2 * c4)));
-  return (x * std::cos(x) - std::sin(x)) / x2;
+  return (x * lm.cos(x) - lm.sin(x)) / x2;
 }
 
 // cosc.f90:15
@@ -65,7 +84,7 @@ double sincc(double x) {
   const double c0 = 1.0 / 6.0, c1 = -1.0 / 120.0, c2 = 1.0 / 5040.0, c3 = -1.0 / 362880.0;
   double x2 = x * x;
   if (std::fabs(x) < 0.1) return c0 + x2 * (c1 + x2 * (c2 + x2 * c3));
-  return (x - std::sin(x)) / (x * x2);
+  return (x - lm.sin(x)) / (x * x2);
 }
 
 // sqrt_one.f90:18
@@ -213,8 +232,8 @@ void tilt_this_multipole(const Ele& ele, int sgn, double* a, double* b, int ix_p
   for (int n = 0; n <= ix_pole_max; n++) {
     if (a[n] == 0 && b[n] == 0) continue;
     double an = a[n], bn = b[n];
-    double cos_t = std::cos((n + 1) * tilt);
-    double sin_t = std::sin((n + 1) * tilt);
+    double cos_t = lm.cos((n + 1) * tilt);
+    double sin_t = lm.sin((n + 1) * tilt);
     b[n] = bn * cos_t + an * sin_t;
     a[n] = -bn * sin_t + an * cos_t;
   }
@@ -224,8 +243,8 @@ void tilt_this_multipole(const Ele& ele, int sgn, double* a, double* b, int ix_p
 void multipole1_kt_to_ab(double knl, double tn, int n, double* an, double* bn) {
   if (knl == 0) { *an = 0; *bn = 0; return; }
   double angle = -tn * (n + 1);
-  *bn = (knl * std::cos(angle) - 0.0 * std::sin(angle)) / factorial(n);
-  *an = (knl * std::sin(angle) + 0.0 * std::cos(angle)) / factorial(n);
+  *bn = (knl * lm.cos(angle) - 0.0 * lm.sin(angle)) / factorial(n);
+  *an = (knl * lm.sin(angle) + 0.0 * lm.cos(angle)) / factorial(n);
 }
 
 // multipole1_ab_to_kt, bmad/low_level/multipole1_ab_to_kt.f90:17
@@ -233,7 +252,7 @@ void multipole1_ab_to_kt(double an, double bn, int n, double* knl, double* tn) {
   if (an == 0 && bn == 0) { *knl = 0; *tn = 0; return; }
   double a = an, b = bn;
   *knl = factorial(n) * std::sqrt(a * a + b * b);
-  *tn = -std::atan2(a, b) / (n + 1);
+  *tn = -lm.atan2(a, b) / (n + 1);
   if (2 * (n + 1) * std::fabs(*tn) > pi) {
     *knl = -*knl;
     double sgn = (*tn < 0) ? -1.0 : 1.0;
@@ -295,7 +314,7 @@ void this_ele_non_multipoles(const Ele& ele, int p_type, double a_kick[4], doubl
   if (key_has_hkick(e->key) && (hk != 0 || vk != 0)) {
     double tilt = (e->key == BMADGPU_SBEND) ? ele.ref_tilt_tot : ele.tilt_tot;
     if (tilt != 0) {
-      double cos_t = std::cos(tilt), sin_t = std::sin(tilt);
+      double cos_t = lm.cos(tilt), sin_t = lm.sin(tilt);
       b_kick[0] = -hk * cos_t - vk * sin_t;
       a_kick[0] = -hk * sin_t + vk * cos_t;
     } else {
@@ -467,8 +486,8 @@ void multipole_kick(double knl, double tilt, int n, Coord& coord, bool ref_orb_o
     x = coord.vec[0];
     y = coord.vec[2];
   } else {
-    sin_ang = std::sin(t);
-    cos_ang = std::cos(t);
+    sin_ang = lm.sin(t);
+    cos_ang = lm.cos(t);
     x = coord.vec[0] * cos_ang + coord.vec[2] * sin_ang;
     y = -coord.vec[0] * sin_ang + coord.vec[2] * cos_ang;
   }
@@ -551,11 +570,11 @@ void quad_mat2_calc(double k1, double length, double rel_p, double mat2[2][2], d
     cx = 1 + k_l2 / 2;
     sx = (1 + k_l2 / 6) * length;
   } else if (k1 < 0) {
-    cx = std::cos(sk_l);
-    sx = std::sin(sk_l) / sqrt_k;
+    cx = lm.cos(sk_l);
+    sx = lm.sin(sk_l) / sqrt_k;
   } else {
-    cx = std::cosh(sk_l);
-    sx = std::sinh(sk_l) / sqrt_k;
+    cx = lm.cosh(sk_l);
+    sx = lm.sinh(sk_l) / sqrt_k;
   }
   mat2[0][0] = cx;
   mat2[0][1] = sx / rel_p;
@@ -589,7 +608,7 @@ double low_energy_z_correction(const Coord& orbit, const Ele& ele, double ds) {
 // tilt_coords, bmad/code/tilt_coords.f90:18-53
 void tilt_coords(double tilt_val, double* coord) {
   if (tilt_val == 0) return;
-  double sin_ang = std::sin(tilt_val), cos_ang = std::cos(tilt_val);
+  double sin_ang = lm.sin(tilt_val), cos_ang = lm.cos(tilt_val);
   double x = coord[0], y = coord[2];
   coord[0] = cos_ang * x + sin_ang * y;
   coord[2] = -sin_ang * x + cos_ang * y;
@@ -600,9 +619,9 @@ void tilt_coords(double tilt_val, double* coord) {
 
 // floor_angles_to_w_mat, bmad/geometry/floor_angles_to_w_mat.f90 (psi = 0 as used here)
 void floor_angles_to_w_mat(double theta, double phi, double psi, double w[3][3], bool inverse) {
-  double s_the = std::sin(theta), c_the = std::cos(theta);
-  double s_phi = std::sin(phi), c_phi = std::cos(phi);
-  double s_psi = std::sin(psi), c_psi = std::cos(psi);
+  double s_the = lm.sin(theta), c_the = lm.cos(theta);
+  double s_phi = lm.sin(phi), c_phi = lm.cos(phi);
+  double s_psi = lm.sin(psi), c_psi = lm.cos(psi);
   if (!inverse) {
     w[0][0] = c_the * c_psi - s_the * s_phi * s_psi;
     w[0][1] = -c_the * s_psi - s_the * s_phi * c_psi;
@@ -847,7 +866,7 @@ void hwang_bend_edge_kick(const Ele& ele, int particle_at, Coord& orb, double* m
     fint_gap = e->fintx * e->hgapx;
   }
   if (fringe_type == BMADGPU_FRINGE_HARD_EDGE_ONLY || fringe_type == BMADGPU_FRINGE_SAD_FULL) fint_gap = 0;
-  double cos_e = std::cos(ee), sin_e = std::sin(ee);
+  double cos_e = lm.cos(ee), sin_e = lm.sin(ee);
   double tan_e = sin_e / cos_e, sec_e = 1 / cos_e;
   double gt = g_tot * tan_e;
   double gt2 = g_tot * (tan_e * tan_e);
@@ -1181,12 +1200,12 @@ void sbend_body_with_k1_map(const Ele& ele, double dg, double b1, int n_step, Co
     c_x = 1 + tau_x * (arg * arg) / 2;
     z2 = g * (length * length) / (2 * rel_p);
   } else if (k_x > 0) {
-    s_x = std::sin(arg) / om_x;
-    c_x = std::cos(arg);
+    s_x = lm.sin(arg) / om_x;
+    c_x = lm.cos(arg);
     z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
   } else {
-    s_x = std::sinh(arg) / om_x;
-    c_x = std::cosh(arg);
+    s_x = lm.sinh(arg) / om_x;
+    c_x = lm.cosh(arg);
     z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
   }
   arg = om_y * length;
@@ -1194,11 +1213,11 @@ void sbend_body_with_k1_map(const Ele& ele, double dg, double b1, int n_step, Co
     s_y = (1 + tau_y * (arg * arg) / 6) * length;
     c_y = 1 + tau_y * (arg * arg) / 2;
   } else if (k1 < 0) {
-    s_y = std::sin(om_y * length) / om_y;
-    c_y = std::cos(om_y * length);
+    s_y = lm.sin(om_y * length) / om_y;
+    c_y = lm.cos(om_y * length);
   } else {
-    s_y = std::sinh(om_y * length) / om_y;
-    c_y = std::cosh(om_y * length);
+    s_y = lm.sinh(om_y * length) / om_y;
+    c_y = lm.cosh(om_y * length);
   }
   double r[6];
   for (int i = 0; i < 6; i++) r[i] = orbit.vec[i];
@@ -1300,7 +1319,7 @@ int track_a_bend(Coord& orbit, const Ele& ele) {
       if (dg == 0 && std::fabs(x * g) < 1e-9 && std::fabs(px) < 1e-9 && std::fabs(py) < 1e-9 &&
           std::fabs(pz) < 1e-9) {
         double ll = step_len;
-        double cos_a = std::cos(angle), sin_a = std::sin(angle);
+        double cos_a = lm.cos(angle), sin_a = lm.sin(angle);
         double sinc_a = sinc(angle), cosc_a = cosc(angle);
         double m2 = p->mass * p->mass;
         double rpp = rel_p * orbit.p0c;
@@ -1320,11 +1339,11 @@ int track_a_bend(Coord& orbit, const Ele& ele) {
           return 0;
         }
         double g_p = g_tot / pt;
-        double phi_1 = std::asin(px / pt);
-        double cos_a = std::cos(angle), sin_a = std::sin(angle);
+        double phi_1 = lm.asin(px / pt);
+        double cos_a = lm.cos(angle), sin_a = lm.sin(angle);
         double cosc_a = cosc(angle);
-        double cos_plus = std::cos(angle + phi_1);
-        double sin_plus = std::sin(angle + phi_1);
+        double cos_plus = lm.cos(angle + phi_1);
+        double sin_plus = lm.sin(angle + phi_1);
         double gx1 = 1 + g * x;
         double ls = gx1 * step_len * sinc_a;
         double alpha = 2 * gx1 * sin_plus * step_len * sinc_a - g_p * (ls * ls);
@@ -1351,9 +1370,9 @@ int track_a_bend(Coord& orbit, const Ele& ele) {
         double L_u = xi;
         double L_v = -1 * (step_len * sinc_a + x * sin_a);
         double L_c = std::sqrt(L_v * L_v + L_u * L_u);
-        double angle_p = 2 * (angle + phi_1 - 1 * std::atan2(L_u, -L_v));
+        double angle_p = 2 * (angle + phi_1 - 1 * lm.atan2(L_u, -L_v));
         double L_p = 1 * L_c / sinc(angle_p / 2);
-        orbit.vec[1] = pt * std::sin(phi_1 + angle - angle_p);
+        orbit.vec[1] = pt * lm.sin(phi_1 + angle - angle_p);
         orbit.vec[2] = y + py * L_p / pt;
         orbit.vec[4] = z + orbit.beta * step_len / beta_ref - rel_p * L_p / pt;
       }
@@ -1406,7 +1425,7 @@ int track_a_rfcavity(Coord& orbit, const Ele& ele) {
   double phase = modulo2(phase0, pi);
   // rf_coupler_kick: coupler_strength = 0 on the path -> no kick
   for (int i = 0; i <= n_slice; i++) {
-    double dE = 1 * voltage * std::sin(phase) / n_slice;
+    double dE = 1 * voltage * lm.sin(phase) / n_slice;
     if (i == 0 || i == n_slice) dE = dE / 2;
     apply_energy_kick(dE, orbit, p);
     if (orbit.vec[5] == -1) {
@@ -1696,6 +1715,15 @@ int oracle_hwang_bend_edge_kick(const bmadgpu_element* e, const bmadgpu_param* p
   hwang_bend_edge_kick(ele, particle_at, o, mat6);
   to_external(o, c);
   return 0;
+}
+
+void oracle_set_libm(double (*f_sin)(double), double (*f_cos)(double), double (*f_asin)(double),
+                     double (*f_atan2)(double, double), double (*f_sinh)(double), double (*f_cosh)(double)) {
+  if (!f_sin || !f_cos || !f_asin || !f_atan2 || !f_sinh || !f_cosh) {
+    lm = Libm{h_sin, h_cos, h_asin, h_atan2, h_sinh, h_cosh};
+    return;
+  }
+  lm = Libm{f_sin, f_cos, f_asin, f_atan2, f_sinh, f_cosh};
 }
 
 int32_t oracle_max_threads(void) {

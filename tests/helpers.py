@@ -75,3 +75,43 @@ def noise_track(elements, param, vec, n_turns):
 def per_particle_err(got, want):
     """Max over coordinates of the RMS-relative error, per particle."""
     return rel_err(got, want, coord_floor(want)).max(axis=0)
+
+
+_CRLIB = None
+
+
+def cr_libm(kind="cr"):
+    """Addresses of six libm functions for oracle_set_libm: "cr", the correctly rounded functions
+    the device maps use (host build of csrc/crmath.cuh); "quad", libquadmath's rounded once, an
+    independent correctly rounded set."""
+    global _CRLIB
+    import os
+    import subprocess
+    from conftest import ROOT
+    if _CRLIB is None:
+        path = os.path.join(ROOT, "bmad-ecosystem_b200", "_build", "libbmadgpu_crmath.so")
+        if not os.path.exists(path):
+            subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "bmad-ecosystem_b200", "csrc"),
+                                   "hostcheck-lib"])
+        _CRLIB = ctypes.CDLL(path)
+    pre = "bmadgpu_cr_" if kind == "cr" else "bmadgpu_q_"
+    return [ctypes.cast(getattr(_CRLIB, pre + f), ctypes.c_void_p) for f in ("sin", "cos", "asin", "atan2", "sinh",
+                                                                            "cosh")]
+
+
+class oracle_libm:
+    """Context manager: the oracle tracks with the given libm ("cr" or "quad"), then the host's."""
+
+    def __init__(self, kind="cr"):
+        self.kind = kind
+
+    def __enter__(self):
+        lib = load_oracle()
+        lib.oracle_set_libm.argtypes = [ctypes.c_void_p] * 6
+        lib.oracle_set_libm(*cr_libm(self.kind))
+        return self
+
+    def __exit__(self, *exc):
+        lib = load_oracle()
+        lib.oracle_set_libm(None, None, None, None, None, None)
+        return False

@@ -12,20 +12,28 @@ lib = importlib.import_module("bmad-ecosystem_b200.lib")
 rings = importlib.import_module("bmad-ecosystem_b200.rings")
 
 
-def test_library_exports_every_declared_symbol():
-    so = lib.load()
+@pytest.mark.parametrize("path", [lib.LIB_PATH, lib.LIB_CR_PATH], ids=["libbmadgpu", "libbmadgpu_cr"])
+def test_library_exports_every_declared_symbol(path):
+    """Both builds (device libm; correctly rounded transcendentals) export the whole C-ABI."""
+    so = lib.load(path)
     declared = lib.declared_symbols()
     assert len(declared) >= 15
     missing = [s for s in declared if not hasattr(so, s)]
     assert not missing, missing
-    out = subprocess.check_output(["nm", "-D", "--defined-only", lib.LIB_PATH]).decode()
+    out = subprocess.check_output(["nm", "-D", "--defined-only", path]).decode()
     for s in declared:
         assert (" T " + s) in out, s
 
 
-def test_struct_layout_matches():
-    lib.check_layout()
-    assert lib.load().bmadgpu_abi_version() == 1
+@pytest.mark.parametrize("math", ["fast", "cr"])
+def test_struct_layout_matches(math):
+    previous = lib.get_math()
+    lib.set_math(math)
+    try:
+        lib.check_layout()
+        assert lib.load().bmadgpu_abi_version() == 1
+    finally:
+        lib.set_math(previous)
 
 
 def test_ring_bookkeeping_matches_oracle():

@@ -10,11 +10,12 @@ import numpy as np
 import pytest
 
 from conftest import ROOT, load_abi
-from helpers import oracle_track
+from helpers import oracle_libm, oracle_track
 
 abi = load_abi()
 rings = importlib.import_module("bmad-ecosystem_b200.rings")
 HC = os.path.join(ROOT, "bmad-ecosystem_b200", "_build", "libbmadgpu_hostcheck.so")
+HC_CR = os.path.join(ROOT, "bmad-ecosystem_b200", "_build", "libbmadgpu_hostcheck_cr.so")
 
 
 @pytest.fixture(scope="module")
@@ -22,6 +23,15 @@ def hc():
     if not os.path.exists(HC):
         subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "bmad-ecosystem_b200", "csrc"), "hostcheck-lib"])
     return ctypes.CDLL(HC)
+
+
+@pytest.fixture(scope="module")
+def hc_cr():
+    if not os.path.exists(HC_CR):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "bmad-ecosystem_b200", "csrc"), "hostcheck-lib"])
+    lib = ctypes.CDLL(HC_CR)
+    lib.bmadgpu_hostcheck_track = lib.bmadgpu_hostcheck_cr_track
+    return lib
 
 
 def host_track(hc, eles, p, vec, nt):
@@ -182,3 +192,49 @@ def test_edge_inputs_on_host_match_oracle(hc):
     assert o["state"][0] == abi.LOST_POS_X and o["state"][1] == abi.LOST_NEG_X
     assert o["state"][2] == abi.LOST_POS_Y and o["state"][3] == abi.LOST_NEG_Y
     assert o["state"][4] == abi.LOST_PZ
+
+
+# ---- correctly rounded transcendentals: the device's arithmetic on the CPU --------------------
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_device_code_with_cr_libm_is_bit_exact(hc_cr, name):
+    """The host build of the device maps with the correctly rounded functions (maps and element
+    invariants, as in the product library) against the oracle with the same functions installed."""
+    ap = dict(x1_limit=0.02, x2_limit=0.02, y1_limit=0.01, y2_limit=0.01)
+    eles = CASES[name](abi.default_element, ap)
+    p = abi.electron_param(3e9)
+    rings.set_ref_time(eles, p)
+    vec = rings.matched_gaussian(rings.ring(50)[0], 1000, seed=11, scale=3.0)
+    with oracle_libm("cr"):
+        o = oracle_track(eles, p, vec, 1)
+    h = host_track(hc_cr, eles, p, vec, 1)
+    for k in ("vec", "beta", "state"):
+        assert np.array_equal(h[k], o[k]), k
+
+
+def test_config1_ring_with_cr_libm_bit_exact(hc_cr):
+    eles, p = rings.ring(200, fringe=True, multipole_sigma=1e-4)
+    vec = rings.matched_gaussian(eles, 200, seed=3, scale=3.0)
+    with oracle_libm("cr"):
+        o = oracle_track(eles, p, vec, 5)
+    h = host_track(hc_cr, eles, p, vec, 5)
+    assert np.array_equal(h["vec"], o["vec"])
+    assert np.array_equal(h["state"], o["state"])
+
+
+def test_cr_libm_equals_an_independent_correctly_rounded_libm():
+    """The oracle tracking the 50-cell ring with the device's correctly rounded functions and with
+    libquadmath's rounded once: the same bits, so the device's functions are correctly rounded on
+    the arguments tracking produces, not only on the random ones of test_crmath_cpu.py."""
+    eles, p = rings.ring(50)
+    vec = rings.matched_gaussian(eles, 64, seed=4, scale=3.0)
+    with oracle_libm("cr"):
+        a = oracle_track(eles, p, vec, 20)
+    with oracle_libm("quad"):
+        b = oracle_track(eles, p, vec, 20)
+    assert np.array_equal(a["vec"], b["vec"])
+    assert np.array_equal(a["state"], b["state"])
+    with oracle_libm("cr"):
+        pass
+    c = oracle_track(eles, p, vec, 20)        # the host's libm again: not correctly rounded
+    assert not np.array_equal(a["vec"], c["vec"])
