@@ -250,15 +250,26 @@ def run_ours(args):
     t, v = device_bunch()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
     turn = 0
+    # several ranks: each step's per-turn moment sums [T, 28] of the rank's shard, added over the
+    # ranks by one all_reduce (the path's only exchange); timed with the kernel
+    mom = torch.zeros((T, abi.N_MOMENTS), dtype=torch.float64, device=dev) if world > 1 else None
+    job_moments = None
 
     def step(timed):
-        nonlocal turn
+        nonlocal turn, job_moments
         alive0 = t["state"] == abi.ALIVE
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        lib.check(lib.load().bmadgpu_track_bunch_device(ctx.handle, lat.handle, ctypes.byref(v), 0, lat.n_ele, turn, T, None))
-        e1.record(stream)
+        lib.check(lib.load().bmadgpu_track_bunch_device(ctx.handle, lat.handle, ctypes.byref(v), 0, lat.n_ele, turn, T,
+                                                        mom.data_ptr() if mom is not None else None))
+        if mom is not None:
+            torch.cuda.current_stream().wait_stream(stream)
+            job_moments = lib.allreduce_moments(mom)
+            e1.record(torch.cuda.current_stream())
+        else:
+            e1.record(stream)
         ctx.synchronize()
+        torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         alive1 = t["state"] == abi.ALIVE
         lost_now = alive0 & ~alive1
@@ -342,6 +353,8 @@ def run_ours(args):
             "clocks": clk,
             "particles_alive_end": n_alive_end,
         }
+        if job_moments is not None:
+            out["job_n_live_end"] = float(job_moments[-1, 0].item())
         if world == 1:
             out["cpu_baseline"] = cpu_baseline(eles, p, scale)
     lat.close()

@@ -134,7 +134,12 @@ interface
 end interface
 
 type(c_ptr), save :: gpu_ctx = c_null_ptr, gpu_lat = c_null_ptr
-integer, save :: gpu_branch = 0, gpu_turn = 0
+integer, save :: gpu_branch = 0
+! Turn index passed to the tracker (coord%ix_turn of particles lost in a call): advanced by
+! bmadgpu_track_turns and, when the hook tracks the branch's last element, by the hook; a caller
+! whose turn loop starts elsewhere sets it with bmadgpu_set_turn.
+integer, save :: gpu_turn = 0
+type (lat_struct), pointer, save :: gpu_lat_f => null()
 
 contains
 
@@ -181,6 +186,8 @@ if (.not. c_associated(gpu_ctx)) then
 endif
 if (bmadgpu_lattice_create(gpu_ctx, eles, int(n, c_int32_t), param, gpu_lat) /= 0) return
 gpu_branch = ix_branch
+gpu_lat_f => lat
+gpu_turn = 0
 track1_bunch_hook_ptr => bmadgpu_track1_bunch_hook
 err = .false.
 
@@ -245,8 +252,20 @@ if (integer_option(1, direction) /= 1 .or. present(bunch_track)) return   ! Bmad
 if (ele%ix_branch /= gpu_branch .or. ele%ix_ele < 1) return
 call track_on_gpu (bunch, ele%ix_ele - 1, ele%ix_ele, 1, err)
 finished = .not. err
+if (finished .and. ele%ix_ele == gpu_lat_f%branch(gpu_branch)%n_ele_track) gpu_turn = gpu_turn + 1
 
 end subroutine bmadgpu_track1_bunch_hook
+
+!+
+! Subroutine bmadgpu_set_turn (ix_turn)
+! Sets the turn index the next tracking call starts at (recorded in coord%ix_turn of the
+! particles it loses).
+!-
+
+subroutine bmadgpu_set_turn (ix_turn)
+integer ix_turn
+gpu_turn = ix_turn
+end subroutine bmadgpu_set_turn
 
 !+
 ! Subroutine bmadgpu_track_turns (bunch, n_turns, err)
@@ -261,6 +280,7 @@ integer n_turns, n_ele_track
 logical err
 
 call track_on_gpu (bunch, 0, n_ele_track, n_turns, err)
+if (.not. err) gpu_turn = gpu_turn + n_turns
 
 end subroutine bmadgpu_track_turns
 
@@ -272,7 +292,11 @@ logical err
 real(c_double), allocatable, target :: vec(:,:), beta(:), t(:)
 integer(c_int32_t), allocatable, target :: state(:), ix_ele(:), ix_turn(:), location(:)
 type (bmadgpu_bunch_t) b
+type (branch_struct), pointer :: branch
+type (ele_struct), pointer :: ele
 integer j, n, i
+
+branch => gpu_lat_f%branch(gpu_branch)
 
 n = size(bunch%particle)
 allocate (vec(n, 6), beta(n), t(n), state(n), ix_ele(n), ix_turn(n), location(n))
@@ -299,10 +323,19 @@ do j = 1, n
   bunch%particle(j)%t = t(j)
   bunch%particle(j)%state = state(j)
   if (ix_ele(j) >= 0) then        ! lost in this call
+    ! as track1 leaves a particle lost at element ix: ix_ele (track1.f90:92), the location, and s
+    ! at the element's end unless the loss was at its entrance (track1_bmad.f90:277-281)
+    ele => branch%ele(ix_ele(j) + 1)
     bunch%particle(j)%ix_ele = ix_ele(j) + 1
+    bunch%particle(j)%ix_turn = ix_turn(j)
     bunch%particle(j)%location = location(j)
-  else
+    bunch%particle(j)%s = merge(ele%s_start, ele%s, location(j) == upstream_end$)
+  elseif (state(j) == alive$) then
+    ! survivors as track1 leaves them after the last element tracked (track1.f90:92, 296-304;
+    ! track1_bmad.f90:277-281)
+    bunch%particle(j)%ix_ele = ix_end
     bunch%particle(j)%location = downstream_end$
+    bunch%particle(j)%s = branch%ele(ix_end)%s
   endif
 enddo
 bunch%n_live = count(bunch%particle%state == alive$)

@@ -290,6 +290,34 @@ def track_bunch(ctx, lat, bunch, n_turns=1, ix_start=0, ix_end=None, turn0=0, mo
     return mom
 
 
+# ---- several GPUs: particle shards, one collective for the moments ----------------------------
+
+def shard(n, rank, world):
+    """[start, stop) of the particles rank tracks when n particles are shared by world ranks:
+    contiguous ranges whose sizes differ by at most one, in rank order. Particles never interact
+    on this path, so the shards are tracked independently (one process per GPU)."""
+    if world < 1 or not 0 <= rank < world:
+        raise BmadGpuError(abi.EINVAL, "bad rank/world")
+    q, r = divmod(n, world)
+    start = rank * q + min(rank, r)
+    return start, start + q + (1 if rank < r else 0)
+
+
+def allreduce_moments(moments, group=None):
+    """The whole job's per-turn moment sums (n_live, sum vec_i, sum vec_i vec_j: [n_turns, 28]) from
+    each rank's sums over its shard: one all_reduce (sum) of all reported turns at once
+    (torch.distributed; NCCL for CUDA tensors, gloo for CPU ones). The reference gathers the same
+    sums from its MPI workers (bsim/long_term_tracking/long_term_tracking_mpi.f90:344, 381).
+    Takes a float64 torch tensor or numpy array and returns the sums as a new one of the same kind."""
+    import torch
+    import torch.distributed as dist
+    as_numpy = isinstance(moments, np.ndarray)
+    t = torch.from_numpy(np.array(moments, dtype=np.float64, copy=True)) if as_numpy else moments.clone()
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.numpy() if as_numpy else t
+
+
 def autotune(ctx, lat, device_bunch_view, sample_n=0):
     """Run the library's launch-shape autotuner on a device-resident bunch view (abi.Bunch of
     device pointers); returns the chosen tuning (also set on the context)."""
