@@ -653,8 +653,10 @@ def run_serve(args, peak=None):
     st = run_stream(pinned_inputs())
     clk = clocks.stop()
     value = st["particle_turns"] / st["elapsed_s"]
-    # plain kernel: jobs one after another (host buffers, synchronous), on a random sample
-    ctx.set_tuning(block=64, ctas_per_sm=12, stage_smem=0, turns_per_launch=64, compact=1)
+    # plain kernel: jobs one after another (host buffers, synchronous), on a random sample, at the
+    # plain kernel's default shape (the fastest measured on the 50- and 200-cell rings), compacting
+    # the live list every 64 turns
+    ctx.set_tuning(block=256, ctas_per_sm=2, stage_smem=1, turns_per_launch=64, compact=1)
     sample = np.random.default_rng(7).choice(len(jobs), size=min(args.plain_sample, len(jobs)), replace=False)
     p_s, p_pt = 0.0, 0
     for k in sample:
@@ -678,7 +680,8 @@ def run_serve(args, peak=None):
                    "host_prep_s": t_prep},
         "fma": fma_summary,
         "latency_s": {"p50": st["latency_p50_s"], "p99": st["latency_p99_s"], "max": st["latency_max_s"]},
-        "server": {k: st[k] for k in ("jobs_done", "rounds", "particle_turns", "capacity", "peak_resident")},
+        "server": {k: st[k] for k in ("jobs_done", "rounds", "particle_turns", "capacity", "peak_resident",
+                                      "gpu_busy_s", "gpu_idle_s", "gpu_max_gap_s")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": n_part * (8 * 8 + 4 * 4),
                 "d2h_bytes_per_step": n_part * (8 * 8 + 4 * 4)},
         "plain_kernel": {"value": plain, "unit": UNIT, "ratio": value / plain,

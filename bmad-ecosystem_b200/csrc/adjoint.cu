@@ -123,7 +123,7 @@ extern "C" int bmadgpu_loss_grad(bmadgpu_ctx* c, const bmadgpu_lattice* lat, con
     if (adj_supported(hdr[i]))
       return fail(BMADGPU_EUNSUPPORTED, "element " + std::to_string(i) +
                                             " is outside the adjoint path (edge fringe, bend k1 or multipoles, thin "
-                                            "multipole, or more than 16 steps)");
+                                            "multipole, pitch or z_offset, or more than 16 steps)");
   std::vector<int32_t> slot_of(n_ele, -1);
   std::vector<double> strength(n_param);
   for (int32_t s = 0; s < n_param; s++) {

@@ -15,7 +15,7 @@ BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b,
   const double* kf = kh + 2 * np;
   const double* mis = b + 3 + 4 * np;
   const bool has_t = h.flags & F_TILT;
-  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, h.flags & F_PITCH);
   const double b1 = b[0], length = b[1], step_len = b[2];
   const int n_step = h.n_step;
   const bool b_from2 = h.flags & F_KICK_B_FROM2;
@@ -23,7 +23,7 @@ BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b,
     if (i > 0) quad_step(p, b1, length, step_len, G);
     if (np) ab_kicks(p, (i == 0 || i == n_step) ? kh : kf, np, b_from2);
   }
-  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, h.flags & F_PITCH);
 }
 
 BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b) {
@@ -33,7 +33,7 @@ BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b
   const double* kf = kh + 2 * np;
   const double* mis = b + 1 + 4 * np;
   const bool has_t = h.flags & F_TILT;
-  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, h.flags & F_PITCH);
   const double step_len = b[0];
   const int n_step = h.n_step;
   const bool b_from2 = h.flags & F_KICK_B_FROM2;
@@ -41,7 +41,7 @@ BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b
     if (i > 0) drift(p, step_len);
     if (np) ab_kicks(p, (i == 0 || i == n_step) ? kh : kf, np, b_from2);
   }
-  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, h.flags & F_PITCH);
 }
 
 BG_HD void bend_kick(Particle& p, const double* __restrict__ b, int np, double coef, const Globals& G) {
@@ -106,7 +106,7 @@ BG_HD void body_rf(Particle& p, const EleHdr& h, const double* __restrict__ b, c
   const double* kh = b + RF_FIXED;
   const double* mis = kh + 2 * np;
   const bool has_t = h.flags & F_TILT;
-  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t);
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, h.flags & F_PITCH);
   if (np) ab_kicks(p, kh, np);
   const double voltage = b[0], f = b[1], slice_len = b[4];
   const int n_slice = h.n_step;
@@ -128,7 +128,7 @@ BG_HD void body_rf(Particle& p, const EleHdr& h, const double* __restrict__ b, c
   }
   refresh(p, G);
   if (np) ab_kicks(p, kh, np);
-  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t);
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, h.flags & F_PITCH);
 }
 
 // track1 around one element: entrance orbit/aperture checks, body, exit checks

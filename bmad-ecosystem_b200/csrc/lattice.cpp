@@ -381,8 +381,8 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
       if (e.key == BMADGPU_MULTIPOLE && any_nonzero(e.a_pole_elec, kNPole))
         fail(BMADGPU_EUNSUPPORTED, "multipole ksl");
       if (e.x_pitch != 0 || e.y_pitch != 0 || e.z_offset != 0)
-        if (e.key != BMADGPU_DRIFT && e.key != BMADGPU_MARKER)
-          fail(BMADGPU_EUNSUPPORTED, "pitch / z_offset misalignment");
+        if (e.key == BMADGPU_SBEND || e.key == BMADGPU_MULTIPOLE || e.key == BMADGPU_AB_MULTIPOLE)
+          fail(BMADGPU_EUNSUPPORTED, "pitch / z_offset misalignment of a bend or thin multipole");
       if (e.key == BMADGPU_SBEND && (e.tilt != 0 || e.roll != 0 || e.x_offset != 0 || e.y_offset != 0))
         fail(BMADGPU_EUNSUPPORTED, "misaligned sbend (bend_shift geometry)");
       if (e.key != BMADGPU_SBEND && e.ref_tilt != 0) fail(BMADGPU_EUNSUPPORTED, "ref_tilt on a non-bend");
@@ -396,9 +396,10 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
       if (e.aperture_at < 1 || e.aperture_at > 4) fail(BMADGPU_EUNSUPPORTED, "aperture_at");
 
       double tilt_tot = (e.key == BMADGPU_SBEND) ? 0.0 : e.tilt;
+      const bool pitched = e.x_pitch != 0 || e.y_pitch != 0 || e.z_offset != 0;
       bool has_misalign = (e.key == BMADGPU_SBEND)
                               ? (e.ref_tilt != 0 || e.roll != 0)
-                              : (e.tilt != 0 || e.x_offset != 0 || e.y_offset != 0);
+                              : (e.tilt != 0 || e.x_offset != 0 || e.y_offset != 0 || pitched);
       double ds_step;
       int num_steps;
       resolve_steps(e, p, tilt_tot, &ds_step, &num_steps);
@@ -437,6 +438,27 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
       auto misalign_block = [&](double tilt) {
         mis = {e.x_offset, e.y_offset, l_cos(tilt), l_sin(tilt)};
         flags |= F_MISALIGN;
+        if (pitched) {
+          // offset_particle.f90:239-245, 279-282 (set) and 437-443, 477-480 (unset), straight
+          // geometry: the offsets, the rotation floor_angles_to_w_mat(x_pitch, y_pitch, 0)
+          // (bmad/geometry/floor_angles_to_w_mat.f90) and its inverse, the drift to the edge
+          const double L_half = 0.5 * e.l;
+          mis.insert(mis.end(), {e.z_offset, L_half, L_half - 0.0, L_half - e.l, (1 + 1) * L_half});
+          const double s_the = l_sin(e.x_pitch), c_the = l_cos(e.x_pitch);
+          const double s_phi = l_sin(e.y_pitch), c_phi = l_cos(e.y_pitch);
+          const double s_psi = l_sin(0.0), c_psi = l_cos(0.0);
+          const double winv[9] = {c_the * c_psi - s_the * s_phi * s_psi, c_phi * s_psi,
+                                  -s_the * c_psi - c_the * s_phi * s_psi, -c_the * s_psi - s_the * s_phi * c_psi,
+                                  c_phi * c_psi, s_the * s_psi - c_the * s_phi * c_psi,
+                                  s_the * c_phi, s_phi, c_the * c_phi};
+          const double w[9] = {c_the * c_psi - s_the * s_phi * s_psi, -c_the * s_psi - s_the * s_phi * c_psi,
+                               s_the * c_phi, c_phi * s_psi, c_phi * c_psi, s_phi,
+                               -s_the * c_psi - c_the * s_phi * s_psi, s_the * s_psi - c_the * s_phi * c_psi,
+                               c_the * c_phi};
+          mis.insert(mis.end(), winv, winv + 9);
+          mis.insert(mis.end(), w, w + 9);
+          flags |= F_PITCH;
+        }
       };
 
       switch (key) {
@@ -599,13 +621,13 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           }
           h.n_step = (uint16_t)std::min(n_slice, 65535);
           if (n_slice > 65535) fail(BMADGPU_EUNSUPPORTED, "too many rf slices");
-          if (e.tilt != 0 || e.x_offset != 0 || e.y_offset != 0) misalign_block(tilt_tot);
+          if (e.tilt != 0 || e.x_offset != 0 || e.y_offset != 0 || pitched) misalign_block(tilt_tot);
           break;
         }
         default:
           fail(BMADGPU_EUNSUPPORTED, "element type");
       }
-      if ((flags & F_MISALIGN) && mis.size() == 4 && mis[3] != 0) flags |= F_TILT;
+      if ((flags & F_MISALIGN) && mis.size() >= 4 && mis[3] != 0) flags |= F_TILT;
       blk.insert(blk.end(), mis.begin(), mis.end());
       h.flags = flags;
       h.param = pk.add_block(blk);

@@ -30,8 +30,10 @@
 // (hostcheck.cpp: op counting and algorithm checks on CPU), for the host.
 #if defined(__CUDACC__)
 #define BG_HD __device__ __forceinline__
+#define BG_COLD static __device__ __noinline__   // rare forms: one out-of-line copy
 #else
 #define BG_HD inline
+#define BG_COLD inline
 #endif
 
 namespace bmadgpu {
@@ -464,10 +466,91 @@ BG_HD void tilt(Particle& p, double c, double s) {
   p.py = (0 + -s * px) + c * py;
 }
 
+// track_a_drift without the reference motion (include_ref_motion = .false.,
+// track_a_drift.f90:25-116): the drift of offset_particle to the element's nominal edge.
+BG_HD void drift_noref(Particle& p, double length) {
+  double rel_pc = 1 + p.pz;
+  double px_rel = div_rcp(p.px, rel_pc, p.e_factor);
+  double py_rel = div_rcp(p.py, rel_pc, p.e_factor);
+  double pxy2 = px_rel * px_rel + py_rel * py_rel;
+  if (pxy2 >= 1) { p.state = S_LOST_PZ; return; }
+  double ps_rel = sqrt(1 - pxy2);
+  const double inv_ps = shared_rcp(ps_rel);
+  p.x = p.x + div_rcp(length * px_rel, ps_rel, inv_ps);
+  p.y = p.y + div_rcp(length * py_rel, ps_rel, inv_ps);
+  p.z = p.z + 1 * div_rcp(-length, ps_rel, inv_ps);
+}
+
+// Fortran matmul(w, r) for a 3x3 w (row-major here), summed in the order of the inlined loop.
+BG_HD void matvec3(const double* __restrict__ w, const double r[3], double out[3]) {
+  for (int i = 0; i < 3; i++) out[i] = ((0 + w[3 * i] * r[0]) + w[3 * i + 1] * r[1]) + w[3 * i + 2] * r[2];
+}
+
+// offset_particle set/unset of straight elements with pitches or z_offset (offset_particle.f90:
+// 239-258, 279-282 set; 437-458, 477-480 unset): the offset position rotated by W^-1 (set) or W
+// (unset), the momentum by the same rotation, then the drift to the nominal edge; the tilt last
+// (set) or first (unset). m: the 27-double misalign block (table.h).
+BG_COLD void offset_set_pitched(Particle& p, const double* __restrict__ m, bool has_tilt) {
+  const double L_half = m[5], ds_center = m[6];
+  const double r[3] = {p.x - m[0], p.y - m[1], 0.0 - (m[4] + 1 * ds_center)};
+  double q[3];
+  matvec3(m + 9, r, q);
+  q[2] = q[2] + L_half;
+  const double s_body = q[2];
+  const double rel_p = 1 + p.pz;
+  const double pz2 = rel_p * rel_p - p.px * p.px - p.py * p.py;
+  if (pz2 <= 0) {
+    p.state = S_LOST_PZ;
+  } else {
+    const double v[3] = {p.px, p.py, 1 * sqrt(pz2)};
+    double pv[3];
+    matvec3(m + 9, v, pv);
+    p.px = pv[0];
+    p.py = pv[1];
+    p.x = q[0];
+    p.y = q[1];
+  }
+  const double ds = (1 - 1) * L_half - s_body;
+  if (fabs(ds) > 1e-14 && p.state == S_ALIVE) drift_noref(p, ds);
+  if (has_tilt) tilt(p, m[2], m[3]);
+}
+BG_COLD void offset_unset_pitched(Particle& p, const double* __restrict__ m, bool has_tilt) {
+  if (has_tilt) tilt(p, m[2], -m[3]);
+  const double L_half = m[5];
+  double r[3] = {p.x, p.y, 0.0};
+  r[2] = r[2] - m[7];
+  double q[3];
+  matvec3(m + 18, r, q);
+  q[0] = q[0] + m[0];
+  q[1] = q[1] + m[1];
+  q[2] = q[2] + (m[4] + L_half);
+  const double s_lab = q[2];
+  const double rel_p = 1 + p.pz;
+  const double pz2 = rel_p * rel_p - p.px * p.px - p.py * p.py;
+  if (pz2 <= 0) {
+    p.state = S_LOST_PZ;
+  } else {
+    const double v[3] = {p.px, p.py, 1 * sqrt(pz2)};
+    double pv[3];
+    matvec3(m + 18, v, pv);
+    p.px = pv[0];
+    p.py = pv[1];
+    p.x = q[0];
+    p.y = q[1];
+  }
+  const double ds = m[8] - s_lab;
+  if (fabs(ds) > 1e-14 && p.state == S_ALIVE) drift_noref(p, ds);
+}
+
 // offset_particle set/unset for straight elements with x/y offsets and tilt, no pitches or
 // z_offset (offset_particle.f90:201-330, 374-459): the transforms reduce to exact shifts, the
-// pz-loss test and tilt_coords; no drift to the edge is needed (s_body = s_target).
-BG_HD void offset_set(Particle& p, const double* __restrict__ m, bool has_tilt) {
+// pz-loss test and tilt_coords; no drift to the edge is needed (s_body = s_target). With
+// pitched, the general form above.
+BG_HD void offset_set(Particle& p, const double* __restrict__ m, bool has_tilt, bool pitched = false) {
+  if (pitched) {
+    offset_set_pitched(p, m, has_tilt);
+    return;
+  }
   if (m[0] != 0 || m[1] != 0) {
     p.x = p.x - m[0];
     p.y = p.y - m[1];
@@ -476,7 +559,11 @@ BG_HD void offset_set(Particle& p, const double* __restrict__ m, bool has_tilt) 
   }
   if (has_tilt) tilt(p, m[2], m[3]);
 }
-BG_HD void offset_unset(Particle& p, const double* __restrict__ m, bool has_tilt) {
+BG_HD void offset_unset(Particle& p, const double* __restrict__ m, bool has_tilt, bool pitched = false) {
+  if (pitched) {
+    offset_unset_pitched(p, m, has_tilt);
+    return;
+  }
   if (has_tilt) tilt(p, m[2], -m[3]);
   if (m[0] != 0 || m[1] != 0) {
     double rel_p = 1 + p.pz;

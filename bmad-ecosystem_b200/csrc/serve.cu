@@ -135,6 +135,7 @@ struct Job {
 struct Round {
   int64_t index;
   cudaEvent_t done;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;  // timing: the round's first and last operation
   int parity;                  // live list the round read
   std::vector<int64_t> jobs;   // jobs with work in the round
 };
@@ -179,6 +180,9 @@ struct bmadgpu_server {
   int64_t peak_resident = 0;
   double t_first = -1, t_last = -1;
   std::vector<double> latencies;
+  // the compute stream's timeline: busy time of the rounds, the gaps between consecutive rounds
+  cudaEvent_t t_ref = nullptr;
+  double prev_end_ms = -1, busy_ms = 0, idle_ms = 0, max_gap_ms = 0;
   bool stop = false;
   int err_code = 0;
   std::string err_msg;
@@ -449,13 +453,16 @@ void worker_main(bmadgpu_server* s) {
       rd.parity = parity;
       rd.jobs = round_jobs;
       rd.done = nullptr;
-      ok = cudaMemcpyAsync(s->d_vars, s->h_vars[buf], sizeof(BatchVar) * n_var, cudaMemcpyHostToDevice, c) ==
+      ok = cudaEventCreate(&rd.t0) == cudaSuccess && cudaEventCreate(&rd.t1) == cudaSuccess &&
+           cudaEventRecord(rd.t0, c) == cudaSuccess &&
+           cudaMemcpyAsync(s->d_vars, s->h_vars[buf], sizeof(BatchVar) * n_var, cudaMemcpyHostToDevice, c) ==
                cudaSuccess &&
            batch_launch_plan(s->d_vars, n_var, a.tile, 0, false, a.n_in, s->d_prefix, s->d_queue, a.n_out, c) ==
                cudaSuccess &&
            batch_launch_track(s->kern, a, c, round_records) == cudaSuccess &&
            cudaMemcpyAsync(s->h_cnt[buf], a.n_out, sizeof(unsigned long long) * n_var, cudaMemcpyDeviceToHost, c) ==
                cudaSuccess &&
+           cudaEventRecord(rd.t1, c) == cudaSuccess &&
            cudaEventCreateWithFlags(&rd.done, cudaEventDisableTiming) == cudaSuccess &&
            cudaEventRecord(rd.done, c) == cudaSuccess;
       if (!ok) {
@@ -481,6 +488,27 @@ void worker_main(bmadgpu_server* s) {
         return;
       }
       const int b = (int)(rd.index % kRoundsInFlight);
+      {
+        // rounds run one after another on the compute stream: their busy time, and the gaps in
+        // which the stream waited for the worker (admission, bookkeeping) or for work
+        if (!s->t_ref) {
+          s->t_ref = rd.t0;
+          rd.t0 = nullptr;
+        }
+        float a_ms = 0, b_ms = 0;
+        if (rd.t0) cudaEventElapsedTime(&a_ms, s->t_ref, rd.t0);
+        cudaEventElapsedTime(&b_ms, s->t_ref, rd.t1);
+        lk.lock();
+        s->busy_ms += b_ms - a_ms;
+        if (s->prev_end_ms >= 0 && a_ms > s->prev_end_ms) {
+          s->idle_ms += a_ms - s->prev_end_ms;
+          s->max_gap_ms = std::max(s->max_gap_ms, (double)(a_ms - s->prev_end_ms));
+        }
+        s->prev_end_ms = b_ms;
+        lk.unlock();
+        if (rd.t0) cudaEventDestroy(rd.t0);
+        cudaEventDestroy(rd.t1);
+      }
       std::vector<Job*> finishing;
       lk.lock();
       for (int64_t id : rd.jobs) {
@@ -595,8 +623,10 @@ int bmadgpu_server_create(bmadgpu_ctx* c, const bmadgpu_server_config* cfg_in, b
   if (cfg.element_steps == 0) cfg.element_steps = 4096;
   if (cfg.target_live == 0) cfg.target_live = 1 << 20;
   if (cfg.block == 0) {
-    cfg.block = 64;
-    if (cfg.ctas_per_sm == 0) cfg.ctas_per_sm = 12;
+    // 128 x 4 measured fastest on the mixed request stream (200 jobs: 1.59e7 particle-turns/s
+    // against 1.45e7 for 64 x 12 and 1.57e7 for 256 x 2)
+    cfg.block = 128;
+    if (cfg.ctas_per_sm == 0) cfg.ctas_per_sm = 4;
   }
   CUDA_TRY(cudaSetDevice(c->device));
   size_t free_b = 0, total_b = 0;
@@ -680,6 +710,10 @@ int bmadgpu_server_destroy(bmadgpu_server* s) {
   if (s->s_copy) cudaStreamSynchronize(s->s_copy);
   for (auto& kv : s->jobs) {
     if (kv.second.ev_up) cudaEventDestroy(kv.second.ev_up);
+    if (s->t_ref) {
+      cudaEventDestroy(s->t_ref);
+      s->t_ref = nullptr;
+    }
     if (kv.second.ev_down) cudaEventDestroy(kv.second.ev_down);
     if (kv.second.h_fma) cudaFreeHost(kv.second.h_fma);
   }
@@ -857,6 +891,9 @@ int bmadgpu_server_get_stats(bmadgpu_server* s, bmadgpu_server_stats* st) {
   st->elapsed_s = (s->t_first >= 0 && s->t_last >= 0) ? s->t_last - s->t_first : 0.0;
   st->capacity = s->capacity;
   st->peak_resident = s->peak_resident;
+  st->gpu_busy_s = s->busy_ms / 1e3;
+  st->gpu_idle_s = s->idle_ms / 1e3;
+  st->gpu_max_gap_s = s->max_gap_ms / 1e3;
   if (!s->latencies.empty()) {
     std::vector<double> l = s->latencies;
     std::sort(l.begin(), l.end());

@@ -38,7 +38,8 @@ enum Flag : uint16_t {
   F_BEND_DRIFT = 1 << 9,   // sbend with g == 0 and dg == 0 or zero step: drift body
   F_ZERO_LEN = 1 << 10,    // element length is zero
   F_TILT = 1 << 11,        // misalign block carries a non-zero tilt rotation
-  F_KICK_B_FROM2 = 1 << 12 // both kick arrays: every a_n zero and b_0 = b_1 = 0, at least 3 orders
+  F_KICK_B_FROM2 = 1 << 12, // both kick arrays: every a_n zero and b_0 = b_1 = 0, at least 3 orders
+  F_PITCH = 1 << 13        // misalign block of the pitched form (pitches and/or z_offset)
 };
 
 struct EleHdr {            // 16 bytes
@@ -69,7 +70,9 @@ struct ApRec {             // 32 bytes: rectangular/elliptical limits (x1_lim = 
 //           [5] n_slice  then kicks (half kicks 0.5*r_step), then misalign
 // kicks: n_pole pairs for the end (half) kick followed, for K_QUAD/K_THICK, by n_pole pairs for
 //        the interior (full) kick: (b_n*scale, a_n*scale), n = 0 .. n_pole-1.
-// misalign: [x_off, y_off, cos_t, sin_t]
+// misalign: [x_off, y_off, cos_t, sin_t]; with F_PITCH (straight elements with x/y pitch or
+//           z_offset) followed by [z_off, L/2, L/2 - 0, L/2 - L, 2 (L/2)] and the rotations W^-1
+//           and W of floor_angles_to_w_mat(x_pitch, y_pitch, 0), row-major: 27 doubles
 constexpr int SB_EDGE_IN = 12, SB_EDGE_OUT = 19, SB_FIXED = 26;
 constexpr int RF_FIXED = 6;
 

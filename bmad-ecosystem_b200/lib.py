@@ -193,7 +193,17 @@ class Context:
         check(load().bmadgpu_measure_fp64_peak(self._h, C.byref(f)))
         return f.value
 
+    def adopt(self, obj):
+        """Objects made on this context (batches, servers) are closed before it: their C destroy
+        calls use the context's stream."""
+        import weakref
+        if not hasattr(self, "_children"):
+            self._children = weakref.WeakSet()
+        self._children.add(obj)
+
     def close(self):
+        for obj in list(getattr(self, "_children", ())):
+            obj.close()
         if self._h:
             load().bmadgpu_ctx_destroy(self._h)
             self._h = C.c_void_p()
@@ -351,6 +361,7 @@ class Batch:
         hc = (C.c_int64 * n)(*self.counts)
         self._h = C.c_void_p()
         check(lib.bmadgpu_batch_create(ctx.handle, n, hl, hc, C.byref(self._h)))
+        ctx.adopt(self)
         self.offsets = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
 
     @property
@@ -469,7 +480,8 @@ class ServerStats(C.Structure):
     _fields_ = [("jobs_submitted", C.c_int64), ("jobs_done", C.c_int64), ("rounds", C.c_int64),
                 ("particle_turns", C.c_int64), ("elapsed_s", C.c_double), ("latency_p50_s", C.c_double),
                 ("latency_p99_s", C.c_double), ("latency_max_s", C.c_double), ("capacity", C.c_int64),
-                ("peak_resident", C.c_int64)]
+                ("peak_resident", C.c_int64), ("gpu_busy_s", C.c_double), ("gpu_idle_s", C.c_double),
+                ("gpu_max_gap_s", C.c_double)]
 
 
 SERVE_SRPT, SERVE_FIFO = 0, 1
@@ -561,6 +573,7 @@ class Server:
             setattr(c, k, v)
         self._h = C.c_void_p()
         check(lib.bmadgpu_server_create(ctx.handle, C.byref(c), C.byref(self._h)))
+        ctx.adopt(self)
         self._keep = {}
 
     def submit(self, lat, bunch, n_turns, turn0=0):

@@ -143,6 +143,8 @@ const char* bmadgpu_last_error(void);
 
 /* One context per host thread and device; it owns a CUDA stream and device scratch. */
 int bmadgpu_ctx_create(int32_t device, bmadgpu_ctx** out);
+/* Destroy a context only after the batches and servers made on it (their destroy calls use the
+ * context's stream); lattices may outlive it. */
 int bmadgpu_ctx_destroy(bmadgpu_ctx* ctx);
 
 /* Packs the element records into the device element table (per-element invariants hoisted,
@@ -340,8 +342,8 @@ typedef struct bmadgpu_server_config {
   int32_t element_steps;   /* element passes per particle per round (0: 4096) */
   int64_t target_live;     /* no admission while this many live particles are resident (0: 1,048,576) */
   int32_t policy;          /* BMADGPU_SERVE_SRPT or BMADGPU_SERVE_FIFO */
-  int32_t block;           /* round kernel shape as bmadgpu_batch_tuning (0: 64) */
-  int32_t ctas_per_sm;     /* (0 with block 0: 12) */
+  int32_t block;           /* round kernel shape as bmadgpu_batch_tuning (0: 128) */
+  int32_t ctas_per_sm;     /* (0 with block 0: 4) */
   int32_t stage_smem;      /* stage element tables of up to 64 KiB in shared memory */
   int32_t record_mib;      /* record arena of frequency-map jobs in MiB (0: a quarter of the device
                               memory still free after the particle arena) */
@@ -361,6 +363,10 @@ typedef struct bmadgpu_server_stats {
   double latency_p50_s, latency_p99_s, latency_max_s;  /* t_done - t_submit over finished jobs */
   int64_t capacity;        /* resident particle capacity */
   int64_t peak_resident;   /* most particles resident at once */
+  /* the compute stream's timeline over the completed rounds (first round's start to the last
+   * one's end): time inside rounds, the sum of the gaps between consecutive rounds (the stream
+   * waiting for the worker's admission and bookkeeping, or for work), and the longest gap */
+  double gpu_busy_s, gpu_idle_s, gpu_max_gap_s;
 } bmadgpu_server_stats;
 
 /* cfg may be NULL (all defaults). The server runs on the context's device with its own streams. */

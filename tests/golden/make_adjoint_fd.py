@@ -1,7 +1,8 @@
 """Generates adjoint_config4_fd.json: central finite differences of the oracle's loss on the
 differentiation workload (50-cell ring, 4,096 matched Gaussian particles from seed 2, 256
-turns, loss = mean over particles of x^2 + y^2), for a few quadrupole k1 and sextupole k2
-values. The GPU test compares the adjoint kernel's gradient with these at full size.
+turns, loss = mean over particles of x^2 + y^2), for 12 quadrupole k1 and 12 sextupole k2 values.
+The GPU test compares the adjoint kernel's gradient with these at full size (all 200 components
+are compared there with finite differences of the GPU's own forward tracking).
 
 Stencil: fourth-order central differences, [8 (L(+h) - L(-h)) - (L(+2h) - L(-2h))] / (12 h k),
 at h = 1e-5 relative for quadrupoles and 2e-3 for sextupoles: over 256 turns a 1e-5 change of a
@@ -30,7 +31,10 @@ abi = importlib.import_module("bmad-ecosystem_b200.abi")
 rings = importlib.import_module("bmad-ecosystem_b200.rings")
 
 N_CELLS, N_PART, SEED, N_TURNS = 50, 4096, 2, 256
-QUAD_SLOTS, SEXT_SLOTS = [0, 102, 198], [1, 103, 199]
+# 12 quadrupoles and 12 sextupoles spread over the ring (slots alternate quadrupole, sextupole,
+# quadrupole, sextupole in each cell), the ring's first and last of each among them
+QUAD_SLOTS = [0, 18, 34, 52, 68, 86, 102, 118, 136, 152, 170, 198]
+SEXT_SLOTS = [1, 19, 35, 53, 69, 87, 103, 119, 137, 153, 171, 199]
 
 
 def loss_of(elements, p, vec):

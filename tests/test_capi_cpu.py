@@ -57,15 +57,15 @@ def test_config1_ring_packs_and_sextupoles_use_one_step():
     assert all(s == 1 for e, s in zip(eles, steps) if e.key == abi.SEXTUPOLE)
 
 
-@pytest.mark.parametrize("bad", ["elec", "pitch", "bend_offset", "abs_time"])
+@pytest.mark.parametrize("bad", ["elec", "bend_pitch", "bend_offset", "abs_time"])
 def test_unsupported_inputs_fail_loudly(bad):
     abi = load_abi()
     p = abi.electron_param(3e9)
     e = abi.default_element(abi.QUADRUPOLE, l=0.4, k1=0.5)
     if bad == "elec":
         e.b_pole_elec[1] = 1e3
-    elif bad == "pitch":
-        e.y_pitch = 1e-3
+    elif bad == "bend_pitch":
+        e = abi.default_element(abi.SBEND, l=1.0, g=0.01, y_pitch=1e-3)
     elif bad == "bend_offset":
         e = abi.default_element(abi.SBEND, l=1.0, g=0.01, x_offset=1e-3)
     else:
@@ -80,3 +80,14 @@ def test_optics_of_benchmark_ring_is_stable():
     tw = rings.periodic_optics(eles)
     assert 0 < tw["tune_a"] < 1 and 0 < tw["tune_b"] < 1
     assert tw["beta_a"] > 0 and tw["beta_b"] > 0
+
+
+def test_pitched_straight_elements_are_accepted():
+    """Pitches and z_offset of straight elements are on the device path (the pitched offset form)."""
+    abi = load_abi()
+    p = abi.electron_param(3e9)
+    for key in (abi.QUADRUPOLE, abi.SEXTUPOLE, abi.RFCAVITY):
+        e = abi.default_element(key, l=0.4, k1=0.5, y_pitch=1e-3, x_pitch=-2e-3, z_offset=0.01)
+        if key == abi.RFCAVITY:
+            e.voltage, e.rf_frequency = 1e6, 5e8
+        lib.lattice_check([e], p)

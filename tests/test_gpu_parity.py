@@ -63,9 +63,7 @@ def assert_close(g, o, tol, floor_frac=1.0, alive_only=True):
 # Golden cases whose element form the device path refuses (BMADGPU_EUNSUPPORTED), by name, with
 # the reason; every other case runs on the GPU against its golden line.
 REFUSED_ON_DEVICE = {
-    "OCTUPOLE1": "pitch and z_offset", "SEXTUPOLE1": "pitch and z_offset", "RFCAVITY1": "pitch and z_offset",
-    "RFCAVITY3": "pitch and z_offset", "QUADRUPOLE1": "electric multipoles", "QUADRUPOLE2": "electric multipoles",
-    "QUADRUPOLE3": "electric multipoles",
+    "QUADRUPOLE1": "electric multipoles", "QUADRUPOLE2": "electric multipoles", "QUADRUPOLE3": "electric multipoles",
 }
 
 
@@ -119,6 +117,12 @@ def _single_element_cases():
         "multipole": [E(abi.MULTIPOLE, a_pole={0: 1e-4, 1: 0.02, 2: 0.5}, b_pole={1: 0.1, 2: 0.2}, x_offset=1e-4)],
         "ab_multipole": [E(abi.AB_MULTIPOLE, a_pole={2: 0.3}, b_pole={1: 0.01, 2: 0.5}, tilt=0.1)],
         "marker": [E(abi.MARKER)],
+        "sextupole_pitched": [E(abi.SEXTUPOLE, l=0.6, k2=1.0, tilt=0.52, num_steps=10, x_offset=0.05, y_pitch=0.001,
+                                z_offset=0.02, **ap)],
+        "quad_pitched": [E(abi.QUADRUPOLE, l=0.4, k1=-0.8, x_pitch=-2e-3, y_pitch=1e-3, z_offset=-0.01, y_offset=1e-4,
+                           **ap)],
+        "rf_pitched": [E(abi.RFCAVITY, l=1.2, voltage=2e6, rf_frequency=500e6, x_pitch=1e-3, tilt=0.1, x_offset=1e-4,
+                         **ap)],
     }
 
 

@@ -63,6 +63,12 @@ CASES = {
     "rf_thick": lambda E, ap: [E(abi.RFCAVITY, l=1.2, voltage=2e6, rf_frequency=500e6, phi0=0.05, **ap)],
     "multipole": lambda E, ap: [E(abi.MULTIPOLE, a_pole={0: 1e-4, 1: 0.02, 2: 0.5}, b_pole={1: 0.1, 2: 0.2}, x_offset=1e-4)],
     "ab_multipole": lambda E, ap: [E(abi.AB_MULTIPOLE, a_pole={2: 0.3}, b_pole={1: 0.01, 2: 0.5}, tilt=0.1)],
+    "sextupole_pitched": lambda E, ap: [E(abi.SEXTUPOLE, l=0.6, k2=1.0, tilt=0.52, num_steps=10, x_offset=0.05,
+                                          y_pitch=0.001, z_offset=0.02, **ap)],
+    "quad_pitched": lambda E, ap: [E(abi.QUADRUPOLE, l=0.4, k1=-0.8, x_pitch=-2e-3, y_pitch=1e-3, z_offset=-0.01,
+                                     y_offset=1e-4, **ap)],
+    "rf_pitched": lambda E, ap: [E(abi.RFCAVITY, l=1.2, voltage=2e6, rf_frequency=500e6, x_pitch=1e-3, tilt=0.1,
+                                   x_offset=1e-4, **ap)],
 }
 
 
