@@ -7,9 +7,8 @@
 // Fortran file and lines it restates (paths inside bmad-sim/bmad-ecosystem). Expressions keep
 // the Fortran operand order; the file is compiled with -ffp-contract=off.
 //
-// Not restated (returns BMADGPU_EUNSUPPORTED): misaligned bends with g != 0 (bend_shift
-// geometry), exact_multipoles, electric multipoles inside bends, fringe_type full /
-// soft_edge_only / sad_full / linear_edge edges, elseparators and kickers, reversed
+// Not restated (returns BMADGPU_EUNSUPPORTED): rolled bends, exact_multipoles, fringe_type
+// full / soft_edge_only / sad_full / linear_edge edges, elseparators and kickers, reversed
 // orientation / direction / time, absolute time tracking, radiation and spin.
 
 #include "bmad_oracle.h"
@@ -654,8 +653,109 @@ void matvec3(const double w[3][3], const double r[3], double out[3]) {
   }
 }
 
-// offset_particle, bmad/code/offset_particle.f90:66-530, for straight-geometry transforms
-// (non-bends, and bends without offsets/pitches/roll); set_hvkicks and set_tilt as given.
+// ---- bend geometry for misaligned bends -----------------------------------------------------
+
+// cos_one, sim_utils/special_functions/cos_one.f90:16-27
+double cos_one(double angle) {
+  double s = lm.sin(angle / 2);
+  return -2 * (s * s);
+}
+
+enum { x_axis = 1, y_axis = 2, z_axis = 3 };
+
+// rotate_vec, sim_utils/math/rotation_3d_mod.f90:737-760
+void rotate_vec(double v[3], int axis, double angle) {
+  if (angle == 0) return;
+  double ca = lm.cos(angle), sa = lm.sin(angle);
+  if (axis == x_axis) {
+    double a = ca * v[1] - sa * v[2], b = sa * v[1] + ca * v[2];
+    v[1] = a; v[2] = b;
+  } else if (axis == y_axis) {
+    double a = sa * v[2] + ca * v[0], b = ca * v[2] - sa * v[0];
+    v[0] = a; v[2] = b;
+  } else {
+    double a = ca * v[0] - sa * v[1], b = sa * v[0] + ca * v[1];
+    v[0] = a; v[1] = b;
+  }
+}
+
+// rotate_mat (rotation applied from the left), rotation_3d_mod.f90:781-845
+void rotate_mat(double m[3][3], int axis, double angle) {
+  if (angle == 0) return;
+  double ca = lm.cos(angle), sa = lm.sin(angle);
+  for (int k = 0; k < 3; k++) {
+    if (axis == x_axis) {
+      double a = ca * m[1][k] - sa * m[2][k], b = sa * m[1][k] + ca * m[2][k];
+      m[1][k] = a; m[2][k] = b;
+    } else if (axis == y_axis) {
+      double a = sa * m[2][k] + ca * m[0][k], b = ca * m[2][k] - sa * m[0][k];
+      m[0][k] = a; m[2][k] = b;
+    } else {
+      double a = ca * m[0][k] - sa * m[1][k], b = sa * m[0][k] + ca * m[1][k];
+      m[0][k] = a; m[1][k] = b;
+    }
+  }
+}
+
+// Fortran matmul of two 3x3 matrices (j-order summation).
+void matmul3(const double a[3][3], const double b[3][3], double out[3][3]) {
+  double t[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int k = 0; k < 3; k++) {
+      double acc = 0;
+      for (int j = 0; j < 3; j++) acc = acc + a[i][j] * b[j][k];
+      t[i][k] = acc;
+    }
+  std::memcpy(out, t, sizeof(t));
+}
+
+struct FloorPos {  // floor_position_struct (r, w)
+  double r[3];
+  double w[3][3];
+};
+
+void apply_w(const double ws[3][3], FloorPos& pos) {  // r = ws r, w = ws w
+  double r2[3];
+  matvec3(ws, pos.r, r2);
+  std::memcpy(pos.r, r2, sizeof(r2));
+  matmul3(ws, pos.w, pos.w);
+}
+
+// bend_shift, bmad/geometry/bend_shift.f90:19-61; has_tilt: the optional ref_tilt is present.
+FloorPos bend_shift(const FloorPos& p1, double g, double delta_s, bool has_tilt = false, double ref_tilt = 0) {
+  double angle = delta_s * g;
+  FloorPos p2 = p1;
+  if (angle == 0) {
+    p2.r[2] = p2.r[2] - delta_s;
+    return p2;
+  }
+  double tlt = has_tilt ? ref_tilt : 0.0;
+  double S[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  if (tlt != 0) {
+    rotate_mat(S, z_axis, -ref_tilt);
+    rotate_mat(S, y_axis, angle);
+    rotate_mat(S, z_axis, ref_tilt);
+  } else {
+    rotate_mat(S, y_axis, angle);
+  }
+  double L[3] = {cos_one(angle) / g, 0.0 / g, -lm.sin(angle) / g};
+  if (has_tilt) rotate_vec(L, z_axis, ref_tilt);
+  double r2[3];
+  matvec3(S, p1.r, r2);
+  for (int i = 0; i < 3; i++) p2.r[i] = r2[i] + L[i];
+  matmul3(S, p1.w, p2.w);
+  return p2;
+}
+
+// w_mat_for_tilt, bmad/geometry/w_mat_for_tilt.f90:14-38
+void w_mat_for_tilt(double tilt, double w[3][3]) {
+  double c = lm.cos(tilt), s = lm.sin(tilt);
+  double m[3][3] = {{c, -s, 0.0}, {s, c, 0.0}, {0.0, 0.0, 1.0}};
+  std::memcpy(w, m, sizeof(m));
+}
+
+// offset_particle, bmad/code/offset_particle.f90:66-530 (drift_to the element ends, no roll);
+// set_hvkicks and set_tilt as given.
 int offset_particle(const Ele& ele, int set, Coord& orbit, bool set_tilt, bool set_hvkicks) {
   const bmadgpu_element* e = ele.e;
   const bmadgpu_param* p = ele.p;
@@ -682,12 +782,47 @@ int offset_particle(const Ele& ele, int set, Coord& orbit, bool set_tilt, bool s
     is_misaligned = (x_off != 0 || y_off != 0 || z_off != 0 || xp != 0 || yp != 0 ||
                      (key == BMADGPU_SBEND && e->roll != 0));
   }
-  if (is_misaligned && key == BMADGPU_SBEND && (e->g != 0 || ele.ref_tilt_tot != 0 || e->roll != 0))
-    return BMADGPU_EUNSUPPORTED;  // bend_shift geometry not restated
+  if (is_misaligned && key == BMADGPU_SBEND && e->roll != 0) return BMADGPU_EUNSUPPORTED;  // roll not restated
+  const bool bend_geom = is_misaligned && key == BMADGPU_SBEND && (e->g != 0 || ele.ref_tilt_tot != 0);
+  const double g = e->g, ref_tilt = ele.ref_tilt_tot;
+  // ele_misalignment_L_S_calc (bmad/geometry/ele_misalignment_L_S_calc.f90:16-50), no roll:
+  // L_mis = the offsets, S_mis = floor_angles_to_w_mat(x_pitch, y_pitch, 0)
+  double L_mis[3] = {x_off, y_off, z_off};
 
   if (set) {
     double s_body;
-    if (is_misaligned) {
+    if (bend_geom) {
+      // offset_particle.f90:204-227, 247-257
+      FloorPos pos = {{orbit.vec[0], orbit.vec[2], 0.0}, {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}};
+      pos = bend_shift(pos, g, 1 * ds_center, true, ref_tilt);
+      double ws[3][3], wt[3][3];
+      floor_angles_to_w_mat(xp, yp, 0.0, ws, false);
+      for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) wt[i][j] = ws[j][i];
+      double d[3] = {pos.r[0] - L_mis[0], pos.r[1] - L_mis[1], pos.r[2] - L_mis[2]};
+      std::memcpy(pos.r, d, sizeof(d));
+      apply_w(wt, pos);
+      if (ref_tilt != 0) {
+        pos = bend_shift(pos, g, -L_half, true, ref_tilt);
+        double wtilt[3][3];
+        w_mat_for_tilt(-ref_tilt, wtilt);
+        apply_w(wtilt, pos);
+        pos = bend_shift(pos, g, L_half);
+      }
+      pos = bend_shift(pos, g, -sign_z_vel * 1 * L_half);
+      pos.r[2] = pos.r[2] + (1 - sign_z_vel * 1) * L_half;
+      s_body = pos.r[2];
+      double pz = rel_p * rel_p - orbit.vec[1] * orbit.vec[1] - orbit.vec[3] * orbit.vec[3];
+      if (pz <= 0) {
+        orbit.state = BMADGPU_LOST_PZ;
+      } else {
+        double p_vec0[3] = {orbit.vec[1], orbit.vec[3], sign_z_vel * std::sqrt(pz)}, p_vec[3];
+        matvec3(pos.w, p_vec0, p_vec);
+        orbit.vec[1] = p_vec[0];
+        orbit.vec[3] = p_vec[1];
+        orbit.vec[0] = pos.r[0];
+        orbit.vec[2] = pos.r[1];
+      }
+    } else if (is_misaligned) {
       double r[3] = {orbit.vec[0] - x_off, orbit.vec[2] - y_off, 0.0 - (z_off + 1 * ds_center)};
       double ws[3][3], w[3][3], r2[3];
       floor_angles_to_w_mat(xp, yp, 0.0, ws, true);
@@ -725,7 +860,36 @@ int offset_particle(const Ele& ele, int set, Coord& orbit, bool set_tilt, bool s
       orbit.vec[3] = orbit.vec[3] + 0.5 * charge_dir * e->vkick;
     }
     double s_lab;
-    if (is_misaligned) {
+    if (bend_geom) {
+      // offset_particle.f90:399-425, 445-457
+      FloorPos pos = {{orbit.vec[0], orbit.vec[2], 0.0}, {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}};
+      pos = bend_shift(pos, g, ds_center);
+      if (ref_tilt != 0) {
+        pos = bend_shift(pos, g, -L_half);
+        double wtilt[3][3];
+        w_mat_for_tilt(ref_tilt, wtilt);
+        apply_w(wtilt, pos);
+        pos = bend_shift(pos, g, L_half, true, ref_tilt);
+      }
+      double ws[3][3];
+      floor_angles_to_w_mat(xp, yp, 0.0, ws, false);
+      apply_w(ws, pos);
+      for (int i = 0; i < 3; i++) pos.r[i] = pos.r[i] + L_mis[i];
+      pos = bend_shift(pos, g, sign_z_vel * 1 * L_half, true, ref_tilt);
+      pos.r[2] = pos.r[2] + (1 + sign_z_vel * 1) * L_half;
+      s_lab = pos.r[2];
+      double pz = rel_p * rel_p - orbit.vec[1] * orbit.vec[1] - orbit.vec[3] * orbit.vec[3];
+      if (pz <= 0) {
+        orbit.state = BMADGPU_LOST_PZ;
+      } else {
+        double p_vec0[3] = {orbit.vec[1], orbit.vec[3], sign_z_vel * std::sqrt(pz)}, p_vec[3];
+        matvec3(pos.w, p_vec0, p_vec);
+        orbit.vec[1] = p_vec[0];
+        orbit.vec[3] = p_vec[1];
+        orbit.vec[0] = pos.r[0];
+        orbit.vec[2] = pos.r[1];
+      }
+    } else if (is_misaligned) {
       double r[3] = {orbit.vec[0], orbit.vec[2], 0.0};
       r[2] = r[2] - ds_center;
       double ws[3][3], r2[3];
@@ -1238,13 +1402,33 @@ void sbend_body_with_k1_map(const Ele& ele, double dg, double b1, int n_step, Co
                  z22 * (r[1] * r[1]) + z33 * (r[2] * r[2]) + z34 * r[2] * r[3] + z44 * (r[3] * r[3]);
 }
 
-// apply_multipole_kicks (contained in track_a_bend), track_a_bend.f90:338-471, magnetic only,
-// exact_multipoles = off.
+// elec_multipole_field, bmad/code/elec_multipole_field.f90:25-60 (field only, no derivatives)
+void elec_multipole_field(double a, double b, int n, const Coord& coord, double* Ex, double* Ey) {
+  *Ex = 0;
+  *Ey = 0;
+  if (a == 0 && b == 0) return;
+  double x = coord.vec[0], y = coord.vec[2];
+  for (int m = 0; m <= n; m += 2) {
+    double f = cm.no_n_fact(n, m) * mexp(x, n - m) * mexp(y, m);
+    *Ex = *Ex - b * f;
+    *Ey = *Ey - a * f;
+  }
+  for (int m = 1; m <= n; m += 2) {
+    double f = cm.no_n_fact(n, m) * mexp(x, n - m) * mexp(y, m);
+    *Ex = *Ex + a * f;
+    *Ey = *Ey - b * f;
+  }
+}
+
+// apply_multipole_kicks (contained in track_a_bend), track_a_bend.f90:338-471, exact_multipoles
+// = off: the fields of both kinds from the incoming orbit, then the magnetic kick, then the
+// electric kick with its energy change.
 void bend_apply_multipole_kicks(const Ele& ele, double coef, double step_len, double r_step, int ix_mag_max,
-                                const double* an, const double* bn, Coord& orbit) {
+                                const double* an, const double* bn, int ix_elec_max, const double* ane,
+                                const double* bne, Coord& orbit) {
   const bmadgpu_element* e = ele.e;
   const bmadgpu_param* p = ele.p;
-  double B1 = 0, B2 = 0;
+  double B1 = 0, B2 = 0, E1 = 0, E2 = 0;
   double f_p0c = r_step * p->p0c / (c_light * p->charge);
   for (int i = 0; i <= ix_mag_max; i++) {
     if (an[i] == 0 && bn[i] == 0) continue;
@@ -1253,13 +1437,35 @@ void bend_apply_multipole_kicks(const Ele& ele, double coef, double step_len, do
     B1 = B1 + f_p0c * ky;
     B2 = B2 - f_p0c * kx;
   }
+  for (int i = 0; i <= ix_elec_max; i++) {
+    if (ane[i] == 0 && bne[i] == 0) continue;
+    double ex, ey;
+    elec_multipole_field(ane[i], bne[i], i, orbit, &ex, &ey);
+    E1 = E1 + ex;
+    E2 = E2 + ey;
+  }
   if (ix_mag_max > -1) {
     double c_dir = 1.0 * p->charge;  // orientation * direction * charge_of(species)
     double f_coef = coef * c_dir * (1 + e->g * orbit.vec[0]) * c_light / orbit.p0c;
     orbit.vec[1] = orbit.vec[1] - f_coef * B2;
     orbit.vec[3] = orbit.vec[3] + f_coef * B1;
   }
-  (void)step_len;
+  if (ix_elec_max > -1) {
+    Coord orb0 = orbit;
+    double rel_p0 = 1 + orb0.vec[5];
+    double ps2 = rel_p0 * rel_p0 - orb0.vec[1] * orb0.vec[1] - orb0.vec[3] * orb0.vec[3];
+    double ps = std::sqrt(ps2) / rel_p0;
+    double f_coef = step_len * coef * (1 + e->g * orb0.vec[0]) * p->charge / (ps * orb0.beta * orb0.p0c);
+    double kx = f_coef * E1, ky = f_coef * E2;
+    double alpha = (kx * (2 * orb0.vec[1] + kx) + ky * (2 * orb0.vec[3] + ky)) / (rel_p0 * rel_p0);
+    orbit.vec[1] = orb0.vec[1] + kx;
+    orbit.vec[3] = orb0.vec[3] + ky;
+    orbit.vec[5] = orb0.vec[5] + rel_p0 * sqrt_one(alpha);
+    double mp = p->mass / orbit.p0c;
+    orbit.beta = (1 + orbit.vec[5]) /
+                 std::sqrt(ps2 + orbit.vec[1] * orbit.vec[1] + orbit.vec[3] * orbit.vec[3] + mp * mp);
+    orbit.vec[4] = orb0.vec[4] * orbit.beta / orb0.beta;
+  }
 }
 
 // track_a_bend, bmad/low_level/track_a_bend.f90:18-333
@@ -1284,7 +1490,6 @@ int track_a_bend(Coord& orbit, const Ele& ele) {
     b1 = 0;
   }
   if ((err = multipole_ele_to_ab(ele, false, &ix_elec_max, ane, bne, electric, false, nullptr))) return err;
-  if (ix_elec_max > -1) return BMADGPU_EUNSUPPORTED;
   double length = 1 * e->l;
   double g = e->g, dg;
   if (length == 0) {
@@ -1304,7 +1509,8 @@ int track_a_bend(Coord& orbit, const Ele& ele) {
   double r_step = 1.0 / n_step;
   double step_len = length / n_step;
   double angle = g * step_len;
-  if (ix_mag_max > -1) bend_apply_multipole_kicks(ele, 0.5, step_len, r_step, ix_mag_max, an, bn, orbit);
+  const bool kicks = ix_mag_max > -1 || ix_elec_max > -1;
+  if (kicks) bend_apply_multipole_kicks(ele, 0.5, step_len, r_step, ix_mag_max, an, bn, ix_elec_max, ane, bne, orbit);
   for (int n = 1; n <= n_step; n++) {
     if (b1 != 0) {
       sbend_body_with_k1_map(ele, dg, b1, n_step, orbit);
@@ -1377,9 +1583,9 @@ int track_a_bend(Coord& orbit, const Ele& ele) {
         orbit.vec[4] = z + orbit.beta * step_len / beta_ref - rel_p * L_p / pt;
       }
     }
-    if (ix_mag_max > -1) {
-      if (n == n_step) bend_apply_multipole_kicks(ele, 0.5, step_len, r_step, ix_mag_max, an, bn, orbit);
-      else bend_apply_multipole_kicks(ele, 1.0, step_len, r_step, ix_mag_max, an, bn, orbit);
+    if (kicks) {
+      double c = (n == n_step) ? 0.5 : 1.0;
+      bend_apply_multipole_kicks(ele, c, step_len, r_step, ix_mag_max, an, bn, ix_elec_max, ane, bne, orbit);
     }
   }
   if (orbit_too_large(orbit, p)) return 0;

@@ -28,6 +28,8 @@ TM_START = [0.001, 0.002, 0.003, 0.004, 0.005, 0.006]
 TM_E_TOT = 1e6
 TM_CHARGE = 1.0
 
+_sb0 = dict(a_pole={0: 0.01, 1: 0.1}, vkick=-0.0001, b_pole_elec={0: -2e3}, a_pole_elec={1: 2e4}, r0_mag=2.0,
+            r0_elec=3.0)  # :79
 _q0 = dict(a_pole={0: 0.01, 1: 0.1}, vkick=-0.0001, b_pole_elec={0: -2e3}, a_pole_elec={1: 2e4})  # :62
 
 TM_ELEMENTS = {
@@ -52,6 +54,12 @@ TM_ELEMENTS = {
                                        y_pitch=0.001), 64),
     "QUADRUPOLE3": ("QUADRUPOLE", dict(_q0, l=0.6, k1=1e-20, tilt=PI / 4.0, num_steps=10, x_offset=0.05,
                                        y_pitch=0.001), 65),
+    # sb0 (:79) with the pieces of sbend3 (:84) and sbend7 (:91): offsets, pitch and ref_tilt on a
+    # bend (the bend_shift frame of offset_particle), magnetic and electric multipoles
+    "SBEND3": ("SBEND", dict(_sb0, l=0.6, k1=0.3, k2=3.0, num_steps=10, x_offset=0.05, y_pitch=0.001,
+                             ref_tilt=0.1), 84),
+    "SBEND7": ("SBEND", dict(_sb0, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, x_offset=0.05, y_pitch=0.001,
+                             ref_tilt=0.1), 91),
 }
 
 # fringe_test.bmad: e_tot 1e6 electrons, particle_start, b: sbend ...

@@ -64,6 +64,7 @@ def assert_close(g, o, tol, floor_frac=1.0, alive_only=True):
 # the reason; every other case runs on the GPU against its golden line.
 REFUSED_ON_DEVICE = {
     "QUADRUPOLE1": "electric multipoles", "QUADRUPOLE2": "electric multipoles", "QUADRUPOLE3": "electric multipoles",
+    "SBEND3": "misaligned bend, electric multipoles", "SBEND7": "misaligned bend, electric multipoles",
 }
 
 
