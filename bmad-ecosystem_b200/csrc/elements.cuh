@@ -7,60 +7,101 @@ namespace bmadgpu {
 
 // ---- element bodies (track1_bmad dispatch, bmad/low_level/track1_bmad.f90:64-272) ----------
 
-BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b, const Globals& G) {
+BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b, const double* __restrict__ el,
+                     const Globals& G) {
   // track_a_quadrupole, bmad/low_level/track_a_quadrupole.f90 (fringe_type none); the kick
-  // before the body and the kick after each step share one call site.
+  // before the body and the kick after each step share one call site. With electric
+  // multipoles (F_ELEC, block el) the edges carry the electric fringe and every magnetic kick
+  // is followed by the electric one.
   const int np = h.n_pole;
   const double* kh = b + 3;
   const double* kf = kh + 2 * np;
   const double* mis = b + 3 + 4 * np;
   const bool has_t = h.flags & F_TILT;
+  const bool elec = h.flags & F_ELEC;
   if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, h.flags & F_PITCH);
+  if (elec) {
+    elec_edge(p, el, true, G);
+    if (p.state != S_ALIVE) return;
+  }
   const double b1 = b[0], length = b[1], step_len = b[2];
   const int n_step = h.n_step;
   const bool b_from2 = h.flags & F_KICK_B_FROM2;
   for (int i = 0; i <= n_step; i++) {
     if (i > 0) quad_step(p, b1, length, step_len, G);
-    if (np) ab_kicks(p, (i == 0 || i == n_step) ? kh : kf, np, b_from2);
+    const bool end = (i == 0 || i == n_step);
+    if (np) ab_kicks(p, end ? kh : kf, np, b_from2);
+    if (elec) elec_kicks(p, el, end ? el[1] : el[2], G);
+  }
+  if (elec) {
+    elec_edge(p, el, false, G);
+    if (p.state != S_ALIVE) return;
   }
   if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, h.flags & F_PITCH);
 }
 
-BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b) {
+BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b, const double* __restrict__ el,
+                      const Globals& G) {
   // track_a_thick_multipole, bmad/low_level/track_a_thick_multipole.f90:18-133
   const int np = h.n_pole;
   const double* kh = b + 1;
   const double* kf = kh + 2 * np;
   const double* mis = b + 1 + 4 * np;
   const bool has_t = h.flags & F_TILT;
+  const bool elec = h.flags & F_ELEC;
   if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, h.flags & F_PITCH);
+  if (elec) {
+    elec_edge(p, el, true, G);
+    if (p.state != S_ALIVE) return;
+  }
   const double step_len = b[0];
   const int n_step = h.n_step;
   const bool b_from2 = h.flags & F_KICK_B_FROM2;
   for (int i = 0; i <= n_step; i++) {
     if (i > 0) drift(p, step_len);
-    if (np) ab_kicks(p, (i == 0 || i == n_step) ? kh : kf, np, b_from2);
+    const bool end = (i == 0 || i == n_step);
+    if (np) ab_kicks(p, end ? kh : kf, np, b_from2);
+    if (elec) elec_kicks(p, el, end ? el[1] : el[2], G);
+  }
+  if (elec) {
+    elec_edge(p, el, false, G);
+    if (p.state != S_ALIVE) return;
   }
   if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, h.flags & F_PITCH);
 }
 
-BG_HD void bend_kick(Particle& p, const double* __restrict__ b, int np, double coef, const Globals& G) {
-  // apply_multipole_kicks (magnetic, exact_multipoles = off), track_a_bend.f90:360-397
-  double B1, B2;
-  ab_field(p, b + SB_FIXED, np, b[11], B1, B2);
-  double f_coef = coef * G.charge * (1 + b[1] * p.x) * kCLight / G.p0c;
-  p.px = p.px - f_coef * B2;
-  p.py = p.py + f_coef * B1;
+BG_HD void bend_kick(Particle& p, const double* __restrict__ b, int np, const double* __restrict__ el, bool half,
+                     const Globals& G) {
+  // apply_multipole_kicks (exact_multipoles = off), track_a_bend.f90:338-471: both fields from
+  // the incoming orbit, then the magnetic kick, then the electric one (el, when present)
+  double B1 = 0, B2 = 0, E1 = 0, E2 = 0;
+  const double coef = half ? 0.5 : 1.0;
+  if (np) ab_field(p, b + SB_FIXED, np, b[11], B1, B2);
+  if (el) elec_field(p, el, E1, E2);
+  if (np) {
+    double f_coef = coef * G.charge * (1 + b[1] * p.x) * kCLight / G.p0c;
+    p.px = p.px - f_coef * B2;
+    p.py = p.py + f_coef * B1;
+  }
+  if (el) bend_elec_kick(p, el, half ? el[1] : el[2], b[1], E1, E2, G);
 }
 
-BG_HD void body_bend(Particle& p, const EleHdr& h, const double* __restrict__ b, const Globals& G) {
+BG_HD void body_bend(Particle& p, const EleHdr& h, const double* __restrict__ b, const double* __restrict__ el,
+                     const Globals& G) {
   // track_a_bend, bmad/low_level/track_a_bend.f90:18-333
   const int np = h.n_pole;
   const double* mis = b + SB_FIXED + 2 * np;
-  if (h.flags & F_MISALIGN) tilt(p, mis[2], mis[3]);   // ref_tilt, offset_particle.f90:263-266
+  const double* e = (h.flags & F_ELEC) ? el : nullptr;
+  if (h.flags & F_MISALIGN) {
+    if (h.flags & F_PITCH) bend_frame(p, mis, true);   // offsets / pitches: the bend frame
+    else tilt(p, mis[2], mis[3]);                     // ref_tilt only, offset_particle.f90:263-266
+  }
+  // apply_element_edge_kick at the entrance: magnetic (Hwang) edge, then the electric fringe
+  if (e && e[3] != 0 && p.beta == 0) p.state = S_LOST;
   if (h.flags & F_EDGE_IN) hwang_edge(p, b + SB_EDGE_IN, true);
+  if (e && e[3] == 2) elec_fringe(p, e, e[5], G);
   if (orbit_too_large(p, G)) return;
-  if (np) bend_kick(p, b, np, 0.5, G);
+  if (np || e) bend_kick(p, b, np, e, true, G);
   for (int n = 1; n <= h.n_step; n++) {
     if (h.flags & F_BEND_K1) {
       bend_k1_step(p, b);
@@ -70,11 +111,17 @@ BG_HD void body_bend(Particle& p, const EleHdr& h, const double* __restrict__ b,
     } else {
       if (!bend_exact_step(p, b, G)) return;
     }
-    if (np) bend_kick(p, b, np, n == h.n_step ? 0.5 : 1.0, G);
+    if (np || e) bend_kick(p, b, np, e, n == h.n_step, G);
   }
   if (orbit_too_large(p, G)) return;
+  // at the exit: the electric fringe, then the magnetic edge
+  if (e && e[4] != 0 && p.beta == 0) p.state = S_LOST;
+  if (e && e[4] == 2) elec_fringe(p, e, e[6], G);
   if (h.flags & F_EDGE_OUT) hwang_edge(p, b + SB_EDGE_OUT, false);
-  if (h.flags & F_MISALIGN) tilt(p, mis[2], -mis[3]);
+  if (h.flags & F_MISALIGN) {
+    if (h.flags & F_PITCH) bend_frame(p, mis, false);
+    else tilt(p, mis[2], -mis[3]);
+  }
 }
 
 BG_HD void body_thin(Particle& p, const EleHdr& h, const double* __restrict__ b) {
@@ -143,11 +190,12 @@ BG_HD int track1(Particle& p, const EleHdr& h, const double* __restrict__ pool,
     if (p.state != S_ALIVE) return L_UPSTREAM;
   }
   const double* b = pool + h.param;
+  const double* el = pool + h.elec;
   switch (h.kind) {
     case K_DRIFT: drift(p, b[0]); break;
-    case K_QUAD: body_quad(p, h, b, G); break;
-    case K_THICK: body_thick(p, h, b); break;
-    case K_SBEND: body_bend(p, h, b, G); break;
+    case K_QUAD: body_quad(p, h, b, el, G); break;
+    case K_THICK: body_thick(p, h, b, el, G); break;
+    case K_SBEND: body_bend(p, h, b, el, G); break;
     case K_THIN: body_thin(p, h, b); break;
     case K_RFCAV: body_rf(p, h, b, G); break;
     default: break;  // K_MARKER

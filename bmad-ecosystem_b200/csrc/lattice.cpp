@@ -277,6 +277,232 @@ void resolve_steps(const bmadgpu_element& e, const bmadgpu_param& p, double tilt
   *n_out = std::max(1, nint(std::fabs(L / ds_step)));
 }
 
+// ---- electric multipoles and the misaligned-bend frame ----------------------------------------
+
+// at_this_ele_end, bmad/code/at_this_ele_end.f90:16-61 (now_at: entrance or exit end)
+bool at_ele_end(int now_at, int where_at) {
+  if (where_at == BMADGPU_NO_END) return false;
+  if (where_at == BMADGPU_CONTINUOUS || where_at == 7) return true;
+  if (now_at == BMADGPU_ENTRANCE_END) return where_at == BMADGPU_ENTRANCE_END || where_at == BMADGPU_BOTH_ENDS;
+  return where_at == BMADGPU_EXIT_END || where_at == BMADGPU_BOTH_ENDS;
+}
+
+// Electric a/b multipoles (multipole_ele_to_ab with pole_type = electric: convert_this_ab with
+// r0_elec scaling, multipole_ele_to_ab.f90:472-520); returns ix_elec_max.
+int elec_ab(const bmadgpu_element& e, double* a, double* b) {
+  for (int i = 0; i < kNPole; i++) { a[i] = 0; b[i] = 0; }
+  if (!e.is_on || e.key == BMADGPU_PIPE || e.key == BMADGPU_MULTIPOLE) return -1;
+  for (int i = 0; i < kNPole; i++) { a[i] = e.a_pole_elec[i]; b[i] = e.b_pole_elec[i]; }
+  if (max_nonzero(a, b, kNPole - 1) < 0) return -1;
+  if (e.scale_multipoles) {
+    const double radius = e.r0_elec;
+    if (radius != 0 && radius != 1) {
+      double factor = radius;
+      for (int n = 0; n < kNPole; n++) {
+        factor = factor / radius;
+        a[n] = factor * a[n];
+        b[n] = factor * b[n];
+      }
+    }
+  }
+  return max_nonzero(a, b, kNPole - 1);
+}
+
+// The electric block (table.h). s_half / s_full: the kick scales of the element's loop; the edge
+// modes from apply_element_edge_kick's gate (at_this_ele_end of fringe_at) and the zero-length
+// exit of electric_longitudinal_fringe (apply_element_edge_kick.f90:290).
+std::vector<double> elec_block(const bmadgpu_element& e, const bmadgpu_param& p, const double* a, const double* b,
+                               int ix_elec_max, double s_half, double s_full) {
+  auto mode = [&](int end) { return at_ele_end(end, e.fringe_at) ? (e.l != 0 ? 2.0 : 1.0) : 0.0; };
+  std::vector<double> blk = {(double)(ix_elec_max + 1), s_half, s_full, mode(BMADGPU_ENTRANCE_END),
+                             mode(BMADGPU_EXIT_END), 1.0 * p.charge, -1.0 * p.charge, p.mass / p.p0c};
+  for (int n = 0; n <= ix_elec_max; n++) blk.insert(blk.end(), {b[n], a[n]});
+  return blk;
+}
+
+typedef double Mat3[3][3];
+
+// Fortran matmul of 3x3 matrices, j-order summation
+void matmul3(const Mat3 a, const Mat3 b, Mat3 out) {
+  Mat3 t;
+  for (int i = 0; i < 3; i++)
+    for (int k = 0; k < 3; k++) {
+      double acc = 0;
+      for (int j = 0; j < 3; j++) acc = acc + a[i][j] * b[j][k];
+      t[i][k] = acc;
+    }
+  std::memcpy(out, t, sizeof(t));
+}
+
+// floor_angles_to_w_mat (bmad/geometry/floor_angles_to_w_mat.f90) with psi = 0, or its inverse
+void w_mat_angles(double theta, double phi, bool inverse, Mat3 w) {
+  const double s_the = l_sin(theta), c_the = l_cos(theta);
+  const double s_phi = l_sin(phi), c_phi = l_cos(phi);
+  const double s_psi = l_sin(0.0), c_psi = l_cos(0.0);
+  const double m[9] = {c_the * c_psi - s_the * s_phi * s_psi, -c_the * s_psi - s_the * s_phi * c_psi,
+                       s_the * c_phi, c_phi * s_psi, c_phi * c_psi, s_phi,
+                       -s_the * c_psi - c_the * s_phi * s_psi, s_the * s_psi - c_the * s_phi * c_psi,
+                       c_the * c_phi};
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) w[i][j] = inverse ? m[3 * j + i] : m[3 * i + j];
+}
+
+// cos_one (sim_utils/special_functions/cos_one.f90:16-27)
+double cos_one(double angle) {
+  const double s = l_sin(angle / 2);
+  return -2 * (s * s);
+}
+
+// rotate_vec / rotate_mat about the x (1), y (2) or z (3) axis, sim_utils/math/rotation_3d_mod.f90:
+// 737-845 (the matrix rotated from the left)
+void rotate_vec(double v[3], int axis, double angle) {
+  if (angle == 0) return;
+  const double ca = l_cos(angle), sa = l_sin(angle);
+  if (axis == 1) {
+    const double a = ca * v[1] - sa * v[2], b = sa * v[1] + ca * v[2];
+    v[1] = a;
+    v[2] = b;
+  } else if (axis == 2) {
+    const double a = sa * v[2] + ca * v[0], b = ca * v[2] - sa * v[0];
+    v[0] = a;
+    v[2] = b;
+  } else {
+    const double a = ca * v[0] - sa * v[1], b = sa * v[0] + ca * v[1];
+    v[0] = a;
+    v[1] = b;
+  }
+}
+void rotate_mat(Mat3 m, int axis, double angle) {
+  if (angle == 0) return;
+  const double ca = l_cos(angle), sa = l_sin(angle);
+  for (int k = 0; k < 3; k++) {
+    if (axis == 1) {
+      const double a = ca * m[1][k] - sa * m[2][k], b = sa * m[1][k] + ca * m[2][k];
+      m[1][k] = a;
+      m[2][k] = b;
+    } else if (axis == 2) {
+      const double a = sa * m[2][k] + ca * m[0][k], b = ca * m[2][k] - sa * m[0][k];
+      m[0][k] = a;
+      m[2][k] = b;
+    } else {
+      const double a = ca * m[0][k] - sa * m[1][k], b = sa * m[0][k] + ca * m[1][k];
+      m[0][k] = a;
+      m[1][k] = b;
+    }
+  }
+}
+
+// One end of the bend frame: the rotation chain w of the floor position and the steps acting on
+// its position r, recorded in the reference's order (offset_particle.f90:204-257, 399-457).
+struct FrameEnd {
+  Mat3 w = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  std::vector<double> steps;
+  int n = 0;
+  void step(int op, const double* v1, const Mat3 m, const double* v2) {
+    double st[BF_STEP] = {0};
+    st[0] = op;
+    for (int i = 0; i < 3; i++) {
+      if (v1) st[1 + i] = v1[i];
+      if (v2) st[13 + i] = v2[i];
+    }
+    if (m)
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) st[4 + 3 * i + j] = m[i][j];
+    steps.insert(steps.end(), st, st + BF_STEP);
+    n++;
+  }
+  void apply_w(const Mat3 m, int extra = 0, const double* v1 = nullptr) {  // r = m (r - v1), w = m w
+    step(FS_MAT | extra, v1, m, nullptr);
+    matmul3(m, w, w);
+  }
+  // bend_shift, bmad/geometry/bend_shift.f90:19-61 (has_tilt: the optional ref_tilt is present)
+  void bend_shift(double g, double delta_s, bool has_tilt = false, double ref_tilt = 0) {
+    const double angle = delta_s * g;
+    if (angle == 0) {
+      const double v[3] = {0, 0, delta_s};
+      step(FS_SUBZ, v, nullptr, nullptr);
+      return;
+    }
+    const double tlt = has_tilt ? ref_tilt : 0.0;
+    Mat3 S = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    if (tlt != 0) {
+      rotate_mat(S, 3, -ref_tilt);
+      rotate_mat(S, 2, angle);
+      rotate_mat(S, 3, ref_tilt);
+    } else {
+      rotate_mat(S, 2, angle);
+    }
+    double L[3] = {cos_one(angle) / g, 0.0 / g, -l_sin(angle) / g};
+    if (has_tilt) rotate_vec(L, 3, ref_tilt);
+    step(FS_MAT | FS_ADD, nullptr, S, L);
+    matmul3(S, w, w);
+  }
+};
+
+// The bend frame block of a bend with offsets, pitches or z_offset (no roll). With g != 0 or a
+// ref_tilt, the bend_shift geometry; otherwise the straight transform of offset_particle
+// (offset_particle.f90:239-245, 279-282, 437-443, 477-480), written as the same kind of steps.
+std::vector<double> bend_frame_block(const bmadgpu_element& e) {
+  const double length = e.l, L_half = 0.5 * length, g = e.g, rt = e.ref_tilt;
+  const double L_mis[3] = {e.x_offset, e.y_offset, e.z_offset};
+  const double ds_set = L_half - 0.0, ds_unset = L_half - length;
+  FrameEnd in, out;
+  if (g != 0 || rt != 0) {
+    in.bend_shift(g, 1 * ds_set, true, rt);
+    Mat3 ws, wt;
+    w_mat_angles(e.x_pitch, e.y_pitch, false, ws);
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) wt[i][j] = ws[j][i];
+    in.apply_w(wt, FS_SUB, L_mis);
+    if (rt != 0) {
+      in.bend_shift(g, -L_half, true, rt);
+      const double c = l_cos(-rt), s = l_sin(-rt);   // w_mat_for_tilt (w_mat_for_tilt.f90:14-38)
+      const Mat3 wm = {{c, -s, 0.0}, {s, c, 0.0}, {0.0, 0.0, 1.0}};
+      in.apply_w(wm);
+      in.bend_shift(g, L_half);
+    }
+    in.bend_shift(g, -1 * 1 * L_half);
+    const double zs[3] = {0, 0, (1 - 1 * 1) * L_half};
+    in.step(FS_ADDZ, nullptr, nullptr, zs);
+
+    out.bend_shift(g, ds_unset);
+    if (rt != 0) {
+      out.bend_shift(g, -L_half);
+      const double c = l_cos(rt), s = l_sin(rt);
+      const Mat3 wm = {{c, -s, 0.0}, {s, c, 0.0}, {0.0, 0.0, 1.0}};
+      out.apply_w(wm);
+      out.bend_shift(g, L_half, true, rt);
+    }
+    out.apply_w(ws);
+    out.step(FS_ADD, nullptr, nullptr, L_mis);
+    out.bend_shift(g, 1 * 1 * L_half, true, rt);
+    const double zu[3] = {0, 0, (1 + 1 * 1) * L_half};
+    out.step(FS_ADDZ, nullptr, nullptr, zu);
+  } else {
+    Mat3 winv, ws;
+    w_mat_angles(e.x_pitch, e.y_pitch, true, winv);
+    w_mat_angles(e.x_pitch, e.y_pitch, false, ws);
+    const double v_in[3] = {e.x_offset, e.y_offset, e.z_offset + 1 * ds_set};
+    in.step(FS_SUB | FS_MAT, v_in, winv, nullptr);
+    std::memcpy(in.w, winv, sizeof(Mat3));
+    const double zs[3] = {0, 0, L_half};
+    in.step(FS_ADDZ, nullptr, nullptr, zs);
+    const double v_out[3] = {0, 0, ds_unset};
+    out.step(FS_SUBZ, v_out, nullptr, nullptr);
+    const double add[3] = {e.x_offset, e.y_offset, e.z_offset + L_half};
+    out.step(FS_MAT | FS_ADD, nullptr, ws, add);
+    std::memcpy(out.w, ws, sizeof(Mat3));
+  }
+  std::vector<double> blk = {(double)in.n, (double)out.n, (1 - 1) * L_half, (1 + 1) * L_half};
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) blk.push_back(in.w[i][j]);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) blk.push_back(out.w[i][j]);
+  blk.insert(blk.end(), in.steps.begin(), in.steps.end());
+  blk.insert(blk.end(), out.steps.begin(), out.steps.end());
+  return blk;
+}
+
 struct Packer {
   std::vector<EleHdr> hdr;
   std::vector<ApRec> ap;
@@ -375,16 +601,21 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
       if (e.orientation != 1 && e.orientation != 0) fail(BMADGPU_EUNSUPPORTED, "orientation -1");
       if (e.field_master) fail(BMADGPU_EUNSUPPORTED, "field_master = T");
       if (e.exact_multipoles != 0 && e.exact_multipoles != 1) fail(BMADGPU_EUNSUPPORTED, "exact_multipoles");
-      if (e.key != BMADGPU_MULTIPOLE &&
-          (any_nonzero(e.a_pole_elec, kNPole) || any_nonzero(e.b_pole_elec, kNPole)))
-        fail(BMADGPU_EUNSUPPORTED, "electric multipoles");
+      const bool raw_elec = any_nonzero(e.a_pole_elec, kNPole) || any_nonzero(e.b_pole_elec, kNPole);
+      if (raw_elec && e.is_on && e.key != BMADGPU_MULTIPOLE && e.key != BMADGPU_QUADRUPOLE &&
+          e.key != BMADGPU_SEXTUPOLE && e.key != BMADGPU_OCTUPOLE && e.key != BMADGPU_THICK_MULTIPOLE &&
+          e.key != BMADGPU_SBEND)
+        fail(BMADGPU_EUNSUPPORTED, "electric multipoles on this element type");
       if (e.key == BMADGPU_MULTIPOLE && any_nonzero(e.a_pole_elec, kNPole))
         fail(BMADGPU_EUNSUPPORTED, "multipole ksl");
       if (e.x_pitch != 0 || e.y_pitch != 0 || e.z_offset != 0)
-        if (e.key == BMADGPU_SBEND || e.key == BMADGPU_MULTIPOLE || e.key == BMADGPU_AB_MULTIPOLE)
-          fail(BMADGPU_EUNSUPPORTED, "pitch / z_offset misalignment of a bend or thin multipole");
-      if (e.key == BMADGPU_SBEND && (e.tilt != 0 || e.roll != 0 || e.x_offset != 0 || e.y_offset != 0))
-        fail(BMADGPU_EUNSUPPORTED, "misaligned sbend (bend_shift geometry)");
+        if (e.key == BMADGPU_MULTIPOLE || e.key == BMADGPU_AB_MULTIPOLE)
+          fail(BMADGPU_EUNSUPPORTED, "pitch / z_offset misalignment of a thin multipole");
+      if (e.key == BMADGPU_SBEND && (e.tilt != 0 || e.roll != 0))
+        fail(BMADGPU_EUNSUPPORTED, "sbend tilt / roll");
+      if ((e.key == BMADGPU_QUADRUPOLE || e.key == BMADGPU_SEXTUPOLE) && e.is_on &&
+          e.fringe_type != BMADGPU_FRINGE_NONE && e.fringe_at != BMADGPU_NO_END)
+        fail(BMADGPU_EUNSUPPORTED, "quadrupole / sextupole fringe_type other than none");
       if (e.key != BMADGPU_SBEND && e.ref_tilt != 0) fail(BMADGPU_EUNSUPPORTED, "ref_tilt on a non-bend");
       if (e.key == BMADGPU_RFCAVITY && (e.hkick != 0 || e.vkick != 0))
         fail(BMADGPU_EUNSUPPORTED, "rfcavity hkick/vkick");
@@ -397,9 +628,8 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
 
       double tilt_tot = (e.key == BMADGPU_SBEND) ? 0.0 : e.tilt;
       const bool pitched = e.x_pitch != 0 || e.y_pitch != 0 || e.z_offset != 0;
-      bool has_misalign = (e.key == BMADGPU_SBEND)
-                              ? (e.ref_tilt != 0 || e.roll != 0)
-                              : (e.tilt != 0 || e.x_offset != 0 || e.y_offset != 0 || pitched);
+      const bool offset = e.x_offset != 0 || e.y_offset != 0 || pitched;
+      bool has_misalign = (e.key == BMADGPU_SBEND) ? (e.ref_tilt != 0 || offset) : (e.tilt != 0 || offset);
       double ds_step;
       int num_steps;
       resolve_steps(e, p, tilt_tot, &ds_step, &num_steps);
@@ -432,9 +662,10 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
         }
       }
 
-      double a[kNPole], b[kNPole];
+      double a[kNPole], b[kNPole], ae[kNPole], be[kNPole];
       int ix_mag_max;
-      std::vector<double> mis;
+      const int ix_elec_max = elec_ab(e, ae, be);
+      std::vector<double> mis, eblk;
       auto misalign_block = [&](double tilt) {
         mis = {e.x_offset, e.y_offset, l_cos(tilt), l_sin(tilt)};
         flags |= F_MISALIGN;
@@ -474,10 +705,11 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           mag_ab(e, tilt_tot, 0, a, b, &ix_mag_max);
           double b1 = pull_b1(a, b, &ix_mag_max);
           int n_step = 1;
-          if (ix_mag_max > -1) n_step = std::max(nint(std::fabs(e.l) / ds_step), 1);
+          if (ix_mag_max > -1 || ix_elec_max > -1) n_step = std::max(nint(std::fabs(e.l) / ds_step), 1);
           double r_step = 1.0 / n_step;
           double step_len = e.l * r_step;
           blk = {b1, e.l, step_len};
+          if (ix_elec_max > -1) eblk = elec_block(e, p, ae, be, ix_elec_max, step_len / 2, step_len);
           if (ix_mag_max > -1) {
             flags |= F_KICKS;
             h.n_pole = (uint8_t)(ix_mag_max + 1);
@@ -493,10 +725,11 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
         case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE: {  // track_a_thick_multipole.f90
           h.kind = K_THICK;
           mag_ab(e, tilt_tot, 0, a, b, &ix_mag_max);
-          int n_step = (ix_mag_max == -1) ? 1 : std::max(nint(std::fabs(e.l / ds_step)), 1);
+          int n_step = (ix_mag_max == -1 && ix_elec_max == -1) ? 1 : std::max(nint(std::fabs(e.l / ds_step)), 1);
           double r_step = 1.0 / n_step;
           double step_len = e.l / n_step;
           blk = {step_len};
+          if (ix_elec_max > -1) eblk = elec_block(e, p, ae, be, ix_elec_max, 1 * step_len / 2, 1 * step_len);
           if (ix_mag_max > -1) {
             flags |= F_KICKS;
             h.n_pole = (uint8_t)(ix_mag_max + 1);
@@ -530,10 +763,11 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
             b1 = 0;
           }
           int n_step = 1;
-          if (ix_mag_max > -1) n_step = std::max(nint(std::fabs(e.l) / ds_step), 1);
+          if (ix_mag_max > -1 || ix_elec_max > -1) n_step = std::max(nint(std::fabs(e.l) / ds_step), 1);
           double r_step = 1.0 / n_step;
           double step_len = e.l / n_step;
           double angle = g * step_len;
+          if (ix_elec_max > -1) eblk = elec_block(e, p, ae, be, ix_elec_max, step_len * 0.5, step_len * 1.0);
           double gl = g * step_len;
           blk = {step_len, g, g_tot, dg, angle, l_cos(angle), l_sin(angle), sinc0(angle), cosc0(angle),
                  (gl * gl) * sincc0(angle), (b1 != 0 && e.l != 0) ? b1 / e.l : 0.0,
@@ -570,7 +804,10 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
             push_kicks(blk, a, b, ix_mag_max + 1, 1.0);
           }
           h.n_step = (uint16_t)n_step;
-          if (has_misalign) {  // ref_tilt only (offsets/roll rejected above)
+          if (offset) {  // offsets, pitches or z_offset: the bend frame
+            mis = bend_frame_block(e);
+            flags |= F_MISALIGN | F_PITCH;
+          } else if (has_misalign) {  // ref_tilt only: tilt_coords
             mis = {0.0, 0.0, l_cos(e.ref_tilt), l_sin(e.ref_tilt)};
             flags |= F_MISALIGN;
           }
@@ -627,8 +864,12 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
         default:
           fail(BMADGPU_EUNSUPPORTED, "element type");
       }
-      if ((flags & F_MISALIGN) && mis.size() >= 4 && mis[3] != 0) flags |= F_TILT;
+      if ((flags & F_MISALIGN) && h.kind != K_SBEND && mis.size() >= 4 && mis[3] != 0) flags |= F_TILT;
       blk.insert(blk.end(), mis.begin(), mis.end());
+      if (!eblk.empty() && (h.kind == K_QUAD || h.kind == K_THICK || h.kind == K_SBEND)) {
+        flags |= F_ELEC;
+        h.elec = pk.add_block(eblk);
+      }
       h.flags = flags;
       h.param = pk.add_block(blk);
       out.n_step[i] = h.n_step;

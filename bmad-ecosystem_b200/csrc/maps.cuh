@@ -816,6 +816,192 @@ BG_HD void energy_kick(Particle& p, double dE, const Globals& G) {
   p.beta = beta_new;
 }
 
+// ---- electric multipoles (bmad_standard field, exact_multipoles = off) -----------------------
+// e: the electric block (table.h): [n_elec, scales, edge modes, at_sign charges, mass/p0c] then
+// (b_n, a_n), n < n_elec.
+
+// ab_multipole_kicks with pole_type = electric (multipole_mod.f90:82-141 with
+// ab_multipole_kick :314-376): kick strengths charge / (beta p0c) times (a_n, -b_n) times scale,
+// summed over the orders, then the energy change that goes with the transverse kick (the
+// particle keeps its total energy in the static field), beta and z rescaled.
+BG_COLD void elec_kicks(Particle& p, const double* __restrict__ e, double scale, const Globals& G) {
+  const int n_pole = (int)e[0];
+  const double* c = e + EL_FIXED;
+  const double f = G.charge / (p.beta * G.p0c);
+  const double x = p.x, y = p.y;
+  double kx_tot = 0, ky_tot = 0;
+  for (int n = 0; n < n_pole; n++) {
+    const double b = c[2 * n], a = c[2 * n + 1];
+    double kx = 0, ky = 0;
+    if (!(a == 0 && b == 0)) {
+      double a2 = a * f, b2 = -b * f;
+      a2 = scale * a2;
+      b2 = scale * b2;
+      for (int m = 0; m <= n; m += 2) {
+        const double t = BG_CMULTI(n, m) * mexp(x, n - m) * mexp(y, m);
+        kx = kx + b2 * t;
+        ky = ky - a2 * t;
+      }
+      for (int m = 1; m <= n; m += 2) {
+        const double t = BG_CMULTI(n, m) * mexp(x, n - m) * mexp(y, m);
+        kx = kx + a2 * t;
+        ky = ky + b2 * t;
+      }
+    }
+    kx_tot = kx_tot + kx;
+    ky_tot = ky_tot + ky;
+  }
+  const double px0 = p.px, py0 = p.py, pz0 = p.pz, z0 = p.z, beta0 = p.beta;
+  p.px = p.px + kx_tot;
+  p.py = p.py + ky_tot;
+  const double rp0 = 1 + pz0;
+  const double alpha = (kx_tot * (2 * px0 + kx_tot) + ky_tot * (2 * py0 + ky_tot)) / (rp0 * rp0);
+  if (alpha < -1) {
+    p.state = S_LOST_PZ;
+    return;
+  }
+  const double dpz = (1 + pz0) * sqrt_one(alpha);
+  p.pz = pz0 + dpz;
+  const double rp1 = 1 + p.pz;
+  const double mp = e[7];
+  p.beta = (1 + p.pz) / sqrt(rp1 * rp1 + mp * mp);
+  p.z = z0 * p.beta / beta0;
+  refresh(p, G);
+}
+
+// electric_longitudinal_fringe (apply_element_edge_kick.f90:283-329, bmad_standard field, non-exact
+// multipoles): the energy kick of the scalar potential phi = -Re sum (b_n - i a_n)(x + i y)^(n+1)/(n+1)
+// at the edge, ff = at_sign * charge.
+BG_COLD void elec_fringe(Particle& p, const double* __restrict__ e, double ff, const Globals& G) {
+  const int n_pole = (int)e[0];
+  const double* c = e + EL_FIXED;
+  const double cr = p.x, ci = p.y;
+  double xr = 1, xi = 0, phi = 0;
+  for (int i = 0; i < n_pole; i++) {
+    const double nr = xr * cr - xi * ci, ni = xr * ci + xi * cr;
+    xr = nr;
+    xi = ni;
+    const double b = c[2 * i], a = c[2 * i + 1];
+    if (a == 0 && b == 0) continue;
+    const double ar = b, ai = -a;
+    const double re_cur = ar * xr - ai * xi;
+    phi = phi - re_cur / (i + 1);
+  }
+  energy_kick(p, -ff * phi, G);
+  refresh(p, G);
+}
+
+// One electric edge of apply_element_edge_kick (apply_element_edge_kick.f90:37-282) for the
+// element types whose only edge field is electric: mode 0 no edge, 1 the beta check of a
+// zero-length element, 2 the beta check and the longitudinal fringe.
+BG_HD void elec_edge(Particle& p, const double* __restrict__ e, bool entering, const Globals& G) {
+  const int mode = (int)e[entering ? 3 : 4];
+  if (mode == 0) return;
+  if (p.beta == 0) p.state = S_LOST;
+  if (mode == 2) elec_fringe(p, e, e[entering ? 5 : 6], G);
+}
+
+// Electric field of the bend's multipoles (elec_multipole_field.f90:25-60), summed over the
+// orders as track_a_bend's apply_multipole_kicks sums it (track_a_bend.f90:384-390).
+BG_COLD void elec_field(const Particle& p, const double* __restrict__ e, double& E1, double& E2) {
+  const int n_pole = (int)e[0];
+  const double* c = e + EL_FIXED;
+  const double x = p.x, y = p.y;
+  E1 = 0;
+  E2 = 0;
+  for (int n = 0; n < n_pole; n++) {
+    const double b = c[2 * n], a = c[2 * n + 1];
+    if (a == 0 && b == 0) continue;
+    double ex = 0, ey = 0;
+    for (int m = 0; m <= n; m += 2) {
+      const double f = BG_CMULTI(n, m) * mexp(x, n - m) * mexp(y, m);
+      ex = ex - b * f;
+      ey = ey - a * f;
+    }
+    for (int m = 1; m <= n; m += 2) {
+      const double f = BG_CMULTI(n, m) * mexp(x, n - m) * mexp(y, m);
+      ex = ex + a * f;
+      ey = ey - b * f;
+    }
+    E1 = E1 + ex;
+    E2 = E2 + ey;
+  }
+}
+
+// The electric kick of track_a_bend's apply_multipole_kicks (track_a_bend.f90:416-432), field
+// E1, E2 taken before the magnetic kick; sc = step_len * coef, g the design curvature.
+BG_COLD void bend_elec_kick(Particle& p, const double* __restrict__ e, double sc, double g, double E1, double E2,
+                            const Globals& G) {
+  const double px0 = p.px, py0 = p.py, pz0 = p.pz, z0 = p.z, beta0 = p.beta;
+  const double rel_p0 = 1 + pz0;
+  const double ps2 = rel_p0 * rel_p0 - px0 * px0 - py0 * py0;
+  const double ps = sqrt(ps2) / rel_p0;
+  const double f_coef = sc * (1 + g * p.x) * G.charge / (ps * beta0 * G.p0c);
+  const double kx = f_coef * E1, ky = f_coef * E2;
+  const double alpha = (kx * (2 * px0 + kx) + ky * (2 * py0 + ky)) / (rel_p0 * rel_p0);
+  p.px = px0 + kx;
+  p.py = py0 + ky;
+  p.pz = pz0 + rel_p0 * sqrt_one(alpha);
+  const double mp = e[7];
+  p.beta = (1 + p.pz) / sqrt(ps2 + p.px * p.px + p.py * p.py + mp * mp);
+  p.z = z0 * p.beta / beta0;
+  refresh(p, G);
+}
+
+// ---- misaligned-bend frame ------------------------------------------------------------------
+// offset_particle for a bend with offsets, pitches or z_offset (offset_particle.f90:204-257 set,
+// 399-457 unset): the chain of bend_shift, misalignment and ref_tilt transforms of the floor
+// position is affine in the particle's (x, y); its rotation part and the translations were
+// folded on the host with the reference's own sequence of operations, and the steps acting on
+// the position are replayed here in the same order (the bend frame block, table.h). The momentum
+// is rotated by the chain's rotation, then the particle drifts to the element's edge.
+BG_COLD void bend_frame(Particle& p, const double* __restrict__ m, bool set) {
+  const int n_set = (int)m[0];
+  const int n = set ? n_set : (int)m[1];
+  const double* w = m + (set ? 4 : 13);
+  const double* st = m + BF_FIXED + (set ? 0 : BF_STEP * n_set);
+  double r[3] = {p.x, p.y, 0.0};
+  for (int k = 0; k < n; k++) {
+    const double* s = st + BF_STEP * k;
+    const int op = (int)s[0];
+    if (op & FS_SUB) {
+      r[0] = r[0] - s[1];
+      r[1] = r[1] - s[2];
+      r[2] = r[2] - s[3];
+    }
+    if (op & FS_SUBZ) r[2] = r[2] - s[3];
+    if (op & FS_MAT) {
+      double q[3];
+      matvec3(s + 4, r, q);
+      r[0] = q[0];
+      r[1] = q[1];
+      r[2] = q[2];
+    }
+    if (op & FS_ADD) {
+      r[0] = r[0] + s[13];
+      r[1] = r[1] + s[14];
+      r[2] = r[2] + s[15];
+    }
+    if (op & FS_ADDZ) r[2] = r[2] + s[15];
+  }
+  const double s_pos = r[2];
+  const double rel_p = 1 + p.pz;
+  const double pz2 = rel_p * rel_p - p.px * p.px - p.py * p.py;
+  if (pz2 <= 0) {
+    p.state = S_LOST_PZ;
+  } else {
+    const double v[3] = {p.px, p.py, 1 * sqrt(pz2)};
+    double pv[3];
+    matvec3(w, v, pv);
+    p.px = pv[0];
+    p.py = pv[1];
+    p.x = r[0];
+    p.y = r[1];
+  }
+  const double ds = m[set ? 2 : 3] - s_pos;
+  if (fabs(ds) > 1e-14 && p.state == S_ALIVE) drift_noref(p, ds);
+}
+
 // modulo2 (sim_utils/special_functions/modulo2_mod.f90:85-100): x + 2 n amp in [-amp, amp)
 BG_HD double modulo2(double x, double amp) {
   double two = 2 * amp;

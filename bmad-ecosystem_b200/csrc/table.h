@@ -39,7 +39,8 @@ enum Flag : uint16_t {
   F_ZERO_LEN = 1 << 10,    // element length is zero
   F_TILT = 1 << 11,        // misalign block carries a non-zero tilt rotation
   F_KICK_B_FROM2 = 1 << 12, // both kick arrays: every a_n zero and b_0 = b_1 = 0, at least 3 orders
-  F_PITCH = 1 << 13        // misalign block of the pitched form (pitches and/or z_offset)
+  F_PITCH = 1 << 13,       // misalign block of the pitched form (straight elements) or the bend frame
+  F_ELEC = 1 << 14         // electric multipoles: EleHdr::elec names their block
 };
 
 struct EleHdr {            // 16 bytes
@@ -49,7 +50,7 @@ struct EleHdr {            // 16 bytes
   uint16_t n_step;
   uint16_t ap_index;       // index into the aperture records
   uint32_t param;          // offset (in doubles) of the parameter block in the pool
-  uint32_t reserved;
+  uint32_t elec;           // offset (in doubles) of the electric block (F_ELEC), else 0
 };
 
 struct ApRec {             // 32 bytes: rectangular/elliptical limits (x1_lim = -x1_limit, ...)
@@ -73,7 +74,21 @@ struct ApRec {             // 32 bytes: rectangular/elliptical limits (x1_lim = 
 // misalign: [x_off, y_off, cos_t, sin_t]; with F_PITCH (straight elements with x/y pitch or
 //           z_offset) followed by [z_off, L/2, L/2 - 0, L/2 - L, 2 (L/2)] and the rotations W^-1
 //           and W of floor_angles_to_w_mat(x_pitch, y_pitch, 0), row-major: 27 doubles
+// bend frame (K_SBEND with F_MISALIGN | F_PITCH: offsets, pitches or z_offset on a bend), in
+//           place of the misalign block: [n_set, n_unset, s_target set, s_target unset, W set (9),
+//           W unset (9)] then n_set + n_unset steps of 16 doubles [op, v1 (3), M (9), v2 (3)]
+//           acting on the position r = (x, y, 0): op & FS_SUB: r -= v1; FS_SUBZ: r_z -= v1_z;
+//           FS_MAT: r = M r; FS_ADD: r += v2; FS_ADDZ: r_z += v2_z (in that order). W rotates the
+//           momentum; the particle then drifts from r_z to s_target.
+// electric block (F_ELEC; quadrupole, sextupole, octupole, thick_multipole, sbend):
+//           [n_elec, scale of the end kicks, scale of the interior kicks, entrance edge mode,
+//           exit edge mode, at_sign charge entrance, at_sign charge exit, mass / p0c] then
+//           (b_n, a_n) for n < n_elec (r0_elec scaled). Edge mode: 0 no edge call, 1 edge call
+//           (beta check only, zero length), 2 edge call with the electric longitudinal fringe.
+//           The scales are step_len / 2 and step_len (bends: step_len * 0.5, step_len * 1.0).
 constexpr int SB_EDGE_IN = 12, SB_EDGE_OUT = 19, SB_FIXED = 26;
+constexpr int EL_FIXED = 8, BF_FIXED = 22, BF_STEP = 16;
+enum FrameOp { FS_SUB = 1, FS_SUBZ = 2, FS_MAT = 4, FS_ADD = 8, FS_ADDZ = 16 };
 constexpr int RF_FIXED = 6;
 
 struct TableInfo {

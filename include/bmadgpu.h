@@ -407,7 +407,8 @@ int bmadgpu_server_get_stats(bmadgpu_server* server, bmadgpu_server_stats* stats
  * with it (no hkick/vkick; multipoles only with scale_multipoles). Computed by a hand-written
  * adjoint of the element maps, one thread per particle, with a checkpoint every checkpoint_every
  * turns and recomputation in between. Lattices with edge fringe, bends with k1 or multipoles,
- * thin multipoles or elements of more than 16 steps give BMADGPU_EUNSUPPORTED. Lost particles
+ * thin multipoles, pitched or offset bends, electric multipoles or elements of more than 16 steps
+ * give BMADGPU_EUNSUPPORTED. Lost particles
  * leave the loss (the set of survivors is held fixed). */
 int bmadgpu_loss_grad(bmadgpu_ctx* ctx, const bmadgpu_lattice* lat, const bmadgpu_bunch* host_bunch, int32_t n_turns,
                       int32_t checkpoint_every, int32_t n_param, const int32_t* param_ele, double* loss,

@@ -57,17 +57,20 @@ def test_config1_ring_packs_and_sextupoles_use_one_step():
     assert all(s == 1 for e, s in zip(eles, steps) if e.key == abi.SEXTUPOLE)
 
 
-@pytest.mark.parametrize("bad", ["elec", "bend_pitch", "bend_offset", "abs_time"])
+@pytest.mark.parametrize("bad", ["elec_on_rfcavity", "bend_roll", "bend_tilt", "quad_fringe_full", "abs_time"])
 def test_unsupported_inputs_fail_loudly(bad):
     abi = load_abi()
     p = abi.electron_param(3e9)
     e = abi.default_element(abi.QUADRUPOLE, l=0.4, k1=0.5)
-    if bad == "elec":
+    if bad == "elec_on_rfcavity":
+        e = abi.default_element(abi.RFCAVITY, l=0.4, voltage=1e6, rf_frequency=5e8)
         e.b_pole_elec[1] = 1e3
-    elif bad == "bend_pitch":
-        e = abi.default_element(abi.SBEND, l=1.0, g=0.01, y_pitch=1e-3)
-    elif bad == "bend_offset":
-        e = abi.default_element(abi.SBEND, l=1.0, g=0.01, x_offset=1e-3)
+    elif bad == "bend_roll":
+        e = abi.default_element(abi.SBEND, l=1.0, g=0.01, roll=1e-3)
+    elif bad == "bend_tilt":
+        e = abi.default_element(abi.SBEND, l=1.0, g=0.01, tilt=1e-3)
+    elif bad == "quad_fringe_full":
+        e.fringe_type = abi.FRINGE_FULL
     else:
         p.absolute_time_tracking = 1
     with pytest.raises(lib.BmadGpuError) as ei:
@@ -90,4 +93,18 @@ def test_pitched_straight_elements_are_accepted():
         e = abi.default_element(key, l=0.4, k1=0.5, y_pitch=1e-3, x_pitch=-2e-3, z_offset=0.01)
         if key == abi.RFCAVITY:
             e.voltage, e.rf_frequency = 1e6, 5e8
+        lib.lattice_check([e], p)
+
+
+def test_misaligned_bends_and_electric_multipoles_are_accepted():
+    """Offsets, pitches and z_offset of bends (the bend_shift frame) and electric multipoles of
+    quadrupoles, sextupoles, octupoles, thick multipoles and bends are on the device path."""
+    abi = load_abi()
+    p = abi.electron_param(3e9)
+    for kw in (dict(g=0.01, x_offset=1e-3), dict(g=0.01, y_pitch=1e-3, ref_tilt=0.1), dict(k1=0.3, z_offset=0.01)):
+        lib.lattice_check([abi.default_element(abi.SBEND, l=1.0, **kw)], p)
+    for key in (abi.QUADRUPOLE, abi.SEXTUPOLE, abi.OCTUPOLE, abi.THICK_MULTIPOLE, abi.SBEND):
+        e = abi.default_element(key, l=0.4, k1=0.5, g=0.01 if key == abi.SBEND else 0.0)
+        e.b_pole_elec[1] = 1e3
+        e.a_pole_elec[0] = -2e3
         lib.lattice_check([e], p)

@@ -69,6 +69,26 @@ CASES = {
                                      y_offset=1e-4, **ap)],
     "rf_pitched": lambda E, ap: [E(abi.RFCAVITY, l=1.2, voltage=2e6, rf_frequency=500e6, x_pitch=1e-3, tilt=0.1,
                                    x_offset=1e-4, **ap)],
+    # electric multipoles (kicks with the energy change, the longitudinal fringe at the edges)
+    "quad_elec": lambda E, ap: [E(abi.QUADRUPOLE, l=0.4, k1=0.8, b_pole_elec={0: 2e5, 1: 3e6}, a_pole_elec={2: 1e6},
+                                  r0_elec=0.05, x_offset=2e-4, tilt=0.05, **ap)],
+    "quad_elec_exit_edge_only": lambda E, ap: [E(abi.QUADRUPOLE, l=0.4, k1=-0.8, b_pole_elec={1: 3e6, 3: 4e7},
+                                                 fringe_at=abi.EXIT_END, **ap)],
+    "sextupole_elec": lambda E, ap: [E(abi.SEXTUPOLE, l=0.3, k2=10.0, a_pole_elec={0: -1e5, 2: 5e6}, num_steps=3,
+                                       y_pitch=1e-3, **ap)],
+    "sbend_elec": lambda E, ap: [E(abi.SBEND, l=1.0, g=0.03, e1=0.02, b_pole={2: 1e-3}, b_pole_elec={0: -2e5},
+                                   a_pole_elec={1: 2e6}, r0_elec=3.0, **ap)],
+    # misaligned bends: the bend_shift frame (g or ref_tilt non-zero) and the straight form
+    "sbend_offsets": lambda E, ap: [E(abi.SBEND, l=1.0, g=0.03, x_offset=1e-3, y_offset=-5e-4, x_pitch=2e-4,
+                                      y_pitch=-1e-4, z_offset=0.01, **ap)],
+    "sbend_ref_tilt_offsets": lambda E, ap: [E(abi.SBEND, l=0.8, g=0.05, e1=0.02, e2=-0.01, ref_tilt=0.3,
+                                               x_offset=1e-3, y_pitch=2e-4, **ap)],
+    "sbend_g0_offsets": lambda E, ap: [E(abi.SBEND, l=0.6, k1=0.2, x_offset=1e-3, y_pitch=1e-3, z_offset=-0.02, **ap)],
+    "sbend_g0_ref_tilt": lambda E, ap: [E(abi.SBEND, l=0.6, k1=0.3, k2=3.0, ref_tilt=0.1, x_offset=2e-3,
+                                          y_pitch=1e-3, num_steps=10, **ap)],
+    "sbend7_like": lambda E, ap: [E(abi.SBEND, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, x_offset=0.002,
+                                    y_pitch=0.001, ref_tilt=0.1, a_pole={0: 0.01, 1: 0.1}, vkick=-1e-4,
+                                    b_pole_elec={0: -2e5}, a_pole_elec={1: 2e6}, r0_mag=2.0, r0_elec=3.0, **ap)],
 }
 
 
