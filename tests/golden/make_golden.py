@@ -7,6 +7,8 @@ Sources (paths inside bmad-sim/bmad-ecosystem):
   regression_tests/tracking_method_test/tracking_method_test.bmad   element definitions, start orbit
   regression_tests/tracking_method_test/output.correct              "NAME: Bmad_Standard" lines
   regression_tests/fringe_test/fringe_test.bmad, output.correct     hwang_bend_edge_kick goldens
+  regression_tests/mat6_calc_method_test/mat6_calc_method_test.bmad, output.correct
+                                                                    transfer matrices by tracking
 
 Element attributes are transcribed below from the .bmad lines cited beside each entry; Bmad's
 parser defaults are applied explicitly (tilt flag -> pi/4 quad, pi/6 sextupole, pi/8 octupole,
@@ -62,6 +64,40 @@ TM_ELEMENTS = {
                              ref_tilt=0.1), 91),
 }
 
+# mat6_calc_method_test.bmad: e_tot 1e6, default species (positron), the same particle_start as
+# tracking_method_test (:9-14). The "Tracking" lines hold the transfer matrix that
+# make_mat6_tracking (bmad/low_level/make_mat6_tracking.f90:26-110) forms by central differences
+# of bmad_standard tracking with steps bmad_com%d_orb = 1e-5 (bmad_struct.f90:2315), and
+# vec0 = end orbit - matrix * start orbit. Elements on the path, with their .bmad lines:
+_m_q0 = dict(a_pole={0: 0.01, 1: 0.1}, vkick=-0.0001, b_pole_elec={0: -2e3}, a_pole_elec={1: 2e5})  # :64
+_m_sb0 = dict(a_pole={0: 0.001, 1: 0.1}, vkick=-0.0001, b_pole_elec={0: -2e3}, a_pole_elec={1: 2e3})  # :80
+FULL = 4  # fringe_type full$ (bmad_struct.f90:168)
+_m_mis = dict(num_steps=10, x_offset=0.05, y_pitch=0.001)
+M6_ELEMENTS = {
+    "AB_MULTIPOLE1": ("AB_MULTIPOLE", dict(a_pole={2: 1e3}, b_pole={2: 1e3}, x_offset=0.02, tilt=0.1), 19),
+    "DRIFT1": ("DRIFT", dict(l=4.5, tilt=0.1, **_m_mis), 23),
+    "INSTRUMENT1": ("INSTRUMENT", dict(l=4.5, num_steps=10), 34),
+    "MONITOR1": ("MONITOR", dict(l=4.5, num_steps=10), 56),
+    "MULTIPOLE1": ("MULTIPOLE", dict(a_pole={1: 1.0, 3: 4.5}, b_pole={1: PI / (2 * 1 + 2), 3: 0.31 * PI},
+                                     x_offset=0.05), 57),
+    "OCTUPOLE1": ("OCTUPOLE", dict(l=4.5, k3=1e3, tilt=PI / 8.0, num_steps=10, x_offset=0.01, y_pitch=0.001), 59),
+    "QUADRUPOLE1": ("QUADRUPOLE", dict(_m_q0, l=0.6, k1=1.0, tilt=0.1, **_m_mis), 65),
+    "QUADRUPOLE2": ("QUADRUPOLE", dict(_m_q0, l=0.6, k1=-1.0, tilt=PI / 4.0, **_m_mis), 66),
+    "QUADRUPOLE3": ("QUADRUPOLE", dict(_m_q0, l=0.6, k1=1e-20, tilt=PI / 4.0, **_m_mis), 67),
+    "QUADRUPOLE4": ("QUADRUPOLE", dict(_m_q0, l=0.6, k1=1.0, tilt=PI / 4.0, fringe_type=FULL, **_m_mis), 68),
+    "QUADRUPOLE5": ("QUADRUPOLE", dict(_m_q0, l=0.6, k1=-1.0, tilt=PI / 4.0, fringe_type=FULL, **_m_mis), 69),
+    "RFCAVITY1": ("RFCAVITY", dict(l=4.5, rf_frequency=500e6, voltage=5e5, phi0=0.1, tilt=0.1, b_pole={2: 0.002},
+                                   **_m_mis), 72),
+    "SBEND3": ("SBEND", dict(_m_sb0, l=0.6, k1=0.3, k2=3.0, ref_tilt=0.1, **_m_mis), 84),
+    "SBEND5": ("SBEND", dict(_m_sb0, l=0.6, g=0.01, e1=0.1, e2=0.2, fringe_type=FULL, ref_tilt=0.1,
+                             a_pole={0: 0.001, 1: 10.0, 3: 100.0}, fint=0.7, hgap=2.0, **_m_mis), 87),
+    "SBEND7": ("SBEND", dict(_m_sb0, l=0.6, g=0.01, e1=0.1, e2=0.2, ref_tilt=0.1, a_pole={0: 0.001, 1: 10.0, 3: 100.0},
+                             **_m_mis), 91),
+    "SEXTUPOLE1": ("SEXTUPOLE", dict(l=0.6, k2=1.0, tilt=PI / 6.0, **_m_mis), 94),
+    "THICK_MULTIPOLE1": ("THICK_MULTIPOLE", dict(l=4.5, a_pole={2: 1.0}, b_pole={2: 20.0}, x_offset=0.02, tilt=0.1),
+                         124),
+}
+
 # fringe_test.bmad: e_tot 1e6 electrons, particle_start, b: sbend ...
 FR_START = [0.01, 0.02, 0.03, 0.04, 0.00, 0.5]
 FR_ELEMENT = dict(e1=0.1, e2=-0.2, k1=0.1, g=0.1, fint=0.5, hgap=0.4)
@@ -87,6 +123,17 @@ def main():
                           tol=g["tol"], expected_vec=g["values"][:6]))
     json.dump(dict(source="regression_tests/tracking_method_test", e_tot=TM_E_TOT, charge=TM_CHARGE, start=TM_START,
                    cases=cases), open(os.path.join(HERE, "tracking_method_bmad_standard.json"), "w"), indent=1)
+
+    m6 = parse_output_correct(os.path.join(REF, "regression_tests/mat6_calc_method_test/output.correct"))
+    mcases = []
+    for name, (key, attrs, src_line) in M6_ELEMENTS.items():
+        rows = [m6["%s:Tracking:MatrixRow%d" % (name, i)] for i in range(1, 7)]
+        vec0 = m6[name + ":Tracking:Vector"]
+        mcases.append(dict(name=name, key=key, attrs=attrs, bmad_line=src_line, output_line=vec0["line"],
+                           tol_matrix=max(r["tol"] for r in rows), tol_vec0=vec0["tol"],
+                           expected_mat6=[r["values"] for r in rows], expected_vec0=vec0["values"]))
+    json.dump(dict(source="regression_tests/mat6_calc_method_test", e_tot=1e6, charge=1.0, start=TM_START, d_orb=1e-5,
+                   cases=mcases), open(os.path.join(HERE, "mat6_calc_method_tracking.json"), "w"), indent=1)
 
     fr = parse_output_correct(os.path.join(REF, "regression_tests/fringe_test/output.correct"))
     fcases = []

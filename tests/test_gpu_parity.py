@@ -93,6 +93,36 @@ def test_golden_vectors_on_gpu(ctx, case, data):
         assert abs(g["vec"][i, 0] - want) <= case["tol"] + 5e-11 * abs(want), (case["name"], i)
 
 
+def _m6_cases():
+    data = json.load(open(os.path.join(ROOT, "tests", "golden", "mat6_calc_method_tracking.json")))
+    return [(c, data) for c in data["cases"]]
+
+
+@pytest.mark.parametrize("case,data", _m6_cases(), ids=_golden_id)
+def test_mat6_by_tracking_on_gpu(ctx, case, data):
+    """Transfer matrix and vec0 of each element by central differences of GPU tracking (thirteen
+    particles, as make_mat6_tracking forms them) against the reference's mat6_calc_method_test
+    "Tracking" lines, ABS 1e-9."""
+    from test_oracle_golden import M6_NOT_RESTATED, matrix_by_tracking
+    p = abi.electron_param(data["e_tot"], charge=data["charge"])
+    e = abi.default_element(getattr(abi, case["key"]), **case["attrs"])
+    if case["name"] in M6_NOT_RESTATED:
+        with pytest.raises(lib.BmadGpuError) as ex:
+            lib.lattice_check([e], p)
+        assert ex.value.code == abi.EUNSUPPORTED
+        return
+
+    def track(starts):
+        g = gpu_track(ctx, [e], p, np.array(starts, dtype=np.float64).T.copy(), 1)
+        return list(g["vec"].T), list(g["state"])
+
+    mat, vec0 = matrix_by_tracking(track, data["start"], data["d_orb"])
+    want = np.asarray(case["expected_mat6"])
+    assert np.all(np.abs(mat - want) <= case["tol_matrix"] + 5e-14 * np.abs(want)), (case["name"], mat - want)
+    want0 = np.asarray(case["expected_vec0"])
+    assert np.all(np.abs(vec0 - want0) <= case["tol_vec0"] + 5e-14 * np.abs(want0)), (case["name"], vec0 - want0)
+
+
 # ---- single elements of every kind against the oracle -----------------------------------------
 
 def _single_element_cases():

@@ -62,3 +62,69 @@ def test_fringe_test_hwang():
                 want = case["expected_dmat"][i][j]
                 got = mat[i * 6 + j] - (1.0 if i == j else 0.0)
                 assert abs(got - want) <= case["tol"] + _printed_tol(want, 7), (case["edge"], i, j, got, want)
+
+
+# ---- transfer matrices by tracking (mat6_calc_method_test) ---------------------------------------
+
+def _m6_cases():
+    return json.load(open(os.path.join(HERE, "golden", "mat6_calc_method_tracking.json")))
+
+
+# Elements whose edge kicks the oracle does not restate (fringe_type full: exact_bend_edge_kick,
+# hard_multipole_edge_kick, soft_quadrupole_edge_kick); the oracle refuses them.
+M6_NOT_RESTATED = {"QUADRUPOLE4", "QUADRUPOLE5", "SBEND5"}
+
+
+def matrix_by_tracking(track, start, d):
+    """make_mat6_tracking (bmad/low_level/make_mat6_tracking.f90:26-110): the central particle and
+    the twelve particles displaced by +-d in one coordinate, tracked through the element; column i
+    of the matrix is the difference of the two end orbits over 2 d, and vec0 = end - matrix start.
+    track(list of 6-vectors) -> (list of end 6-vectors, list of states)."""
+    import numpy as np
+    starts = [list(start)]
+    for i in range(6):
+        for sgn in (1, -1):
+            v = list(start)
+            v[i] = v[i] + sgn * d
+            starts.append(v)
+    ends, states = track(starts)
+    ends = np.asarray(ends, dtype=np.float64)
+    assert all(s == 1 for s in states), states
+    mat = np.empty((6, 6))
+    for i in range(6):
+        mat[:, i] = (ends[1 + 2 * i] - ends[2 + 2 * i]) / (2 * d)
+    vec0 = ends[0] - mat @ np.asarray(start)
+    return mat, vec0
+
+
+def _oracle_tracker(abi, lib, ele, p):
+    def track(starts):
+        ends, states = [], []
+        for v in starts:
+            c = OracleCoord()
+            lib.oracle_init_coord(ctypes.byref(c), (ctypes.c_double * 6)(*v), ctypes.byref(p))
+            assert lib.oracle_track1(ctypes.byref(c), ctypes.byref(ele), 1, ctypes.byref(p)) == 0
+            ends.append([c.vec[i] for i in range(6)])
+            states.append(c.state)
+        return ends, states
+    return track
+
+
+@pytest.mark.parametrize("case", _m6_cases()["cases"], ids=lambda c: c["name"])
+def test_mat6_by_tracking(case):
+    """The oracle's transfer matrix and vec0 by central differences against the reference's
+    "Tracking" lines of mat6_calc_method_test (ABS 1e-9 on every entry)."""
+    import numpy as np
+    if case["name"] in M6_NOT_RESTATED:
+        pytest.skip("edge kick of fringe_type full not restated")
+    abi, lib = load_abi(), load_oracle()
+    data = _m6_cases()
+    p = abi.electron_param(data["e_tot"], charge=data["charge"])
+    ele = abi.default_element(getattr(abi, case["key"]), **case["attrs"])
+    mat, vec0 = matrix_by_tracking(_oracle_tracker(abi, lib, ele, p), data["start"], data["d_orb"])
+    want = np.asarray(case["expected_mat6"])
+    tol = case["tol_matrix"] + 5e-14 * np.abs(want)
+    bad = np.argwhere(np.abs(mat - want) > tol)
+    assert bad.size == 0, (case["name"], [(tuple(ij), mat[tuple(ij)], want[tuple(ij)]) for ij in bad[:4]])
+    want0 = np.asarray(case["expected_vec0"])
+    assert np.all(np.abs(vec0 - want0) <= case["tol_vec0"] + 5e-14 * np.abs(want0)), (case["name"], vec0, want0)
