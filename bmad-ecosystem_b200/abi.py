@@ -52,7 +52,8 @@ class Element(C.Structure):
                                   "orientation reserved").split()]
         + [(n, C.c_double) for n in _DOUBLE_FIELDS]
         + [("a_pole", C.c_double * N_POLE), ("b_pole", C.c_double * N_POLE),
-           ("a_pole_elec", C.c_double * N_POLE), ("b_pole_elec", C.c_double * N_POLE)]
+           ("a_pole_elec", C.c_double * N_POLE), ("b_pole_elec", C.c_double * N_POLE),
+           ("fq1", C.c_double), ("fq2", C.c_double)]
     )
 
 

@@ -360,8 +360,9 @@ struct AdjTape {
 
 // Which element bodies the adjoint covers (elements.cuh forms). 0 if supported.
 BG_HOST_DEVICE int adj_supported(const EleHdr& h) {
-  if (h.flags & (F_PITCH | F_ELEC)) return 1;  // pitched / bend-frame misalignment, electric multipoles:
-                                               // no vector-Jacobian product written
+  if (h.flags & (F_PITCH | F_EXTRA)) return 1;  // pitched / bend-frame misalignment, electric
+                                                // multipoles, higher-order edges: no
+                                                // vector-Jacobian product written
   switch (h.kind) {
     case K_MARKER:
     case K_DRIFT:

@@ -335,8 +335,8 @@ CR_HD dd sc_phase1(int i, double dh, const ScPoly& q, bool want_cos) {
   return {w.h, lo};
 }
 
-// Phase 2 of the same in double-double throughout, and the rounding of its result.
-CR_SLOW double sc_slow(int i, double dh, double dl, bool want_cos) {
+// Phase 2 of the same in double-double throughout.
+CR_HD dd sc_phase2(int i, double dh, double dl, bool want_cos) {
   const dd d{dh, dl};
   const dd d2 = dd_mul(d, d);
   dd ps = dd_ld(kSinCoef + 12);
@@ -349,7 +349,12 @@ CR_SLOW double sc_slow(int i, double dh, double dl, bool want_cos) {
   const dd cd = dd_add(dd{1.0, 0.0}, pc);
   const double* t = kSinCos + 4 * i;
   const dd S = dd_ld(t), C = dd_ld(t + 2);
-  const dd v = want_cos ? dd_add(dd_mul(C, cd), dd_neg(dd_mul(S, sd))) : dd_add(dd_mul(S, cd), dd_mul(C, sd));
+  return want_cos ? dd_add(dd_mul(C, cd), dd_neg(dd_mul(S, sd))) : dd_add(dd_mul(S, cd), dd_mul(C, sd));
+}
+
+// Phase 2 and the rounding of its result.
+CR_SLOW double sc_slow(int i, double dh, double dl, bool want_cos) {
+  const dd v = sc_phase2(i, dh, dl, want_cos);
   double out;
   if (!rounds(v.h, v.l, fabs(v.h) * kErr2, &out)) out = v.h + v.l;
   return out;
@@ -426,6 +431,57 @@ CR_API void sincos(double x, double* s, double* c) {
   if (!rounds(vc.h, vc.l, vc.h * kErr1, &cr)) cr = sc_slow(i, dh, dl, true);
   *s = x < 0 ? -sr : sr;
   *c = cr;
+}
+
+// ---- tan ---------------------------------------------------------------------------------------
+
+// tan of r = rh + rl, |r| <= pi/4 + a rounding (odd: -1/tan r, the cotangent branch of the
+// quadrants k = 1, 3): sin and cos of |r| as double-doubles and their double-double quotient. The
+// quotient's relative error is below the sum of the two phase errors and the division's (< 2^-100),
+// so the rounding test takes 3 times the phase bound.
+CR_SLOW double tan_slow(int i, double dh, double dl, bool odd) {
+  const dd s2 = sc_phase2(i, dh, dl, false), c2 = sc_phase2(i, dh, dl, true);
+  const dd s = fast_two_sum(s2.h, s2.l), c = fast_two_sum(c2.h, c2.l);
+  const dd v = odd ? dd_div(c, s) : dd_div(s, c);
+  double out;
+  if (!rounds(v.h, v.l, v.h * (3 * kErr2), &out)) out = v.h + v.l;
+  return out;
+}
+CR_HD double tan_reduced(double rh, double rl, bool odd) {
+  const bool neg = rh < 0;
+  if (neg) {
+    rh = -rh;
+    rl = -rl;
+  }
+  double dh, dl;
+  const int i = sc_split(rh, rl, dh, dl);
+  const ScPoly q = sc_poly1(dh, dl);
+  // phase 1 leaves low parts up to 2^-26 of the high ones: normalised before the division, whose
+  // correction step assumes both operands' low parts below an ulp
+  const dd s1 = sc_phase1(i, dh, q, false), c1 = sc_phase1(i, dh, q, true);
+  const dd s = fast_two_sum(s1.h, s1.l), c = fast_two_sum(c1.h, c1.l);
+  const dd v = odd ? dd_div(c, s) : dd_div(s, c);
+  double out;
+  if (!rounds(v.h, v.l, v.h * (3 * kErr1), &out)) out = tan_slow(i, dh, dl, odd);
+  return (neg != odd) ? -out : out;
+}
+
+// tan x = x (1 + x^2/3 + ...) rounds to x below 2^-27; beyond pi/4 the reduction by pi/2 (the
+// nearest multiple of pi/2 to any double is more than 2^-70 away, so sin r stays far inside the
+// range of the reciprocal).
+CR_SLOW double tan_cold(double x) {
+  const double ax = fabs(x);
+  if (!(ax <= 1.79769313486231570815e308)) return x - x;  // NaN, +-inf -> NaN
+  if (ax < 0x1p-27) return x;
+  double rh, rl;
+  const int k = reduce_pio2(x, rh, rl);
+  return tan_reduced(rh, rl, (k & 1) != 0);
+}
+
+CR_API double tan(double x) {
+  const double ax = fabs(x);
+  if (ax >= 0x1p-27 && ax <= 0x1.921fb54442d18p-1) return tan_reduced(x, 0.0, false);
+  return tan_cold(x);
 }
 
 // ---- atan2 and asin ----------------------------------------------------------------------------
@@ -764,6 +820,73 @@ CR_API void sinhcosh(double x, double* sh, double* ch) {
   os = os * sc;
   *sh = x < 0 ? -os : os;
   *ch = oc * sc;
+}
+
+// ---- exp ---------------------------------------------------------------------------------------
+
+// e^x below 2^-1022 (x < -708.3): F 2^m rounded on the grid of 2^-1074 that the subnormals and the
+// lowest binade share, as the integer nearest to W = F 2^(m+1074) < 2^53 (exact scaling), decided
+// by the same error test as the rounding to a double.
+CR_SLOW double exp_tiny(double x) {
+  if (x < -746.0) return 0.0;  // e^x < 2^-1076 rounds to +0
+  int m, j;
+  double rh, rl;
+  exp_reduce(x, m, j, rh, rl);
+  for (int phase = 1; phase <= 2; phase++) {
+    const dd F = phase == 1 ? exp_phase1(j, rh, rl, false) : exp_phase2(j, rh, rl, false);
+    const double sc = pow2(m + 1074);
+    const double wh = F.h * sc, wl = F.l * sc;
+    const double n = rint(wh);
+    const double f = wh - n;             // exact, |f| <= 1/2
+    const double up = (f - 0.5) + wl, down = (f + 0.5) + wl;  // distances to the midpoints
+    const double err = wh * (phase == 1 ? kErr1 : kErr2);
+    if (phase == 1 && (fabs(up) <= err || fabs(down) <= err)) continue;  // too close to decide
+    const double adj = up > 0 ? 1 : (down < 0 ? -1 : 0);
+    return (n + adj) * 0x1p-1074;
+  }
+  return 0.0;  // not reached
+}
+
+// e^x for |x| < 2^-26: D = e^x - 1 = x + x^2/2 + x^3/6 + x^4/24 (the rest below 2^-130) as a
+// double-double, rounded on the grid of the doubles next to 1 (2^-52 above, 2^-53 below) as the
+// integer nearest to D / grid. Near x = 2^-53 the value lies 2^-107 above a midpoint, which this
+// form resolves and a phase working to 2^-95 of the value would not.
+CR_SLOW double exp_small(double x) {
+  const dd q = two_prod(x, x);
+  const double c3 = x * (x * x) * (1.0 / 6), c4 = (q.h * q.h) * (1.0 / 24);
+  const dd D = two_sum(x, 0.5 * q.h);
+  const double dl = D.l + ((0.5 * q.l + c4) + c3);
+  const double grid = D.h >= 0 ? 0x1p52 : 0x1p53;
+  const double uh = D.h * grid, ul = dl * grid;
+  const double n = rint(uh);
+  const double f = uh - n;                  // exact, |f| <= 1/2
+  // the side of the midpoints n +- 1/2 (f -+ 1/2 exact for |f| >= 1/4; elsewhere far from them)
+  const double k = ((f - 0.5) + ul > 0) ? n + 1 : (((f + 0.5) + ul < 0) ? n - 1 : n);
+  return 1.0 + k / grid;
+}
+
+CR_SLOW double exp_cold(double x) {
+  if (x != x) return x + x;
+  if (x > 709.79) return 0x1p1023 * 2.0;  // overflow (and +inf)
+  if (x < -708.3) return exp_tiny(x);
+  return exp_small(x);                    // |x| < 2^-26
+}
+
+// e^x = 2^m 2^(j/64) e^r for -708.3 <= x <= 709.79 (a normal result): phase 1 of F, the rounding
+// test, phase 2 on failure, then the exact scaling (overflow to infinity at the top).
+CR_API double exp(double x) {
+  const double ax = fabs(x);
+  if (!(ax >= 0x1p-26 && x >= -708.3 && x <= 709.79)) return exp_cold(x);
+  int m, j;
+  double rh, rl;
+  exp_reduce(x, m, j, rh, rl);
+  const dd F = exp_phase1(j, rh, rl, false);
+  double out;
+  if (!rounds(F.h, F.l, F.h * kErr1, &out)) {
+    const dd G = exp_phase2(j, rh, rl, false);
+    if (!rounds(G.h, G.l, G.h * kErr2, &out)) out = G.h + G.l;
+  }
+  return scale_up(out, m);
 }
 
 }  // namespace cr

@@ -9,19 +9,20 @@ namespace bmadgpu {
 
 BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b, const double* __restrict__ el,
                      const Globals& G) {
-  // track_a_quadrupole, bmad/low_level/track_a_quadrupole.f90 (fringe_type none); the kick
-  // before the body and the kick after each step share one call site. With electric
-  // multipoles (F_ELEC, block el) the edges carry the electric fringe and every magnetic kick
-  // is followed by the electric one.
+  // track_a_quadrupole, bmad/low_level/track_a_quadrupole.f90; the kick before the body and the
+  // kick after each step share one call site. With an extra block (F_EXTRA) the edges carry the
+  // hard/soft quadrupole fringe and the electric fringe, and with electric multipoles every
+  // magnetic kick is followed by the electric one.
   const int np = h.n_pole;
   const double* kh = b + 3;
   const double* kf = kh + 2 * np;
   const double* mis = b + 3 + 4 * np;
   const bool has_t = h.flags & F_TILT;
-  const bool elec = h.flags & F_ELEC;
+  const double* xb = (h.flags & F_EXTRA) ? el : nullptr;
+  const bool elec = xb && xb[0] != 0;
   if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, h.flags & F_PITCH);
-  if (elec) {
-    elec_edge(p, el, true, G);
+  if (xb) {
+    straight_edge(p, xb, true, G);
     if (p.state != S_ALIVE) return;
   }
   const double b1 = b[0], length = b[1], step_len = b[2];
@@ -33,8 +34,8 @@ BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b,
     if (np) ab_kicks(p, end ? kh : kf, np, b_from2);
     if (elec) elec_kicks(p, el, end ? el[1] : el[2], G);
   }
-  if (elec) {
-    elec_edge(p, el, false, G);
+  if (xb) {
+    straight_edge(p, xb, false, G);
     if (p.state != S_ALIVE) return;
   }
   if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, h.flags & F_PITCH);
@@ -48,10 +49,11 @@ BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b
   const double* kf = kh + 2 * np;
   const double* mis = b + 1 + 4 * np;
   const bool has_t = h.flags & F_TILT;
-  const bool elec = h.flags & F_ELEC;
+  const double* xb = (h.flags & F_EXTRA) ? el : nullptr;
+  const bool elec = xb && xb[0] != 0;
   if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, h.flags & F_PITCH);
-  if (elec) {
-    elec_edge(p, el, true, G);
+  if (xb) {
+    straight_edge(p, xb, true, G);
     if (p.state != S_ALIVE) return;
   }
   const double step_len = b[0];
@@ -63,8 +65,8 @@ BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b
     if (np) ab_kicks(p, end ? kh : kf, np, b_from2);
     if (elec) elec_kicks(p, el, end ? el[1] : el[2], G);
   }
-  if (elec) {
-    elec_edge(p, el, false, G);
+  if (xb) {
+    straight_edge(p, xb, false, G);
     if (p.state != S_ALIVE) return;
   }
   if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, h.flags & F_PITCH);
@@ -91,15 +93,20 @@ BG_HD void body_bend(Particle& p, const EleHdr& h, const double* __restrict__ b,
   // track_a_bend, bmad/low_level/track_a_bend.f90:18-333
   const int np = h.n_pole;
   const double* mis = b + SB_FIXED + 2 * np;
-  const double* e = (h.flags & F_ELEC) ? el : nullptr;
+  const double* xb = (h.flags & F_EXTRA) ? el : nullptr;   // electric multipoles / fringe_type full
+  const double* e = (xb && xb[0] != 0) ? xb : nullptr;      // electric multipoles
+  const int in = xb ? (int)xb[3] : 0, out = xb ? (int)xb[4] : 0;
   if (h.flags & F_MISALIGN) {
     if (h.flags & F_PITCH) bend_frame(p, mis, true);   // offsets / pitches: the bend frame
     else tilt(p, mis[2], mis[3]);                     // ref_tilt only, offset_particle.f90:263-266
   }
-  // apply_element_edge_kick at the entrance: magnetic (Hwang) edge, then the electric fringe
-  if (e && e[3] != 0 && p.beta == 0) p.state = S_LOST;
-  if (h.flags & F_EDGE_IN) hwang_edge(p, b + SB_EDGE_IN, true);
-  if (e && e[3] == 2) elec_fringe(p, e, e[5], G);
+  // apply_element_edge_kick at the entrance (bend_edge_kick, fringe_mod.f90:40-128): hard-edge
+  // multipole, then the exact (fringe_type full) or Hwang edge, then the electric fringe
+  if ((in & EX_CALL) && p.beta == 0) p.state = S_LOST;
+  if (in & EX_HARD) hard_edge(p, xb, true);
+  if (in & EX_EXACT) exact_bend_edge(p, xb, true);
+  else if (h.flags & F_EDGE_IN) hwang_edge(p, b + SB_EDGE_IN, true);
+  if (in & EX_ELEC) elec_fringe(p, xb, xb[5], G);
   if (orbit_too_large(p, G)) return;
   if (np || e) bend_kick(p, b, np, e, true, G);
   for (int n = 1; n <= h.n_step; n++) {
@@ -114,10 +121,12 @@ BG_HD void body_bend(Particle& p, const EleHdr& h, const double* __restrict__ b,
     if (np || e) bend_kick(p, b, np, e, n == h.n_step, G);
   }
   if (orbit_too_large(p, G)) return;
-  // at the exit: the electric fringe, then the magnetic edge
-  if (e && e[4] != 0 && p.beta == 0) p.state = S_LOST;
-  if (e && e[4] == 2) elec_fringe(p, e, e[6], G);
-  if (h.flags & F_EDGE_OUT) hwang_edge(p, b + SB_EDGE_OUT, false);
+  // at the exit: the electric fringe, then the exact or Hwang edge, then the hard-edge multipole
+  if ((out & EX_CALL) && p.beta == 0) p.state = S_LOST;
+  if (out & EX_ELEC) elec_fringe(p, xb, xb[6], G);
+  if (out & EX_EXACT) exact_bend_edge(p, xb, false);
+  else if (h.flags & F_EDGE_OUT) hwang_edge(p, b + SB_EDGE_OUT, false);
+  if (out & EX_HARD) hard_edge(p, xb, false);
   if (h.flags & F_MISALIGN) {
     if (h.flags & F_PITCH) bend_frame(p, mis, false);
     else tilt(p, mis[2], -mis[3]);
@@ -190,7 +199,7 @@ BG_HD int track1(Particle& p, const EleHdr& h, const double* __restrict__ pool,
     if (p.state != S_ALIVE) return L_UPSTREAM;
   }
   const double* b = pool + h.param;
-  const double* el = pool + h.elec;
+  const double* el = pool + h.extra;
   switch (h.kind) {
     case K_DRIFT: drift(p, b[0]); break;
     case K_QUAD: body_quad(p, h, b, el, G); break;

@@ -1,7 +1,7 @@
 // hostcheck_count.cpp -- TEST/MEASUREMENT-ONLY: the device element code compiled for the host with
 // every floating-point value replaced by a counting type, to obtain the algorithmic FP64
 // operation count per particle-turn (the roofline numerator) from the very source the GPU runs.
-// Counts: add/sub, mul, div, sqrt, and transcendental calls (sin, cos, asin, atan2, sinh, cosh,
+// Counts: add/sub, mul, div, sqrt, and transcendental calls (sin, cos, asin, atan2, sinh, cosh, exp, tan,
 // fmod, fma), each counted once.
 #include <math.h>
 #include <stdint.h>
@@ -61,6 +61,8 @@ inline CD asin(CD a) { g_ops.trans++; return CD(std::asin(a.v)); }
 inline CD atan2(CD a, CD b) { g_ops.trans++; return CD(std::atan2(a.v, b.v)); }
 inline CD sinh(CD a) { g_ops.trans++; return CD(std::sinh(a.v)); }
 inline CD cosh(CD a) { g_ops.trans++; return CD(std::cosh(a.v)); }
+inline CD exp(CD a) { g_ops.trans++; return CD(std::exp(a.v)); }
+inline CD tan(CD a) { g_ops.trans++; return CD(std::tan(a.v)); }
 inline CD fmod(CD a, CD b) { g_ops.trans++; return CD(std::fmod(a.v, b.v)); }
 inline CD floor(CD a) { g_ops.trans++; return CD(std::floor(a.v)); }
 inline CD fma(CD a, CD b, CD c) { g_ops.trans++; return CD(std::fma(a.v, b.v, c.v)); }

@@ -308,15 +308,48 @@ int elec_ab(const bmadgpu_element& e, double* a, double* b) {
   return max_nonzero(a, b, kNPole - 1);
 }
 
-// The electric block (table.h). s_half / s_full: the kick scales of the element's loop; the edge
-// modes from apply_element_edge_kick's gate (at_this_ele_end of fringe_at) and the zero-length
-// exit of electric_longitudinal_fringe (apply_element_edge_kick.f90:290).
-std::vector<double> elec_block(const bmadgpu_element& e, const bmadgpu_param& p, const double* a, const double* b,
-                               int ix_elec_max, double s_half, double s_full) {
-  auto mode = [&](int end) { return at_ele_end(end, e.fringe_at) ? (e.l != 0 ? 2.0 : 1.0) : 0.0; };
-  std::vector<double> blk = {(double)(ix_elec_max + 1), s_half, s_full, mode(BMADGPU_ENTRANCE_END),
-                             mode(BMADGPU_EXIT_END), 1.0 * p.charge, -1.0 * p.charge, p.mass / p.p0c};
-  for (int n = 0; n <= ix_elec_max; n++) blk.insert(blk.end(), {b[n], a[n]});
+// The extra block (table.h) of a quadrupole, sextupole, octupole, thick multipole or sbend, or an
+// empty vector when the element needs none. Straight elements: apply_element_edge_kick runs when
+// init_fringe_info finds a fringe (fringe_type != none with fringe_at != no_end, or electric
+// multipoles; init_fringe_info.f90:22-55); bends: always, with the block only for electric
+// multipoles or fringe_type full (the Hwang edges are in the bend's own block). At each end the
+// edge acts when at_this_ele_end(fringe_at); fringe_here adds fringe_type != none
+// (fringe_here.f90:15-35); the electric fringe needs a length (apply_element_edge_kick.f90:290);
+// hard_multipole_edge_kick acts for full and hard_edge_only (not on bends), soft_quadrupole_
+// edge_kick for full and soft_edge_only (fringe_mod.f90:556-577, 692-722), exact_bend_edge_kick
+// for full (:40-99). s_half / s_full: the electric kick scales of the element's loop.
+std::vector<double> extra_block(const bmadgpu_element& e, const bmadgpu_param& p, const double* a, const double* b,
+                                int ix_elec_max, double s_half, double s_full) {
+  const bool raw_elec = any_nonzero(e.a_pole_elec, kNPole) || any_nonzero(e.b_pole_elec, kNPole);
+  const int ft = e.fringe_type;
+  const bool bend = e.key == BMADGPU_SBEND;
+  if (bend) {
+    if (ix_elec_max < 0 && ft != BMADGPU_FRINGE_FULL) return {};
+  } else {
+    const bool has_fringe = (ft != BMADGPU_FRINGE_NONE && e.fringe_at != BMADGPU_NO_END) || raw_elec;
+    if (!has_fringe) return {};
+  }
+  auto bits = [&](int end) {
+    if (!at_ele_end(end, e.fringe_at)) return 0.0;
+    int m = EX_CALL;
+    if (ix_elec_max > -1 && e.l != 0) m |= EX_ELEC;
+    if (ft != BMADGPU_FRINGE_NONE) {
+      const bool hard = ft == BMADGPU_FRINGE_FULL || (ft == BMADGPU_FRINGE_HARD_EDGE_ONLY && !bend);
+      if (hard && (bend || e.key == BMADGPU_QUADRUPOLE || e.key == BMADGPU_SEXTUPOLE)) m |= EX_HARD;
+      if ((ft == BMADGPU_FRINGE_FULL || ft == BMADGPU_FRINGE_SOFT_EDGE_ONLY) && e.key == BMADGPU_QUADRUPOLE)
+        m |= EX_SOFT;
+      if (bend && ft == BMADGPU_FRINGE_FULL) m |= EX_EXACT;
+    }
+    return (double)m;
+  };
+  const int n_elec = ix_elec_max + 1;
+  std::vector<double> blk = {(double)n_elec, s_half, s_full, bits(BMADGPU_ENTRANCE_END), bits(BMADGPU_EXIT_END),
+                             1.0 * p.charge, -1.0 * p.charge, p.mass / p.p0c,
+                             e.key == BMADGPU_SEXTUPOLE ? 2.0 : 1.0, e.key == BMADGPU_SEXTUPOLE ? e.k2 : e.k1,
+                             e.k1, e.fq1, e.fq2,
+                             e.is_on ? e.g + e.dg : 0.0, p.p0c / p.e_tot,
+                             1 * e.e1, 1 * e.fint, e.hgap, 1 * e.e2, 1 * e.fintx, e.hgapx, 0.0};
+  for (int n = 0; n < n_elec; n++) blk.insert(blk.end(), {b[n], a[n]});
   return blk;
 }
 
@@ -613,9 +646,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           fail(BMADGPU_EUNSUPPORTED, "pitch / z_offset misalignment of a thin multipole");
       if (e.key == BMADGPU_SBEND && (e.tilt != 0 || e.roll != 0))
         fail(BMADGPU_EUNSUPPORTED, "sbend tilt / roll");
-      if ((e.key == BMADGPU_QUADRUPOLE || e.key == BMADGPU_SEXTUPOLE) && e.is_on &&
-          e.fringe_type != BMADGPU_FRINGE_NONE && e.fringe_at != BMADGPU_NO_END)
-        fail(BMADGPU_EUNSUPPORTED, "quadrupole / sextupole fringe_type other than none");
+
       if (e.key != BMADGPU_SBEND && e.ref_tilt != 0) fail(BMADGPU_EUNSUPPORTED, "ref_tilt on a non-bend");
       if (e.key == BMADGPU_RFCAVITY && (e.hkick != 0 || e.vkick != 0))
         fail(BMADGPU_EUNSUPPORTED, "rfcavity hkick/vkick");
@@ -709,7 +740,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           double r_step = 1.0 / n_step;
           double step_len = e.l * r_step;
           blk = {b1, e.l, step_len};
-          if (ix_elec_max > -1) eblk = elec_block(e, p, ae, be, ix_elec_max, step_len / 2, step_len);
+          eblk = extra_block(e, p, ae, be, ix_elec_max, step_len / 2, step_len);
           if (ix_mag_max > -1) {
             flags |= F_KICKS;
             h.n_pole = (uint8_t)(ix_mag_max + 1);
@@ -729,7 +760,8 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           double r_step = 1.0 / n_step;
           double step_len = e.l / n_step;
           blk = {step_len};
-          if (ix_elec_max > -1) eblk = elec_block(e, p, ae, be, ix_elec_max, 1 * step_len / 2, 1 * step_len);
+          if (key != BMADGPU_MONITOR && key != BMADGPU_INSTRUMENT && key != BMADGPU_PIPE)
+            eblk = extra_block(e, p, ae, be, ix_elec_max, 1 * step_len / 2, 1 * step_len);
           if (ix_mag_max > -1) {
             flags |= F_KICKS;
             h.n_pole = (uint8_t)(ix_mag_max + 1);
@@ -767,7 +799,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           double r_step = 1.0 / n_step;
           double step_len = e.l / n_step;
           double angle = g * step_len;
-          if (ix_elec_max > -1) eblk = elec_block(e, p, ae, be, ix_elec_max, step_len * 0.5, step_len * 1.0);
+          eblk = extra_block(e, p, ae, be, ix_elec_max, step_len * 0.5, step_len * 1.0);
           double gl = g * step_len;
           blk = {step_len, g, g_tot, dg, angle, l_cos(angle), l_sin(angle), sinc0(angle), cosc0(angle),
                  (gl * gl) * sincc0(angle), (b1 != 0 && e.l != 0) ? b1 / e.l : 0.0,
@@ -795,8 +827,8 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           if (e.fringe_type == BMADGPU_FRINGE_BASIC_BEND || e.fringe_type == BMADGPU_FRINGE_HARD_EDGE_ONLY) {
             if (e.fringe_at == BMADGPU_ENTRANCE_END || e.fringe_at == BMADGPU_BOTH_ENDS) flags |= F_EDGE_IN;
             if (e.fringe_at == BMADGPU_EXIT_END || e.fringe_at == BMADGPU_BOTH_ENDS) flags |= F_EDGE_OUT;
-          } else if (e.fringe_type != BMADGPU_FRINGE_NONE) {
-            fail(BMADGPU_EUNSUPPORTED, "sbend fringe_type other than none/basic_bend/hard_edge_only");
+          } else if (e.fringe_type != BMADGPU_FRINGE_NONE && e.fringe_type != BMADGPU_FRINGE_FULL) {
+            fail(BMADGPU_EUNSUPPORTED, "sbend fringe_type other than none/basic_bend/hard_edge_only/full");
           }
           if (ix_mag_max > -1) {
             flags |= F_KICKS;
@@ -867,8 +899,8 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
       if ((flags & F_MISALIGN) && h.kind != K_SBEND && mis.size() >= 4 && mis[3] != 0) flags |= F_TILT;
       blk.insert(blk.end(), mis.begin(), mis.end());
       if (!eblk.empty() && (h.kind == K_QUAD || h.kind == K_THICK || h.kind == K_SBEND)) {
-        flags |= F_ELEC;
-        h.elec = pk.add_block(eblk);
+        flags |= F_EXTRA;
+        h.extra = pk.add_block(eblk);
       }
       h.flags = flags;
       h.param = pk.add_block(blk);

@@ -68,6 +68,8 @@ BG_HD double m_asin(double x) { return cr::asin(x); }
 BG_HD double m_atan2(double y, double x) { return cr::atan2(y, x); }
 BG_HD void m_sincos(double x, double& s, double& c) { cr::sincos(x, &s, &c); }
 BG_HD void m_sinhcosh(double x, double& s, double& c) { cr::sinhcosh(x, &s, &c); }
+BG_HD double m_exp(double x) { return cr::exp(x); }
+BG_HD double m_tan(double x) { return cr::tan(x); }
 #else
 BG_HD double m_sin(double x) { return sin(x); }
 BG_HD double m_cos(double x) { return cos(x); }
@@ -81,6 +83,8 @@ BG_HD void m_sinhcosh(double x, double& s, double& c) {
   s = sinh(x);
   c = cosh(x);
 }
+BG_HD double m_exp(double x) { return exp(x); }
+BG_HD double m_tan(double x) { return tan(x); }
 #endif
 
 struct Particle {
@@ -891,14 +895,215 @@ BG_COLD void elec_fringe(Particle& p, const double* __restrict__ e, double ff, c
   refresh(p, G);
 }
 
-// One electric edge of apply_element_edge_kick (apply_element_edge_kick.f90:37-282) for the
-// element types whose only edge field is electric: mode 0 no edge, 1 the beta check of a
-// zero-length element, 2 the beta check and the longitudinal fringe.
-BG_HD void elec_edge(Particle& p, const double* __restrict__ e, bool entering, const Globals& G) {
-  const int mode = (int)e[entering ? 3 : 4];
-  if (mode == 0) return;
+// ---- higher-order edge fringes (fringe_mod.f90) ----------------------------------------------
+// x: the extra block (table.h).
+
+// hard_multipole_edge_kick (fringe_mod.f90:692-865, no matrix): the hard-edge fringe of the
+// order-n (1 quadrupole, 2 sextupole) component, strength x[9], as a transverse map with the
+// Jacobian's determinant correcting the momenta. Complex arithmetic written out.
+BG_COLD void hard_edge(Particle& p, const double* __restrict__ xb, bool entering) {
+  const int n_max = (int)xb[8];
+  const double x = p.x, y = p.y;
+  double pr = x, pi = y;          // poly
+  double fx = 0, dfx_dx = 0, dfx_dy = 0, fy = 0, dfy_dx = 0, dfy_dy = 0;
+  const double rel_p = 1 + p.pz;
+  for (int n = 1; n <= n_max; n++) {
+    const double n1r = pr, n1i = pi;                       // poly_n1
+    const double qr = pr * x - pi * y, qi = pr * y + pi * x;  // poly * xy
+    pr = qr;
+    pi = qi;
+    if (n != n_max) continue;     // only the order of the element's own field is non-zero
+    const double dxr = (n + 1) * n1r, dxi = (n + 1) * n1i;  // dpoly_dx
+    const double dyr = -dxi, dyi = dxr;                      // i dpoly_dx
+    const double div = 4 * (n + 2) * rel_p;
+    double cr = 1.0 * xb[9], ci = 1.0 * 0.0;
+    cr = cr / div;
+    ci = ci / div;
+    if (entering) {
+      cr = -cr;
+      ci = -ci;
+    }
+    const double cn = (double)(n + 3) / (n + 1);
+    // f = Re(cab * poly * xny) and its x, y derivatives, xny = x - i cn y
+    double xr = x, xi = -cn * y;
+    double ar = cr * pr - ci * pi, ai = cr * pi + ci * pr;   // cab * poly
+    fx = fx + (ar * xr - ai * xi);
+    double tr = (dxr * xr - dxi * xi) + pr, ti = (dxr * xi + dxi * xr) + pi;
+    dfx_dx = dfx_dx + (cr * tr - ci * ti);
+    {
+      const double ur = dyr * xr - dyi * xi, ui = dyr * xi + dyi * xr;
+      const double wr = pr * 0.0 - pi * -cn, wi = pr * -cn + pi * 0.0;  // poly * dxny_dy
+      tr = ur + wr;
+      ti = ui + wi;
+      dfx_dy = dfx_dy + (cr * tr - ci * ti);
+    }
+    xr = y;
+    xi = cn * x;                  // xny = y + i cn x
+    fy = fy + (ar * xr - ai * xi);
+    {
+      const double ur = dxr * xr - dxi * xi, ui = dxr * xi + dxi * xr;
+      const double wr = pr * 0.0 - pi * cn, wi = pr * cn + pi * 0.0;    // poly * dxny_dx
+      tr = ur + wr;
+      ti = ui + wi;
+      dfy_dx = dfy_dx + (cr * tr - ci * ti);
+    }
+    tr = (dyr * xr - dyi * xi) + pr;
+    ti = (dyr * xi + dyi * xr) + pi;
+    dfy_dy = dfy_dy + (cr * tr - ci * ti);
+  }
+  const double px = p.px, py = p.py;
+  const double denom = (1 - dfx_dx) * (1 - dfy_dy) - dfx_dy * dfy_dx;
+  p.x = p.x - fx;
+  p.px = px + ((1.0 - dfy_dy - denom) * px + dfy_dx * py) / denom;
+  p.y = p.y - fy;
+  p.py = py + (dfx_dy * px + (1.0 - dfx_dx - denom) * py) / denom;
+  p.z = p.z + (p.px * fx + p.py * fy) / rel_p;
+}
+
+// soft_quadrupole_edge_kick (fringe_mod.f90:556-661, no matrix): the soft-edge quadrupole fringe
+// with the integrals fq1, fq2.
+BG_COLD void soft_quad_edge(Particle& p, const double* __restrict__ xb, bool entering) {
+  const double rel_p = 1 + p.pz;
+  const double k1_rel = 1.0 * xb[10] / rel_p;
+  double f1 = k1_rel * xb[11];
+  const double f2 = k1_rel * xb[12];
+  if (f1 == 0 && f2 == 0) return;
+  if (!entering) f1 = -f1;
+  const double ef1 = m_exp(f1);
+  const double v0 = p.x, v1 = p.px, v2 = p.y, v3 = p.py;
+  const double vx = v1 / rel_p, vy = v3 / rel_p;
+  p.z = p.z - (f1 * v0 + f2 * (1 + f1 / 2) * vx / ef1) * vx + (f1 * v2 + f2 * (1 - f1 / 2) * vy * ef1) * vy;
+  p.x = v0 * ef1 + vx * f2;
+  p.px = v1 / ef1;
+  p.y = v2 / ef1 - vy * f2;
+  p.py = v3 * ef1;
+}
+
+// bmad_rot_xz (fringe_mod.f90:1691-1771) and bmad_wedger (:1563-1690), no matrix: the rotation of
+// the reference frame by the edge angle, in a field g_tot for the wedger.
+BG_HD bool rot_xz(double a, double* __restrict__ v) {
+  const double x = v[0], px = v[1], py = v[3];
+  const double pp = 1 + v[5];
+  double ps = pp * pp - px * px - py * py;
+  if (ps <= 0) return false;
+  ps = sqrt(ps);
+  const double ca = m_cos(a), sa = m_sin(a);
+  const double den = ps * ca - px * sa;
+  const double L = x * sa / den;
+  v[0] = x * ps / den;
+  v[1] = px * ca + ps * sa;
+  v[2] = v[2] + py * L;
+  v[4] = v[4] - pp * L;
+  return true;
+}
+BG_HD bool wedger(double a, double g_tot, double* __restrict__ v) {
+  const double b1 = g_tot;
+  if (b1 == 0) return rot_xz(a, v);
+  const double x = v[0], px = v[1], py = v[3];
+  const double pp = 1 + v[5];
+  double ps = pp * pp - px * px - py * py;
+  if (ps <= 0) return false;
+  ps = sqrt(ps);
+  double pt = pp * pp - py * py;
+  if (pt < 1e-10) return false;
+  pt = sqrt(pt);
+  const double ca = m_cos(a), sa = m_sin(a), s2a = m_sin(2.0 * a), s2 = sa * sa;
+  const double pxn = px * ca + (ps - b1 * x) * sa;
+  double psn = pt * pt - pxn * pxn;
+  if (psn < 1e-10) return false;
+  psn = sqrt(psn);
+  const double den = psn + ps * ca - px * sa;
+  const double num = x * px * s2a + s2 * (2 * x * ps - b1 * (x * x));
+  const double L = (a + m_asin(px / pt) - m_asin(pxn / pt)) / b1;
+  v[0] = x * ca + num / den;
+  v[1] = pxn;
+  v[2] = v[2] + py * L;
+  v[4] = v[4] - pp * L;
+  return true;
+}
+
+// bmad_fringe_dipoler (fringe_mod.f90:1772-1933, no matrix): the hard-edge dipole fringe with the
+// fringe integral fint hgap.
+BG_HD bool fringe_dipoler(double* __restrict__ v, double g_tot, double beta0, double fint, double hgap,
+                          bool entering) {
+  const double b = entering ? g_tot : -g_tot;
+  const double x = v[0], px = v[1], y = v[2], py = v[3], z = v[4];
+  const double pp = 1 + v[5];
+  double ps = pp * pp - px * px - py * py;
+  if (ps <= 0) return false;
+  ps = sqrt(ps);
+  const double ee = sqrt(pp * pp + 1 / (beta0 * beta0) - 1);
+  const double beta = pp / ee;
+  const double xp = px / ps, yp = py / ps;
+  const double kap = b * fint * hgap;
+  const double fac2 = 1 + yp * yp;
+  const double d11 = (1 + xp * xp) / ps, d21 = xp * yp / ps, d31 = -xp;
+  const double d12 = xp * yp / ps, d22 = fac2 / ps, d32 = -yp;
+  const double d13 = -(ee * xp / (ps * ps)), d23 = -(ee * yp / (ps * ps)), d33 = ee / ps;
+  const double xf = xp / fac2;
+  const double fi0 = m_atan2(xf, 1.0) - 2 * kap * (1 + xp * xp * (2 + yp * yp)) * ps;  // atan(xp/fac2)
+  const double cf = m_cos(fi0);
+  const double co2 = b / (cf * cf);
+  const double co1 = co2 / (1 + xf * xf);
+  const double fi1 = co1 / fac2 - 4 * kap * co2 * xp * (2 + yp * yp) * ps;
+  const double fi2 = -(2 * co1 * xp * yp / (fac2 * fac2)) - 4 * kap * co2 * (xp * xp) * yp * ps;
+  const double fi3 = -(2 * kap * co2 * (1 + xp * xp * (2 + yp * yp)));
+  const double fi0t = b * m_tan(fi0);
+  const double bb2 = fi1 * d12 + fi2 * d22 + fi3 * d32;
+  double sq = 1 - 2 * bb2 * y;
+  if (sq < 0) return false;
+  sq = sqrt(sq);
+  const double ynew = 2 * y / (1 + sq);
+  const double bb1 = fi1 * d11 + fi2 * d21 + fi3 * d31;
+  const double bb3 = fi1 * d13 + fi2 * d23 + fi3 * d33;
+  v[0] = x + 0.5 * bb1 * (ynew * ynew);
+  v[2] = ynew;
+  v[3] = py - fi0t * ynew;
+  v[4] = z + 0.5 * beta * bb3 * (ynew * ynew);
+  return true;
+}
+
+// exact_bend_edge_kick (fringe_mod.f90:1474-1562, no matrix): wedge, dipole fringe, wedge.
+BG_COLD void exact_bend_edge(Particle& p, const double* __restrict__ xb, bool entering) {
+  const double g_tot = xb[13], beta0 = xb[14];
+  const double* q = xb + (entering ? 15 : 18);
+  const double edge_angle = q[0], fint = q[1], hgap = q[2];
+  double v[6] = {p.x, p.px, p.y, p.py, p.z, p.pz};
+  bool ok;
+  if (entering)
+    ok = wedger(edge_angle, 0.0, v) && fringe_dipoler(v, g_tot, beta0, 1 * fint, hgap, true) &&
+         wedger(-edge_angle, g_tot, v);
+  else
+    ok = wedger(-edge_angle, g_tot, v) && fringe_dipoler(v, g_tot, beta0, 1 * fint, hgap, false) &&
+         wedger(edge_angle, 0.0, v);
+  if (!ok) {
+    p.state = S_LOST_PZ;
+    return;
+  }
+  p.x = v[0];
+  p.px = v[1];
+  p.y = v[2];
+  p.py = v[3];
+  p.z = v[4];
+}
+
+// One edge of apply_element_edge_kick (apply_element_edge_kick.f90:37-282) for a quadrupole,
+// sextupole, octupole or thick multipole with an extra block: the beta check, the electric
+// fringe after the magnetic edge at the entrance and before it at the exit, and the hard and
+// soft fringes of the quadrupole (hard then soft entering, soft then hard leaving) or sextupole.
+BG_COLD void straight_edge(Particle& p, const double* __restrict__ xb, bool entering, const Globals& G) {
+  const int bits = (int)xb[entering ? 3 : 4];
+  if (!(bits & EX_CALL)) return;
   if (p.beta == 0) p.state = S_LOST;
-  if (mode == 2) elec_fringe(p, e, e[entering ? 5 : 6], G);
+  if (!entering && (bits & EX_ELEC)) elec_fringe(p, xb, xb[6], G);
+  if (entering) {
+    if (bits & EX_HARD) hard_edge(p, xb, true);
+    if (bits & EX_SOFT) soft_quad_edge(p, xb, true);
+  } else {
+    if (bits & EX_SOFT) soft_quad_edge(p, xb, false);
+    if (bits & EX_HARD) hard_edge(p, xb, false);
+  }
+  if (entering && (bits & EX_ELEC)) elec_fringe(p, xb, xb[5], G);
 }
 
 // Electric field of the bend's multipoles (elec_multipole_field.f90:25-60), summed over the

@@ -73,6 +73,8 @@ __global__ void k_cr_eval(int fn, const double* __restrict__ a, const double* __
       case 3: r = cr::atan2(x, b[i]); break;
       case 4: r = cr::sinh(x); break;
       case 5: r = cr::cosh(x); break;
+      case 8: r = cr::exp(x); break;
+      case 9: r = cr::tan(x); break;
       case 6: {  // sincos: sin in out[i], cos in out[n + i]
         double c;
         cr::sincos(x, &r, &c);
@@ -93,7 +95,7 @@ __global__ void k_cr_eval(int fn, const double* __restrict__ a, const double* __
 }  // namespace
 
 extern "C" int bmadgpu_cr_eval(bmadgpu_ctx* c, int32_t fn, const double* a, const double* b, double* out, int64_t n) {
-  if (!c || !a || !out || n < 0 || fn < 0 || fn > 7 || (fn == 3 && !b)) return fail(BMADGPU_EINVAL, "bad argument");
+  if (!c || !a || !out || n < 0 || fn < 0 || fn > 9 || (fn == 3 && !b)) return fail(BMADGPU_EINVAL, "bad argument");
   CUDA_TRY(cudaSetDevice(c->device));
   if (n == 0) return BMADGPU_OK;
   const int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)c->sm_count * 8);

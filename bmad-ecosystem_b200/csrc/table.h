@@ -40,7 +40,7 @@ enum Flag : uint16_t {
   F_TILT = 1 << 11,        // misalign block carries a non-zero tilt rotation
   F_KICK_B_FROM2 = 1 << 12, // both kick arrays: every a_n zero and b_0 = b_1 = 0, at least 3 orders
   F_PITCH = 1 << 13,       // misalign block of the pitched form (straight elements) or the bend frame
-  F_ELEC = 1 << 14         // electric multipoles: EleHdr::elec names their block
+  F_EXTRA = 1 << 14        // extra block (EleHdr::extra): electric multipoles, higher-order edge fringes
 };
 
 struct EleHdr {            // 16 bytes
@@ -50,7 +50,7 @@ struct EleHdr {            // 16 bytes
   uint16_t n_step;
   uint16_t ap_index;       // index into the aperture records
   uint32_t param;          // offset (in doubles) of the parameter block in the pool
-  uint32_t elec;           // offset (in doubles) of the electric block (F_ELEC), else 0
+  uint32_t extra;          // offset (in doubles) of the extra block (F_EXTRA), else 0
 };
 
 struct ApRec {             // 32 bytes: rectangular/elliptical limits (x1_lim = -x1_limit, ...)
@@ -80,14 +80,21 @@ struct ApRec {             // 32 bytes: rectangular/elliptical limits (x1_lim = 
 //           acting on the position r = (x, y, 0): op & FS_SUB: r -= v1; FS_SUBZ: r_z -= v1_z;
 //           FS_MAT: r = M r; FS_ADD: r += v2; FS_ADDZ: r_z += v2_z (in that order). W rotates the
 //           momentum; the particle then drifts from r_z to s_target.
-// electric block (F_ELEC; quadrupole, sextupole, octupole, thick_multipole, sbend):
-//           [n_elec, scale of the end kicks, scale of the interior kicks, entrance edge mode,
-//           exit edge mode, at_sign charge entrance, at_sign charge exit, mass / p0c] then
-//           (b_n, a_n) for n < n_elec (r0_elec scaled). Edge mode: 0 no edge call, 1 edge call
-//           (beta check only, zero length), 2 edge call with the electric longitudinal fringe.
-//           The scales are step_len / 2 and step_len (bends: step_len * 0.5, step_len * 1.0).
+// extra block (F_EXTRA; quadrupole, sextupole, octupole, thick_multipole with electric multipoles
+//           or an edge fringe, sbend with electric multipoles or fringe_type full):
+//           [0] n_elec  [1] electric kick scale at the ends  [2] scale of the interior kicks
+//           (step_len / 2 and step_len; bends step_len * 0.5 and step_len * 1.0)  [3] entrance
+//           edge bits  [4] exit edge bits  [5] at_sign charge entrance  [6] at_sign charge exit
+//           [7] mass / p0c  [8] hard-edge multipole order n (1 or 2)  [9] its strength (k1 or k2)
+//           [10] k1 [11] fq1 [12] fq2 (soft quadrupole edge)  [13] g_tot [14] beta0 (exact bend
+//           edge)  [15..17] entrance e1, fint, hgap  [18..20] exit e2, fintx, hgapx
+//           then (b_n, a_n) for n < n_elec (r0_elec scaled). Edge bits (EdgeBit): EX_CALL the
+//           element's apply_element_edge_kick acts at this end (beta check), EX_ELEC the electric
+//           longitudinal fringe, EX_HARD hard_multipole_edge_kick, EX_SOFT
+//           soft_quadrupole_edge_kick, EX_EXACT exact_bend_edge_kick (in place of Hwang's).
 constexpr int SB_EDGE_IN = 12, SB_EDGE_OUT = 19, SB_FIXED = 26;
-constexpr int EL_FIXED = 8, BF_FIXED = 22, BF_STEP = 16;
+constexpr int EL_FIXED = 22, BF_FIXED = 22, BF_STEP = 16;
+enum EdgeBit { EX_CALL = 1, EX_ELEC = 2, EX_HARD = 4, EX_SOFT = 8, EX_EXACT = 16 };
 enum FrameOp { FS_SUB = 1, FS_SUBZ = 2, FS_MAT = 4, FS_ADD = 8, FS_ADDZ = 16 };
 constexpr int RF_FIXED = 6;
 

@@ -38,6 +38,7 @@ type, bind(c) :: bmadgpu_element_t
   real(c_double) :: delta_ref_time
   real(c_double) :: a_pole(0:bmadgpu_n_pole-1), b_pole(0:bmadgpu_n_pole-1)
   real(c_double) :: a_pole_elec(0:bmadgpu_n_pole-1), b_pole_elec(0:bmadgpu_n_pole-1)
+  real(c_double) :: fq1, fq2
 end type
 
 type, bind(c) :: bmadgpu_param_t
@@ -222,6 +223,10 @@ e%voltage = ele%value(voltage$);  e%rf_frequency = ele%value(rf_frequency$)
 e%phi0 = ele%value(phi0$);  e%phi0_multipass = ele%value(phi0_multipass$)
 e%ds_step = ele%value(ds_step$);  e%r0_mag = ele%value(r0_mag$);  e%r0_elec = ele%value(r0_elec$)
 e%delta_ref_time = ele%value(delta_ref_time$)
+e%fq1 = 0;  e%fq2 = 0
+if (ele%key == quadrupole$) then
+  e%fq1 = ele%value(fq1$);  e%fq2 = ele%value(fq2$)
+endif
 e%a_pole = 0;  e%b_pole = 0;  e%a_pole_elec = 0;  e%b_pole_elec = 0
 if (associated(ele%a_pole)) then
   e%a_pole = ele%a_pole(0:bmadgpu_n_pole-1);  e%b_pole = ele%b_pole(0:bmadgpu_n_pole-1)

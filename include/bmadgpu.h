@@ -106,6 +106,7 @@ typedef struct bmadgpu_element {
   double delta_ref_time;      /* ele%value(delta_ref_time$); used only for the time coordinate */
   double a_pole[BMADGPU_N_POLE], b_pole[BMADGPU_N_POLE];
   double a_pole_elec[BMADGPU_N_POLE], b_pole_elec[BMADGPU_N_POLE];
+  double fq1, fq2;            /* quadrupole soft-edge fringe integrals (soft_quadrupole_edge_kick) */
 } bmadgpu_element;
 
 /* Branch/global parameters: lat_param_struct + the bmad_common_struct switches on the path. */
@@ -251,9 +252,10 @@ int bmadgpu_selftest_division(bmadgpu_ctx* ctx, int64_t n, uint64_t seed, int64_
 
 /* The correctly rounded transcendentals the element maps use, evaluated on the device for n
  * arguments (device memory): fn 0 sin(a), 1 cos(a), 2 asin(a), 3 atan2(a, b), 4 sinh(a),
- * 5 cosh(a), 6 sincos(a) (sin in out[0, n), cos in out[n, 2n)), 7 sinhcosh(a) (likewise). The
- * reference calls its libm here (sin, cos, asin, atan2, sinh, cosh in track_a_bend.f90:163-209,
- * quad_mat2_calc.f90:34-47, track_a_rfcavity.f90:117); the device's are correctly rounded so that
+ * 5 cosh(a), 6 sincos(a) (sin in out[0, n), cos in out[n, 2n)), 7 sinhcosh(a) (likewise),
+ * 8 exp(a), 9 tan(a). The reference calls its libm here (sin, cos, asin, atan2, sinh, cosh in
+ * track_a_bend.f90:163-209, quad_mat2_calc.f90:34-47, track_a_rfcavity.f90:117; exp and tan in
+ * the edge kicks of fringe_mod.f90); the device's are correctly rounded so that
  * its results equal the reference algorithm's with a correctly rounded libm, bit for bit. */
 int bmadgpu_cr_eval(bmadgpu_ctx* ctx, int32_t fn, const double* a, const double* b, double* out, int64_t n);
 

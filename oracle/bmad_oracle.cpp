@@ -28,14 +28,17 @@ namespace {
 typedef __float128 qp;
 
 // The libm of the restated routines: the host's (default: glibc, as a gfortran build of the
-// reference on Linux uses), or six functions the caller installs with oracle_set_libm (the tests
-// install correctly rounded ones to compare with the device, whose maps are correctly rounded).
+// reference on Linux uses), or eight functions the caller installs with oracle_set_libm (the
+// tests install correctly rounded ones to compare with the device, whose maps are correctly
+// rounded). atan(v) is taken as atan2(v, 1), the same value.
 double h_sin(double x) { return std::sin(x); }
 double h_cos(double x) { return std::cos(x); }
 double h_asin(double x) { return std::asin(x); }
 double h_atan2(double y, double x) { return std::atan2(y, x); }
 double h_sinh(double x) { return std::sinh(x); }
 double h_cosh(double x) { return std::cosh(x); }
+double h_exp(double x) { return std::exp(x); }
+double h_tan(double x) { return std::tan(x); }
 struct Libm {
   double (*sin)(double);
   double (*cos)(double);
@@ -43,8 +46,10 @@ struct Libm {
   double (*atan2)(double, double);
   double (*sinh)(double);
   double (*cosh)(double);
+  double (*exp)(double);
+  double (*tan)(double);
 };
-Libm lm = {h_sin, h_cos, h_asin, h_atan2, h_sinh, h_cosh};
+Libm lm = {h_sin, h_cos, h_asin, h_atan2, h_sinh, h_cosh, h_exp, h_tan};
 
 // sim_utils/interfaces/physical_constants.f90:12-13, 34
 const double pi = 3.141592653589793238462643383279;
@@ -1175,6 +1180,231 @@ void electric_longitudinal_fringe(Coord& orb, const Ele& ele, const double* a_po
   (void)E_r0; (void)E_r1;  // only enter the transfer matrix
 }
 
+// fringe_here, bmad/code/fringe_here.f90:15-35
+bool fringe_here(const Ele& ele, int particle_at) {
+  int physical_end = (particle_at == first_track_edge) ? BMADGPU_ENTRANCE_END : BMADGPU_EXIT_END;
+  if (ele.e->fringe_type == BMADGPU_FRINGE_NONE) return false;
+  return at_this_ele_end(physical_end, ele.e->fringe_at);
+}
+
+// Complex numbers with gfortran's operations (products written out, no special-value rules).
+struct Cx {
+  double re, im;
+};
+Cx cmul(Cx a, Cx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+Cx cadd(Cx a, Cx b) { return {a.re + b.re, a.im + b.im}; }
+Cx cscale(double f, Cx a) { return {f * a.re, f * a.im}; }
+
+// hard_multipole_edge_kick, bmad/modules/fringe_mod.f90:692-865 (no matrix): the hard-edge
+// fringe of the quadrupole (n = 1) or sextupole (n = 2) component of a quadrupole, sbend or
+// sextupole with fringe_type full (or hard_edge_only, not for sbends).
+void hard_multipole_edge_kick(const Ele& ele, int particle_at, Coord& orbit) {
+  const bmadgpu_element* e = ele.e;
+  switch (e->fringe_type) {
+    case BMADGPU_FRINGE_HARD_EDGE_ONLY:
+      if (e->key == BMADGPU_SBEND) return;
+      break;
+    case BMADGPU_FRINGE_FULL:
+      break;
+    default:
+      return;
+  }
+  if (!fringe_here(ele, particle_at)) return;
+  const double charge_dir = 1.0 * 1.0 * 1.0;  // orientation * direction * rel_tracking_charge
+  int n_max;
+  switch (e->key) {
+    case BMADGPU_QUADRUPOLE: case BMADGPU_SBEND: n_max = 1; break;
+    case BMADGPU_SEXTUPOLE: n_max = 2; break;
+    default: return;
+  }
+  const double x = orbit.vec[0], y = orbit.vec[2];
+  const Cx xy = {x, y};
+  Cx poly_n1 = {1, 0}, poly = xy;
+  const double rel_p = 1 + orbit.vec[5];
+  double fx = 0, dfx_dx = 0, dfx_dy = 0, fy = 0, dfy_dx = 0, dfy_dy = 0;
+  for (int n = 1; n <= n_max; n++) {
+    poly_n1 = poly;
+    poly = cmul(poly, xy);
+    double ap, bp;
+    if (e->key == BMADGPU_SEXTUPOLE) {
+      ap = 0;
+      bp = e->k2;
+      if (n != 2) continue;
+    } else {
+      ap = 0;
+      bp = e->k1;
+    }
+    const Cx dpoly_dx = cscale(n + 1, poly_n1);
+    const Cx dpoly_dy = {-dpoly_dx.im, dpoly_dx.re};  // i_imag * dpoly_dx
+    const double div = 4 * (n + 2) * rel_p;
+    Cx cab = cscale(charge_dir, Cx{bp, ap});
+    cab = {cab.re / div, cab.im / div};
+    if (particle_at == first_track_edge) cab = {-cab.re, -cab.im};
+    const double cn = (double)(n + 3) / (n + 1);
+    Cx xny = {x, -cn * y};
+    const Cx dxny_dy = {0.0, -cn};
+    fx = fx + cmul(cmul(cab, poly), xny).re;
+    dfx_dx = dfx_dx + cmul(cab, cadd(cmul(dpoly_dx, xny), poly)).re;
+    dfx_dy = dfx_dy + cmul(cab, cadd(cmul(dpoly_dy, xny), cmul(poly, dxny_dy))).re;
+    xny = {y, cn * x};
+    const Cx dxny_dx = {0.0, cn};
+    fy = fy + cmul(cmul(cab, poly), xny).re;
+    dfy_dx = dfy_dx + cmul(cab, cadd(cmul(dpoly_dx, xny), cmul(poly, dxny_dx))).re;
+    dfy_dy = dfy_dy + cmul(cab, cadd(cmul(dpoly_dy, xny), poly)).re;
+  }
+  const double px = orbit.vec[1], py = orbit.vec[3];
+  const double denom = (1 - dfx_dx) * (1 - dfy_dy) - dfx_dy * dfy_dx;
+  orbit.vec[0] = orbit.vec[0] - fx;
+  orbit.vec[1] = px + ((1.0 - dfy_dy - denom) * px + dfy_dx * py) / denom;
+  orbit.vec[2] = orbit.vec[2] - fy;
+  orbit.vec[3] = py + (dfx_dy * px + (1.0 - dfx_dx - denom) * py) / denom;
+  orbit.vec[4] = orbit.vec[4] + (orbit.vec[1] * fx + orbit.vec[3] * fy) / rel_p;
+}
+
+// soft_quadrupole_edge_kick, bmad/modules/fringe_mod.f90:556-661 (no matrix; quadrupoles, tilt1 = 0)
+void soft_quadrupole_edge_kick(const Ele& ele, int particle_at, Coord& orbit) {
+  const bmadgpu_element* e = ele.e;
+  if (e->fringe_type != BMADGPU_FRINGE_SOFT_EDGE_ONLY && e->fringe_type != BMADGPU_FRINGE_FULL) return;
+  if (!fringe_here(ele, particle_at)) return;
+  if (e->key != BMADGPU_QUADRUPOLE) return;
+  const double charge_dir = 1.0 * 1.0 * 1.0;
+  const double rel_p = 1 + orbit.vec[5];
+  const double k1_rel = charge_dir * e->k1 / rel_p;
+  double f1 = k1_rel * e->fq1;
+  const double f2 = k1_rel * e->fq2;
+  if (f1 == 0 && f2 == 0) return;
+  if (particle_at == second_track_edge) f1 = -f1;
+  const double ef1 = lm.exp(f1);
+  tilt_coords(0.0, orbit.vec);
+  const double v0 = orbit.vec[0], v1 = orbit.vec[1], v2 = orbit.vec[2], v3 = orbit.vec[3];
+  const double vx = v1 / rel_p, vy = v3 / rel_p;
+  orbit.vec[4] = orbit.vec[4] - (f1 * v0 + f2 * (1 + f1 / 2) * vx / ef1) * vx +
+                 (f1 * v2 + f2 * (1 - f1 / 2) * vy * ef1) * vy;
+  orbit.vec[0] = v0 * ef1 + vx * f2;
+  orbit.vec[1] = v1 / ef1;
+  orbit.vec[2] = v2 / ef1 - vy * f2;
+  orbit.vec[3] = v3 * ef1;
+  tilt_coords(-0.0, orbit.vec);
+}
+
+// bmad_rot_xz, fringe_mod.f90:1691-1771 (no matrix). Returns false on a lost particle.
+bool bmad_rot_xz(double a, double vec[6]) {
+  const double x = vec[0], px = vec[1], py = vec[3], delta = vec[5];
+  const double pp = 1 + delta;
+  double ps = pp * pp - px * px - py * py;
+  if (ps <= 0) return false;
+  ps = std::sqrt(ps);
+  const double ca = lm.cos(a), sa = lm.sin(a);
+  const double den = ps * ca - px * sa;
+  const double L = x * sa / den;
+  vec[0] = x * ps / den;
+  vec[1] = px * ca + ps * sa;
+  vec[2] = vec[2] + py * L;
+  vec[4] = vec[4] - pp * L;
+  return true;
+}
+
+// bmad_wedger, fringe_mod.f90:1563-1690 (no matrix): a wedge of angle a in a field g_tot.
+bool bmad_wedger(double a, double g_tot, double vec[6]) {
+  const double b1 = g_tot;
+  if (b1 == 0) return bmad_rot_xz(a, vec);
+  const double x = vec[0], px = vec[1], py = vec[3], delta = vec[5];
+  const double pp = 1 + delta;
+  double ps = pp * pp - px * px - py * py;
+  if (ps <= 0) return false;
+  ps = std::sqrt(ps);
+  double pt = pp * pp - py * py;
+  if (pt < 1e-10) return false;
+  pt = std::sqrt(pt);
+  const double ca = lm.cos(a), sa = lm.sin(a), s2a = lm.sin(2.0 * a), s2 = sa * sa;
+  const double pxn = px * ca + (ps - b1 * x) * sa;
+  double psn = pt * pt - pxn * pxn;
+  if (psn < 1e-10) return false;
+  psn = std::sqrt(psn);
+  const double den = psn + ps * ca - px * sa;
+  const double num = x * px * s2a + s2 * (2 * x * ps - b1 * (x * x));
+  const double L = (a + lm.asin(px / pt) - lm.asin(pxn / pt)) / b1;
+  vec[0] = x * ca + num / den;
+  vec[1] = pxn;
+  vec[2] = vec[2] + py * L;
+  vec[4] = vec[4] - pp * L;
+  return true;
+}
+
+// bmad_fringe_dipoler, fringe_mod.f90:1772-1933 (no matrix): the hard-edge dipole fringe with
+// the fringe integral fint * hgap.
+bool bmad_fringe_dipoler(double vec[6], double g_tot, double beta0, double fint, double hgap, int particle_at) {
+  const double b = (particle_at == second_track_edge) ? -g_tot : g_tot;
+  const double x = vec[0], px = vec[1], y = vec[2], py = vec[3], z = vec[4], delta = vec[5];
+  const double pp = 1 + delta;
+  double ps = pp * pp - px * px - py * py;
+  if (ps <= 0) return false;
+  ps = std::sqrt(ps);
+  const double ee = std::sqrt(pp * pp + 1 / (beta0 * beta0) - 1);
+  const double beta = pp / ee;
+  const double xp = px / ps, yp = py / ps;
+  const double kap = b * fint * hgap;
+  const double fac2 = 1 + yp * yp;
+  const double d11 = (1 + xp * xp) / ps, d21 = xp * yp / ps, d31 = -xp;
+  const double d12 = xp * yp / ps, d22 = fac2 / ps, d32 = -yp;
+  const double d13 = -(ee * xp / (ps * ps)), d23 = -(ee * yp / (ps * ps)), d33 = ee / ps;
+  const double xf = xp / fac2;
+  const double fi0 = lm.atan2(xf, 1.0) - 2 * kap * (1 + xp * xp * (2 + yp * yp)) * ps;  // atan(xp/fac2)
+  const double cf = lm.cos(fi0);
+  const double co2 = b / (cf * cf);
+  const double co1 = co2 / (1 + xf * xf);
+  const double fi1 = co1 / fac2 - 4 * kap * co2 * xp * (2 + yp * yp) * ps;
+  const double fi2 = -(2 * co1 * xp * yp / (fac2 * fac2)) - 4 * kap * co2 * (xp * xp) * yp * ps;
+  const double fi3 = -(2 * kap * co2 * (1 + xp * xp * (2 + yp * yp)));
+  const double fi0t = b * lm.tan(fi0);
+  const double bb2 = fi1 * d12 + fi2 * d22 + fi3 * d32;
+  double sq = 1 - 2 * bb2 * y;
+  if (sq < 0) return false;
+  sq = std::sqrt(sq);
+  const double ynew = 2 * y / (1 + sq);
+  const double bb1 = fi1 * d11 + fi2 * d21 + fi3 * d31;
+  const double bb3 = fi1 * d13 + fi2 * d23 + fi3 * d33;
+  vec[0] = x + 0.5 * bb1 * (ynew * ynew);
+  vec[2] = ynew;
+  vec[3] = py - fi0t * ynew;
+  vec[4] = z + 0.5 * beta * bb3 * (ynew * ynew);
+  return true;
+}
+
+// exact_bend_edge_kick, fringe_mod.f90:1474-1562 (no matrix; the time coordinate follows from
+// the element's end orbit): wedge, hard-edge dipole fringe, wedge.
+void exact_bend_edge_kick(const Ele& ele, int particle_at, Coord& orb) {
+  const bmadgpu_element* e = ele.e;
+  const bmadgpu_param* p = ele.p;
+  const double beta0 = p->p0c / p->e_tot;
+  const double g_tot = e->is_on ? e->g + e->dg : 0.0;
+  double edge_angle, fint, hgap;
+  if (particle_at == first_track_edge) {
+    edge_angle = 1 * e->e1;
+    fint = e->fint;
+    hgap = e->hgap;
+  } else {
+    edge_angle = 1 * e->e2;
+    fint = e->fintx;
+    hgap = e->hgapx;
+  }
+  double vec[6];
+  for (int i = 0; i < 6; i++) vec[i] = orb.vec[i];
+  bool ok;
+  if (particle_at == first_track_edge) {
+    ok = bmad_wedger(edge_angle, 0.0, vec) && bmad_fringe_dipoler(vec, g_tot, beta0, 1 * fint, hgap, particle_at) &&
+         bmad_wedger(-edge_angle, g_tot, vec);
+  } else {
+    ok = bmad_wedger(-edge_angle, g_tot, vec) && bmad_fringe_dipoler(vec, g_tot, beta0, 1 * fint, hgap, particle_at) &&
+         bmad_wedger(edge_angle, 0.0, vec);
+  }
+  if (!ok) {
+    orb.state = BMADGPU_LOST_PZ;
+    return;
+  }
+  for (int i = 0; i < 6; i++) orb.vec[i] = vec[i];
+}
+
 // apply_element_edge_kick, bmad/low_level/apply_element_edge_kick.f90:37-282, for the
 // element types on the path with bmad_standard field_calc.
 int apply_element_edge_kick(Coord& orb, const Ele& ele, int particle_at) {
@@ -1189,23 +1419,33 @@ int apply_element_edge_kick(Coord& orb, const Ele& ele, int particle_at) {
   if (err) return err;
   if (particle_at == second_track_edge) electric_longitudinal_fringe(orb, ele, a_el, b_el, ix_elec_max, at_sign);
   switch (e->key) {
-    case BMADGPU_QUADRUPOLE: case BMADGPU_SEXTUPOLE:
-      // hard_multipole_edge_kick / soft_quadrupole_edge_kick act only for fringe_type full,
-      // hard_edge_only or soft_edge_only (fringe_mod.f90:576-577, 715-722).
-      if (e->fringe_type != BMADGPU_FRINGE_NONE) return BMADGPU_EUNSUPPORTED;
+    case BMADGPU_QUADRUPOLE:  // apply_element_edge_kick.f90:171-179
+      if (particle_at == first_track_edge) {
+        hard_multipole_edge_kick(ele, particle_at, orb);
+        soft_quadrupole_edge_kick(ele, particle_at, orb);
+      } else {
+        soft_quadrupole_edge_kick(ele, particle_at, orb);
+        hard_multipole_edge_kick(ele, particle_at, orb);
+      }
+      break;
+    case BMADGPU_SEXTUPOLE:
+      hard_multipole_edge_kick(ele, particle_at, orb);
       break;
     case BMADGPU_SBEND: {
       // bend_edge_kick, fringe_mod.f90:40-128
-      bool here = at_this_ele_end(physical_end, e->fringe_at) && e->fringe_type != BMADGPU_FRINGE_NONE;
-      if (here) {
-        switch (e->fringe_type) {
-          case BMADGPU_FRINGE_BASIC_BEND: case BMADGPU_FRINGE_HARD_EDGE_ONLY:
-            hwang_bend_edge_kick(ele, particle_at, orb, nullptr);
-            break;
-          default:
-            return BMADGPU_EUNSUPPORTED;
-        }
+      if (!fringe_here(ele, particle_at)) break;
+      if (particle_at == first_track_edge) hard_multipole_edge_kick(ele, particle_at, orb);
+      switch (e->fringe_type) {
+        case BMADGPU_FRINGE_FULL:
+          exact_bend_edge_kick(ele, particle_at, orb);
+          break;
+        case BMADGPU_FRINGE_BASIC_BEND: case BMADGPU_FRINGE_HARD_EDGE_ONLY:
+          hwang_bend_edge_kick(ele, particle_at, orb, nullptr);
+          break;
+        default:
+          return BMADGPU_EUNSUPPORTED;
       }
+      if (particle_at == second_track_edge) hard_multipole_edge_kick(ele, particle_at, orb);
       break;
     }
     default:
@@ -1924,12 +2164,13 @@ int oracle_hwang_bend_edge_kick(const bmadgpu_element* e, const bmadgpu_param* p
 }
 
 void oracle_set_libm(double (*f_sin)(double), double (*f_cos)(double), double (*f_asin)(double),
-                     double (*f_atan2)(double, double), double (*f_sinh)(double), double (*f_cosh)(double)) {
-  if (!f_sin || !f_cos || !f_asin || !f_atan2 || !f_sinh || !f_cosh) {
-    lm = Libm{h_sin, h_cos, h_asin, h_atan2, h_sinh, h_cosh};
+                     double (*f_atan2)(double, double), double (*f_sinh)(double), double (*f_cosh)(double),
+                     double (*f_exp)(double), double (*f_tan)(double)) {
+  if (!f_sin || !f_cos || !f_asin || !f_atan2 || !f_sinh || !f_cosh || !f_exp || !f_tan) {
+    lm = Libm{h_sin, h_cos, h_asin, h_atan2, h_sinh, h_cosh, h_exp, h_tan};
     return;
   }
-  lm = Libm{f_sin, f_cos, f_asin, f_atan2, f_sinh, f_cosh};
+  lm = Libm{f_sin, f_cos, f_asin, f_atan2, f_sinh, f_cosh, f_exp, f_tan};
 }
 
 int32_t oracle_max_threads(void) {

@@ -73,11 +73,12 @@ int oracle_track_ring(const bmadgpu_element* eles, int32_t n_ele, const bmadgpu_
 /* Number of OpenMP threads the oracle would use with n_threads <= 0. */
 int32_t oracle_max_threads(void);
 
-/* The six libm functions the restated routines call (sin, cos, asin, atan2, sinh, cosh): by
- * default the host's; the given ones if all six are non-NULL; the host's again if any is NULL.
- * Not thread-safe against a tracking call in progress. */
+/* The eight libm functions the restated routines call (sin, cos, asin, atan2, sinh, cosh, exp,
+ * tan; atan(v) is atan2(v, 1)): by default the host's; the given ones if all eight are non-NULL;
+ * the host's again if any is NULL. Not thread-safe against a tracking call in progress. */
 void oracle_set_libm(double (*f_sin)(double), double (*f_cos)(double), double (*f_asin)(double),
-                     double (*f_atan2)(double, double), double (*f_sinh)(double), double (*f_cosh)(double));
+                     double (*f_atan2)(double, double), double (*f_sinh)(double), double (*f_cosh)(double),
+                     double (*f_exp)(double), double (*f_tan)(double));
 
 #ifdef __cplusplus
 }

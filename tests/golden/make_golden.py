@@ -62,6 +62,9 @@ TM_ELEMENTS = {
                              ref_tilt=0.1), 84),
     "SBEND7": ("SBEND", dict(_sb0, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, x_offset=0.05, y_pitch=0.001,
                              ref_tilt=0.1), 91),
+    # fringe_type full: exact_bend_edge_kick with fint = 0.7, hgap = 2 (:87-88)
+    "SBEND5": ("SBEND", dict(_sb0, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, fringe_type=4, x_offset=0.05,
+                             y_pitch=0.001, ref_tilt=0.1, fint=0.7, hgap=2.0), 87),
 }
 
 # mat6_calc_method_test.bmad: e_tot 1e6, default species (positron), the same particle_start as

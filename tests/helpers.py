@@ -81,7 +81,7 @@ _CRLIB = None
 
 
 def cr_libm(kind="cr"):
-    """Addresses of six libm functions for oracle_set_libm: "cr", the correctly rounded functions
+    """Addresses of the eight libm functions for oracle_set_libm: "cr", the correctly rounded functions
     the device maps use (host build of csrc/crmath.cuh); "quad", libquadmath's rounded once, an
     independent correctly rounded set."""
     global _CRLIB
@@ -96,7 +96,7 @@ def cr_libm(kind="cr"):
         _CRLIB = ctypes.CDLL(path)
     pre = "bmadgpu_cr_" if kind == "cr" else "bmadgpu_q_"
     return [ctypes.cast(getattr(_CRLIB, pre + f), ctypes.c_void_p) for f in ("sin", "cos", "asin", "atan2", "sinh",
-                                                                            "cosh")]
+                                                                            "cosh", "exp", "tan")]
 
 
 class oracle_libm:
@@ -107,11 +107,11 @@ class oracle_libm:
 
     def __enter__(self):
         lib = load_oracle()
-        lib.oracle_set_libm.argtypes = [ctypes.c_void_p] * 6
+        lib.oracle_set_libm.argtypes = [ctypes.c_void_p] * 8
         lib.oracle_set_libm(*cr_libm(self.kind))
         return self
 
     def __exit__(self, *exc):
         lib = load_oracle()
-        lib.oracle_set_libm(None, None, None, None, None, None)
+        lib.oracle_set_libm(*([None] * 8))
         return False

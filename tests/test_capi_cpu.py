@@ -57,7 +57,7 @@ def test_config1_ring_packs_and_sextupoles_use_one_step():
     assert all(s == 1 for e, s in zip(eles, steps) if e.key == abi.SEXTUPOLE)
 
 
-@pytest.mark.parametrize("bad", ["elec_on_rfcavity", "bend_roll", "bend_tilt", "quad_fringe_full", "abs_time"])
+@pytest.mark.parametrize("bad", ["elec_on_rfcavity", "bend_roll", "bend_tilt", "bend_soft_edge", "abs_time"])
 def test_unsupported_inputs_fail_loudly(bad):
     abi = load_abi()
     p = abi.electron_param(3e9)
@@ -69,8 +69,8 @@ def test_unsupported_inputs_fail_loudly(bad):
         e = abi.default_element(abi.SBEND, l=1.0, g=0.01, roll=1e-3)
     elif bad == "bend_tilt":
         e = abi.default_element(abi.SBEND, l=1.0, g=0.01, tilt=1e-3)
-    elif bad == "quad_fringe_full":
-        e.fringe_type = abi.FRINGE_FULL
+    elif bad == "bend_soft_edge":
+        e = abi.default_element(abi.SBEND, l=1.0, g=0.01, fringe_type=abi.FRINGE_SOFT_EDGE_ONLY)
     else:
         p.absolute_time_tracking = 1
     with pytest.raises(lib.BmadGpuError) as ei:
@@ -108,3 +108,16 @@ def test_misaligned_bends_and_electric_multipoles_are_accepted():
         e.b_pole_elec[1] = 1e3
         e.a_pole_elec[0] = -2e3
         lib.lattice_check([e], p)
+
+
+def test_edge_fringes_are_accepted():
+    """fringe_type full / hard_edge_only / soft_edge_only of quadrupoles and sextupoles and full of
+    sbends (hard_multipole_edge_kick, soft_quadrupole_edge_kick, exact_bend_edge_kick)."""
+    abi = load_abi()
+    p = abi.electron_param(3e9)
+    for ft in (abi.FRINGE_FULL, abi.FRINGE_HARD_EDGE_ONLY, abi.FRINGE_SOFT_EDGE_ONLY):
+        for key in (abi.QUADRUPOLE, abi.SEXTUPOLE):
+            lib.lattice_check([abi.default_element(key, l=0.4, k1=0.5, k2=3.0, fringe_type=ft, fq1=0.01)], p)
+    lib.lattice_check([abi.default_element(abi.SBEND, l=1.0, g=0.01, e1=0.1, fint=0.5, hgap=0.02,
+                                           fringe_type=abi.FRINGE_FULL)], p)
+

@@ -18,7 +18,7 @@ import pytest
 from conftest import ROOT
 
 LIB = os.path.join(ROOT, "bmad-ecosystem_b200", "_build", "libbmadgpu_crmath.so")
-FN = {"sin": 0, "cos": 1, "asin": 2, "atan2": 3, "sinh": 4, "cosh": 5}
+FN = {"sin": 0, "cos": 1, "asin": 2, "atan2": 3, "sinh": 4, "cosh": 5, "exp": 8, "tan": 9}
 
 
 @pytest.fixture(scope="module")
@@ -45,7 +45,9 @@ def exact(name, a, b=0.0):
     """mpmath's value rounded to the nearest double (ties to even)."""
     if a == 0 and name in ("sin", "asin", "sinh"):
         return a                     # odd functions keep the sign of zero (mpmath has no -0)
-    prec = 1300 if name in ("sin", "cos") and abs(a) >= 2.0 ** 20 else 200
+    if a == 0 and name == "tan":
+        return a
+    prec = 1300 if name in ("sin", "cos", "tan") and abs(a) >= 2.0 ** 20 else 200
     with mp.workprec(prec):
         x = mp.mpf(a)
         if name == "sin":
@@ -58,6 +60,15 @@ def exact(name, a, b=0.0):
             v = mp.atan2(x, mp.mpf(b))
         elif name == "sinh":
             v = mp.sinh(x)
+        elif name == "exp":
+            v = mp.exp(x)
+            if v < mp.mpf(2) ** -1022:   # subnormal range: round on the grid of 2^-1074
+                q = v / mp.mpf(2) ** -1074
+                n = mp.floor(q)
+                n = n + 1 if (q - n > 0.5 or (q - n == 0.5 and int(n) % 2)) else n
+                return float(n) * 2.0 ** -1074
+        elif name == "tan":
+            v = mp.tan(x)
         else:
             v = mp.cosh(x)
         if abs(v) > mp.mpf(2) ** 1024 * (1 - mp.mpf(2) ** -54):
@@ -168,3 +179,26 @@ def test_sinhcosh_same_bits(cr):
     for i, v in enumerate(a):
         cr.bmadgpu_cr_sinhcosh(v, ctypes.byref(s), ctypes.byref(c))
         assert s.value == s_ref[i] and c.value == c_ref[i], v
+
+
+def test_tan(cr):
+    rng = np.random.default_rng(17)
+    for a in (rng.uniform(-0.8, 0.8, N), rng.uniform(-4, 4, N), rng.uniform(-1e5, 1e5, N),
+              logu(rng, -40, 20, N), logu(rng, 20, 1023, N // 3),
+              # next to odd multiples of pi/2 (the poles) and to multiples of pi (the zeros)
+              np.array([k * math.pi / 2 * (1 + e) for k in range(1, 40) for e in (-3e-16, 0, 3e-16, 1e-12)]),
+              np.array([0.0, -0.0, 5e-324, 2.0 ** -27, -(2.0 ** -28), 1e-300])):
+        check(cr, "tan", a)
+    assert np.all(np.isnan(evaluate(cr, "tan", np.array([math.inf, -math.inf, math.nan]))))
+
+
+def test_exp(cr):
+    rng = np.random.default_rng(18)
+    for a in (rng.uniform(-1, 1, N), rng.uniform(-700, 700, N), logu(rng, -60, 0, N),
+              rng.uniform(709.0, 709.79, N // 3), rng.uniform(-745.2, -700.0, N),
+              np.array([0.0, -0.0, 5e-324, 2.0 ** -54, -(2.0 ** -54), 2.0 ** -53, 1.0, -1.0,
+                        709.782712893384, 709.7827128933841, -708.3, -708.39, -745.13, -745.14, -746.0, -800.0])):
+        check(cr, "exp", a)
+    out = evaluate(cr, "exp", np.array([math.inf, -math.inf, 710.0, math.nan]))
+    assert out[0] == math.inf and out[1] == 0.0 and out[2] == math.inf and math.isnan(out[3])
+

@@ -43,6 +43,12 @@ def arguments(name, rng, n):
                                [1.0, -1.0, 0.0, -0.0, 2.0, np.nan]])
     if name == "atan2":
         return np.concatenate([lu(-60, 60, n), rng.uniform(-1, 1, n), lu(-1000, 1000, n // 8), [0.0, -0.0, np.inf]])
+    if name == "tan":
+        return np.concatenate([rng.uniform(-0.8, 0.8, n), rng.uniform(-4, 4, n), lu(-60, 30, n), lu(20, 1023, n // 8),
+                               [0.0, -0.0, 5e-324, np.inf, -np.inf, np.nan, np.pi / 2]])
+    if name == "exp":
+        return np.concatenate([rng.uniform(-1, 1, n), rng.uniform(-745, 709.7, n), lu(-60, -20, n),
+                               [0.0, -0.0, np.inf, -np.inf, np.nan, 2.0 ** -53, -708.39, 709.78]])
     return np.concatenate([rng.uniform(-0.3, 0.3, n), rng.uniform(-3, 3, n), rng.uniform(-711, 711, n),
                            lu(-60, 0, n), [0.0, -0.0, np.inf, -np.inf, np.nan, 2.0 ** -26]])
 
@@ -53,7 +59,7 @@ def same_bits(x, y):
     return np.array_equal(nx, ny) and np.array_equal(x[~nx].view(np.uint64), y[~ny].view(np.uint64))
 
 
-@pytest.mark.parametrize("name", ["sin", "cos", "asin", "atan2", "sinh", "cosh"])
+@pytest.mark.parametrize("name", ["sin", "cos", "asin", "atan2", "sinh", "cosh", "exp", "tan"])
 def test_device_equals_host_build(ctx, cr_host, name):
     rng = np.random.default_rng(100 + H.FN[name])
     a = arguments(name, rng, 250000)

@@ -5,7 +5,7 @@ libm.
 The device maps keep the reference's operation order (no FMA contraction); in this build they
 call correctly rounded sin, cos, asin, atan2, sinh and cosh (csrc/crmath.cuh), and the element
 invariants are packed with the same functions. The oracle -- the restatement of the reference's Fortran --
-takes its six libm functions from oracle_set_libm; installed with the same correctly rounded set
+takes its libm functions from oracle_set_libm; installed with the same correctly rounded set
 (checked against mpmath and against libquadmath on the CPU), it is the reference's algorithm
 with a correctly rounded libm, and the GPU must reproduce it exactly: every coordinate, beta,
 state, loss element, loss turn and location, after 1 and after 1000 turns, at 10,000 particles

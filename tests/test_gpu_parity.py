@@ -62,8 +62,8 @@ def assert_close(g, o, tol, floor_frac=1.0, alive_only=True):
 
 # Golden cases whose element form the device path refuses (BMADGPU_EUNSUPPORTED), by name, with
 # the reason; every other case runs on the GPU against its golden line. None is refused: the
-# electric multipoles of QUADRUPOLE1-3, SBEND3 and SBEND7 and the misaligned-bend frame of the
-# last two are on the device.
+# electric multipoles of QUADRUPOLE1-3 and SBEND3/5/7, the misaligned-bend frame of the bends
+# and SBEND5's exact edge (fringe_type full) are on the device.
 REFUSED_ON_DEVICE = {}
 
 
@@ -166,6 +166,16 @@ def _single_element_cases():
         "sbend_ref_tilt_offsets": [E(abi.SBEND, l=0.8, g=0.05, e1=0.02, e2=-0.01, ref_tilt=0.3, x_offset=1e-3,
                                      y_pitch=2e-4, **ap)],
         "sbend_g0_offsets": [E(abi.SBEND, l=0.6, k1=0.2, x_offset=1e-3, y_pitch=1e-3, z_offset=-0.02, **ap)],
+        "quad_fringe_full": [E(abi.QUADRUPOLE, l=0.4, k1=0.8, fringe_type=abi.FRINGE_FULL, fq1=0.02, fq2=-0.01, tilt=0.3,
+                               **ap)],
+        "quad_soft_edge": [E(abi.QUADRUPOLE, l=0.4, k1=0.8, fringe_type=abi.FRINGE_SOFT_EDGE_ONLY, fq1=0.05, fq2=0.01,
+                             **ap)],
+        "sextupole_fringe_full": [E(abi.SEXTUPOLE, l=0.3, k2=20.0, fringe_type=abi.FRINGE_FULL, x_offset=1e-3, **ap)],
+        "sbend_fringe_full": [E(abi.SBEND, l=1.0, g=0.05, k1=0.2, e1=0.1, e2=-0.05, fint=0.5, hgap=0.03,
+                                fringe_type=abi.FRINGE_FULL, **ap)],
+        "sbend5_like": [E(abi.SBEND, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, fringe_type=abi.FRINGE_FULL,
+                          x_offset=0.002, y_pitch=0.001, ref_tilt=0.1, fint=0.7, hgap=2.0,
+                          a_pole={0: 0.001, 1: 10.0, 3: 100.0}, b_pole_elec={0: -2e5}, a_pole_elec={1: 2e6}, **ap)],
         "sbend7_like": [E(abi.SBEND, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, x_offset=0.002, y_pitch=0.001,
                           ref_tilt=0.1, a_pole={0: 0.01, 1: 0.1}, vkick=-1e-4, b_pole_elec={0: -2e5},
                           a_pole_elec={1: 2e6}, r0_mag=2.0, r0_elec=3.0, **ap)],

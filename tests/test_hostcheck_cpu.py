@@ -86,6 +86,21 @@ CASES = {
     "sbend_g0_offsets": lambda E, ap: [E(abi.SBEND, l=0.6, k1=0.2, x_offset=1e-3, y_pitch=1e-3, z_offset=-0.02, **ap)],
     "sbend_g0_ref_tilt": lambda E, ap: [E(abi.SBEND, l=0.6, k1=0.3, k2=3.0, ref_tilt=0.1, x_offset=2e-3,
                                           y_pitch=1e-3, num_steps=10, **ap)],
+    # higher-order edge fringes: hard-edge multipole, soft quadrupole edge, exact bend edge
+    "quad_fringe_full": lambda E, ap: [E(abi.QUADRUPOLE, l=0.4, k1=0.8, fringe_type=abi.FRINGE_FULL, fq1=0.02, fq2=-0.01,
+                                         tilt=0.3, **ap)],
+    "quad_hard_edge_exit": lambda E, ap: [E(abi.QUADRUPOLE, l=0.4, k1=-0.8, fringe_type=abi.FRINGE_HARD_EDGE_ONLY,
+                                            fringe_at=abi.EXIT_END, b_pole_elec={1: 3e6}, **ap)],
+    "quad_soft_edge": lambda E, ap: [E(abi.QUADRUPOLE, l=0.4, k1=0.8, fringe_type=abi.FRINGE_SOFT_EDGE_ONLY, fq1=0.05,
+                                       fq2=0.01, **ap)],
+    "sextupole_fringe_full": lambda E, ap: [E(abi.SEXTUPOLE, l=0.3, k2=20.0, fringe_type=abi.FRINGE_FULL,
+                                              x_offset=1e-3, **ap)],
+    "octupole_fringe_full": lambda E, ap: [E(abi.OCTUPOLE, l=0.3, k3=200.0, fringe_type=abi.FRINGE_FULL, **ap)],
+    "sbend_fringe_full": lambda E, ap: [E(abi.SBEND, l=1.0, g=0.05, k1=0.2, e1=0.1, e2=-0.05, fint=0.5, hgap=0.03,
+                                          fringe_type=abi.FRINGE_FULL, **ap)],
+    "sbend5_like": lambda E, ap: [E(abi.SBEND, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, fringe_type=abi.FRINGE_FULL,
+                                    x_offset=0.002, y_pitch=0.001, ref_tilt=0.1, fint=0.7, hgap=2.0,
+                                    a_pole={0: 0.001, 1: 10.0, 3: 100.0}, b_pole_elec={0: -2e5}, a_pole_elec={1: 2e6}, **ap)],
     "sbend7_like": lambda E, ap: [E(abi.SBEND, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, x_offset=0.002,
                                     y_pitch=0.001, ref_tilt=0.1, a_pole={0: 0.01, 1: 0.1}, vkick=-1e-4,
                                     b_pole_elec={0: -2e5}, a_pole_elec={1: 2e6}, r0_mag=2.0, r0_elec=3.0, **ap)],

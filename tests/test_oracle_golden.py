@@ -72,7 +72,7 @@ def _m6_cases():
 
 # Elements whose edge kicks the oracle does not restate (fringe_type full: exact_bend_edge_kick,
 # hard_multipole_edge_kick, soft_quadrupole_edge_kick); the oracle refuses them.
-M6_NOT_RESTATED = {"QUADRUPOLE4", "QUADRUPOLE5", "SBEND5"}
+M6_NOT_RESTATED = set()
 
 
 def matrix_by_tracking(track, start, d):
