@@ -587,11 +587,12 @@ BG_HD void adj_load(const double* buf, int64_t row, int64_t N, int64_t j, Partic
   refresh(p, G);
 }
 
-// One turn of track1 over every element; false if the particle was lost.
+// One turn of track1 over every element; false if the particle was lost. The adjoint accepts no
+// element with an extra block or a pitched offset (adj_supported), so the lean track1 serves.
 BG_HD bool adj_turn(Particle& p, const AdjArgs& a, bool first_turn, double* store, int64_t j) {
   for (int ie = 0; ie < a.n_ele; ++ie) {
     if (store) adj_store(store, ie, a.N, j, p);
-    if (track1(p, a.hdr[ie], a.pool, a.ap, a.G, first_turn && ie == 0)) return false;
+    if (track1<false>(p, a.hdr[ie], a.pool, a.ap, a.G, first_turn && ie == 0)) return false;
   }
   return true;
 }

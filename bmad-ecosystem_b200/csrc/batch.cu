@@ -86,8 +86,10 @@ __global__ void k_batch_init_list(int32_t* __restrict__ list, int64_t n, unsigne
 struct Variant {
   int block, minb;
   const void* fn;
+  const void* fn_lean;
 };
-#define BG_BATCH_VARIANT(B, M) {B, M, (const void*)k_batch_track<B, M, false>}
+#define BG_BATCH_VARIANT(B, M) \
+  {B, M, (const void*)k_batch_track<B, M, false, true>, (const void*)k_batch_track<B, M, false, false>}
 const Variant kVariants[] = {
     BG_BATCH_VARIANT(64, 8),  BG_BATCH_VARIANT(64, 12), BG_BATCH_VARIANT(128, 3), BG_BATCH_VARIANT(128, 4),
     BG_BATCH_VARIANT(128, 5), BG_BATCH_VARIANT(128, 6), BG_BATCH_VARIANT(256, 1), BG_BATCH_VARIANT(256, 2),
@@ -134,6 +136,14 @@ cudaError_t batch_resolve(const BatchLaunch& cfg, uint32_t smem_bytes, int sm_co
   err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_rec, fn_rec, cfg.block, smem_bytes);
   if (err != cudaSuccess) return err;
   if (per_sm_rec < 1) per_sm_rec = 1;
+  err = cudaFuncSetAttribute(v->fn_lean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  if (err != cudaSuccess) return err;
+  int per_sm_lean = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_lean, v->fn_lean, cfg.block, smem_bytes);
+  if (err != cudaSuccess) return err;
+  if (per_sm_lean < 1) per_sm_lean = 1;
+  out->fn_lean = v->fn_lean;
+  out->grid_lean = sm_count * per_sm_lean;
   out->fn = v->fn;
   out->fn_rec = fn_rec;
   out->grid_rec = sm_count * per_sm_rec;
@@ -149,6 +159,8 @@ cudaError_t batch_launch_track(const BatchKernel& k, const BatchArgs& a, cudaStr
   void* args[] = {(void*)&a, (void*)&ppt};
   if (record)
     return cudaLaunchKernel(k.fn_rec, dim3((unsigned)k.grid_rec), dim3((unsigned)k.block), args, k.smem, stream);
+  if (!a.rare)
+    return cudaLaunchKernel(k.fn_lean, dim3((unsigned)k.grid_lean), dim3((unsigned)k.block), args, k.smem, stream);
   return cudaLaunchKernel(k.fn, dim3((unsigned)k.grid), dim3((unsigned)k.block), args, k.smem, stream);
 }
 

@@ -49,6 +49,7 @@ struct BatchArgs {
   unsigned long long* queue;         // work-item counter, zero at launch
   int32_t* err_flag;                 // bit 0: table staging wait timed out
   uint32_t smem_bytes;               // dynamic shared memory for staging (0: read tables from global)
+  int32_t rare;                      // some variant's table has extra blocks / pitched offsets
 };
 
 struct BatchLaunch {
@@ -64,6 +65,8 @@ struct BatchKernel {
   uint32_t smem = 0;
   const void* fn_rec = nullptr;  // the same shape with the frequency-map record path
   int grid_rec = 0;
+  const void* fn_lean = nullptr; // the same shape for tables without rare forms (TableInfo::rare)
+  int grid_lean = 0;
 };
 
 cudaError_t batch_upload_constants();

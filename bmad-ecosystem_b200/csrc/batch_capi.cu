@@ -34,6 +34,7 @@ struct bmadgpu_batch {
   int64_t* d_prefix = nullptr;          // [n_var + 1]
   unsigned long long* d_queue = nullptr;
   uint32_t smem_bytes = 0;        // largest stageable table
+  int32_t rare = 0;               // some variant's table has extra blocks / pitched offsets
   bmadgpu_batch_tuning tuning;
   cudaGraphExec_t exec = nullptr;
   int32_t graph_turns = -1;
@@ -106,6 +107,7 @@ int enqueue_calls(bmadgpu_batch* b, const BatchKernel& k, int32_t n_turns, int64
   a.queue = b->d_queue;
   a.err_flag = b->ctx->d_err;
   a.smem_bytes = smem;
+  a.rare = b->rare;
   for (int32_t c = 0; c < n_chunks; ++c) {
     const bool last = c == n_chunks - 1;
     a.turn_off = c * tpl;
@@ -212,6 +214,7 @@ int bmadgpu_batch_create(bmadgpu_ctx* c, int32_t n_var, const bmadgpu_lattice* c
   int64_t off = 0;
   for (int32_t v = 0; v < n_var; ++v) {
     const bmadgpu_lattice* L = lats[v];
+    if (L->pk.info.rare) b->rare = 1;
     b->offs[v] = off;
     BatchVar& d = hv[v];
     std::memset(&d, 0, sizeof(d));

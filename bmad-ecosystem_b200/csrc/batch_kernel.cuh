@@ -37,7 +37,7 @@ __device__ __noinline__ void fma_record(const BatchVar& v, int64_t j, int32_t t_
 
 // REC: the instantiation for rounds that hold a frequency-map job; every other launch uses the
 // REC = false code, which has no record path at all.
-template <int BLOCK, int MINB, bool REC>
+template <int BLOCK, int MINB, bool REC, bool FULL = true>
 __global__ void __launch_bounds__(BLOCK, MINB) k_batch_track(const BatchArgs a, int ppt) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_batch_track(const BatchArgs a, 
       if (alive) {
         refresh(p, G);
         for (int turn = 0; turn < nt && alive; ++turn) {
-          alive = track_turn(p, hdr, pool, ap, G, 0, n_ele, turn == 0, turn_no0 + turn, li);
+          alive = track_turn<FULL>(p, hdr, pool, ap, G, 0, n_ele, turn == 0, turn_no0 + turn, li);
           if (REC && sv.rec && alive)
             fma_record(sv, j, turn_no0 + turn - sv.rec_turn0, p.x, p.px, p.y, p.py, p.z, p.pz);
         }

@@ -106,6 +106,7 @@ int track_device(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bunch
   std::memset(&a, 0, sizeof(a));
   a.table = lat->d_table;
   a.table_bytes = lat->pk.info.total_bytes;
+  a.rare = (int32_t)lat->pk.info.rare;
   a.hdr_bytes = lat->pk.info.hdr_bytes;
   a.ap_bytes = lat->pk.info.ap_bytes;
   a.ix_start = ix_start;
@@ -194,6 +195,7 @@ int noalloc_prepare(bmadgpu_ctx* c, const bmadgpu_lattice* lat, const bmadgpu_bu
   std::memset(a, 0, sizeof(*a));
   a->table = lat->d_table;
   a->table_bytes = lat->pk.info.total_bytes;
+  a->rare = (int32_t)lat->pk.info.rare;
   a->hdr_bytes = lat->pk.info.hdr_bytes;
   a->ap_bytes = lat->pk.info.ap_bytes;
   a->ix_start = 0;

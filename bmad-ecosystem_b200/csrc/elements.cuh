@@ -7,6 +7,11 @@ namespace bmadgpu {
 
 // ---- element bodies (track1_bmad dispatch, bmad/low_level/track1_bmad.f90:64-272) ----------
 
+// Each body and track1 come in two forms: FULL = true handles every element form; FULL = false,
+// for tables without any extra block or pitched offset (TableInfo::rare = 0, the common rings),
+// leaves those forms out, so that their out-of-line helpers add nothing to the kernels that
+// track such rings.
+template <bool FULL>
 BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b, const double* __restrict__ el,
                      const Globals& G) {
   // track_a_quadrupole, bmad/low_level/track_a_quadrupole.f90; the kick before the body and the
@@ -18,9 +23,10 @@ BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b,
   const double* kf = kh + 2 * np;
   const double* mis = b + 3 + 4 * np;
   const bool has_t = h.flags & F_TILT;
-  const double* xb = (h.flags & F_EXTRA) ? el : nullptr;
+  const double* xb = (FULL && (h.flags & F_EXTRA)) ? el : nullptr;
   const bool elec = xb && xb[0] != 0;
-  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, h.flags & F_PITCH);
+  const bool pitched = FULL && (h.flags & F_PITCH);
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, pitched);
   if (xb) {
     straight_edge(p, xb, true, G);
     if (p.state != S_ALIVE) return;
@@ -38,9 +44,10 @@ BG_HD void body_quad(Particle& p, const EleHdr& h, const double* __restrict__ b,
     straight_edge(p, xb, false, G);
     if (p.state != S_ALIVE) return;
   }
-  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, h.flags & F_PITCH);
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, pitched);
 }
 
+template <bool FULL>
 BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b, const double* __restrict__ el,
                       const Globals& G) {
   // track_a_thick_multipole, bmad/low_level/track_a_thick_multipole.f90:18-133
@@ -49,9 +56,10 @@ BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b
   const double* kf = kh + 2 * np;
   const double* mis = b + 1 + 4 * np;
   const bool has_t = h.flags & F_TILT;
-  const double* xb = (h.flags & F_EXTRA) ? el : nullptr;
+  const double* xb = (FULL && (h.flags & F_EXTRA)) ? el : nullptr;
   const bool elec = xb && xb[0] != 0;
-  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, h.flags & F_PITCH);
+  const bool pitched = FULL && (h.flags & F_PITCH);
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, pitched);
   if (xb) {
     straight_edge(p, xb, true, G);
     if (p.state != S_ALIVE) return;
@@ -69,7 +77,7 @@ BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b
     straight_edge(p, xb, false, G);
     if (p.state != S_ALIVE) return;
   }
-  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, h.flags & F_PITCH);
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, pitched);
 }
 
 BG_HD void bend_kick(Particle& p, const double* __restrict__ b, int np, const double* __restrict__ el, bool half,
@@ -88,16 +96,17 @@ BG_HD void bend_kick(Particle& p, const double* __restrict__ b, int np, const do
   if (el) bend_elec_kick(p, el, half ? el[1] : el[2], b[1], E1, E2, G);
 }
 
+template <bool FULL>
 BG_HD void body_bend(Particle& p, const EleHdr& h, const double* __restrict__ b, const double* __restrict__ el,
                      const Globals& G) {
   // track_a_bend, bmad/low_level/track_a_bend.f90:18-333
   const int np = h.n_pole;
   const double* mis = b + SB_FIXED + 2 * np;
-  const double* xb = (h.flags & F_EXTRA) ? el : nullptr;   // electric multipoles / fringe_type full
+  const double* xb = (FULL && (h.flags & F_EXTRA)) ? el : nullptr;   // electric multipoles / fringe_type full
   const double* e = (xb && xb[0] != 0) ? xb : nullptr;      // electric multipoles
   const int in = xb ? (int)xb[3] : 0, out = xb ? (int)xb[4] : 0;
   if (h.flags & F_MISALIGN) {
-    if (h.flags & F_PITCH) bend_frame(p, mis, true);   // offsets / pitches: the bend frame
+    if (FULL && (h.flags & F_PITCH)) bend_frame(p, mis, true);   // offsets / pitches: the bend frame
     else tilt(p, mis[2], mis[3]);                     // ref_tilt only, offset_particle.f90:263-266
   }
   // apply_element_edge_kick at the entrance (bend_edge_kick, fringe_mod.f90:40-128): hard-edge
@@ -128,7 +137,7 @@ BG_HD void body_bend(Particle& p, const EleHdr& h, const double* __restrict__ b,
   else if (h.flags & F_EDGE_OUT) hwang_edge(p, b + SB_EDGE_OUT, false);
   if (out & EX_HARD) hard_edge(p, xb, false);
   if (h.flags & F_MISALIGN) {
-    if (h.flags & F_PITCH) bend_frame(p, mis, false);
+    if (FULL && (h.flags & F_PITCH)) bend_frame(p, mis, false);
     else tilt(p, mis[2], -mis[3]);
   }
 }
@@ -156,13 +165,15 @@ BG_HD void body_thin(Particle& p, const EleHdr& h, const double* __restrict__ b)
   if (h.flags & F_MISALIGN) offset_unset(p, mis, false);
 }
 
+template <bool FULL>
 BG_HD void body_rf(Particle& p, const EleHdr& h, const double* __restrict__ b, const Globals& G) {
   // track_a_rfcavity, bmad/low_level/track_a_rfcavity.f90:17-146 (relative time tracking)
   const int np = h.n_pole;
   const double* kh = b + RF_FIXED;
   const double* mis = kh + 2 * np;
   const bool has_t = h.flags & F_TILT;
-  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, h.flags & F_PITCH);
+  const bool pitched = FULL && (h.flags & F_PITCH);
+  if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, pitched);
   if (np) ab_kicks(p, kh, np);
   const double voltage = b[0], f = b[1], slice_len = b[4];
   const int n_slice = h.n_step;
@@ -184,13 +195,14 @@ BG_HD void body_rf(Particle& p, const EleHdr& h, const double* __restrict__ b, c
   }
   refresh(p, G);
   if (np) ab_kicks(p, kh, np);
-  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, h.flags & F_PITCH);
+  if (h.flags & F_MISALIGN) offset_unset(p, mis, has_t, pitched);
 }
 
 // track1 around one element: entrance orbit/aperture checks, body, exit checks
 // (track1.f90:179-196, 221-236, 289-329). Returns 0 if the particle survived, else its
 // coord%location at the loss. The entrance orbit_too_large test repeats the previous element's
 // exit test on unchanged coordinates, so it runs only for the first element of a launch.
+template <bool FULL = true>
 BG_HD int track1(Particle& p, const EleHdr& h, const double* __restrict__ pool,
                                       const ApRec* __restrict__ ap, const Globals& G, bool entry_check) {
   if (entry_check && orbit_too_large(p, G)) return L_UPSTREAM;
@@ -202,11 +214,11 @@ BG_HD int track1(Particle& p, const EleHdr& h, const double* __restrict__ pool,
   const double* el = pool + h.extra;
   switch (h.kind) {
     case K_DRIFT: drift(p, b[0]); break;
-    case K_QUAD: body_quad(p, h, b, el, G); break;
-    case K_THICK: body_thick(p, h, b, el, G); break;
-    case K_SBEND: body_bend(p, h, b, el, G); break;
+    case K_QUAD: body_quad<FULL>(p, h, b, el, G); break;
+    case K_THICK: body_thick<FULL>(p, h, b, el, G); break;
+    case K_SBEND: body_bend<FULL>(p, h, b, el, G); break;
     case K_THIN: body_thin(p, h, b); break;
-    case K_RFCAV: body_rf(p, h, b, G); break;
+    case K_RFCAV: body_rf<FULL>(p, h, b, G); break;
     default: break;  // K_MARKER
   }
   if (orbit_too_large(p, G)) return L_UPSTREAM;

@@ -919,6 +919,9 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
     total = (total + 15) & ~size_t(15);
     ti.total_bytes = (uint32_t)total;
     ti.turn_ref_time = turn_ref;
+    ti.rare = 0;
+    for (const EleHdr& h : pk.hdr)
+      if (h.flags & (F_EXTRA | F_PITCH)) ti.rare = 1;
     out.image.assign(total, 0);
     std::memcpy(out.image.data(), pk.hdr.data(), ti.hdr_bytes);
     if (ti.ap_bytes) std::memcpy(out.image.data() + ti.hdr_bytes, pk.ap.data(), ti.ap_bytes);

@@ -44,13 +44,14 @@ __device__ __forceinline__ void load_particle(const SoA& s, int64_t j, Particle&
 }
 
 // One turn over elements [ix_start, ix_end). Returns false (and fills li) if the particle is lost.
+template <bool FULL = true>
 __device__ __forceinline__ bool track_turn(Particle& p, const EleHdr* __restrict__ hdr, const double* __restrict__ pool,
                                            const ApRec* __restrict__ ap, const Globals& G, int ix_start, int ix_end,
                                            bool first_turn, int turn_no, LossInfo& li) {
   for (int ie = ix_start; ie < ix_end; ++ie) {
     EleHdr h;
     load_hdr(hdr, ie, h);
-    int loc = track1(p, h, pool, ap, G, first_turn && ie == ix_start);
+    int loc = track1<FULL>(p, h, pool, ap, G, first_turn && ie == ix_start);
     if (loc) {
       li.loc = loc;
       li.ele = ie;

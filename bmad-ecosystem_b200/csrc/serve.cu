@@ -384,6 +384,7 @@ void worker_main(bmadgpu_server* s) {
     int32_t n_var = 0;
     std::vector<int64_t> round_jobs;
     bool round_records = false;
+    int32_t round_rare = 0;
     for (int32_t slot = 0; slot < (int32_t)s->slot_job.size(); ++slot) {
       const int64_t id = s->slot_job[slot];
       BatchVar& hv = s->h_vars[buf][slot];
@@ -392,6 +393,7 @@ void worker_main(bmadgpu_server* s) {
       Job& j = s->jobs[id];
       n_var = slot + 1;
       hv = make_var(j);
+      if (j.lat->pk.info.rare) round_rare = 1;
       if (j.fma) set_rec(hv, j, s->d_rec);
       const int32_t left = j.n_turns - j.done_turns;
       if (left <= 0 || j.retiring || j.live == 0) continue;
@@ -448,6 +450,7 @@ void worker_main(bmadgpu_server* s) {
       a.queue = s->d_queue;
       a.err_flag = s->ctx->d_err;
       a.smem_bytes = s->smem;
+      a.rare = round_rare;
       Round rd;
       rd.index = r;
       rd.parity = parity;

@@ -106,6 +106,7 @@ struct TableInfo {
   uint32_t pool_doubles;
   uint32_t total_bytes;    // whole image, 16-aligned
   double turn_ref_time;    // sum of delta_ref_time over the elements
+  uint32_t rare;           // some element has an extra block or a pitched offset / bend frame
 };
 
 struct Globals {            // branch constants (lat_param_struct / bmad_com) and derived terms

@@ -57,7 +57,7 @@ __device__ void add_moments(const Particle& p, bool alive, double* __restrict__ 
   }
 }
 
-template <int BLOCK, int MINB>
+template <int BLOCK, int MINB, bool FULL>
 __global__ void __launch_bounds__(BLOCK, MINB) k_track(const TrackArgs a, int stage_smem) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_track(const TrackArgs a, int st
     LossInfo li;
     if (alive) refresh(p, G);
     for (int turn = 0; turn < a.n_turns; ++turn) {
-      if (alive) alive = track_turn(p, hdr, pool, ap, G, a.ix_start, a.ix_end, turn == 0, a.turn0 + turn, li);
+      if (alive) alive = track_turn<FULL>(p, hdr, pool, ap, G, a.ix_start, a.ix_end, turn == 0, a.turn0 + turn, li);
       if (a.moments) add_moments(p, alive, a.moments + (int64_t)turn * 28);
     }
     if (valid) store_particle(soa, j, p, alive, li, z_in, beta_in, a.n_turns, a.turn0, seg_ref, a.ref_prefix, a.ix_start);
@@ -188,16 +188,15 @@ cudaError_t upload_constants() {
 // thread follows: 65536 / (BLOCK * MINB), capped at 255).
 struct Variant {
   int block, minb;
-  const void* fn;
+  const void* fn;       // the kernel for every element form
+  const void* fn_lean;  // the kernel for tables without rare forms (TableInfo::rare = 0)
 };
+#define BG_VARIANT(B, M) {B, M, (const void*)k_track<B, M, true>, (const void*)k_track<B, M, false>}
 static const Variant kVariants[] = {
-    {64, 8, (const void*)k_track<64, 8>},    {64, 12, (const void*)k_track<64, 12>},
-    {128, 3, (const void*)k_track<128, 3>},  {128, 4, (const void*)k_track<128, 4>},
-    {128, 5, (const void*)k_track<128, 5>},
-    {128, 6, (const void*)k_track<128, 6>},  {256, 2, (const void*)k_track<256, 2>},
-    {256, 1, (const void*)k_track<256, 1>},  {256, 3, (const void*)k_track<256, 3>},
-    {512, 1, (const void*)k_track<512, 1>},
+    BG_VARIANT(64, 8),   BG_VARIANT(64, 12), BG_VARIANT(128, 3), BG_VARIANT(128, 4), BG_VARIANT(128, 5),
+    BG_VARIANT(128, 6),  BG_VARIANT(256, 2), BG_VARIANT(256, 1), BG_VARIANT(256, 3), BG_VARIANT(512, 1),
 };
+#undef BG_VARIANT
 
 cudaError_t launch_track(const TrackArgs& a, const LaunchCfg& cfg, int sm_count, cudaStream_t stream) {
   int stage = (cfg.stage_smem && table_fits_smem(a.table_bytes)) ? 1 : 0;
@@ -214,7 +213,7 @@ cudaError_t launch_track(const TrackArgs& a, const LaunchCfg& cfg, int sm_count,
     for (const Variant& k : kVariants)
       if (k.block == cfg.block && (!v || k.minb < v->minb)) v = &k;
   if (!v) return cudaErrorInvalidValue;
-  const void* fn = v->fn;
+  const void* fn = a.rare ? v->fn : v->fn_lean;
   int per_sm = 0;
   cudaError_t err;
   if (stage) {

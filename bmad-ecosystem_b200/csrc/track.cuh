@@ -27,6 +27,7 @@ struct TrackArgs {
   const double* ref_prefix;    // [n_ele + 1] sums of delta_ref_time
   Globals G;
   int32_t* err_flag;           // device: bit 0 = table staging wait timed out
+  int32_t rare;                // the table has extra blocks / pitched offsets: the full kernel
 };
 
 struct LaunchCfg {
