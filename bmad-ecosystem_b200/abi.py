@@ -19,6 +19,7 @@ STATUS_NAMES = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ETIMEDOUT
 # element keys (bmad_struct.f90:1696-1710)
 DRIFT, SBEND, QUADRUPOLE, SEXTUPOLE, RFCAVITY, MARKER = 1, 2, 3, 5, 9, 14
 OCTUPOLE, MULTIPOLE, AB_MULTIPOLE, MONITOR, INSTRUMENT, PIPE, THICK_MULTIPOLE = 17, 19, 22, 31, 32, 44, 67
+RCOLLIMATOR, ECOLLIMATOR = 35, 36
 # particle states (bmad_struct.f90:525-532)
 ALIVE, LOST, LOST_NEG_X, LOST_POS_X, LOST_NEG_Y, LOST_POS_Y, LOST_Z, LOST_PZ = 1, 2, 3, 4, 5, 6, 7, 8
 # locations (bmad_struct.f90:376-377)
@@ -53,7 +54,11 @@ class Element(C.Structure):
         + [(n, C.c_double) for n in _DOUBLE_FIELDS]
         + [("a_pole", C.c_double * N_POLE), ("b_pole", C.c_double * N_POLE),
            ("a_pole_elec", C.c_double * N_POLE), ("b_pole_elec", C.c_double * N_POLE),
-           ("fq1", C.c_double), ("fq2", C.c_double)]
+           ("fq1", C.c_double), ("fq2", C.c_double),
+           ("px_aperture_width2", C.c_double), ("px_aperture_center", C.c_double),
+           ("py_aperture_width2", C.c_double), ("py_aperture_center", C.c_double),
+           ("z_aperture_width2", C.c_double), ("z_aperture_center", C.c_double),
+           ("pz_aperture_width2", C.c_double), ("pz_aperture_center", C.c_double)]
     )
 
 
@@ -83,7 +88,7 @@ def default_element(key, **kw):
     e.fringe_type = FRINGE_BASIC_BEND if key == SBEND else FRINGE_NONE
     e.fringe_at = BOTH_ENDS
     e.aperture_at = EXIT_END
-    e.aperture_type = APERTURE_RECTANGULAR
+    e.aperture_type = APERTURE_ELLIPTICAL if key == ECOLLIMATOR else APERTURE_RECTANGULAR
     e.scale_multipoles = 1
     e.exact_multipoles = 1   # off$
     e.orientation = 1

@@ -206,8 +206,9 @@ template <bool FULL = true>
 BG_HD int track1(Particle& p, const EleHdr& h, const double* __restrict__ pool,
                                       const ApRec* __restrict__ ap, const Globals& G, bool entry_check) {
   if (entry_check && orbit_too_large(p, G)) return L_UPSTREAM;
+  const bool windows = FULL && (h.flags & F_AP_WINDOW);
   if (h.flags & F_AP_ENTRANCE) {
-    aperture(p, ap[h.ap_index], h.flags & F_AP_ELLIPTICAL);
+    aperture(p, ap[h.ap_index], h.flags & F_AP_ELLIPTICAL, windows);
     if (p.state != S_ALIVE) return L_UPSTREAM;
   }
   const double* b = pool + h.param;
@@ -224,7 +225,7 @@ BG_HD int track1(Particle& p, const EleHdr& h, const double* __restrict__ pool,
   if (orbit_too_large(p, G)) return L_UPSTREAM;
   if (p.state != S_ALIVE) return L_INSIDE;
   if (h.flags & F_AP_EXIT) {
-    aperture(p, ap[h.ap_index], h.flags & F_AP_ELLIPTICAL);
+    aperture(p, ap[h.ap_index], h.flags & F_AP_ELLIPTICAL, windows);
     if (p.state != S_ALIVE) return L_DOWNSTREAM;
   }
   return 0;

@@ -86,16 +86,18 @@ bool key_supported(int key) {
     case BMADGPU_DRIFT: case BMADGPU_SBEND: case BMADGPU_QUADRUPOLE: case BMADGPU_SEXTUPOLE:
     case BMADGPU_RFCAVITY: case BMADGPU_MARKER: case BMADGPU_OCTUPOLE: case BMADGPU_MULTIPOLE:
     case BMADGPU_AB_MULTIPOLE: case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE:
-    case BMADGPU_THICK_MULTIPOLE:
+    case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:
       return true;
   }
   return false;
 }
 
+// has_hkick_attributes (attribute_mod.f90:746-765, 1879) for the keys on the path
 bool key_has_hkick(int key) {
   switch (key) {
     case BMADGPU_QUADRUPOLE: case BMADGPU_SBEND: case BMADGPU_SEXTUPOLE: case BMADGPU_OCTUPOLE:
-    case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RFCAVITY:
+    case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RFCAVITY: case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT:
+    case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:
       return true;
   }
   return false;
@@ -236,6 +238,7 @@ void resolve_steps(const bmadgpu_element& e, const bmadgpu_param& p, double tilt
   if (ds_step == 0 && num_steps == 0) {
     switch (e.key) {
       case BMADGPU_DRIFT: case BMADGPU_PIPE: case BMADGPU_INSTRUMENT: case BMADGPU_MONITOR:
+      case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:
         num_steps = 1;
         ds_step = L;
         break;
@@ -555,7 +558,8 @@ struct Packer {
     return off;
   }
   uint16_t add_ap(const ApRec& r) {
-    std::vector<double> k = {r.x1_lim, r.x2_lim, r.y1_lim, r.y2_lim};
+    std::vector<double> k = {r.x1_lim, r.x2_lim, r.y1_lim, r.y2_lim, r.win_kind};
+    k.insert(k.end(), r.win, r.win + 8);
     auto it = ap_dedupe.find(k);
     if (it != ap_dedupe.end()) return it->second;
     uint16_t ix = (uint16_t)ap.size();
@@ -641,6 +645,11 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
         fail(BMADGPU_EUNSUPPORTED, "electric multipoles on this element type");
       if (e.key == BMADGPU_MULTIPOLE && any_nonzero(e.a_pole_elec, kNPole))
         fail(BMADGPU_EUNSUPPORTED, "multipole ksl");
+      // convert_this_ab has no scale for other keys (multipole_ele_to_ab.f90:534-580)
+      if (e.scale_multipoles && (any_nonzero(e.a_pole, kNPole) || any_nonzero(e.b_pole, kNPole)) &&
+          (e.key == BMADGPU_MONITOR || e.key == BMADGPU_INSTRUMENT || e.key == BMADGPU_RCOLLIMATOR ||
+           e.key == BMADGPU_ECOLLIMATOR || e.key == BMADGPU_DRIFT || e.key == BMADGPU_MARKER))
+        fail(BMADGPU_EUNSUPPORTED, "scaled multipoles on an element type without a reference strength");
       if (e.x_pitch != 0 || e.y_pitch != 0 || e.z_offset != 0)
         if (e.key == BMADGPU_MULTIPOLE || e.key == BMADGPU_AB_MULTIPOLE)
           fail(BMADGPU_EUNSUPPORTED, "pitch / z_offset misalignment of a thin multipole");
@@ -679,17 +688,54 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
 
       // aperture (check_aperture_limit.f90), offset_moves_aperture = F
       if (p.aperture_limit_on && e.aperture_at != BMADGPU_NO_END) {
-        ApRec r{-e.x1_limit, e.x2_limit, -e.y1_limit, e.y2_limit};
+        ApRec r;
+        std::memset(&r, 0, sizeof(r));
+        r.x1_lim = -e.x1_limit;
+        r.x2_lim = e.x2_limit;
+        r.y1_lim = -e.y1_limit;
+        r.y2_lim = e.y2_limit;
         bool any = (r.x1_lim != 0 || r.x2_lim != 0 || r.y1_lim != 0 || r.y2_lim != 0);
         if (e.aperture_type == BMADGPU_APERTURE_ELLIPTICAL) {
-          if (e.x1_limit != e.x2_limit || e.y1_limit != e.y2_limit || e.x1_limit == 0 || e.y1_limit == 0)
-            fail(BMADGPU_EUNSUPPORTED, "elliptical aperture with asymmetric or zero limits");
-          flags |= F_AP_ELLIPTICAL;
+          // elliptical_params_setup (check_aperture_limit.f90:361-387): limits set on one side
+          // only skip the check; otherwise half width (max_aperture_limit for none) and centre
+          auto setup = [&](double lim1, double lim2, double* w, double* c) {
+            if ((lim1 == 0 && lim2 != 0) || (lim1 != 0 && lim2 == 0)) return false;
+            *w = (lim2 - lim1) / 2;
+            *c = (lim2 + lim1) / 2;
+            if (*w == 0) *w = p.max_aperture_limit;
+            *w = std::max(*w, 0.0);
+            return true;
+          };
+          double xw, x0, yw, y0;
+          if (setup(r.x1_lim, r.x2_lim, &xw, &x0) && setup(r.y1_lim, r.y2_lim, &yw, &y0)) {
+            r.x1_lim = xw;
+            r.x2_lim = x0;
+            r.y1_lim = yw;
+            r.y2_lim = y0;
+            any = true;
+            flags |= F_AP_ELLIPTICAL;
+          } else {
+            any = false;
+          }
+        }
+        const bool coll = e.key == BMADGPU_ECOLLIMATOR || e.key == BMADGPU_RCOLLIMATOR;
+        if (coll) {
+          const double w[8] = {e.px_aperture_width2, e.px_aperture_center, e.py_aperture_width2,
+                                e.py_aperture_center, e.z_aperture_width2, e.z_aperture_center,
+                                e.pz_aperture_width2, e.pz_aperture_center};
+          if (w[0] != 0 || w[2] != 0 || w[4] != 0 || w[6] != 0) {
+            std::memcpy(r.win, w, sizeof(w));
+            r.win_kind = e.key == BMADGPU_ECOLLIMATOR ? 1 : 2;
+            flags |= F_AP_WINDOW;
+            any = true;
+          }
         }
         if (any) {
           h.ap_index = pk.add_ap(r);
           if (e.aperture_at == BMADGPU_ENTRANCE_END || e.aperture_at == BMADGPU_BOTH_ENDS) flags |= F_AP_ENTRANCE;
           if (e.aperture_at == BMADGPU_EXIT_END || e.aperture_at == BMADGPU_BOTH_ENDS) flags |= F_AP_EXIT;
+        } else {
+          flags &= (uint16_t)~(F_AP_ELLIPTICAL | F_AP_WINDOW);
         }
       }
 
@@ -753,14 +799,16 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           break;
         }
         case BMADGPU_SEXTUPOLE: case BMADGPU_OCTUPOLE: case BMADGPU_THICK_MULTIPOLE:
-        case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE: {  // track_a_thick_multipole.f90
+        case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE:
+        case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR: {  // track_a_thick_multipole.f90
           h.kind = K_THICK;
           mag_ab(e, tilt_tot, 0, a, b, &ix_mag_max);
           int n_step = (ix_mag_max == -1 && ix_elec_max == -1) ? 1 : std::max(nint(std::fabs(e.l / ds_step)), 1);
           double r_step = 1.0 / n_step;
           double step_len = e.l / n_step;
           blk = {step_len};
-          if (key != BMADGPU_MONITOR && key != BMADGPU_INSTRUMENT && key != BMADGPU_PIPE)
+          if (key != BMADGPU_MONITOR && key != BMADGPU_INSTRUMENT && key != BMADGPU_PIPE &&
+              key != BMADGPU_RCOLLIMATOR && key != BMADGPU_ECOLLIMATOR)
             eblk = extra_block(e, p, ae, be, ix_elec_max, 1 * step_len / 2, 1 * step_len);
           if (ix_mag_max > -1) {
             flags |= F_KICKS;
@@ -921,7 +969,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
     ti.turn_ref_time = turn_ref;
     ti.rare = 0;
     for (const EleHdr& h : pk.hdr)
-      if (h.flags & (F_EXTRA | F_PITCH)) ti.rare = 1;
+      if (h.flags & (F_EXTRA | F_PITCH | F_AP_WINDOW)) ti.rare = 1;
     out.image.assign(total, 0);
     std::memcpy(out.image.data(), pk.hdr.data(), ti.hdr_bytes);
     if (ti.ap_bytes) std::memcpy(out.image.data() + ti.hdr_bytes, pk.ap.data(), ti.ap_bytes);

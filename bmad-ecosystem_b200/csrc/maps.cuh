@@ -176,21 +176,65 @@ BG_HD bool orbit_too_large(Particle& p, const Globals& g) {
   return false;
 }
 
-// check_aperture_limit (rectangular / elliptical branch), check_aperture_limit.f90:256-324
-BG_HD void aperture(Particle& p, const ApRec& a, bool elliptical) {
+// check_this_limit (check_aperture_limit.f90:344-356) on one coordinate
+BG_HD void window_limit(Particle& p, double coord, double width2, double center, double& uf) {
+  if (width2 == 0) return;
+  if (coord > center - width2 && coord < center + width2) return;
+  p.state = S_LOST;
+  const double lo = (center - width2) - coord, hi = coord - (center + width2);
+  uf = (lo < hi) ? hi : lo;  // max(lo, hi)
+}
+
+// The collimators' momentum and longitudinal windows (check_aperture_limit.f90:113-151):
+// elliptical in (px, py) and (z, pz) for an ecollimator with both half widths set, else one
+// check_this_limit per coordinate. Returns the unstable factor they leave.
+BG_COLD double aperture_windows(Particle& p, const ApRec& a) {
+  double uf = 0;
+  const auto* w = a.win;
+  if (a.win_kind == 1) {
+    for (int k = 0; k < 2; k++) {
+      const double xw = w[4 * k], x0 = w[4 * k + 1], yw = w[4 * k + 2], y0 = w[4 * k + 3];
+      const double u = k == 0 ? p.px : p.z, v = k == 0 ? p.py : p.pz;
+      if (xw == 0 || yw == 0) {
+        window_limit(p, u, xw, x0, uf);
+        window_limit(p, v, yw, y0, uf);
+      } else {
+        const double r = ((u - x0) / xw) * ((u - x0) / xw) + ((v - y0) / yw) * ((v - y0) / yw);
+        if (r > 1) {
+          p.state = S_LOST;
+          uf = sqrt(r) - 1;
+        }
+      }
+    }
+  } else {
+    window_limit(p, p.px, w[0], w[1], uf);
+    window_limit(p, p.py, w[2], w[3], uf);
+    window_limit(p, p.z, w[4], w[5], uf);
+    window_limit(p, p.pz, w[6], w[7], uf);
+  }
+  return uf;
+}
+
+// check_aperture_limit (bmad/low_level/check_aperture_limit.f90:30-387), rectangular and
+// elliptical x/y limits (offset_moves_aperture = F), after the collimator windows when present.
+BG_HD void aperture(Particle& p, const ApRec& a, bool elliptical, bool windows = false) {
+  double uf = 0;
+  if (windows) uf = aperture_windows(p, a);
   double xp = p.x, yp = p.y;
-  if (elliptical) {
-    double rx = xp / a.x2_lim, ry = yp / a.y2_lim;
+  if (elliptical) {  // elliptical_params_setup packed: (x_width2, x0, y_width2, y0)
+    const double xw = a.x1_lim, yw = a.y1_lim;
+    xp = xp - a.x2_lim;
+    yp = yp - a.y2_lim;
+    double rx = xp / xw, ry = yp / yw;
     double r = rx * rx + ry * ry;
     if (r < 1) return;
-    if (fabs(xp / a.x2_lim) > fabs(yp / a.y2_lim)) p.state = (xp > 0) ? S_POS_X : S_NEG_X;
+    if (fabs(xp / xw) > fabs(yp / yw)) p.state = (xp > 0) ? S_POS_X : S_NEG_X;
     else p.state = (yp > 0) ? S_POS_Y : S_NEG_Y;
     return;
   }
   bool out = (a.x1_lim != 0 && xp < a.x1_lim) || (a.x2_lim != 0 && xp > a.x2_lim) ||
              (a.y1_lim != 0 && yp < a.y1_lim) || (a.y2_lim != 0 && yp > a.y2_lim);
   if (!out) return;
-  double uf = 0;
   if (a.x1_lim != 0 && xp < a.x1_lim) {
     double f = fabs((xp - a.x1_lim) / (a.x2_lim - a.x1_lim));
     if (f > uf) { p.state = S_NEG_X; uf = f; }

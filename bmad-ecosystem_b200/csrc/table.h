@@ -40,7 +40,8 @@ enum Flag : uint16_t {
   F_TILT = 1 << 11,        // misalign block carries a non-zero tilt rotation
   F_KICK_B_FROM2 = 1 << 12, // both kick arrays: every a_n zero and b_0 = b_1 = 0, at least 3 orders
   F_PITCH = 1 << 13,       // misalign block of the pitched form (straight elements) or the bend frame
-  F_EXTRA = 1 << 14        // extra block (EleHdr::extra): electric multipoles, higher-order edge fringes
+  F_EXTRA = 1 << 14,       // extra block (EleHdr::extra): electric multipoles, higher-order edge fringes
+  F_AP_WINDOW = 1 << 15    // the aperture record carries collimator phase-space windows
 };
 
 struct EleHdr {            // 16 bytes
@@ -53,8 +54,15 @@ struct EleHdr {            // 16 bytes
   uint32_t extra;          // offset (in doubles) of the extra block (F_EXTRA), else 0
 };
 
-struct ApRec {             // 32 bytes: rectangular/elliptical limits (x1_lim = -x1_limit, ...)
+struct ApRec {             // 112 bytes
+  // rectangular: the limits (x1_lim = -x1_limit, x2_lim = x2_limit, ...); elliptical: the
+  // half widths and centres of elliptical_params_setup (x1_lim = x_width2, x2_lim = x0,
+  // y1_lim = y_width2, y2_lim = y0)
   double x1_lim, x2_lim, y1_lim, y2_lim;
+  // collimator phase-space windows (F_AP_WINDOW): half width and centre in px, py, z, pz
+  double win[8];
+  double win_kind;         // 1 ecollimator (elliptical px-py and z-pz windows), 2 rcollimator
+  double pad;
 };
 
 // Parameter block layouts (indices in doubles from EleHdr::param).

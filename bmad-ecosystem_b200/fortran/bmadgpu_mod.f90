@@ -39,6 +39,8 @@ type, bind(c) :: bmadgpu_element_t
   real(c_double) :: a_pole(0:bmadgpu_n_pole-1), b_pole(0:bmadgpu_n_pole-1)
   real(c_double) :: a_pole_elec(0:bmadgpu_n_pole-1), b_pole_elec(0:bmadgpu_n_pole-1)
   real(c_double) :: fq1, fq2
+  real(c_double) :: px_aperture_width2, px_aperture_center, py_aperture_width2, py_aperture_center
+  real(c_double) :: z_aperture_width2, z_aperture_center, pz_aperture_width2, pz_aperture_center
 end type
 
 type, bind(c) :: bmadgpu_param_t
@@ -226,6 +228,14 @@ e%delta_ref_time = ele%value(delta_ref_time$)
 e%fq1 = 0;  e%fq2 = 0
 if (ele%key == quadrupole$) then
   e%fq1 = ele%value(fq1$);  e%fq2 = ele%value(fq2$)
+endif
+e%px_aperture_width2 = 0;  e%px_aperture_center = 0;  e%py_aperture_width2 = 0;  e%py_aperture_center = 0
+e%z_aperture_width2 = 0;  e%z_aperture_center = 0;  e%pz_aperture_width2 = 0;  e%pz_aperture_center = 0
+if (ele%key == ecollimator$ .or. ele%key == rcollimator$) then
+  e%px_aperture_width2 = ele%value(px_aperture_width2$);  e%px_aperture_center = ele%value(px_aperture_center$)
+  e%py_aperture_width2 = ele%value(py_aperture_width2$);  e%py_aperture_center = ele%value(py_aperture_center$)
+  e%z_aperture_width2 = ele%value(z_aperture_width2$);  e%z_aperture_center = ele%value(z_aperture_center$)
+  e%pz_aperture_width2 = ele%value(pz_aperture_width2$);  e%pz_aperture_center = ele%value(pz_aperture_center$)
 endif
 e%a_pole = 0;  e%b_pole = 0;  e%a_pole_elec = 0;  e%b_pole_elec = 0
 if (associated(ele%a_pole)) then

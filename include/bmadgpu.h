@@ -52,7 +52,7 @@ enum {
   BMADGPU_DRIFT = 1, BMADGPU_SBEND = 2, BMADGPU_QUADRUPOLE = 3, BMADGPU_SEXTUPOLE = 5,
   BMADGPU_RFCAVITY = 9, BMADGPU_MARKER = 14, BMADGPU_OCTUPOLE = 17, BMADGPU_MULTIPOLE = 19,
   BMADGPU_AB_MULTIPOLE = 22, BMADGPU_MONITOR = 31, BMADGPU_INSTRUMENT = 32, BMADGPU_PIPE = 44,
-  BMADGPU_THICK_MULTIPOLE = 67
+  BMADGPU_THICK_MULTIPOLE = 67, BMADGPU_RCOLLIMATOR = 35, BMADGPU_ECOLLIMATOR = 36
 };
 /* particle states, bmad_struct.f90:525-532 */
 enum {
@@ -107,6 +107,10 @@ typedef struct bmadgpu_element {
   double a_pole[BMADGPU_N_POLE], b_pole[BMADGPU_N_POLE];
   double a_pole_elec[BMADGPU_N_POLE], b_pole_elec[BMADGPU_N_POLE];
   double fq1, fq2;            /* quadrupole soft-edge fringe integrals (soft_quadrupole_edge_kick) */
+  /* collimator phase-space windows (check_aperture_limit.f90:115-151): half widths and centres in
+   * px, py, z, pz; a zero half width leaves that coordinate unchecked */
+  double px_aperture_width2, px_aperture_center, py_aperture_width2, py_aperture_center;
+  double z_aperture_width2, z_aperture_center, pz_aperture_width2, pz_aperture_center;
 } bmadgpu_element;
 
 /* Branch/global parameters: lat_param_struct + the bmad_common_struct switches on the path. */

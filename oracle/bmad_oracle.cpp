@@ -210,10 +210,12 @@ struct Ele {
   bool has_mag;    // associated(ele%a_pole)
 };
 
+// has_hkick_attributes (attribute_mod.f90:746-765, 1879) for the keys on the path
 bool key_has_hkick(int key) {
   switch (key) {
     case BMADGPU_QUADRUPOLE: case BMADGPU_SBEND: case BMADGPU_SEXTUPOLE: case BMADGPU_OCTUPOLE:
-    case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RFCAVITY:
+    case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RFCAVITY: case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT:
+    case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:
       return true;
   }
   return false;
@@ -959,17 +961,65 @@ bool at_this_ele_end(int now_at, int where_at) {
   return false;
 }
 
+// check_this_limit (check_aperture_limit.f90:344-356): a phase-space window centre +- width2
+void check_this_limit(Coord& orb, double coord, double width2, double center, double* unstable_factor) {
+  if (width2 == 0) return;
+  if (coord > center - width2 && coord < center + width2) return;
+  orb.state = BMADGPU_LOST;
+  *unstable_factor = std::max((center - width2) - coord, coord - (center + width2));
+}
+
+// elliptical_params_setup (check_aperture_limit.f90:361-387); false on limits set on one side only
+bool elliptical_params_setup(double lim1, double lim2, double* pos, double* width2, double* center,
+                             const bmadgpu_param* p) {
+  if ((lim1 == 0 && lim2 != 0) || (lim1 != 0 && lim2 == 0)) return false;
+  *width2 = (lim2 - lim1) / 2;
+  *center = (lim2 + lim1) / 2;
+  *pos = *pos - *center;
+  if (*width2 == 0) *width2 = p->max_aperture_limit;
+  *width2 = std::max(*width2, 0.0);
+  return true;
+}
+
 // check_aperture_limit, bmad/low_level/check_aperture_limit.f90:30-387 (rectangular and
-// elliptical apertures, offset_moves_aperture = F, no wall_transition).
-int check_aperture_limit(Coord& orb, const Ele& ele, int particle_at) {
+// elliptical apertures with the collimators' phase-space windows, offset_moves_aperture = F, no
+// wall_transition). unstable: param%unstable_factor on return (may be null).
+int check_aperture_limit(Coord& orb, const Ele& ele, int particle_at, double* unstable = nullptr) {
   const bmadgpu_element* e = ele.e;
+  double unstable_factor = 0;
+  if (unstable) *unstable = 0;
   if (orbit_too_large(orb, ele.p)) return 0;
   if (!ele.p->aperture_limit_on) return 0;
   int physical_end = (particle_at == first_track_edge) ? BMADGPU_ENTRANCE_END : BMADGPU_EXIT_END;
   if (!at_this_ele_end(physical_end, e->aperture_at)) return 0;
+  // momentum and longitudinal windows, :113-151
+  if (e->key == BMADGPU_ECOLLIMATOR) {
+    const double pairs[2][4] = {{e->px_aperture_width2, e->py_aperture_width2, e->px_aperture_center,
+                                 e->py_aperture_center},
+                                {e->z_aperture_width2, e->pz_aperture_width2, e->z_aperture_center,
+                                 e->pz_aperture_center}};
+    for (int k = 0; k < 2; k++) {
+      const double xw = pairs[k][0], yw = pairs[k][1], x0 = pairs[k][2], y0 = pairs[k][3];
+      const double u = orb.vec[k == 0 ? 1 : 4], v = orb.vec[k == 0 ? 3 : 5];
+      if (xw == 0 || yw == 0) {
+        check_this_limit(orb, u, xw, x0, &unstable_factor);
+        check_this_limit(orb, v, yw, y0, &unstable_factor);
+      } else {
+        const double r = ((u - x0) / xw) * ((u - x0) / xw) + ((v - y0) / yw) * ((v - y0) / yw);
+        if (r > 1) {
+          orb.state = BMADGPU_LOST;
+          unstable_factor = std::sqrt(r) - 1;
+        }
+      }
+    }
+  } else if (e->key == BMADGPU_RCOLLIMATOR) {
+    check_this_limit(orb, orb.vec[1], e->px_aperture_width2, e->px_aperture_center, &unstable_factor);
+    check_this_limit(orb, orb.vec[3], e->py_aperture_width2, e->py_aperture_center, &unstable_factor);
+    check_this_limit(orb, orb.vec[4], e->z_aperture_width2, e->z_aperture_center, &unstable_factor);
+    check_this_limit(orb, orb.vec[5], e->pz_aperture_width2, e->pz_aperture_center, &unstable_factor);
+  }
   double x_particle = orb.vec[0], y_particle = orb.vec[2];
   double x1_lim = -e->x1_limit, x2_lim = e->x2_limit, y1_lim = -e->y1_limit, y2_lim = e->y2_limit;
-  double unstable_factor = 0;
   if (e->aperture_type == BMADGPU_APERTURE_RECTANGULAR || e->aperture_type == BMADGPU_APERTURE_AUTO) {
     if (x1_lim != 0 && x_particle < x1_lim) {
       double f = std::fabs((x_particle - x1_lim) / (x2_lim - x1_lim));
@@ -987,21 +1037,26 @@ int check_aperture_limit(Coord& orb, const Ele& ele, int particle_at) {
       double f = std::fabs((y_particle - y2_lim) / (y2_lim - y1_lim));
       if (f > unstable_factor) { orb.state = BMADGPU_LOST_POS_Y; unstable_factor = f; }
     }
+    if (unstable) *unstable = unstable_factor;
     return 0;
   }
   if (e->aperture_type == BMADGPU_APERTURE_ELLIPTICAL) {
-    // elliptical_params_setup: symmetric limits only (x1 = x2, y1 = y2)
-    if (e->x1_limit != e->x2_limit || e->y1_limit != e->y2_limit || e->x1_limit == 0 || e->y1_limit == 0)
-      return BMADGPU_EUNSUPPORTED;
-    double x_width2 = e->x2_limit, y_width2 = e->y2_limit;
-    double rx = x_particle / x_width2, ry = y_particle / y_width2;
-    double r = rx * rx + ry * ry;
-    if (r < 1) return 0;
+    double x_width2, x0, y_width2, y0;
+    if (!elliptical_params_setup(x1_lim, x2_lim, &x_particle, &x_width2, &x0, ele.p)) return 0;
+    if (!elliptical_params_setup(y1_lim, y2_lim, &y_particle, &y_width2, &y0, ele.p)) return 0;
+    const double rx = x_particle / x_width2, ry = y_particle / y_width2;
+    const double r = rx * rx + ry * ry;
+    if (r < 1) {
+      if (unstable) *unstable = unstable_factor;
+      return 0;
+    }
     if (std::fabs(x_particle / x_width2) > std::fabs(y_particle / y_width2)) {
       orb.state = (x_particle > 0) ? BMADGPU_LOST_POS_X : BMADGPU_LOST_NEG_X;
     } else {
       orb.state = (y_particle > 0) ? BMADGPU_LOST_POS_Y : BMADGPU_LOST_NEG_Y;
     }
+    unstable_factor = std::sqrt(r) - 1;
+    if (unstable) *unstable = unstable_factor;
     return 0;
   }
   return BMADGPU_EUNSUPPORTED;
@@ -1929,6 +1984,7 @@ int track1_bmad(Coord& orbit, const Ele& ele) {
     case -1: break;
     case BMADGPU_DRIFT: track_a_drift(orbit, e->l * 1, ele.p); break;
     case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE:
+    case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:  // track1_bmad.f90:87-88
     case BMADGPU_OCTUPOLE: case BMADGPU_THICK_MULTIPOLE: case BMADGPU_SEXTUPOLE:
       err = track_a_thick_multipole(orbit, ele);
       break;
@@ -2001,6 +2057,7 @@ int make_ele(const bmadgpu_element* e, const bmadgpu_param* p, int ix_ele, Ele& 
   if (ds_step == 0 && num_steps == 0) {
     switch (e->key) {
       case BMADGPU_DRIFT: case BMADGPU_PIPE: case BMADGPU_INSTRUMENT: case BMADGPU_MONITOR:
+      case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:
         num_steps = 1;
         ds_step = L;
         break;
@@ -2161,6 +2218,18 @@ int oracle_hwang_bend_edge_kick(const bmadgpu_element* e, const bmadgpu_param* p
   hwang_bend_edge_kick(ele, particle_at, o, mat6);
   to_external(o, c);
   return 0;
+}
+
+int oracle_check_aperture(const bmadgpu_element* e, const bmadgpu_param* p, int32_t particle_at, oracle_coord* c,
+                          double* unstable_factor) {
+  Ele ele;
+  int err = make_ele(e, p, 0, ele);
+  if (err) return err;
+  Coord o;
+  to_internal(c, o);
+  err = check_aperture_limit(o, ele, particle_at, unstable_factor);
+  to_external(o, c);
+  return err;
 }
 
 void oracle_set_libm(double (*f_sin)(double), double (*f_cos)(double), double (*f_asin)(double),

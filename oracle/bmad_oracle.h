@@ -59,6 +59,12 @@ int oracle_track1(oracle_coord* orb, const bmadgpu_element* ele, int32_t ix_ele,
 /* hwang_bend_edge_kick (fringe_mod.f90:241-419) with make_matrix = T.
  * particle_at: 11 = first_track_edge$, 12 = second_track_edge$. mat6 is 6x6 row-major
  * (mat6[i*6+j] = Fortran mat6(i+1, j+1)), premultiplied by the edge matrix. */
+/* check_aperture_limit (bmad/low_level/check_aperture_limit.f90:30-387) of one element at
+ * particle_at (11 first_track_edge, 12 second_track_edge) on the coordinate c: its state after the
+ * check and param%unstable_factor. */
+int oracle_check_aperture(const bmadgpu_element* ele, const bmadgpu_param* param, int32_t particle_at,
+                          oracle_coord* c, double* unstable_factor);
+
 int oracle_hwang_bend_edge_kick(const bmadgpu_element* ele, const bmadgpu_param* param,
                                 int32_t particle_at, oracle_coord* orb, double* mat6);
 

@@ -9,6 +9,8 @@ Sources (paths inside bmad-sim/bmad-ecosystem):
   regression_tests/fringe_test/fringe_test.bmad, output.correct     hwang_bend_edge_kick goldens
   regression_tests/mat6_calc_method_test/mat6_calc_method_test.bmad, output.correct
                                                                     transfer matrices by tracking
+  regression_tests/aperture_test/aperture_test.bmad, .f90, output.correct
+                                                                    collimator aperture states
 
 Element attributes are transcribed below from the .bmad lines cited beside each entry; Bmad's
 parser defaults are applied explicitly (tilt flag -> pi/4 quad, pi/6 sextupole, pi/8 octupole,
@@ -38,6 +40,10 @@ TM_ELEMENTS = {
     # name: (key, attributes, source line in tracking_method_test.bmad)
     "DRIFT1": ("DRIFT", dict(l=4.5, num_steps=10, x_offset=0.05, y_pitch=0.001, tilt=0.1), 27),
     "INSTRUMENT1": ("INSTRUMENT", dict(l=4.5, num_steps=10), 41),
+    "ECOLLIMATOR1": ("ECOLLIMATOR", dict(l=4.5, x1_limit=0.2, x2_limit=0.2, y1_limit=0.1, y2_limit=0.1, num_steps=10,
+                                         x_offset=0.02, y_pitch=0.001, tilt=0.1, hkick=0.01, vkick=0.002), 29),
+    "RCOLLIMATOR1": ("RCOLLIMATOR", dict(l=4.5, x1_limit=0.2, x2_limit=0.2, y1_limit=0.1, y2_limit=0.1, num_steps=10,
+                                         x_offset=0.02, y_pitch=0.001, tilt=0.1), 68),
     "MONITOR1": ("MONITOR", dict(l=4.5, num_steps=10), 55),
     "MULTIPOLE1": ("MULTIPOLE", dict(a_pole={1: 1.0, 3: 4.5}, b_pole={1: PI / (2 * 1 + 2), 3: 0.31 * PI},
                                      x_offset=0.05), 56),
@@ -80,6 +86,10 @@ M6_ELEMENTS = {
     "AB_MULTIPOLE1": ("AB_MULTIPOLE", dict(a_pole={2: 1e3}, b_pole={2: 1e3}, x_offset=0.02, tilt=0.1), 19),
     "DRIFT1": ("DRIFT", dict(l=4.5, tilt=0.1, **_m_mis), 23),
     "INSTRUMENT1": ("INSTRUMENT", dict(l=4.5, num_steps=10), 34),
+    "ECOLLIMATOR1": ("ECOLLIMATOR", dict(l=4.5, x1_limit=0.2, x2_limit=0.2, y1_limit=0.1, y2_limit=0.1, num_steps=10,
+                                         x_offset=0.02, y_pitch=0.001, tilt=0.1, hkick=0.01, vkick=0.002), 25),
+    "RCOLLIMATOR1": ("RCOLLIMATOR", dict(l=4.5, x1_limit=0.2, x2_limit=0.2, y1_limit=0.1, y2_limit=0.1, num_steps=10,
+                                         x_offset=0.02, y_pitch=0.001, tilt=0.1), 71),
     "MONITOR1": ("MONITOR", dict(l=4.5, num_steps=10), 56),
     "MULTIPOLE1": ("MULTIPOLE", dict(a_pole={1: 1.0, 3: 4.5}, b_pole={1: PI / (2 * 1 + 2), 3: 0.31 * PI},
                                      x_offset=0.05), 57),
@@ -100,6 +110,44 @@ M6_ELEMENTS = {
     "THICK_MULTIPOLE1": ("THICK_MULTIPOLE", dict(l=4.5, a_pole={2: 1.0}, b_pole={2: 20.0}, x_offset=0.02, tilt=0.1),
                          124),
 }
+
+# aperture_test.bmad:23-35 (ec, rc) and check_this_aperture (aperture_test.f90:116-220), which
+# calls check_aperture_limit at second_track_edge on 9-point grids around each window's edges
+# and prints the states (S lines) and param%unstable_factor (U lines, 3 digits). The driver's
+# grid constants (xw2 = 0.01, x0, eps = 1e-5, ...) are default-kind REAL literals, i.e. single
+# precision widened to double; that rounding shows in the printed unstable factors (9.98E-06 in
+# RC_U_zPz+), so the grid is built here with the same float32 values.
+_win = dict(px_aperture_width2=0.01, px_aperture_center=0.01, py_aperture_width2=0.015, z_aperture_width2=0.2,
+            z_aperture_center=-0.6, pz_aperture_width2=0.03, pz_aperture_center=0.02, x1_limit=1e-10,
+            x2_limit=0.02, y1_limit=0.015, y2_limit=0.015)
+AP_ELEMENTS = {"EC": ("ECOLLIMATOR", _win, 23), "RC": ("RCOLLIMATOR", _win, 30)}
+
+
+def aperture_grids():
+    """The six grids of check_this_aperture: name -> 9 phase-space vectors (i outer, j inner)."""
+    import numpy as np
+    f = lambda v: float(np.float32(v))
+    out = {}
+    for sign, tag in ((-1, "-"), (1, "+")):
+        xw2, x0, yw2, y0, eps = f(0.01), f(0.01), f(0.015), 0.0, f(1e-5)
+        g = []
+        for i in (-1, 0, 1):
+            for j in (-1, 0, 1):
+                g.append([0.0, x0 + i * (xw2 + sign * eps), 0.0, y0 + j * (yw2 + sign * eps), -0.6, 0.02])
+        out["Pxy" + tag] = g
+        g = []
+        for i in (-1, 0, 1):
+            for j in (-1, 0, 1):
+                g.append([x0 + i * (xw2 + sign * eps), 0.1 if sign < 0 else 0.0, y0 + j * (yw2 + sign * eps), 0.0,
+                          -0.6, 0.02])
+        out["xy" + tag] = g
+        xw2, x0, yw2, y0 = f(0.2), f(-0.6), f(0.03), f(0.02)
+        g = []
+        for i in (-1, 0, 1):
+            for j in (-1, 0, 1):
+                g.append([0.0, 0.01, 0.0, 0.0, x0 + i * (xw2 + sign * eps), y0 + j * (yw2 + sign * eps)])
+        out["zPz" + tag] = g
+    return out
 
 # fringe_test.bmad: e_tot 1e6 electrons, particle_start, b: sbend ...
 FR_START = [0.01, 0.02, 0.03, 0.04, 0.00, 0.5]
@@ -137,6 +185,18 @@ def main():
                            expected_mat6=[r["values"] for r in rows], expected_vec0=vec0["values"]))
     json.dump(dict(source="regression_tests/mat6_calc_method_test", e_tot=1e6, charge=1.0, start=TM_START, d_orb=1e-5,
                    cases=mcases), open(os.path.join(HERE, "mat6_calc_method_tracking.json"), "w"), indent=1)
+
+    ap = parse_output_correct(os.path.join(REF, "regression_tests/aperture_test/output.correct"))
+    grids = aperture_grids()
+    acases = []
+    for name, (key, attrs, src_line) in AP_ELEMENTS.items():
+        for g, vecs in grids.items():
+            st, un = ap["%s_S_%s" % (name, g)], ap["%s_U_%s" % (name, g)]
+            acases.append(dict(name="%s_%s" % (name, g), key=key, attrs=attrs, bmad_line=src_line,
+                               output_line=st["line"], vecs=vecs, expected_state=[int(v) for v in st["values"]],
+                               expected_unstable=un["values"], tol=un["tol"]))
+    json.dump(dict(source="regression_tests/aperture_test", particle_at="second_track_edge", cases=acases),
+              open(os.path.join(HERE, "aperture_test_collimators.json"), "w"), indent=1)
 
     fr = parse_output_correct(os.path.join(REF, "regression_tests/fringe_test/output.correct"))
     fcases = []

@@ -121,3 +121,18 @@ def test_edge_fringes_are_accepted():
     lib.lattice_check([abi.default_element(abi.SBEND, l=1.0, g=0.01, e1=0.1, fint=0.5, hgap=0.02,
                                            fringe_type=abi.FRINGE_FULL)], p)
 
+
+
+def test_collimators_and_kicked_monitors_are_accepted():
+    """ecollimator / rcollimator (track_a_thick_multipole with phase-space windows) and monitors or
+    instruments with hkick/vkick (has_hkick_attributes) are on the device path; scaled multipoles
+    on an element without a reference strength are refused (convert_this_ab has no scale)."""
+    abi = load_abi()
+    p = abi.electron_param(3e9)
+    lib.lattice_check([abi.default_element(abi.ECOLLIMATOR, l=0.5, x1_limit=1e-3, x2_limit=0.02, y1_limit=0.01,
+                                           y2_limit=0.01, px_aperture_width2=1e-3, hkick=1e-5)], p)
+    lib.lattice_check([abi.default_element(abi.RCOLLIMATOR, l=0.5, pz_aperture_width2=1e-3)], p)
+    lib.lattice_check([abi.default_element(abi.MONITOR, l=0.2, hkick=1e-5, vkick=2e-5)], p)
+    with pytest.raises(lib.BmadGpuError) as ei:
+        lib.lattice_check([abi.default_element(abi.MONITOR, l=0.2, b_pole={2: 1e-3})], p)
+    assert ei.value.code == abi.EUNSUPPORTED

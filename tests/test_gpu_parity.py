@@ -123,6 +123,21 @@ def test_mat6_by_tracking_on_gpu(ctx, case, data):
     assert np.all(np.abs(vec0 - want0) <= case["tol_vec0"] + 5e-14 * np.abs(want0)), (case["name"], vec0 - want0)
 
 
+def _ap_cases():
+    return json.load(open(os.path.join(ROOT, "tests", "golden", "aperture_test_collimators.json")))["cases"]
+
+
+@pytest.mark.parametrize("case", _ap_cases(), ids=lambda c: c["name"])
+def test_aperture_test_collimators_on_gpu(ctx, case):
+    """The reference's zero-length ecollimator / rcollimator (aperture checked at the exit) tracked on
+    the GPU from each aperture_test grid point: the loss states of its S lines."""
+    p = abi.electron_param(3.1e9, charge=1.0)
+    e = abi.default_element(getattr(abi, case["key"]), **case["attrs"])
+    vec = np.array(case["vecs"], dtype=np.float64).T.copy()
+    g = gpu_track(ctx, [e], p, vec, 1)
+    assert list(g["state"]) == case["expected_state"], (case["name"], list(g["state"]))
+
+
 # ---- single elements of every kind against the oracle -----------------------------------------
 
 def _single_element_cases():
@@ -176,6 +191,15 @@ def _single_element_cases():
         "sbend5_like": [E(abi.SBEND, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, fringe_type=abi.FRINGE_FULL,
                           x_offset=0.002, y_pitch=0.001, ref_tilt=0.1, fint=0.7, hgap=2.0,
                           a_pole={0: 0.001, 1: 10.0, 3: 100.0}, b_pole_elec={0: -2e5}, a_pole_elec={1: 2e6}, **ap)],
+        "ecollimator_windows": [E(abi.ECOLLIMATOR, l=0.5, x1_limit=1e-3, x2_limit=0.02, y1_limit=0.01, y2_limit=0.008,
+                                  px_aperture_width2=4e-4, px_aperture_center=1e-5, py_aperture_width2=3e-4,
+                                  pz_aperture_width2=2e-3, hkick=1e-5, x_offset=1e-4, tilt=0.05)],
+        "rcollimator_windows": [E(abi.RCOLLIMATOR, l=0.5, x1_limit=0.02, x2_limit=0.02, y1_limit=0.01, y2_limit=0.01,
+                                  px_aperture_width2=3e-4, py_aperture_width2=2e-4, py_aperture_center=-1e-5,
+                                  z_aperture_width2=5e-3, pz_aperture_width2=1.5e-3, vkick=-1e-5)],
+        "monitor_kicks": [E(abi.MONITOR, l=0.2, hkick=2e-5, vkick=-1e-5, x_offset=1e-4, **ap)],
+        "elliptical_asymmetric": [E(abi.DRIFT, l=1.0, aperture_type=abi.APERTURE_ELLIPTICAL, x1_limit=0.004, x2_limit=0.006,
+                                    y1_limit=0.002, y2_limit=0.003)],
         "sbend7_like": [E(abi.SBEND, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, x_offset=0.002, y_pitch=0.001,
                           ref_tilt=0.1, a_pole={0: 0.01, 1: 0.1}, vkick=-1e-4, b_pole_elec={0: -2e5},
                           a_pole_elec={1: 2e6}, r0_mag=2.0, r0_elec=3.0, **ap)],

@@ -86,6 +86,18 @@ CASES = {
     "sbend_g0_offsets": lambda E, ap: [E(abi.SBEND, l=0.6, k1=0.2, x_offset=1e-3, y_pitch=1e-3, z_offset=-0.02, **ap)],
     "sbend_g0_ref_tilt": lambda E, ap: [E(abi.SBEND, l=0.6, k1=0.3, k2=3.0, ref_tilt=0.1, x_offset=2e-3,
                                           y_pitch=1e-3, num_steps=10, **ap)],
+    # collimators: phase-space windows before the x/y limits, asymmetric elliptical limits
+    "ecollimator_windows": lambda E, ap: [E(abi.ECOLLIMATOR, l=0.5, x1_limit=1e-3, x2_limit=0.02, y1_limit=0.01,
+                                            y2_limit=0.008, px_aperture_width2=4e-4, px_aperture_center=1e-5,
+                                            py_aperture_width2=3e-4, pz_aperture_width2=2e-3, hkick=1e-5,
+                                            x_offset=1e-4, tilt=0.05)],
+    "rcollimator_windows": lambda E, ap: [E(abi.RCOLLIMATOR, l=0.5, x1_limit=0.02, x2_limit=0.02, y1_limit=0.01,
+                                            y2_limit=0.01, px_aperture_width2=3e-4, py_aperture_width2=2e-4,
+                                            py_aperture_center=-1e-5, z_aperture_width2=5e-3, pz_aperture_width2=1.5e-3,
+                                            vkick=-1e-5)],
+    "monitor_kicks": lambda E, ap: [E(abi.MONITOR, l=0.2, hkick=2e-5, vkick=-1e-5, x_offset=1e-4, **ap)],
+    "elliptical_asymmetric": lambda E, ap: [E(abi.DRIFT, l=1.0, aperture_type=abi.APERTURE_ELLIPTICAL, x1_limit=0.004,
+                                              x2_limit=0.006, y1_limit=0.002, y2_limit=0.003)],
     # higher-order edge fringes: hard-edge multipole, soft quadrupole edge, exact bend edge
     "quad_fringe_full": lambda E, ap: [E(abi.QUADRUPOLE, l=0.4, k1=0.8, fringe_type=abi.FRINGE_FULL, fq1=0.02, fq2=-0.01,
                                          tilt=0.3, **ap)],

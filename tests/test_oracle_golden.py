@@ -128,3 +128,30 @@ def test_mat6_by_tracking(case):
     assert bad.size == 0, (case["name"], [(tuple(ij), mat[tuple(ij)], want[tuple(ij)]) for ij in bad[:4]])
     want0 = np.asarray(case["expected_vec0"])
     assert np.all(np.abs(vec0 - want0) <= case["tol_vec0"] + 5e-14 * np.abs(want0)), (case["name"], vec0, want0)
+
+
+# ---- collimator apertures (aperture_test) --------------------------------------------------------
+
+def _ap_cases():
+    return json.load(open(os.path.join(HERE, "golden", "aperture_test_collimators.json")))["cases"]
+
+
+def _printed3(x):
+    import math
+    return 0.0 if x == 0 else 0.5 * 10.0 ** (math.floor(math.log10(abs(x))) - 2)
+
+
+@pytest.mark.parametrize("case", _ap_cases(), ids=lambda c: c["name"])
+def test_aperture_test_collimators(case):
+    """check_aperture_limit at the exit of the reference's ecollimator / rcollimator on each 9-point
+    grid: the states (S lines) exactly, param%unstable_factor (U lines, printed with 3 digits)."""
+    abi, lib = load_abi(), load_oracle()
+    p = abi.electron_param(3.1e9, charge=1.0)
+    ele = abi.default_element(getattr(abi, case["key"]), **case["attrs"])
+    for v, want_state, want_u in zip(case["vecs"], case["expected_state"], case["expected_unstable"]):
+        c = OracleCoord()
+        lib.oracle_init_coord(ctypes.byref(c), (ctypes.c_double * 6)(*v), ctypes.byref(p))
+        u = ctypes.c_double()
+        assert lib.oracle_check_aperture(ctypes.byref(ele), ctypes.byref(p), 12, ctypes.byref(c), ctypes.byref(u)) == 0
+        assert c.state == want_state, (case["name"], v, c.state, want_state)
+        assert abs(u.value - want_u) <= case["tol"] + _printed3(want_u), (case["name"], v, u.value, want_u)
