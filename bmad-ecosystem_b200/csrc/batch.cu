@@ -144,6 +144,16 @@ cudaError_t batch_resolve(const BatchLaunch& cfg, uint32_t smem_bytes, int sm_co
   if (per_sm_lean < 1) per_sm_lean = 1;
   out->fn_lean = v->fn_lean;
   out->grid_lean = sm_count * per_sm_lean;
+  const void* fn_rec_lean = batch_rec_kernel(v->block, v->minb, false);
+  if (!fn_rec_lean) return cudaErrorInvalidValue;
+  err = cudaFuncSetAttribute(fn_rec_lean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  if (err != cudaSuccess) return err;
+  int per_sm_rec_lean = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_rec_lean, fn_rec_lean, cfg.block, smem_bytes);
+  if (err != cudaSuccess) return err;
+  if (per_sm_rec_lean < 1) per_sm_rec_lean = 1;
+  out->fn_rec_lean = fn_rec_lean;
+  out->grid_rec_lean = sm_count * per_sm_rec_lean;
   out->fn = v->fn;
   out->fn_rec = fn_rec;
   out->grid_rec = sm_count * per_sm_rec;
@@ -157,6 +167,9 @@ cudaError_t batch_resolve(const BatchLaunch& cfg, uint32_t smem_bytes, int sm_co
 cudaError_t batch_launch_track(const BatchKernel& k, const BatchArgs& a, cudaStream_t stream, bool record) {
   int ppt = k.ppt;
   void* args[] = {(void*)&a, (void*)&ppt};
+  if (record && !a.rare)
+    return cudaLaunchKernel(k.fn_rec_lean, dim3((unsigned)k.grid_rec_lean), dim3((unsigned)k.block), args, k.smem,
+                            stream);
   if (record)
     return cudaLaunchKernel(k.fn_rec, dim3((unsigned)k.grid_rec), dim3((unsigned)k.block), args, k.smem, stream);
   if (!a.rare)

@@ -67,11 +67,14 @@ struct BatchKernel {
   int grid_rec = 0;
   const void* fn_lean = nullptr; // the same shape for tables without rare forms (TableInfo::rare)
   int grid_lean = 0;
+  const void* fn_rec_lean = nullptr;
+  int grid_rec_lean = 0;
 };
 
 cudaError_t batch_upload_constants();
 cudaError_t batch_rec_upload_constants();            // batch_rec.cu's copy of the tables
-const void* batch_rec_kernel(int block, int minb);  // record-path instantiation of a shape
+// record-path instantiation of a shape (full: every element form; else the lean one)
+const void* batch_rec_kernel(int block, int minb, bool full = true);
 cudaError_t batch_resolve(const BatchLaunch& cfg, uint32_t smem_bytes, int sm_count, BatchKernel* out);
 // record: use the instantiation with the frequency-map record path (rounds with an FMA job).
 cudaError_t batch_launch_track(const BatchKernel& k, const BatchArgs& a, cudaStream_t stream, bool record = false);

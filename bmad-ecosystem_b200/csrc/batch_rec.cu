@@ -8,12 +8,13 @@
 
 namespace bmadgpu {
 
-const void* batch_rec_kernel(int block, int minb) {
+const void* batch_rec_kernel(int block, int minb, bool full) {
   struct Entry {
     int block, minb;
     const void* fn;
+    const void* fn_lean;
   };
-#define BG_BATCH_REC(B, M) {B, M, (const void*)k_batch_track<B, M, true>}
+#define BG_BATCH_REC(B, M) {B, M, (const void*)k_batch_track<B, M, true, true>, (const void*)k_batch_track<B, M, true, false>}
   static const Entry kRec[] = {
       BG_BATCH_REC(64, 8),  BG_BATCH_REC(64, 12), BG_BATCH_REC(128, 3), BG_BATCH_REC(128, 4),
       BG_BATCH_REC(128, 5), BG_BATCH_REC(128, 6), BG_BATCH_REC(256, 1), BG_BATCH_REC(256, 2),
@@ -21,7 +22,7 @@ const void* batch_rec_kernel(int block, int minb) {
   };
 #undef BG_BATCH_REC
   for (const Entry& e : kRec)
-    if (e.block == block && e.minb == minb) return e.fn;
+    if (e.block == block && e.minb == minb) return full ? e.fn : e.fn_lean;
   return nullptr;
 }
 
