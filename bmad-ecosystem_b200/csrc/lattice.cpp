@@ -370,11 +370,11 @@ void matmul3(const Mat3 a, const Mat3 b, Mat3 out) {
   std::memcpy(out, t, sizeof(t));
 }
 
-// floor_angles_to_w_mat (bmad/geometry/floor_angles_to_w_mat.f90) with psi = 0, or its inverse
-void w_mat_angles(double theta, double phi, bool inverse, Mat3 w) {
+// floor_angles_to_w_mat (bmad/geometry/floor_angles_to_w_mat.f90), or its inverse
+void w_mat_angles(double theta, double phi, bool inverse, Mat3 w, double psi = 0.0) {
   const double s_the = l_sin(theta), c_the = l_cos(theta);
   const double s_phi = l_sin(phi), c_phi = l_cos(phi);
-  const double s_psi = l_sin(0.0), c_psi = l_cos(0.0);
+  const double s_psi = l_sin(psi), c_psi = l_cos(psi);
   const double m[9] = {c_the * c_psi - s_the * s_phi * s_psi, -c_the * s_psi - s_the * s_phi * c_psi,
                        s_the * c_phi, c_phi * s_psi, c_phi * c_psi, s_phi,
                        -s_the * c_psi - c_the * s_phi * s_psi, s_the * s_psi - c_the * s_phi * c_psi,
@@ -475,18 +475,30 @@ struct FrameEnd {
   }
 };
 
-// The bend frame block of a bend with offsets, pitches or z_offset (no roll). With g != 0 or a
-// ref_tilt, the bend_shift geometry; otherwise the straight transform of offset_particle
-// (offset_particle.f90:239-245, 279-282, 437-443, 477-480), written as the same kind of steps.
+// The bend frame block of a bend with offsets, pitches, z_offset or roll. With g != 0, a ref_tilt
+// or a roll, the bend_shift geometry, with the misalignment of ele_misalignment_L_S_calc
+// (bmad/geometry/ele_misalignment_L_S_calc.f90:16-50: the offsets moved by the roll about the
+// chord, the rotation floor_angles_to_w_mat(x_pitch, y_pitch, roll)); otherwise the straight
+// transform of offset_particle (offset_particle.f90:239-245, 279-282, 437-443, 477-480), written
+// as the same kind of steps.
 std::vector<double> bend_frame_block(const bmadgpu_element& e) {
-  const double length = e.l, L_half = 0.5 * length, g = e.g, rt = e.ref_tilt;
-  const double L_mis[3] = {e.x_offset, e.y_offset, e.z_offset};
+  const double length = e.l, L_half = 0.5 * length, g = e.g, rt = e.ref_tilt, roll = e.roll;
+  double L_mis[3] = {e.x_offset, e.y_offset, e.z_offset};
   const double ds_set = L_half - 0.0, ds_unset = L_half - length;
   FrameEnd in, out;
-  if (g != 0 || rt != 0) {
+  if (g != 0 || rt != 0 || roll != 0) {
+    if (roll != 0) {  // angle = l g, rho = 1/g (0 for g = 0), attribute_bookkeeper.f90:763-770
+      const double angle = e.l * g, rho = (g == 0) ? 0.0 : 1 / g;
+      double Lc[3] = {rho * cos_one(angle / 2), rho * 0.0, rho * l_sin(angle / 2)};
+      rotate_vec(Lc, 2, angle / 2);
+      rotate_vec(Lc, 3, rt);
+      for (int i = 0; i < 3; i++) L_mis[i] = L_mis[i] - Lc[i];
+      rotate_vec(Lc, 3, roll);
+      for (int i = 0; i < 3; i++) L_mis[i] = L_mis[i] + Lc[i];
+    }
     in.bend_shift(g, 1 * ds_set, true, rt);
     Mat3 ws, wt;
-    w_mat_angles(e.x_pitch, e.y_pitch, false, ws);
+    w_mat_angles(e.x_pitch, e.y_pitch, false, ws, roll);
     for (int i = 0; i < 3; i++)
       for (int j = 0; j < 3; j++) wt[i][j] = ws[j][i];
     in.apply_w(wt, FS_SUB, L_mis);
@@ -653,8 +665,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
       if (e.x_pitch != 0 || e.y_pitch != 0 || e.z_offset != 0)
         if (e.key == BMADGPU_MULTIPOLE || e.key == BMADGPU_AB_MULTIPOLE)
           fail(BMADGPU_EUNSUPPORTED, "pitch / z_offset misalignment of a thin multipole");
-      if (e.key == BMADGPU_SBEND && (e.tilt != 0 || e.roll != 0))
-        fail(BMADGPU_EUNSUPPORTED, "sbend tilt / roll");
+      if (e.key == BMADGPU_SBEND && e.tilt != 0) fail(BMADGPU_EUNSUPPORTED, "sbend tilt (use ref_tilt)");
 
       if (e.key != BMADGPU_SBEND && e.ref_tilt != 0) fail(BMADGPU_EUNSUPPORTED, "ref_tilt on a non-bend");
       if (e.key == BMADGPU_RFCAVITY && (e.hkick != 0 || e.vkick != 0))
@@ -668,7 +679,7 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
 
       double tilt_tot = (e.key == BMADGPU_SBEND) ? 0.0 : e.tilt;
       const bool pitched = e.x_pitch != 0 || e.y_pitch != 0 || e.z_offset != 0;
-      const bool offset = e.x_offset != 0 || e.y_offset != 0 || pitched;
+      const bool offset = e.x_offset != 0 || e.y_offset != 0 || pitched || (e.key == BMADGPU_SBEND && e.roll != 0);
       bool has_misalign = (e.key == BMADGPU_SBEND) ? (e.ref_tilt != 0 || offset) : (e.tilt != 0 || offset);
       double ds_step;
       int num_steps;

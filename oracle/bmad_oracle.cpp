@@ -2,13 +2,14 @@
 //
 // A scalar restatement of Bmad's bmad_standard tracking of one charged particle through
 // drift / quadrupole / sbend / sextupole / octupole / thick_multipole / multipole /
-// ab_multipole / rfcavity / marker / monitor / instrument / pipe elements, with rectangular and
-// elliptical exit/entrance apertures, and of the bunch loop around it. Every routine names the
+// ab_multipole / rfcavity / marker / monitor / instrument / pipe / ecollimator / rcollimator
+// elements, with rectangular and elliptical apertures and the collimators' phase-space windows,
+// and of the bunch loop around it. Every routine names the
 // Fortran file and lines it restates (paths inside bmad-sim/bmad-ecosystem). Expressions keep
 // the Fortran operand order; the file is compiled with -ffp-contract=off.
 //
-// Not restated (returns BMADGPU_EUNSUPPORTED): rolled bends, exact_multipoles, fringe_type
-// full / soft_edge_only / sad_full / linear_edge edges, elseparators and kickers, reversed
+// Not restated (returns BMADGPU_EUNSUPPORTED): exact_multipoles, sbend fringe_type
+// soft_edge_only / sad_full / linear_edge edges, elseparators and kickers, reversed
 // orientation / direction / time, absolute time tracking, radiation and spin.
 
 #include "bmad_oracle.h"
@@ -623,7 +624,7 @@ void tilt_coords(double tilt_val, double* coord) {
   coord[3] = -sin_ang * px + cos_ang * py;
 }
 
-// floor_angles_to_w_mat, bmad/geometry/floor_angles_to_w_mat.f90 (psi = 0 as used here)
+// floor_angles_to_w_mat, bmad/geometry/floor_angles_to_w_mat.f90
 void floor_angles_to_w_mat(double theta, double phi, double psi, double w[3][3], bool inverse) {
   double s_the = lm.sin(theta), c_the = lm.cos(theta);
   double s_phi = lm.sin(phi), c_phi = lm.cos(phi);
@@ -789,12 +790,22 @@ int offset_particle(const Ele& ele, int set, Coord& orbit, bool set_tilt, bool s
     is_misaligned = (x_off != 0 || y_off != 0 || z_off != 0 || xp != 0 || yp != 0 ||
                      (key == BMADGPU_SBEND && e->roll != 0));
   }
-  if (is_misaligned && key == BMADGPU_SBEND && e->roll != 0) return BMADGPU_EUNSUPPORTED;  // roll not restated
-  const bool bend_geom = is_misaligned && key == BMADGPU_SBEND && (e->g != 0 || ele.ref_tilt_tot != 0);
+  const double roll = (key == BMADGPU_SBEND) ? e->roll : 0.0;
+  const bool bend_geom = is_misaligned && key == BMADGPU_SBEND && (e->g != 0 || ele.ref_tilt_tot != 0 || roll != 0);
   const double g = e->g, ref_tilt = ele.ref_tilt_tot;
-  // ele_misalignment_L_S_calc (bmad/geometry/ele_misalignment_L_S_calc.f90:16-50), no roll:
-  // L_mis = the offsets, S_mis = floor_angles_to_w_mat(x_pitch, y_pitch, 0)
+  // ele_misalignment_L_S_calc (bmad/geometry/ele_misalignment_L_S_calc.f90:16-50): L_mis = the
+  // offsets, moved by the roll about the bend's chord; S_mis = floor_angles_to_w_mat(x_pitch,
+  // y_pitch, roll). angle = l g, rho = 1/g (0 for g = 0), attribute_bookkeeper.f90:763-770.
   double L_mis[3] = {x_off, y_off, z_off};
+  if (bend_geom && roll != 0) {
+    const double angle = e->l * g, rho = (g == 0) ? 0.0 : 1 / g;
+    double Lc[3] = {rho * cos_one(angle / 2), rho * 0.0, rho * lm.sin(angle / 2)};
+    rotate_vec(Lc, y_axis, angle / 2);
+    rotate_vec(Lc, z_axis, ref_tilt);
+    for (int i = 0; i < 3; i++) L_mis[i] = L_mis[i] - Lc[i];
+    rotate_vec(Lc, z_axis, roll);
+    for (int i = 0; i < 3; i++) L_mis[i] = L_mis[i] + Lc[i];
+  }
 
   if (set) {
     double s_body;
@@ -803,7 +814,7 @@ int offset_particle(const Ele& ele, int set, Coord& orbit, bool set_tilt, bool s
       FloorPos pos = {{orbit.vec[0], orbit.vec[2], 0.0}, {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}};
       pos = bend_shift(pos, g, 1 * ds_center, true, ref_tilt);
       double ws[3][3], wt[3][3];
-      floor_angles_to_w_mat(xp, yp, 0.0, ws, false);
+      floor_angles_to_w_mat(xp, yp, roll, ws, false);
       for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) wt[i][j] = ws[j][i];
       double d[3] = {pos.r[0] - L_mis[0], pos.r[1] - L_mis[1], pos.r[2] - L_mis[2]};
       std::memcpy(pos.r, d, sizeof(d));
@@ -879,7 +890,7 @@ int offset_particle(const Ele& ele, int set, Coord& orbit, bool set_tilt, bool s
         pos = bend_shift(pos, g, L_half, true, ref_tilt);
       }
       double ws[3][3];
-      floor_angles_to_w_mat(xp, yp, 0.0, ws, false);
+      floor_angles_to_w_mat(xp, yp, roll, ws, false);
       apply_w(ws, pos);
       for (int i = 0; i < 3; i++) pos.r[i] = pos.r[i] + L_mis[i];
       pos = bend_shift(pos, g, sign_z_vel * 1 * L_half, true, ref_tilt);
@@ -2218,6 +2229,17 @@ int oracle_hwang_bend_edge_kick(const bmadgpu_element* e, const bmadgpu_param* p
   hwang_bend_edge_kick(ele, particle_at, o, mat6);
   to_external(o, c);
   return 0;
+}
+
+int oracle_offset_particle(const bmadgpu_element* e, const bmadgpu_param* p, int32_t set, oracle_coord* c) {
+  Ele ele;
+  int err = make_ele(e, p, 0, ele);
+  if (err) return err;
+  Coord o;
+  to_internal(c, o);
+  err = offset_particle(ele, set ? set_ : unset_, o, true, true);
+  to_external(o, c);
+  return err;
 }
 
 int oracle_check_aperture(const bmadgpu_element* e, const bmadgpu_param* p, int32_t particle_at, oracle_coord* c,

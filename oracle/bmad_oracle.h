@@ -59,6 +59,10 @@ int oracle_track1(oracle_coord* orb, const bmadgpu_element* ele, int32_t ix_ele,
 /* hwang_bend_edge_kick (fringe_mod.f90:241-419) with make_matrix = T.
  * particle_at: 11 = first_track_edge$, 12 = second_track_edge$. mat6 is 6x6 row-major
  * (mat6[i*6+j] = Fortran mat6(i+1, j+1)), premultiplied by the edge matrix. */
+/* offset_particle (bmad/code/offset_particle.f90:66-530) of one element, set (1) or unset (0),
+ * drifting to the element's end, set_tilt and set_hvkicks true. */
+int oracle_offset_particle(const bmadgpu_element* ele, const bmadgpu_param* param, int32_t set, oracle_coord* c);
+
 /* check_aperture_limit (bmad/low_level/check_aperture_limit.f90:30-387) of one element at
  * particle_at (11 first_track_edge, 12 second_track_edge) on the coordinate c: its state after the
  * check and param%unstable_factor. */

@@ -11,6 +11,7 @@ Sources (paths inside bmad-sim/bmad-ecosystem):
                                                                     transfer matrices by tracking
   regression_tests/aperture_test/aperture_test.bmad, .f90, output.correct
                                                                     collimator aperture states
+  regression_tests/coord_test/coord_test.bmad, .f90, output.correct offset_particle of bends
 
 Element attributes are transcribed below from the .bmad lines cited beside each entry; Bmad's
 parser defaults are applied explicitly (tilt flag -> pi/4 quad, pi/6 sextupole, pi/8 octupole,
@@ -149,6 +150,18 @@ def aperture_grids():
         out["zPz" + tag] = g
     return out
 
+# coord_test.bmad:38-40 (line l2: e_tot 1e8 electrons): b0, b1 (offsets, pitches, roll) and b2
+# (the same with ref_tilt = 2), and offset_track_drift (coord_test.f90:124-160) at orientation 1,
+# direction 1: offset_particle set ("Drift-In"), track1 through the element with its offsets,
+# pitches, roll and ref_tilt zeroed (zero_ele_offsets.f90:14-54, "Drift-Xfer"), offset_particle
+# unset ("Drift-Out").
+CT_ELEMENTS = {
+    "B0": ("SBEND", dict(l=2.0, g=0.1, dg=-0.1), 38),
+    "B1": ("SBEND", dict(l=2.0, g=0.1, dg=-0.1, x_offset=0.2, y_offset=0.3, x_pitch=0.1, y_pitch=0.2, roll=0.3), 39),
+    "B2": ("SBEND", dict(l=2.0, g=0.1, dg=-0.1, x_offset=0.2, y_offset=0.3, x_pitch=0.1, y_pitch=0.2, roll=0.3,
+                         ref_tilt=2.0), 40),
+}
+
 # fringe_test.bmad: e_tot 1e6 electrons, particle_start, b: sbend ...
 FR_START = [0.01, 0.02, 0.03, 0.04, 0.00, 0.5]
 FR_ELEMENT = dict(e1=0.1, e2=-0.2, k1=0.1, g=0.1, fint=0.5, hgap=0.4)
@@ -197,6 +210,17 @@ def main():
                                expected_unstable=un["values"], tol=un["tol"]))
     json.dump(dict(source="regression_tests/aperture_test", particle_at="second_track_edge", cases=acases),
               open(os.path.join(HERE, "aperture_test_collimators.json"), "w"), indent=1)
+
+    ct = parse_output_correct(os.path.join(REF, "regression_tests/coord_test/output.correct"))
+    ccases = []
+    for name, (key, attrs, src_line) in CT_ELEMENTS.items():
+        st = ct["%s:O:1:D:1:Drift-Start-orb" % name]
+        ccases.append(dict(name=name, key=key, attrs=attrs, bmad_line=src_line, output_line=st["line"],
+                           tol=st["tol"], start=st["values"][:6],
+                           expected={stage: ct["%s:O:1:D:1:Drift-%s-orb" % (name, stage)]["values"][:6]
+                                     for stage in ("In:", "Xfer", "Out")}))
+    json.dump(dict(source="regression_tests/coord_test", e_tot=1e8, charge=-1.0, cases=ccases),
+              open(os.path.join(HERE, "coord_test_bend_offsets.json"), "w"), indent=1)
 
     fr = parse_output_correct(os.path.join(REF, "regression_tests/fringe_test/output.correct"))
     fcases = []

@@ -57,7 +57,7 @@ def test_config1_ring_packs_and_sextupoles_use_one_step():
     assert all(s == 1 for e, s in zip(eles, steps) if e.key == abi.SEXTUPOLE)
 
 
-@pytest.mark.parametrize("bad", ["elec_on_rfcavity", "bend_roll", "bend_tilt", "bend_soft_edge", "abs_time"])
+@pytest.mark.parametrize("bad", ["elec_on_rfcavity", "bend_tilt", "bend_soft_edge", "abs_time"])
 def test_unsupported_inputs_fail_loudly(bad):
     abi = load_abi()
     p = abi.electron_param(3e9)
@@ -65,8 +65,6 @@ def test_unsupported_inputs_fail_loudly(bad):
     if bad == "elec_on_rfcavity":
         e = abi.default_element(abi.RFCAVITY, l=0.4, voltage=1e6, rf_frequency=5e8)
         e.b_pole_elec[1] = 1e3
-    elif bad == "bend_roll":
-        e = abi.default_element(abi.SBEND, l=1.0, g=0.01, roll=1e-3)
     elif bad == "bend_tilt":
         e = abi.default_element(abi.SBEND, l=1.0, g=0.01, tilt=1e-3)
     elif bad == "bend_soft_edge":
@@ -101,7 +99,8 @@ def test_misaligned_bends_and_electric_multipoles_are_accepted():
     quadrupoles, sextupoles, octupoles, thick multipoles and bends are on the device path."""
     abi = load_abi()
     p = abi.electron_param(3e9)
-    for kw in (dict(g=0.01, x_offset=1e-3), dict(g=0.01, y_pitch=1e-3, ref_tilt=0.1), dict(k1=0.3, z_offset=0.01)):
+    for kw in (dict(g=0.01, x_offset=1e-3), dict(g=0.01, y_pitch=1e-3, ref_tilt=0.1), dict(k1=0.3, z_offset=0.01),
+               dict(g=0.01, roll=1e-3)):
         lib.lattice_check([abi.default_element(abi.SBEND, l=1.0, **kw)], p)
     for key in (abi.QUADRUPOLE, abi.SEXTUPOLE, abi.OCTUPOLE, abi.THICK_MULTIPOLE, abi.SBEND):
         e = abi.default_element(key, l=0.4, k1=0.5, g=0.01 if key == abi.SBEND else 0.0)

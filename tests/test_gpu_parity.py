@@ -181,6 +181,8 @@ def _single_element_cases():
         "sbend_ref_tilt_offsets": [E(abi.SBEND, l=0.8, g=0.05, e1=0.02, e2=-0.01, ref_tilt=0.3, x_offset=1e-3,
                                      y_pitch=2e-4, **ap)],
         "sbend_g0_offsets": [E(abi.SBEND, l=0.6, k1=0.2, x_offset=1e-3, y_pitch=1e-3, z_offset=-0.02, **ap)],
+        "sbend_roll": [E(abi.SBEND, l=1.0, g=0.03, roll=0.02, x_offset=1e-3, y_pitch=2e-4, **ap)],
+        "sbend_roll_ref_tilt": [E(abi.SBEND, l=1.0, g=0.03, e1=0.02, roll=-0.01, ref_tilt=0.2, **ap)],
         "quad_fringe_full": [E(abi.QUADRUPOLE, l=0.4, k1=0.8, fringe_type=abi.FRINGE_FULL, fq1=0.02, fq2=-0.01, tilt=0.3,
                                **ap)],
         "quad_soft_edge": [E(abi.QUADRUPOLE, l=0.4, k1=0.8, fringe_type=abi.FRINGE_SOFT_EDGE_ONLY, fq1=0.05, fq2=0.01,

@@ -84,6 +84,8 @@ CASES = {
     "sbend_ref_tilt_offsets": lambda E, ap: [E(abi.SBEND, l=0.8, g=0.05, e1=0.02, e2=-0.01, ref_tilt=0.3,
                                                x_offset=1e-3, y_pitch=2e-4, **ap)],
     "sbend_g0_offsets": lambda E, ap: [E(abi.SBEND, l=0.6, k1=0.2, x_offset=1e-3, y_pitch=1e-3, z_offset=-0.02, **ap)],
+    "sbend_roll": lambda E, ap: [E(abi.SBEND, l=1.0, g=0.03, roll=0.02, x_offset=1e-3, y_pitch=2e-4, **ap)],
+    "sbend_roll_ref_tilt": lambda E, ap: [E(abi.SBEND, l=1.0, g=0.03, e1=0.02, roll=-0.01, ref_tilt=0.2, **ap)],
     "sbend_g0_ref_tilt": lambda E, ap: [E(abi.SBEND, l=0.6, k1=0.3, k2=3.0, ref_tilt=0.1, x_offset=2e-3,
                                           y_pitch=1e-3, num_steps=10, **ap)],
     # collimators: phase-space windows before the x/y limits, asymmetric elliptical limits

@@ -155,3 +155,39 @@ def test_aperture_test_collimators(case):
         assert lib.oracle_check_aperture(ctypes.byref(ele), ctypes.byref(p), 12, ctypes.byref(c), ctypes.byref(u)) == 0
         assert c.state == want_state, (case["name"], v, c.state, want_state)
         assert abs(u.value - want_u) <= case["tol"] + _printed3(want_u), (case["name"], v, u.value, want_u)
+
+
+# ---- offset_particle of bends (coord_test) ------------------------------------------------------
+
+def _ct():
+    return json.load(open(os.path.join(HERE, "golden", "coord_test_bend_offsets.json")))
+
+
+@pytest.mark.parametrize("case", _ct()["cases"], ids=lambda c: c["name"])
+def test_coord_test_bend_offsets(case):
+    """offset_particle set, track1 through the unmisaligned bend, offset_particle unset, for the
+    reference's b0 / b1 (offsets, pitches, roll) / b2 (also ref_tilt) against its coord_test
+    lines (8 printed decimals, ABS 1e-8)."""
+    abi, lib = load_abi(), load_oracle()
+    data = _ct()
+    p = abi.electron_param(data["e_tot"], charge=data["charge"])
+    ele = abi.default_element(abi.SBEND, **case["attrs"])
+    bare = dict(case["attrs"])
+    for k in ("x_offset", "y_offset", "x_pitch", "y_pitch", "roll", "ref_tilt", "z_offset"):
+        bare.pop(k, None)
+    ele2 = abi.default_element(abi.SBEND, **bare)   # zero_ele_offsets
+    c = OracleCoord()
+    lib.oracle_init_coord(ctypes.byref(c), (ctypes.c_double * 6)(*case["start"]), ctypes.byref(p))
+    tol = case["tol"] + 5e-9
+
+    def check(stage):
+        want = case["expected"][stage]
+        got = [c.vec[i] for i in range(6)]
+        assert all(abs(g - w) <= tol for g, w in zip(got, want)), (case["name"], stage, got, want)
+
+    assert lib.oracle_offset_particle(ctypes.byref(ele), ctypes.byref(p), 1, ctypes.byref(c)) == 0
+    check("In:")
+    assert lib.oracle_track1(ctypes.byref(c), ctypes.byref(ele2), 1, ctypes.byref(p)) == 0
+    check("Xfer")
+    assert lib.oracle_offset_particle(ctypes.byref(ele), ctypes.byref(p), 0, ctypes.byref(c)) == 0
+    check("Out")
