@@ -35,6 +35,29 @@ TM_CHARGE = 1.0
 
 _sb0 = dict(a_pole={0: 0.01, 1: 0.1}, vkick=-0.0001, b_pole_elec={0: -2e3}, a_pole_elec={1: 2e4}, r0_mag=2.0,
             r0_elec=3.0)  # :79
+def rbend_to_sbend(attrs):
+    """The parser's rbend conversion (bmad_parser_mod.f90:5186-5225, fiducial_pt none): the given
+    l is the chord; the arc length follows from g, the angle is g l, e1 and e2 each gain half the
+    angle, and the element is an sbend from then on."""
+    import math
+    a = dict(attrs)
+    l_chord, g = a.pop("l"), a.get("g", 0.0)
+    if g != 0:
+        ang = 2.0 * math.asin(0.5 * l_chord * g)
+        l = l_chord * ang / (2.0 * math.sin(0.5 * ang))
+    else:
+        l = l_chord
+    angle = g * l
+    a["l"] = l
+    a["e1"] = a.get("e1", 0.0) + 0.5 * angle
+    a["e2"] = a.get("e2", 0.0) + 0.5 * angle
+    if angle != 0:
+        a["g"] = angle / l
+    return a
+
+
+_rb0 = dict(a_pole={0: 0.01, 1: 0.1}, vkick=-0.0001, b_pole_elec={0: -2e3}, a_pole_elec={1: 2e4}, r0_mag=2.0,
+            r0_elec=3.0)  # :80
 _q0 = dict(a_pole={0: 0.01, 1: 0.1}, vkick=-0.0001, b_pole_elec={0: -2e3}, a_pole_elec={1: 2e4})  # :62
 
 TM_ELEMENTS = {
@@ -69,6 +92,11 @@ TM_ELEMENTS = {
                              ref_tilt=0.1), 84),
     "SBEND7": ("SBEND", dict(_sb0, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, x_offset=0.05, y_pitch=0.001,
                              ref_tilt=0.1), 91),
+    # rbends (l = the chord), converted as the parser converts them
+    "RBEND4": ("SBEND", rbend_to_sbend(dict(_rb0, l=0.6, g=0.01, dg=-0.0099, e1=0.1, e2=0.2, num_steps=10,
+                                            fringe_type=4, x_offset=0.05, y_pitch=0.001, ref_tilt=0.1)), 85),
+    "RBEND6": ("SBEND", rbend_to_sbend(dict(_rb0, l=0.6, g=0.01, dg=-0.0099999, e1=0.1, e2=0.2, num_steps=10,
+                                            x_offset=0.05, y_pitch=0.001, ref_tilt=0.1)), 89),
     # fringe_type full: exact_bend_edge_kick with fint = 0.7, hgap = 2 (:87-88)
     "SBEND5": ("SBEND", dict(_sb0, l=0.6, g=0.01, e1=0.1, e2=0.2, num_steps=10, fringe_type=4, x_offset=0.05,
                              y_pitch=0.001, ref_tilt=0.1, fint=0.7, hgap=2.0), 87),
@@ -83,6 +111,7 @@ _m_q0 = dict(a_pole={0: 0.01, 1: 0.1}, vkick=-0.0001, b_pole_elec={0: -2e3}, a_p
 _m_sb0 = dict(a_pole={0: 0.001, 1: 0.1}, vkick=-0.0001, b_pole_elec={0: -2e3}, a_pole_elec={1: 2e3})  # :80
 FULL = 4  # fringe_type full$ (bmad_struct.f90:168)
 _m_mis = dict(num_steps=10, x_offset=0.05, y_pitch=0.001)
+_m_rb0 = dict(a_pole={0: 0.001, 1: 0.1}, vkick=-0.0001, b_pole_elec={0: -2e3}, a_pole_elec={1: 2e3})  # :81
 M6_ELEMENTS = {
     "AB_MULTIPOLE1": ("AB_MULTIPOLE", dict(a_pole={2: 1e3}, b_pole={2: 1e3}, x_offset=0.02, tilt=0.1), 19),
     "DRIFT1": ("DRIFT", dict(l=4.5, tilt=0.1, **_m_mis), 23),
@@ -108,6 +137,10 @@ M6_ELEMENTS = {
     "SBEND7": ("SBEND", dict(_m_sb0, l=0.6, g=0.01, e1=0.1, e2=0.2, ref_tilt=0.1, a_pole={0: 0.001, 1: 10.0, 3: 100.0},
                              **_m_mis), 91),
     "SEXTUPOLE1": ("SEXTUPOLE", dict(l=0.6, k2=1.0, tilt=PI / 6.0, **_m_mis), 94),
+    "RBEND4": ("SBEND", rbend_to_sbend(dict(_m_rb0, l=0.6, g=0.01, dg=-0.009999, e1=0.1, e2=0.2, fringe_type=FULL,
+                                            ref_tilt=0.1, b_pole={1: 10.0, 3: 100.0}, **_m_mis)), 85),
+    "RBEND6": ("SBEND", rbend_to_sbend(dict(_m_rb0, l=0.6, g=0.01, dg=-0.009999999, e1=0.1, e2=0.2, ref_tilt=0.1,
+                                            **_m_mis)), 89),
     "THICK_MULTIPOLE1": ("THICK_MULTIPOLE", dict(l=4.5, a_pole={2: 1.0}, b_pole={2: 20.0}, x_offset=0.02, tilt=0.1),
                          124),
 }
@@ -194,7 +227,7 @@ def main():
         rows = [m6["%s:Tracking:MatrixRow%d" % (name, i)] for i in range(1, 7)]
         vec0 = m6[name + ":Tracking:Vector"]
         mcases.append(dict(name=name, key=key, attrs=attrs, bmad_line=src_line, output_line=vec0["line"],
-                           tol_matrix=max(r["tol"] for r in rows), tol_vec0=vec0["tol"],
+                           tol_matrix=max(r["tol"] for r in rows), tol_rows=[r["tol"] for r in rows], tol_vec0=vec0["tol"],
                            expected_mat6=[r["values"] for r in rows], expected_vec0=vec0["values"]))
     json.dump(dict(source="regression_tests/mat6_calc_method_test", e_tot=1e6, charge=1.0, start=TM_START, d_orb=1e-5,
                    cases=mcases), open(os.path.join(HERE, "mat6_calc_method_tracking.json"), "w"), indent=1)
