@@ -87,6 +87,7 @@ bool key_supported(int key) {
     case BMADGPU_RFCAVITY: case BMADGPU_MARKER: case BMADGPU_OCTUPOLE: case BMADGPU_MULTIPOLE:
     case BMADGPU_AB_MULTIPOLE: case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE:
     case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:
+    case BMADGPU_KICKER: case BMADGPU_HKICKER: case BMADGPU_VKICKER:
       return true;
   }
   return false;
@@ -97,7 +98,7 @@ bool key_has_hkick(int key) {
   switch (key) {
     case BMADGPU_QUADRUPOLE: case BMADGPU_SBEND: case BMADGPU_SEXTUPOLE: case BMADGPU_OCTUPOLE:
     case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RFCAVITY: case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT:
-    case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:
+    case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR: case BMADGPU_KICKER:
       return true;
   }
   return false;
@@ -133,6 +134,13 @@ void mag_ab(const bmadgpu_element& e, double tilt_tot, double ref_tilt_tot, doub
         case BMADGPU_QUADRUPOLE: cnst = e.k1 * e.l; ref_exp = 1; break;
         case BMADGPU_SEXTUPOLE: cnst = e.k2 * e.l; ref_exp = 2; break;
         case BMADGPU_OCTUPOLE: cnst = e.k3 * e.l; ref_exp = 3; break;
+        case BMADGPU_KICKER:
+          if (e.hkick == 0) cnst = e.vkick;
+          else if (e.vkick == 0) cnst = e.hkick;
+          else cnst = std::sqrt(e.hkick * e.hkick + e.vkick * e.vkick);
+          ref_exp = 0;
+          break;
+        case BMADGPU_HKICKER: case BMADGPU_VKICKER: cnst = e.kick; ref_exp = 0; break;
         default: scale = false;
       }
       if (scale) {
@@ -151,7 +159,14 @@ void mag_ab(const bmadgpu_element& e, double tilt_tot, double ref_tilt_tot, doub
   }
   // this_ele_non_multipoles (multipole_ele_to_ab.f90:326-405)
   double ak[4] = {0, 0, 0, 0}, bk[4] = {0, 0, 0, 0};
-  if (key_has_hkick(e.key) && (e.hkick != 0 || e.vkick != 0)) {
+  if (e.key == BMADGPU_HKICKER) {         // multipole_ele_to_ab.f90:339-346
+    bk[0] = -e.kick;
+  } else if (e.key == BMADGPU_VKICKER) {
+    ak[0] = e.kick;
+  } else if (e.key == BMADGPU_KICKER) {
+    bk[0] = -e.hkick;
+    ak[0] = e.vkick;
+  } else if (key_has_hkick(e.key) && (e.hkick != 0 || e.vkick != 0)) {
     double tilt = (e.key == BMADGPU_SBEND) ? ref_tilt_tot : tilt_tot;
     if (tilt != 0) {
       double c = l_cos(tilt), s = l_sin(tilt);
@@ -811,7 +826,8 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
         }
         case BMADGPU_SEXTUPOLE: case BMADGPU_OCTUPOLE: case BMADGPU_THICK_MULTIPOLE:
         case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE:
-        case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR: {  // track_a_thick_multipole.f90
+        case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:
+        case BMADGPU_KICKER: case BMADGPU_HKICKER: case BMADGPU_VKICKER: {  // track_a_thick_multipole.f90
           h.kind = K_THICK;
           mag_ab(e, tilt_tot, 0, a, b, &ix_mag_max);
           int n_step = (ix_mag_max == -1 && ix_elec_max == -1) ? 1 : std::max(nint(std::fabs(e.l / ds_step)), 1);
@@ -819,7 +835,8 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
           double step_len = e.l / n_step;
           blk = {step_len};
           if (key != BMADGPU_MONITOR && key != BMADGPU_INSTRUMENT && key != BMADGPU_PIPE &&
-              key != BMADGPU_RCOLLIMATOR && key != BMADGPU_ECOLLIMATOR)
+              key != BMADGPU_RCOLLIMATOR && key != BMADGPU_ECOLLIMATOR && key != BMADGPU_KICKER &&
+              key != BMADGPU_HKICKER && key != BMADGPU_VKICKER)
             eblk = extra_block(e, p, ae, be, ix_elec_max, 1 * step_len / 2, 1 * step_len);
           if (ix_mag_max > -1) {
             flags |= F_KICKS;

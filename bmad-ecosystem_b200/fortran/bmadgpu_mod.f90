@@ -41,6 +41,7 @@ type, bind(c) :: bmadgpu_element_t
   real(c_double) :: fq1, fq2
   real(c_double) :: px_aperture_width2, px_aperture_center, py_aperture_width2, py_aperture_center
   real(c_double) :: z_aperture_width2, z_aperture_center, pz_aperture_width2, pz_aperture_center
+  real(c_double) :: kick
 end type
 
 type, bind(c) :: bmadgpu_param_t
@@ -231,6 +232,8 @@ if (ele%key == quadrupole$) then
 endif
 e%px_aperture_width2 = 0;  e%px_aperture_center = 0;  e%py_aperture_width2 = 0;  e%py_aperture_center = 0
 e%z_aperture_width2 = 0;  e%z_aperture_center = 0;  e%pz_aperture_width2 = 0;  e%pz_aperture_center = 0
+e%kick = 0
+if (ele%key == hkicker$ .or. ele%key == vkicker$) e%kick = ele%value(kick$)
 if (ele%key == ecollimator$ .or. ele%key == rcollimator$) then
   e%px_aperture_width2 = ele%value(px_aperture_width2$);  e%px_aperture_center = ele%value(px_aperture_center$)
   e%py_aperture_width2 = ele%value(py_aperture_width2$);  e%py_aperture_center = ele%value(py_aperture_center$)

@@ -52,7 +52,8 @@ enum {
   BMADGPU_DRIFT = 1, BMADGPU_SBEND = 2, BMADGPU_QUADRUPOLE = 3, BMADGPU_SEXTUPOLE = 5,
   BMADGPU_RFCAVITY = 9, BMADGPU_MARKER = 14, BMADGPU_OCTUPOLE = 17, BMADGPU_MULTIPOLE = 19,
   BMADGPU_AB_MULTIPOLE = 22, BMADGPU_MONITOR = 31, BMADGPU_INSTRUMENT = 32, BMADGPU_PIPE = 44,
-  BMADGPU_THICK_MULTIPOLE = 67, BMADGPU_RCOLLIMATOR = 35, BMADGPU_ECOLLIMATOR = 36
+  BMADGPU_THICK_MULTIPOLE = 67, BMADGPU_RCOLLIMATOR = 35, BMADGPU_ECOLLIMATOR = 36,
+  BMADGPU_KICKER = 15, BMADGPU_HKICKER = 33, BMADGPU_VKICKER = 34
 };
 /* particle states, bmad_struct.f90:525-532 */
 enum {
@@ -111,6 +112,7 @@ typedef struct bmadgpu_element {
    * px, py, z, pz; a zero half width leaves that coordinate unchecked */
   double px_aperture_width2, px_aperture_center, py_aperture_width2, py_aperture_center;
   double z_aperture_width2, z_aperture_center, pz_aperture_width2, pz_aperture_center;
+  double kick;                /* hkicker / vkicker: ele%value(kick$) */
 } bmadgpu_element;
 
 /* Branch/global parameters: lat_param_struct + the bmad_common_struct switches on the path. */

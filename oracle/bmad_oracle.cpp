@@ -216,7 +216,7 @@ bool key_has_hkick(int key) {
   switch (key) {
     case BMADGPU_QUADRUPOLE: case BMADGPU_SBEND: case BMADGPU_SEXTUPOLE: case BMADGPU_OCTUPOLE:
     case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RFCAVITY: case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT:
-    case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:
+    case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR: case BMADGPU_KICKER:
       return true;
   }
   return false;
@@ -295,6 +295,13 @@ int convert_this_ab(const Ele& ele, int p_type, const double* a_pole, const doub
     case BMADGPU_QUADRUPOLE: cnst = e->k1 * e->l; ref_exp = 1; break;
     case BMADGPU_SEXTUPOLE: cnst = e->k2 * e->l; ref_exp = 2; break;
     case BMADGPU_OCTUPOLE: cnst = e->k3 * e->l; ref_exp = 3; break;
+    case BMADGPU_KICKER:
+      if (e->hkick == 0) cnst = e->vkick;
+      else if (e->vkick == 0) cnst = e->hkick;
+      else cnst = std::sqrt(e->hkick * e->hkick + e->vkick * e->vkick);
+      ref_exp = 0;
+      break;
+    case BMADGPU_HKICKER: case BMADGPU_VKICKER: cnst = e->kick; ref_exp = 0; break;
     case BMADGPU_AB_MULTIPOLE: case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RFCAVITY: return 0;
     default: return BMADGPU_EUNSUPPORTED;
   }
@@ -317,6 +324,14 @@ void this_ele_non_multipoles(const Ele& ele, int p_type, double a_kick[4], doubl
   const bmadgpu_element* e = ele.e;
   for (int i = 0; i < 4; i++) { a_kick[i] = 0; b_kick[i] = 0; }
   if (p_type != magnetic) return;
+  switch (e->key) {  // multipole_ele_to_ab.f90:339-346
+    case BMADGPU_HKICKER: b_kick[0] = -e->kick; return;
+    case BMADGPU_VKICKER: a_kick[0] = e->kick; return;
+    case BMADGPU_KICKER:
+      b_kick[0] = -e->hkick;
+      a_kick[0] = e->vkick;
+      return;
+  }
   double hk = e->hkick, vk = e->vkick;
   if (key_has_hkick(e->key) && (hk != 0 || vk != 0)) {
     double tilt = (e->key == BMADGPU_SBEND) ? ele.ref_tilt_tot : ele.tilt_tot;
@@ -1996,6 +2011,7 @@ int track1_bmad(Coord& orbit, const Ele& ele) {
     case BMADGPU_DRIFT: track_a_drift(orbit, e->l * 1, ele.p); break;
     case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE:
     case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:  // track1_bmad.f90:87-88
+    case BMADGPU_KICKER: case BMADGPU_HKICKER: case BMADGPU_VKICKER:
     case BMADGPU_OCTUPOLE: case BMADGPU_THICK_MULTIPOLE: case BMADGPU_SEXTUPOLE:
       err = track_a_thick_multipole(orbit, ele);
       break;

@@ -135,3 +135,13 @@ def test_collimators_and_kicked_monitors_are_accepted():
     with pytest.raises(lib.BmadGpuError) as ei:
         lib.lattice_check([abi.default_element(abi.MONITOR, l=0.2, b_pole={2: 1e-3})], p)
     assert ei.value.code == abi.EUNSUPPORTED
+
+
+def test_kickers_are_accepted():
+    """hkicker / vkicker (kick) and kicker (hkick, vkick, scaled multipoles) are thick multipoles
+    on the device path."""
+    abi = load_abi()
+    p = abi.electron_param(3e9)
+    lib.lattice_check([abi.default_element(abi.HKICKER, l=0.2, kick=1e-4, tilt=0.1)], p)
+    lib.lattice_check([abi.default_element(abi.VKICKER, l=0.2, kick=-1e-4)], p)
+    lib.lattice_check([abi.default_element(abi.KICKER, l=0.2, hkick=1e-4, vkick=2e-4, b_pole={1: 2.0})], p)
