@@ -181,3 +181,15 @@ def test_batched_variants_bit_exact(ctx):
         assert np.array_equal(g["ix_ele"][lost], o["ix_ele"][lost])
         assert np.array_equal(g["ix_turn"][lost], o["ix_turn"][lost])
     batch.close()
+
+
+def test_ring_with_rare_forms_bit_exact(ctx):
+    """The full kernel instance over many turns: a ring with electric multipoles, full edge
+    fringes, a rolled bend frame, a pitched sextupole, a collimator with phase-space windows and
+    kickers, bit-identical to the oracle with a correctly rounded libm, losses included."""
+    from test_hostcheck_cpu import _rare_ring
+    eles, p = _rare_ring()
+    vec = rings.matched_gaussian(rings.ring(20)[0], 4096, seed=17, scale=6.0)
+    g, o = gpu_track(ctx, eles, p, vec, 100), oracle_cr(eles, p, vec, 100)
+    assert (o["state"] != abi.ALIVE).sum() > 0
+    assert_identical(g, o)

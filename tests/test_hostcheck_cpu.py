@@ -297,3 +297,48 @@ def test_cr_libm_equals_an_independent_correctly_rounded_libm():
         pass
     c = oracle_track(eles, p, vec, 20)        # the host's libm again: not correctly rounded
     assert not np.array_equal(a["vec"], c["vec"])
+
+
+def _rare_ring():
+    """A 20-cell ring carrying every rare element form at once: a quadrupole with electric
+    multipoles, a full (hard and soft) edge fringe and fq1/fq2, a rolled and offset bend with
+    fringe_type full, a pitched sextupole, an ecollimator with phase-space windows, kickers."""
+    E = abi.default_element
+    eles, p = rings.ring(20)
+    quads = [i for i, e in enumerate(eles) if e.key == abi.QUADRUPOLE]
+    bends = [i for i, e in enumerate(eles) if e.key == abi.SBEND]
+    sexts = [i for i, e in enumerate(eles) if e.key == abi.SEXTUPOLE]
+    q = eles[quads[3]]
+    q.b_pole_elec[1] = 2e5
+    q.a_pole_elec[2] = 1e6
+    q.fringe_type = abi.FRINGE_FULL
+    q.fq1, q.fq2 = 0.01, -0.005
+    b = eles[bends[5]]
+    b.x_offset, b.roll, b.y_pitch = 2e-4, 1e-3, 1e-4
+    b.fringe_type, b.e1, b.fint, b.hgap = abi.FRINGE_FULL, 0.01, 0.5, 0.02
+    b.fintx, b.hgapx = b.fint, b.hgap
+    eles[sexts[4]].z_offset = 1e-3
+    eles[sexts[4]].x_pitch = 2e-4
+    extra = [E(abi.ECOLLIMATOR, l=0.1, x1_limit=0.015, x2_limit=0.015, y1_limit=0.008, y2_limit=0.008,
+               px_aperture_width2=2e-3, py_aperture_width2=1.5e-3),
+             E(abi.HKICKER, l=0.1, kick=1e-6), E(abi.KICKER, l=0.1, hkick=-1e-6, vkick=5e-7)]
+    eles = eles[:10] + extra + eles[10:]
+    rings.set_ref_time(eles, p)
+    return eles, p
+
+
+def test_ring_with_rare_forms_on_host(hc, hc_cr):
+    """Many turns of a ring with every rare form (the full kernel's path), bit-identical to the
+    oracle with glibc and with the correctly rounded libm, losses included."""
+    eles, p = _rare_ring()
+    vec = rings.matched_gaussian(rings.ring(20)[0], 400, seed=17, scale=6.0)
+    o = oracle_track(eles, p, vec, 30)
+    h = host_track(hc, eles, p, vec, 30)
+    for k in ("vec", "beta", "state", "ix_ele", "ix_turn"):
+        assert np.array_equal(h[k], o[k]), k
+    assert (o["state"] != abi.ALIVE).sum() > 0 and (o["state"] == abi.ALIVE).sum() > 100
+    with oracle_libm("cr"):
+        o = oracle_track(eles, p, vec, 30)
+    h = host_track(hc_cr, eles, p, vec, 30)
+    for k in ("vec", "beta", "state", "ix_ele", "ix_turn"):
+        assert np.array_equal(h[k], o[k]), k
