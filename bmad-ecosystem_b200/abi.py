@@ -20,7 +20,7 @@ STATUS_NAMES = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ETIMEDOUT
 DRIFT, SBEND, QUADRUPOLE, SEXTUPOLE, RFCAVITY, MARKER = 1, 2, 3, 5, 9, 14
 OCTUPOLE, MULTIPOLE, AB_MULTIPOLE, MONITOR, INSTRUMENT, PIPE, THICK_MULTIPOLE = 17, 19, 22, 31, 32, 44, 67
 RCOLLIMATOR, ECOLLIMATOR = 35, 36
-KICKER, HKICKER, VKICKER = 15, 33, 34
+KICKER, HKICKER, VKICKER, ELSEPARATOR = 15, 33, 34, 10
 # particle states (bmad_struct.f90:525-532)
 ALIVE, LOST, LOST_NEG_X, LOST_POS_X, LOST_NEG_Y, LOST_POS_Y, LOST_Z, LOST_PZ = 1, 2, 3, 4, 5, 6, 7, 8
 # locations (bmad_struct.f90:376-377)

@@ -58,7 +58,10 @@ BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b
   const bool has_t = h.flags & F_TILT;
   const double* xb = (FULL && (h.flags & F_EXTRA)) ? el : nullptr;
   const bool elec = xb && xb[0] != 0;
+  const bool elsep = xb && xb[21] != 0;   // elseparator field steps
   const bool pitched = FULL && (h.flags & F_PITCH);
+  Particle start;
+  if (elsep) start = p;
   if (h.flags & F_MISALIGN) offset_set(p, mis, has_t, pitched);
   if (xb) {
     straight_edge(p, xb, true, G);
@@ -68,7 +71,13 @@ BG_HD void body_thick(Particle& p, const EleHdr& h, const double* __restrict__ b
   const int n_step = h.n_step;
   const bool b_from2 = h.flags & F_KICK_B_FROM2;
   for (int i = 0; i <= n_step; i++) {
-    if (i > 0) drift(p, step_len);
+    if (i > 0) {
+      if (elsep) {
+        if (!elsep_step(p, xb, step_len, start, G)) return;
+      } else {
+        drift(p, step_len);
+      }
+    }
     const bool end = (i == 0 || i == n_step);
     if (np) ab_kicks(p, end ? kh : kf, np, b_from2);
     if (elec) elec_kicks(p, el, end ? el[1] : el[2], G);

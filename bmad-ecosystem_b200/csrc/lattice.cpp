@@ -87,7 +87,7 @@ bool key_supported(int key) {
     case BMADGPU_RFCAVITY: case BMADGPU_MARKER: case BMADGPU_OCTUPOLE: case BMADGPU_MULTIPOLE:
     case BMADGPU_AB_MULTIPOLE: case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE:
     case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:
-    case BMADGPU_KICKER: case BMADGPU_HKICKER: case BMADGPU_VKICKER:
+    case BMADGPU_KICKER: case BMADGPU_HKICKER: case BMADGPU_VKICKER: case BMADGPU_ELSEPARATOR:
       return true;
   }
   return false;
@@ -134,7 +134,7 @@ void mag_ab(const bmadgpu_element& e, double tilt_tot, double ref_tilt_tot, doub
         case BMADGPU_QUADRUPOLE: cnst = e.k1 * e.l; ref_exp = 1; break;
         case BMADGPU_SEXTUPOLE: cnst = e.k2 * e.l; ref_exp = 2; break;
         case BMADGPU_OCTUPOLE: cnst = e.k3 * e.l; ref_exp = 3; break;
-        case BMADGPU_KICKER:
+        case BMADGPU_KICKER: case BMADGPU_ELSEPARATOR:
           if (e.hkick == 0) cnst = e.vkick;
           else if (e.vkick == 0) cnst = e.hkick;
           else cnst = std::sqrt(e.hkick * e.hkick + e.vkick * e.vkick);
@@ -166,6 +166,8 @@ void mag_ab(const bmadgpu_element& e, double tilt_tot, double ref_tilt_tot, doub
   } else if (e.key == BMADGPU_KICKER) {
     bk[0] = -e.hkick;
     ak[0] = e.vkick;
+  } else if (e.key == BMADGPU_ELSEPARATOR) {
+    // the separator's kick is its electric field (track_this_elsep), not a multipole
   } else if (key_has_hkick(e.key) && (e.hkick != 0 || e.vkick != 0)) {
     double tilt = (e.key == BMADGPU_SBEND) ? ref_tilt_tot : tilt_tot;
     if (tilt != 0) {
@@ -344,7 +346,9 @@ std::vector<double> extra_block(const bmadgpu_element& e, const bmadgpu_param& p
   if (bend) {
     if (ix_elec_max < 0 && ft != BMADGPU_FRINGE_FULL) return {};
   } else {
-    const bool has_fringe = (ft != BMADGPU_FRINGE_NONE && e.fringe_at != BMADGPU_NO_END) || raw_elec;
+    // init_fringe_info: an elseparator always has a fringe (its longitudinal field)
+    const bool has_fringe = (ft != BMADGPU_FRINGE_NONE && e.fringe_at != BMADGPU_NO_END) || raw_elec ||
+                            e.key == BMADGPU_ELSEPARATOR;
     if (!has_fringe) return {};
   }
   auto bits = [&](int end) {
@@ -358,6 +362,7 @@ std::vector<double> extra_block(const bmadgpu_element& e, const bmadgpu_param& p
         m |= EX_SOFT;
       if (bend && ft == BMADGPU_FRINGE_FULL) m |= EX_EXACT;
     }
+    if (e.key == BMADGPU_ELSEPARATOR && e.l != 0) m |= EX_ESEP;
     return (double)m;
   };
   const int n_elec = ix_elec_max + 1;
@@ -366,7 +371,10 @@ std::vector<double> extra_block(const bmadgpu_element& e, const bmadgpu_param& p
                              e.key == BMADGPU_SEXTUPOLE ? 2.0 : 1.0, e.key == BMADGPU_SEXTUPOLE ? e.k2 : e.k1,
                              e.k1, e.fq1, e.fq2,
                              e.is_on ? e.g + e.dg : 0.0, p.p0c / p.e_tot,
-                             1 * e.e1, 1 * e.fint, e.hgap, 1 * e.e2, 1 * e.fintx, e.hgapx, 0.0};
+                             1 * e.e1, 1 * e.fint, e.hgap, 1 * e.e2, 1 * e.fintx, e.hgapx,
+                             0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0,   // elseparator steps, set by the caller
+                             e.l != 0 ? 1.0 * p.charge * (p.p0c / e.l) : 0.0,
+                             e.l != 0 ? -1.0 * p.charge * (p.p0c / e.l) : 0.0, e.hkick, e.vkick};
   for (int n = 0; n < n_elec; n++) blk.insert(blk.end(), {b[n], a[n]});
   return blk;
 }
@@ -685,7 +693,8 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
       if (e.key != BMADGPU_SBEND && e.ref_tilt != 0) fail(BMADGPU_EUNSUPPORTED, "ref_tilt on a non-bend");
       if (e.key == BMADGPU_RFCAVITY && (e.hkick != 0 || e.vkick != 0))
         fail(BMADGPU_EUNSUPPORTED, "rfcavity hkick/vkick");
-      if (!key_has_hkick(e.key) && (e.hkick != 0 || e.vkick != 0) && e.key != BMADGPU_DRIFT)
+      if (!key_has_hkick(e.key) && (e.hkick != 0 || e.vkick != 0) && e.key != BMADGPU_DRIFT &&
+          e.key != BMADGPU_ELSEPARATOR)
         fail(BMADGPU_EUNSUPPORTED, "hkick/vkick on this element type");
       if (e.aperture_type != BMADGPU_APERTURE_RECTANGULAR && e.aperture_type != BMADGPU_APERTURE_AUTO &&
           e.aperture_type != BMADGPU_APERTURE_ELLIPTICAL)
@@ -827,10 +836,20 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
         case BMADGPU_SEXTUPOLE: case BMADGPU_OCTUPOLE: case BMADGPU_THICK_MULTIPOLE:
         case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE:
         case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:
-        case BMADGPU_KICKER: case BMADGPU_HKICKER: case BMADGPU_VKICKER: {  // track_a_thick_multipole.f90
+        case BMADGPU_KICKER: case BMADGPU_HKICKER: case BMADGPU_VKICKER:
+        case BMADGPU_ELSEPARATOR: {  // track_a_thick_multipole.f90
           h.kind = K_THICK;
           mag_ab(e, tilt_tot, 0, a, b, &ix_mag_max);
-          int n_step = (ix_mag_max == -1 && ix_elec_max == -1) ? 1 : std::max(nint(std::fabs(e.l / ds_step)), 1);
+          // the separator's field, :49-65: kick = |(hk, vk)| (charge sign), angle atan2(vk, hk)
+          double sep_kick = 0, sep_angle = 0;
+          if (key == BMADGPU_ELSEPARATOR) {
+            const double rtc = 1.0 * (p.charge < 0 ? -1.0 : 1.0);
+            const double hk = e.hkick * rtc, vk = e.vkick * rtc;
+            sep_kick = std::sqrt(hk * hk + vk * vk);
+            sep_angle = l_atan2(vk, hk);
+          }
+          int n_step = (sep_kick == 0 && ix_mag_max == -1 && ix_elec_max == -1)
+                           ? 1 : std::max(nint(std::fabs(e.l / ds_step)), 1);
           double r_step = 1.0 / n_step;
           double step_len = e.l / n_step;
           blk = {step_len};
@@ -838,6 +857,17 @@ int pack_lattice(const bmadgpu_element* eles, int n_ele, const bmadgpu_param& p,
               key != BMADGPU_RCOLLIMATOR && key != BMADGPU_ECOLLIMATOR && key != BMADGPU_KICKER &&
               key != BMADGPU_HKICKER && key != BMADGPU_VKICKER)
             eblk = extra_block(e, p, ae, be, ix_elec_max, 1 * step_len / 2, 1 * step_len);
+          if (key == BMADGPU_ELSEPARATOR) {
+            eblk = extra_block(e, p, ae, be, ix_elec_max, 1 * step_len / 2, 1 * step_len);
+            const double mr = p.mass / p.p0c;
+            eblk[21] = sep_kick != 0 ? 1.0 : 0.0;
+            eblk[22] = l_cos(sep_angle);
+            eblk[23] = l_sin(sep_angle);
+            eblk[24] = sep_angle != 0 ? 1.0 : 0.0;
+            eblk[25] = (e.l == 0) ? 1.0 : sep_kick / e.l;
+            eblk[26] = p.p0c / p.e_tot;
+            eblk[27] = mr * mr;
+          }
           if (ix_mag_max > -1) {
             flags |= F_KICKS;
             h.n_pole = (uint8_t)(ix_mag_max + 1);

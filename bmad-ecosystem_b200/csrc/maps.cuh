@@ -1131,6 +1131,59 @@ BG_COLD void exact_bend_edge(Particle& p, const double* __restrict__ xb, bool en
   p.z = v[4];
 }
 
+// track_this_elsep (track_a_thick_multipole.f90:137-240, no matrix): one step through an
+// elseparator's transverse electric field in the frame turned by the field angle; false if the
+// particle is lost (lost_pz returns it to the element's entrance coordinates, start).
+BG_COLD bool elsep_step(Particle& p, const double* __restrict__ xb, double step_len, const Particle& start,
+                        const Globals& G) {
+  const bool rot = xb[24] != 0;
+  if (rot) tilt(p, xb[22], xb[23]);
+  const double k_E = xb[25], beta_ref = xb[26];
+  const double beta = p.beta, px = p.px, py = p.py, pz = p.pz;
+  const double pc = G.p0c * (1 + pz);
+  const double E_tot = pc / beta;
+  const double E_rel = E_tot / G.p0c;
+  const double p_factor = xb[27] + px * px + py * py;
+  if (E_rel * E_rel < p_factor) {
+    p = start;
+    p.state = S_LOST_PZ;
+    return false;
+  }
+  const double ps2 = E_rel * E_rel - p_factor;
+  const double ps = sqrt(ps2);
+  const double coef = k_E * step_len / ps;
+  if (fabs(coef) > 10) {
+    p.state = S_LOST;
+    return false;
+  }
+  double sinh_k, cosh_k, cosh1_k;
+  const double c2 = coef * coef, c4 = c2 * c2;
+  if (fabs(coef) < 1e-3) {
+    const double alpha = step_len / ps;
+    sinh_k = alpha * (1 + c2 / 6 + c4 / 120);
+    cosh1_k = alpha * coef * (1.0 / 2 + c2 / 24 + c4 / 720);
+    double sh, ch;
+    m_sinhcosh(coef, sh, ch);
+    cosh_k = ch / k_E;
+  } else {
+    double sh, ch;
+    m_sinhcosh(coef, sh, ch);
+    cosh_k = ch / k_E;
+    sinh_k = sh / k_E;
+    cosh1_k = cosh_k - 1 / k_E;
+  }
+  const double dx = E_rel * cosh1_k + px * sinh_k;
+  p.x = p.x + dx;
+  p.px = k_E * (E_rel * sinh_k + px * cosh_k);
+  p.y = p.y + step_len * py / ps;
+  const double dct = E_rel * sinh_k + px * cosh1_k;
+  p.z = p.z + p.beta * (step_len / beta_ref - dct);
+  energy_kick(p, dx * k_E * G.p0c, G);
+  refresh(p, G);
+  if (rot) tilt(p, xb[22], -xb[23]);
+  return true;
+}
+
 // One edge of apply_element_edge_kick (apply_element_edge_kick.f90:37-282) for a quadrupole,
 // sextupole, octupole or thick multipole with an extra block: the beta check, the electric
 // fringe after the magnetic edge at the entrance and before it at the exit, and the hard and
@@ -1146,6 +1199,11 @@ BG_COLD void straight_edge(Particle& p, const double* __restrict__ xb, bool ente
   } else {
     if (bits & EX_SOFT) soft_quad_edge(p, xb, false);
     if (bits & EX_HARD) hard_edge(p, xb, false);
+  }
+  if (bits & EX_ESEP) {  // the elseparator's longitudinal fringe, :263-272
+    const double ff = xb[entering ? 28 : 29];
+    energy_kick(p, ff * (xb[30] * p.x + xb[31] * p.y), G);
+    refresh(p, G);
   }
   if (entering && (bits & EX_ELEC)) elec_fringe(p, xb, xb[5], G);
 }

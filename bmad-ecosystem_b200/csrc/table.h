@@ -96,13 +96,18 @@ struct ApRec {             // 112 bytes
 //           [7] mass / p0c  [8] hard-edge multipole order n (1 or 2)  [9] its strength (k1 or k2)
 //           [10] k1 [11] fq1 [12] fq2 (soft quadrupole edge)  [13] g_tot [14] beta0 (exact bend
 //           edge)  [15..17] entrance e1, fint, hgap  [18..20] exit e2, fintx, hgapx
+//           elseparator: [21] steps through the separator field (kick != 0)  [22] cos, [23] sin
+//           of the field angle atan2(vk, hk)  [24] angle != 0  [25] k_E = kick / l  [26] beta0
+//           [27] (mass / p0c)^2  [28] at_sign charge p0c / l entrance  [29] the same, exit
+//           [30] hkick [31] vkick
 //           then (b_n, a_n) for n < n_elec (r0_elec scaled). Edge bits (EdgeBit): EX_CALL the
 //           element's apply_element_edge_kick acts at this end (beta check), EX_ELEC the electric
 //           longitudinal fringe, EX_HARD hard_multipole_edge_kick, EX_SOFT
-//           soft_quadrupole_edge_kick, EX_EXACT exact_bend_edge_kick (in place of Hwang's).
+//           soft_quadrupole_edge_kick, EX_EXACT exact_bend_edge_kick (in place of Hwang's), EX_ESEP
+//           the elseparator's longitudinal fringe.
 constexpr int SB_EDGE_IN = 12, SB_EDGE_OUT = 19, SB_FIXED = 26;
-constexpr int EL_FIXED = 22, BF_FIXED = 22, BF_STEP = 16;
-enum EdgeBit { EX_CALL = 1, EX_ELEC = 2, EX_HARD = 4, EX_SOFT = 8, EX_EXACT = 16 };
+constexpr int EL_FIXED = 32, BF_FIXED = 22, BF_STEP = 16;
+enum EdgeBit { EX_CALL = 1, EX_ELEC = 2, EX_HARD = 4, EX_SOFT = 8, EX_EXACT = 16, EX_ESEP = 32 };
 enum FrameOp { FS_SUB = 1, FS_SUBZ = 2, FS_MAT = 4, FS_ADD = 8, FS_ADDZ = 16 };
 constexpr int RF_FIXED = 6;
 

@@ -53,7 +53,7 @@ enum {
   BMADGPU_RFCAVITY = 9, BMADGPU_MARKER = 14, BMADGPU_OCTUPOLE = 17, BMADGPU_MULTIPOLE = 19,
   BMADGPU_AB_MULTIPOLE = 22, BMADGPU_MONITOR = 31, BMADGPU_INSTRUMENT = 32, BMADGPU_PIPE = 44,
   BMADGPU_THICK_MULTIPOLE = 67, BMADGPU_RCOLLIMATOR = 35, BMADGPU_ECOLLIMATOR = 36,
-  BMADGPU_KICKER = 15, BMADGPU_HKICKER = 33, BMADGPU_VKICKER = 34
+  BMADGPU_KICKER = 15, BMADGPU_HKICKER = 33, BMADGPU_VKICKER = 34, BMADGPU_ELSEPARATOR = 10
 };
 /* particle states, bmad_struct.f90:525-532 */
 enum {

@@ -9,7 +9,7 @@
 // the Fortran operand order; the file is compiled with -ffp-contract=off.
 //
 // Not restated (returns BMADGPU_EUNSUPPORTED): exact_multipoles, sbend fringe_type
-// soft_edge_only / sad_full / linear_edge edges, elseparators and kickers, reversed
+// soft_edge_only / sad_full / linear_edge edges, ac_kickers, reversed
 // orientation / direction / time, absolute time tracking, radiation and spin.
 
 #include "bmad_oracle.h"
@@ -216,7 +216,7 @@ bool key_has_hkick(int key) {
   switch (key) {
     case BMADGPU_QUADRUPOLE: case BMADGPU_SBEND: case BMADGPU_SEXTUPOLE: case BMADGPU_OCTUPOLE:
     case BMADGPU_THICK_MULTIPOLE: case BMADGPU_RFCAVITY: case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT:
-    case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR: case BMADGPU_KICKER:
+    case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR: case BMADGPU_KICKER: case BMADGPU_ELSEPARATOR:
       return true;
   }
   return false;
@@ -295,7 +295,7 @@ int convert_this_ab(const Ele& ele, int p_type, const double* a_pole, const doub
     case BMADGPU_QUADRUPOLE: cnst = e->k1 * e->l; ref_exp = 1; break;
     case BMADGPU_SEXTUPOLE: cnst = e->k2 * e->l; ref_exp = 2; break;
     case BMADGPU_OCTUPOLE: cnst = e->k3 * e->l; ref_exp = 3; break;
-    case BMADGPU_KICKER:
+    case BMADGPU_KICKER: case BMADGPU_ELSEPARATOR:
       if (e->hkick == 0) cnst = e->vkick;
       else if (e->vkick == 0) cnst = e->hkick;
       else cnst = std::sqrt(e->hkick * e->hkick + e->vkick * e->vkick);
@@ -331,6 +331,7 @@ void this_ele_non_multipoles(const Ele& ele, int p_type, double a_kick[4], doubl
       b_kick[0] = -e->hkick;
       a_kick[0] = e->vkick;
       return;
+    case BMADGPU_ELSEPARATOR: return;
   }
   double hk = e->hkick, vk = e->vkick;
   if (key_has_hkick(e->key) && (hk != 0 || vk != 0)) {
@@ -1512,6 +1513,13 @@ int apply_element_edge_kick(Coord& orb, const Ele& ele, int particle_at) {
     case BMADGPU_SEXTUPOLE:
       hard_multipole_edge_kick(ele, particle_at, orb);
       break;
+    case BMADGPU_ELSEPARATOR:  // longitudinal fringe of the separator's field, :263-272
+      if (e->l != 0) {
+        const double ff = at_sign * ele.p->charge * (ele.p->p0c / e->l);
+        const double phi = ff * (e->hkick * orb.vec[0] + e->vkick * orb.vec[2]);
+        apply_energy_kick(phi, orb, ele.p);
+      }
+      break;
     case BMADGPU_SBEND: {
       // bend_edge_kick, fringe_mod.f90:40-128
       if (!fringe_here(ele, particle_at)) break;
@@ -1540,7 +1548,7 @@ int apply_element_edge_kick(Coord& orb, const Ele& ele, int particle_at) {
 bool has_fringe(const Ele& ele) {
   const bmadgpu_element* e = ele.e;
   switch (e->key) {
-    case BMADGPU_RFCAVITY: return true;
+    case BMADGPU_RFCAVITY: case BMADGPU_ELSEPARATOR: return true;
     case BMADGPU_QUADRUPOLE: case BMADGPU_SBEND: case BMADGPU_SEXTUPOLE: case BMADGPU_OCTUPOLE:
     case BMADGPU_THICK_MULTIPOLE:
       if ((e->fringe_type == BMADGPU_FRINGE_NONE || e->fringe_at == BMADGPU_NO_END) && !ele.has_elec) return false;
@@ -1616,17 +1624,76 @@ int track_a_quadrupole(Coord& orbit, const Ele& ele) {
   return 0;
 }
 
-// track_a_thick_multipole, bmad/low_level/track_a_thick_multipole.f90:18-133 (no elseparator)
+// track_this_elsep (contained in track_a_thick_multipole, track_a_thick_multipole.f90:137-240, no
+// matrix): one step through the separator's transverse electric field, in the frame turned by
+// angle_E; false if the particle was lost (on lost_pz the orbit returns to the element's start).
+bool track_this_elsep(Coord& orbit, const Coord& start_orb, const Ele& ele, double step_len, double angle_E,
+                      double k_E, double beta_ref) {
+  const bmadgpu_param* p = ele.p;
+  const double p0c = p->p0c, mc2 = p->mass;
+  tilt_coords(angle_E, orbit.vec);
+  const double beta = orbit.beta, px = orbit.vec[1], py = orbit.vec[3], pz = orbit.vec[5];
+  const double pc = p0c * (1 + pz);
+  const double E_tot = pc / beta;
+  const double E_rel = E_tot / p0c;
+  const double mr = mc2 / p0c;
+  const double p_factor = mr * mr + px * px + py * py;
+  if (E_rel * E_rel < p_factor) {
+    orbit = start_orb;
+    orbit.state = BMADGPU_LOST_PZ;
+    return false;
+  }
+  const double ps2 = E_rel * E_rel - p_factor;
+  const double ps = std::sqrt(ps2);
+  const double coef = k_E * step_len / ps;
+  if (std::fabs(coef) > 10) {
+    orbit.state = BMADGPU_LOST;
+    return false;
+  }
+  double sinh_k, cosh_k, cosh1_k;
+  const double c2 = coef * coef, c4 = c2 * c2;
+  if (std::fabs(coef) < 1e-3) {
+    const double alpha = step_len / ps;
+    sinh_k = alpha * (1 + c2 / 6 + c4 / 120);
+    cosh1_k = alpha * coef * (1.0 / 2 + c2 / 24 + c4 / 720);
+    cosh_k = lm.cosh(coef) / k_E;
+  } else {
+    cosh_k = lm.cosh(coef) / k_E;
+    sinh_k = lm.sinh(coef) / k_E;
+    cosh1_k = cosh_k - 1 / k_E;
+  }
+  const double dx = E_rel * cosh1_k + px * sinh_k;
+  orbit.vec[0] = orbit.vec[0] + dx;
+  orbit.vec[1] = k_E * (E_rel * sinh_k + px * cosh_k);
+  orbit.vec[2] = orbit.vec[2] + step_len * py / ps;
+  const double dct = E_rel * sinh_k + px * cosh1_k;
+  orbit.vec[4] = orbit.vec[4] + orbit.beta * (step_len / beta_ref - dct);
+  apply_energy_kick(dx * k_E * p0c, orbit, p);
+  tilt_coords(-angle_E, orbit.vec);
+  return true;
+}
+
+// track_a_thick_multipole, bmad/low_level/track_a_thick_multipole.f90:18-133
 int track_a_thick_multipole(Coord& orbit, const Ele& ele) {
   const bmadgpu_element* e = ele.e;
   Coord start_orb = orbit;
   double length = e->l * 1;
   double an[n_pole_maxx + 1], bn[n_pole_maxx + 1], ane[n_pole_maxx + 1], bne[n_pole_maxx + 1];
   int ix_mag_max, ix_elec_max, err;
+  // the separator's field (:49-65): strength k_E = kick / l along the angle atan2(vk, hk)
+  double kick = 0, angle_E = 0, k_E = 0, beta_ref = 0;
+  if (e->key == BMADGPU_ELSEPARATOR) {
+    const double rtc = 1.0 * (ele.p->charge < 0 ? -1.0 : 1.0);  // |rel_tracking_charge| sign_of(charge)
+    beta_ref = ele.p->p0c / ele.p->e_tot;
+    const double hk = e->hkick * rtc, vk = e->vkick * rtc;
+    kick = std::sqrt(hk * hk + vk * vk);
+    angle_E = lm.atan2(vk, hk);
+    k_E = (length == 0) ? 1.0 : kick / e->l;
+  }
   if ((err = multipole_ele_to_ab(ele, false, &ix_mag_max, an, bn, magnetic, true, nullptr))) return err;
   if ((err = multipole_ele_to_ab(ele, false, &ix_elec_max, ane, bne, electric, false, nullptr))) return err;
   int n_step;
-  if (ix_mag_max == -1 && ix_elec_max == -1) n_step = 1;
+  if (kick == 0 && ix_mag_max == -1 && ix_elec_max == -1) n_step = 1;
   else n_step = std::max(nint(std::fabs(length / ele.ds_step)), 1);
   double r_step = 1.0 / n_step;
   double step_len = length / n_step;
@@ -1642,7 +1709,11 @@ int track_a_thick_multipole(Coord& orbit, const Ele& ele) {
   if (ix_mag_max > -1) ab_multipole_kicks(an, bn, ix_mag_max, ele, orbit, magnetic, ac_amp * r_step / 2);
   if (ix_elec_max > -1) ab_multipole_kicks(ane, bne, ix_elec_max, ele, orbit, electric, ac_amp * step_len / 2);
   for (int i = 1; i <= n_step; i++) {
-    track_a_drift(orbit, step_len, ele.p);
+    if (e->key == BMADGPU_ELSEPARATOR && kick != 0) {
+      if (!track_this_elsep(orbit, start_orb, ele, step_len, angle_E, k_E, beta_ref)) return 0;
+    } else {
+      track_a_drift(orbit, step_len, ele.p);
+    }
     if (i == n_step) {
       if (ix_mag_max > -1) ab_multipole_kicks(an, bn, ix_mag_max, ele, orbit, magnetic, ac_amp * r_step / 2);
       if (ix_elec_max > -1) ab_multipole_kicks(ane, bne, ix_elec_max, ele, orbit, electric, ac_amp * step_len / 2);
@@ -2011,7 +2082,7 @@ int track1_bmad(Coord& orbit, const Ele& ele) {
     case BMADGPU_DRIFT: track_a_drift(orbit, e->l * 1, ele.p); break;
     case BMADGPU_MONITOR: case BMADGPU_INSTRUMENT: case BMADGPU_PIPE:
     case BMADGPU_RCOLLIMATOR: case BMADGPU_ECOLLIMATOR:  // track1_bmad.f90:87-88
-    case BMADGPU_KICKER: case BMADGPU_HKICKER: case BMADGPU_VKICKER:
+    case BMADGPU_KICKER: case BMADGPU_HKICKER: case BMADGPU_VKICKER: case BMADGPU_ELSEPARATOR:
     case BMADGPU_OCTUPOLE: case BMADGPU_THICK_MULTIPOLE: case BMADGPU_SEXTUPOLE:
       err = track_a_thick_multipole(orbit, ele);
       break;

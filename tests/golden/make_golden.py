@@ -65,6 +65,8 @@ TM_ELEMENTS = {
     "DRIFT1": ("DRIFT", dict(l=4.5, num_steps=10, x_offset=0.05, y_pitch=0.001, tilt=0.1), 27),
     "INSTRUMENT1": ("INSTRUMENT", dict(l=4.5, num_steps=10), 41),
     "HKICKER1": ("HKICKER", dict(l=4.5, kick=0.005, num_steps=10, x_offset=0.05, y_pitch=0.001, tilt=0.1), 40),
+    "ELSEPARATOR1": ("ELSEPARATOR", dict(l=4.5, hkick=0.005, num_steps=10, x_offset=0.05, y_pitch=0.001, tilt=0.1), 30),
+    "ELSEPARATOR2": ("ELSEPARATOR", dict(l=4.5, vkick=0.005, num_steps=10, x_offset=0.05, y_pitch=0.001, tilt=0.1), 31),
     "VKICKER1": ("VKICKER", dict(l=4.5, kick=0.005, num_steps=10, x_offset=0.05, y_pitch=0.001, tilt=0.1), 124),
     "KICKER1": ("KICKER", dict(l=4.5, b_pole={0: 0.002}, vkick=0.003, num_steps=10, x_offset=0.05, y_pitch=0.001,
                                tilt=0.1), 42),
@@ -121,6 +123,8 @@ M6_ELEMENTS = {
     "DRIFT1": ("DRIFT", dict(l=4.5, tilt=0.1, **_m_mis), 23),
     "INSTRUMENT1": ("INSTRUMENT", dict(l=4.5, num_steps=10), 34),
     "HKICKER1": ("HKICKER", dict(l=4.5, kick=0.005, tilt=0.1, **_m_mis), 33),
+    "ELSEPARATOR1": ("ELSEPARATOR", dict(l=4.5, hkick=0.005, tilt=0.1, **_m_mis), 26),
+    "ELSEPARATOR2": ("ELSEPARATOR", dict(l=4.5, vkick=0.005, tilt=0.1, **_m_mis), 27),
     "VKICKER1": ("VKICKER", dict(l=4.5, kick=0.005, tilt=0.1, **_m_mis), 125),
     "KICKER1": ("KICKER", dict(l=4.5, hkick=0.003, vkick=0.003, tilt=0.1, **_m_mis), 35),
     "ECOLLIMATOR1": ("ECOLLIMATOR", dict(l=4.5, x1_limit=0.2, x2_limit=0.2, y1_limit=0.1, y2_limit=0.1, num_steps=10,

@@ -145,3 +145,10 @@ def test_kickers_are_accepted():
     lib.lattice_check([abi.default_element(abi.HKICKER, l=0.2, kick=1e-4, tilt=0.1)], p)
     lib.lattice_check([abi.default_element(abi.VKICKER, l=0.2, kick=-1e-4)], p)
     lib.lattice_check([abi.default_element(abi.KICKER, l=0.2, hkick=1e-4, vkick=2e-4, b_pole={1: 2.0})], p)
+
+
+def test_elseparators_are_accepted():
+    """Elseparators (track_this_elsep with the longitudinal fringe) are on the device path."""
+    abi = load_abi()
+    p = abi.electron_param(3e9)
+    lib.lattice_check([abi.default_element(abi.ELSEPARATOR, l=1.0, hkick=1e-5, vkick=2e-5, tilt=0.1)], p)

@@ -200,6 +200,7 @@ def _single_element_cases():
                                   px_aperture_width2=3e-4, py_aperture_width2=2e-4, py_aperture_center=-1e-5,
                                   z_aperture_width2=5e-3, pz_aperture_width2=1.5e-3, vkick=-1e-5)],
         "monitor_kicks": [E(abi.MONITOR, l=0.2, hkick=2e-5, vkick=-1e-5, x_offset=1e-4, **ap)],
+        "elseparator_hv": [E(abi.ELSEPARATOR, l=1.0, hkick=-1e-5, vkick=2e-5, num_steps=3, y_pitch=1e-4, **ap)],
         "hkicker": [E(abi.HKICKER, l=0.3, kick=3e-5, num_steps=4, x_offset=1e-4, tilt=0.1, **ap)],
         "kicker_multipole": [E(abi.KICKER, l=0.3, hkick=1e-5, vkick=2e-5, b_pole={0: 0.2, 1: 3.0}, num_steps=3,
                                tilt=-0.05, **ap)],
