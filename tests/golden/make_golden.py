@@ -92,6 +92,13 @@ TM_ELEMENTS = {
                                        y_pitch=0.001), 64),
     "QUADRUPOLE3": ("QUADRUPOLE", dict(_q0, l=0.6, k1=1e-20, tilt=PI / 4.0, num_steps=10, x_offset=0.05,
                                        y_pitch=0.001), 65),
+    # fringe_type full: hard_multipole_edge_kick at both edges (soft edge without fq1/fq2)
+    "QUADRUPOLE4": ("QUADRUPOLE", dict(_q0, l=0.6, k1=1.0, tilt=PI / 4.0, num_steps=10, x_offset=0.05,
+                                       y_pitch=0.001, fringe_type=4), 66),
+    "QUADRUPOLE5": ("QUADRUPOLE", dict(_q0, l=0.6, k1=-1.0, tilt=PI / 4.0, num_steps=10, x_offset=0.05,
+                                       y_pitch=0.001, fringe_type=4), 67),
+    "THICK_MULTIPOLE1": ("THICK_MULTIPOLE", dict(l=4.5, a_pole={2: 1.0}, b_pole={3: 20.0}, x_offset=0.02, tilt=0.1),
+                         123),
     # sb0 (:79) with the pieces of sbend3 (:84) and sbend7 (:91): offsets, pitch and ref_tilt on a
     # bend (the bend_shift frame of offset_particle), magnetic and electric multipoles
     "SBEND3": ("SBEND", dict(_sb0, l=0.6, k1=0.3, k2=3.0, num_steps=10, x_offset=0.05, y_pitch=0.001,
