@@ -345,3 +345,19 @@ def test_ring_with_rare_forms_on_host(hc, hc_cr):
     h = host_track(hc_cr, eles, p, vec, 30)
     for k in ("vec", "beta", "state", "ix_ele", "ix_turn"):
         assert np.array_equal(h[k], o[k]), k
+
+
+def test_edge_inputs_through_rare_forms_on_host(hc):
+    """The edge inputs (beyond the aperture limits, NaN and infinite coordinates) through the ring
+    with every rare element form: the host build of the device code equals the oracle."""
+    eles, p = _rare_ring()
+    vec = _edge_bunch()
+    with np.errstate(invalid="ignore"):
+        o = oracle_track(eles, p, vec, 2)
+        h = host_track(hc, eles, p, vec, 2)
+    for k in ("vec", "beta", "state", "ix_ele", "ix_turn"):
+        a, b = h[k], o[k]
+        if a.dtype.kind == "f":
+            assert np.array_equal(np.isnan(a), np.isnan(b)), k
+            a, b = a[~np.isnan(a)], b[~np.isnan(b)]
+        assert np.array_equal(a, b), k
