@@ -4,7 +4,7 @@
  * A scalar C++ restatement of Bmad's bmad_standard single-particle tracking
  * (bmad/code/track1.f90 -> bmad/low_level/track1_bmad.f90 -> track_a_*) and of the OpenMP
  * bunch loop (bmad/multiparticle/beam_utils.f90:81-86). Only tests/, __graft_entry__.smoke()
- * and bench.py's CPU-baseline leg may load it, and only as the checker.
+ * and bench.py's CPU-baseline leg may load it, and only to check the device results.
  *
  * Parity pinning: the element maps are checked against the Bmad_Standard golden lines of
  * regression_tests/tracking_method_test/output.correct and against

@@ -1,4 +1,4 @@
-"""numpy restatement of the long-term-tracking bunch data (test infrastructure, the checker):
+"""numpy restatement of the long-term-tracking bunch data (test infrastructure, for checking the device path):
 
   ltt_calc_bunch_data            bsim/modules/lt_tracking_mod.f90:2369-2421
   calc_bunch_params              bmad/multiparticle/beam_utils.f90:1326-1431

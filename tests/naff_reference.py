@@ -1,4 +1,4 @@
-"""numpy restatement of NAFF (test infrastructure, the checker): sim_utils/math/naff.f90:72-131
+"""numpy restatement of NAFF (test infrastructure, for checking the device path): sim_utils/math/naff.f90:72-131
 (naff), :140-150 (projdd, ed), :160-205 (maximize_projection with a Hanning window), :230-290
 (interpolated_fft_gsl: Gaussian window r = 8, FFT backward, log-parabola peak interpolation).
 

@@ -1,4 +1,4 @@
-"""numpy restatement of the optics set-up before tracking (test infrastructure, the checker):
+"""numpy restatement of the optics set-up before tracking (test infrastructure, for checking the device path):
 
   closed_orbit_calc          bmad/code/closed_orbit_calc.f90:192-862: the fixed point of the
                              one-turn map, here Newton's method on the ORACLE's tracking

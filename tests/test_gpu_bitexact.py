@@ -2,8 +2,8 @@
 rounded transcendentals (libbmadgpu_cr.so) against the CPU oracle run with a correctly rounded
 libm.
 
-The device maps keep the reference's operation order (no FMA contraction); in this build they
-call correctly rounded sin, cos, asin, atan2, sinh and cosh (csrc/crmath.cuh), and the element
+The device maps keep the reference's operation order (no FMA contraction); in that library they
+call correctly rounded sin, cos, asin, atan2, sinh, cosh, exp and tan (csrc/crmath.cuh), and the element
 invariants are packed with the same functions. The oracle -- the restatement of the reference's Fortran --
 takes its libm functions from oracle_set_libm; installed with the same correctly rounded set
 (checked against mpmath and against libquadmath on the CPU), it is the reference's algorithm
