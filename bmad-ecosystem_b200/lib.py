@@ -818,6 +818,30 @@ def beam_read(path, param):
     return b
 
 
+def beam_write_hdf5(path, bunch, param, s_position=0.0, flags=0):
+    """Bmad openPMD beam file (HDF5) of a HostBunch, as hdf5_write_beam lays it out."""
+    lib = load()
+    lib.bmadgpu_beam_write_hdf5.argtypes = [C.c_char_p, C.POINTER(abi.Bunch), C.POINTER(abi.Param), C.c_double,
+                                            C.c_int32]
+    v = bunch.view()
+    check_host(lib.bmadgpu_beam_write_hdf5(path.encode(), C.byref(v), C.byref(param), s_position, flags))
+
+
+def beam_read_hdf5(path, param, ix_bunch=0):
+    """(HostBunch of bunch ix_bunch, number of bunches) from a Bmad openPMD beam file, as
+    hdf5_read_beam reads it without an element."""
+    lib = load()
+    lib.bmadgpu_beam_read_hdf5.argtypes = [C.c_char_p, C.POINTER(abi.Param), C.c_int32, C.POINTER(abi.Bunch),
+                                           C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+    n, nb = C.c_int64(), C.c_int32()
+    check_host(lib.bmadgpu_beam_read_hdf5(path.encode(), C.byref(param), ix_bunch, None, C.byref(n), C.byref(nb)))
+    b = HostBunch(np.zeros((6, n.value)), np.zeros(n.value), t=np.zeros(n.value))
+    v = b.view()
+    check_host(lib.bmadgpu_beam_read_hdf5(path.encode(), C.byref(param), ix_bunch, C.byref(v), C.byref(n),
+                                          C.byref(nb)))
+    return b, nb.value
+
+
 def check_host(code):
     """Status check for the host-only calls (they set no last-error message)."""
     if code != 0:

@@ -659,6 +659,25 @@ int bmadgpu_beam_write_ascii(const char* path, const bmadgpu_bunch* host_bunch, 
 int bmadgpu_beam_read_ascii(const char* path, const bmadgpu_param* param, bmadgpu_bunch* host_bunch,
                             int64_t* n_particle);
 
+/* Bmad's openPMD beam file in HDF5 (hdf5_write_beam, bmad/hdf5/hdf5_write_beam.f90:20-245), written
+ * without the HDF5 library in the classic file structures libhdf5 writes by default. One bunch as
+ * /data/00001/particles/<species>/; records whose values are all equal become constant record
+ * components, as in the reference. flags: ALIVE_ONLY; APPEND gives BMADGPU_EUNSUPPORTED. The
+ * species name comes from param's mass and charge (electron, positron, proton, anti-proton;
+ * other species give BMADGPU_EUNSUPPORTED). Spin and macro-charge are written as 0. */
+int bmadgpu_beam_write_hdf5(const char* path, const bmadgpu_bunch* host_bunch, const bmadgpu_param* param,
+                            double s_position, int32_t flags);
+/* hdf5_read_beam (bmad/hdf5/hdf5_read_beam.f90:24-474) without an element: bunch ix_bunch
+ * (0-based, in the order of the bunch groups' names) of a file written by Bmad or by the call above,
+ * the old layout (records directly in particles/) included. *n_bunch (nullable) is set to the
+ * number of bunches and *n_particle to the bunch's size; with host_bunch NULL or host_bunch->vec
+ * NULL nothing else is read, otherwise host_bunch->n must equal *n_particle. beta comes from the
+ * momentum and param's mass. Files using HDF5 structures outside the classic set (superblock
+ * version 2 or 3, version-2 object headers, link messages, chunked or filtered storage) and photon
+ * bunches give BMADGPU_EUNSUPPORTED. */
+int bmadgpu_beam_read_hdf5(const char* path, const bmadgpu_param* param, int32_t ix_bunch,
+                           bmadgpu_bunch* host_bunch, int64_t* n_particle, int32_t* n_bunch);
+
 /* Page-locked host memory for bunch arrays (cudaHostAlloc / cudaFreeHost). */
 int bmadgpu_host_alloc(int64_t bytes, void** ptr);
 int bmadgpu_host_free(void* ptr);

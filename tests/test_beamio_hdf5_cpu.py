@@ -1,0 +1,134 @@
+"""HDF5 (openPMD) beam files (bmadgpu_beam_read_hdf5 / bmadgpu_beam_write_hdf5), host-only, on CPU.
+
+Pinned to the reference's hdf5_test (regression_tests/hdf5_test): its old-layout beam file
+bunch_old.h5 (committed as tests/golden/hdf5_test_bunch_old.h5) holds the ten particles of
+beam_1.dat (tests/golden/hdf5_test_beam_1.dat) as bunch 1 and a photon bunch as bunch 2; the test
+checks that reading the file gives back the particles of the ASCII beam ("Old-Bunch1" TTTTTTTTTT,
+output.correct:11) and prints particle 7 of that beam (output.correct:2-5)."""
+import importlib
+import os
+
+import numpy as np
+import pytest
+
+lib = importlib.import_module("bmad-ecosystem_b200.lib")
+abi = importlib.import_module("bmad-ecosystem_b200.abi")
+rings = importlib.import_module("bmad-ecosystem_b200.rings")
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+OLD_H5 = os.path.join(GOLDEN, "hdf5_test_bunch_old.h5")
+BEAM_1 = os.path.join(GOLDEN, "hdf5_test_beam_1.dat")
+
+# regression_tests/hdf5_test/output.correct:2-5 (particle 7 of bunch 1, REL 1e-10)
+P7_VEC = [1.6387488057E-03, -2.9985054496E-06, 1.8144481648E-03, -7.8926417700E-05, -1.5942344121E-04,
+          5.2241291487E-04]
+P7_T, P7_P0C, P7_BETA = 5.3177942856E-13, 9.9999986944E+08, 9.9999986958E-01
+
+
+def positron_1gev():
+    """lat.bmad of hdf5_test: positron (Bmad's default species), beginning e_tot = 1e9."""
+    p = abi.Param()
+    p.mass, p.charge, p.e_tot = 0.51099895069e6, 1.0, 1e9
+    p.p0c = (p.e_tot ** 2 - p.mass ** 2) ** 0.5
+    return p
+
+
+def rel(a, b):
+    return abs(a - b) / abs(b)
+
+
+def test_old_layout_particle_7_matches_reference_output():
+    p = positron_1gev()
+    assert rel(p.p0c, P7_P0C) < 1e-10
+    b, n_bunch = lib.beam_read_hdf5(OLD_H5, p, 0)
+    assert n_bunch == 2 and b.vec.shape == (6, 10)
+    for i in range(6):
+        assert rel(b.vec[i, 6], P7_VEC[i]) < 1e-10, i
+    assert rel(b.t[6], P7_T) < 1e-10
+    assert rel(b.beta[6], P7_BETA) < 1e-10
+    # output.correct:5: state alive, location downstream_end
+    assert b.state[6] == abi.ALIVE and b.location[6] == abi.DOWNSTREAM_END
+
+
+def test_old_layout_bunch_equals_ascii_beam():
+    """The reference's Old-Bunch1 check: the HDF5 bunch equals the ASCII beam particle for particle."""
+    p = positron_1gev()
+    b, _ = lib.beam_read_hdf5(OLD_H5, p, 0)
+    a = lib.beam_read(BEAM_1, p)
+    assert np.allclose(b.vec, a.vec, rtol=1e-12, atol=1e-18)
+    assert np.array_equal(b.state, a.state)
+
+
+def test_photon_bunch_and_bad_index_are_refused():
+    p = positron_1gev()
+    with pytest.raises(lib.BmadGpuError) as e:
+        lib.beam_read_hdf5(OLD_H5, p, 1)          # bunch 2 of the file is a photon bunch
+    assert e.value.code == abi.EUNSUPPORTED
+    with pytest.raises(lib.BmadGpuError) as e:
+        lib.beam_read_hdf5(OLD_H5, p, 2)
+    assert e.value.code == abi.EINVAL
+
+
+def sample(n=300, seed=3):
+    eles, p = rings.ring(10)
+    rng = np.random.default_rng(seed)
+    b = lib.HostBunch.from_vec(rings.matched_gaussian(eles, n, seed=seed), p, t=rng.normal(0, 1e-9, n))
+    b.state[[3, 10, 11]] = [abi.LOST_POS_X, abi.LOST_NEG_Y, abi.LOST_PZ]
+    b.ix_ele[[3, 10, 11]] = [17, 0, 35]
+    b.location[:] = abi.DOWNSTREAM_END
+    b.location[[3, 10, 11]] = [abi.DOWNSTREAM_END, abi.UPSTREAM_END, abi.INSIDE]
+    return b, p
+
+
+def test_round_trip(tmp_path):
+    b, p = sample()
+    path = str(tmp_path / "beam.h5")
+    lib.beam_write_hdf5(path, b, p, s_position=12.5)
+    r, n_bunch = lib.beam_read_hdf5(path, p)
+    assert n_bunch == 1
+    # px, py and z pass through px * p0c, py * p0c and t - t_ref as in the reference's file
+    assert np.allclose(r.vec, b.vec, rtol=4e-16, atol=1e-300)
+    assert np.array_equal(r.beta, b.beta)
+    assert np.allclose(r.t, b.t, rtol=4e-16, atol=1e-300)
+    lost = b.state != abi.ALIVE
+    assert np.array_equal(r.state, b.state)
+    assert np.array_equal(r.ix_ele[lost], b.ix_ele[lost])
+    assert np.array_equal(r.location, b.location)
+
+
+def test_alive_only_and_constant_records(tmp_path):
+    b, p = sample()
+    path = str(tmp_path / "alive.h5")
+    lib.beam_write_hdf5(path, b, p, flags=lib.BEAM_ALIVE_ONLY)
+    r, _ = lib.beam_read_hdf5(path, p)
+    alive = b.state == abi.ALIVE
+    assert r.vec.shape[1] == alive.sum()
+    assert np.all(r.state == abi.ALIVE)            # particleStatus all equal: a constant record
+    assert np.allclose(r.vec, b.vec[:, alive], rtol=4e-16, atol=1e-300)
+    # a bunch with one particle: every record is a constant record component
+    one = lib.HostBunch.from_vec(b.vec[:, :1].copy(), p, t=b.t[:1].copy())
+    lib.beam_write_hdf5(path, one, p)
+    r1, _ = lib.beam_read_hdf5(path, p)
+    assert np.allclose(r1.vec, one.vec, rtol=4e-16, atol=1e-300)
+
+
+def test_append_and_unknown_species_are_refused(tmp_path):
+    b, p = sample(20)
+    path = str(tmp_path / "x.h5")
+    with pytest.raises(lib.BmadGpuError) as e:
+        lib.beam_write_hdf5(path, b, p, flags=lib.BEAM_APPEND)
+    assert e.value.code == abi.EUNSUPPORTED
+    q = abi.Param()
+    q.p0c, q.e_tot, q.mass, q.charge = p.p0c, p.e_tot, 105.6583755e6, -1.0     # a muon
+    with pytest.raises(lib.BmadGpuError) as e:
+        lib.beam_write_hdf5(path, b, q)
+    assert e.value.code == abi.EUNSUPPORTED
+
+
+def test_truncated_file_is_an_error(tmp_path):
+    data = open(OLD_H5, "rb").read()
+    path = str(tmp_path / "cut.h5")
+    for cut in (50, 4000, len(data) // 2):
+        open(path, "wb").write(data[:cut])
+        with pytest.raises(lib.BmadGpuError):
+            lib.beam_read_hdf5(path, positron_1gev(), 0)
