@@ -430,10 +430,12 @@ int read_hdf5(const char* path, const bmadgpu_param* param, int32_t ix_bunch, bm
   const bool have_loc = read_int_record(r, species, "locationInElement", n, loc);
 
   for (int64_t j = 0; j < n; j++) {
-    const double pc0 = p0c[j];
+    // a particle without a reference momentum in the file takes the lattice's, as the reference's
+    // reader does when it is given the element (p0c_initial = ele%value(p0c$))
+    const double pc0 = p0c[j] != 0 ? p0c[j] : param->p0c;
     if (pc0 == 0) return BMADGPU_EINVAL;                       // reference momentum not present
     int st = have_state ? (int)state[j] : 1;
-    if (st != 1 && st != 13 && software != "Bmad") st = 2;    // pre_born$ = 13; others lost$ (non-Bmad files)
+    if (st != 1 && st != 0 && software != "Bmad") st = 2;     // alive$, pre_born$ = 0 kept; others lost$ (non-Bmad files)
     double pz;
     if (!have_tot)
       pz = (std::sqrt(v[1][j] * v[1][j] + v[3][j] * v[3][j] + v[5][j] * v[5][j]) - pc0) / pc0;
@@ -844,4 +846,26 @@ extern "C" int bmadgpu_beam_read_hdf5(const char* path, const bmadgpu_param* par
   } catch (const Err& e) {
     return e.code;
   }
+}
+
+// write_beam_file / read_beam_file (bmad/multiparticle/beam_file_io.f90:29-106, 380-420): the file
+// name picks the format, HDF5 for names ending in ".h5" or ".hdf5", else Bmad's ASCII layout.
+static bool is_hdf5_name(const char* path) {
+  const size_t n = std::strlen(path);
+  return (n > 3 && std::strcmp(path + n - 3, ".h5") == 0) || (n > 5 && std::strcmp(path + n - 5, ".hdf5") == 0);
+}
+
+extern "C" int bmadgpu_beam_write_file(const char* path, const bmadgpu_bunch* host_bunch, const bmadgpu_param* param,
+                                       double s_position, int32_t flags) {
+  if (!path) return BMADGPU_EINVAL;
+  if (is_hdf5_name(path))   // doubles are stored as they are: BMADGPU_BEAM_EXACT has nothing to add
+    return bmadgpu_beam_write_hdf5(path, host_bunch, param, s_position, flags & ~BMADGPU_BEAM_EXACT);
+  return bmadgpu_beam_write_ascii(path, host_bunch, param, s_position, flags);
+}
+
+extern "C" int bmadgpu_beam_read_file(const char* path, const bmadgpu_param* param, bmadgpu_bunch* host_bunch,
+                                      int64_t* n_particle) {
+  if (!path) return BMADGPU_EINVAL;
+  if (is_hdf5_name(path)) return bmadgpu_beam_read_hdf5(path, param, 0, host_bunch, n_particle, nullptr);
+  return bmadgpu_beam_read_ascii(path, param, host_bunch, n_particle);
 }

@@ -1008,7 +1008,7 @@ extern "C" int bmadgpu_ltt_run(bmadgpu_ctx* c, const bmadgpu_lattice* lat, bmadg
     std::string name;
     const size_t dot = beam_base.find_last_of('.');
     name = dot == std::string::npos ? beam_base + "-" + num : beam_base.substr(0, dot) + "-" + num + beam_base.substr(dot);
-    if (bmadgpu_beam_write_ascii(name.c_str(), &h, &lat->param, 0.0, P->beam_exact ? BMADGPU_BEAM_EXACT : 0))
+    if (bmadgpu_beam_write_file(name.c_str(), &h, &lat->param, 0.0, P->beam_exact ? BMADGPU_BEAM_EXACT : 0))
       return fail(BMADGPU_EINVAL, "cannot write the beam file " + name);
     return BMADGPU_OK;
   };

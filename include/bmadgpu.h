@@ -677,6 +677,13 @@ int bmadgpu_beam_write_hdf5(const char* path, const bmadgpu_bunch* host_bunch, c
  * bunches give BMADGPU_EUNSUPPORTED. */
 int bmadgpu_beam_read_hdf5(const char* path, const bmadgpu_param* param, int32_t ix_bunch,
                            bmadgpu_bunch* host_bunch, int64_t* n_particle, int32_t* n_bunch);
+/* write_beam_file / read_beam_file (bmad/multiparticle/beam_file_io.f90:29-106, 380-420): HDF5
+ * (the two calls above; the first bunch on reading) when the name ends in ".h5" or ".hdf5", else
+ * the ASCII calls. The long-term-tracking beam files go through the writer. */
+int bmadgpu_beam_write_file(const char* path, const bmadgpu_bunch* host_bunch, const bmadgpu_param* param,
+                            double s_position, int32_t flags);
+int bmadgpu_beam_read_file(const char* path, const bmadgpu_param* param, bmadgpu_bunch* host_bunch,
+                           int64_t* n_particle);
 
 /* Page-locked host memory for bunch arrays (cudaHostAlloc / cudaFreeHost). */
 int bmadgpu_host_alloc(int64_t bytes, void** ptr);

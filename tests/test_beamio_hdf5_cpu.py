@@ -132,3 +132,75 @@ def test_truncated_file_is_an_error(tmp_path):
         open(path, "wb").write(data[:cut])
         with pytest.raises(lib.BmadGpuError):
             lib.beam_read_hdf5(path, positron_1gev(), 0)
+
+
+def test_file_name_picks_the_format(tmp_path):
+    """write_beam_file / read_beam_file: HDF5 for .h5 and .hdf5 names, ASCII otherwise."""
+    import ctypes as C
+    so = lib.load()
+    so.bmadgpu_beam_write_file.argtypes = [C.c_char_p, C.POINTER(abi.Bunch), C.POINTER(abi.Param), C.c_double,
+                                           C.c_int32]
+    so.bmadgpu_beam_read_file.argtypes = [C.c_char_p, C.POINTER(abi.Param), C.POINTER(abi.Bunch),
+                                          C.POINTER(C.c_int64)]
+    b, p = sample(50)
+    v = b.view()
+    for name, hdf5 in (("a.h5", True), ("a.hdf5", True), ("a.dat", False), ("a_h5", False)):
+        path = str(tmp_path / name)
+        assert so.bmadgpu_beam_write_file(path.encode(), C.byref(v), C.byref(p), 0.0, lib.BEAM_EXACT) == 0
+        head = open(path, "rb").read(8)
+        assert (head == b"\x89HDF\r\n\x1a\n") == hdf5, name
+        n = C.c_int64()
+        assert so.bmadgpu_beam_read_file(path.encode(), C.byref(p), None, C.byref(n)) == 0 and n.value == 50
+        r = lib.HostBunch(np.zeros((6, 50)), np.zeros(50), t=np.zeros(50))
+        rv = r.view()
+        assert so.bmadgpu_beam_read_file(path.encode(), C.byref(p), C.byref(rv), C.byref(n)) == 0
+        assert np.allclose(r.vec, b.vec, rtol=4e-16, atol=1e-300), name
+        assert np.array_equal(r.state, b.state), name
+
+
+def test_writer_uses_the_encodings_of_the_reference_file(tmp_path):
+    """The writer's superblock fields, datatypes, dataspaces and fill-value message are byte for byte
+    those libhdf5 wrote into the reference's bunch_old.h5 (independent of this library's reader)."""
+    ref = open(OLD_H5, "rb").read()
+    eles, p = rings.ring(10)
+    b = lib.HostBunch.from_vec(rings.matched_gaussian(eles, 10, seed=1), p, t=np.zeros(10))
+    path = str(tmp_path / "enc.h5")
+    lib.beam_write_hdf5(path, b, p)
+    ours = open(path, "rb").read()
+    assert ours[:24] == ref[:24]                                    # signature, versions, sizes, K values
+    pieces = [
+        "11203f000800000000004000340b0034ff030000",                # IEEE f64 little-endian
+        "100800000400000000002000",                                # signed i32 little-endian
+        "0202020100000000",                                        # fill value message
+        "0100000000000000",                                        # scalar dataspace (string attributes)
+        "01010100000000000a000000000000000a00000000000000",        # 1-D dataspace of 10 with max 10
+        "13000000",                                                # fixed-length null-terminated string
+    ]
+    for h in pieces:
+        assert bytes.fromhex(h) in ref and bytes.fromhex(h) in ours, h
+    for sig in (b"TREE", b"HEAP", b"SNOD"):
+        assert sig in ours
+
+
+def test_files_of_other_openpmd_writers():
+    """Two more of the reference's particle files, written by another openPMD writer (null-padded
+    strings, 64-bit integer attributes, basePath "/" without %T, particlesPath "." or "particles/",
+    no totalMomentumOffset): regression_tests/pytao/sr_wakes/particles3.h5 (3 positrons, read by
+    tao.startup with the lattice's e_tot = 10e6) and regression_tests/space_charge_test/
+    initial_particles.h5 (10 electrons before cathode emission)."""
+    p = abi.Param()
+    p.mass, p.charge, p.e_tot = 0.51099895069e6, 1.0, 10e6
+    p.p0c = (p.e_tot ** 2 - p.mass ** 2) ** 0.5
+    b, n_bunch = lib.beam_read_hdf5(os.path.join(GOLDEN, "sr_wakes_particles3.h5"), p)
+    assert n_bunch == 1 and b.vec.shape == (6, 3)
+    assert np.all(b.state == abi.ALIVE)
+    # no reference momentum in the file: pz relative to the lattice's p0c (sig_pz ~ 6e-3 in tao.startup)
+    assert np.all(np.abs(b.vec[5]) < 0.05)
+    pc = p.p0c * (1 + b.vec[5])
+    assert np.allclose(b.beta, pc / np.sqrt(pc * pc + p.mass ** 2), rtol=1e-15)
+    # no timeOffset record: t = time and z = -beta c time
+    assert np.array_equal(b.vec[4], -b.beta * 2.99792458e8 * b.t)
+    p.charge = -1.0
+    g, _ = lib.beam_read_hdf5(os.path.join(GOLDEN, "space_charge_initial_particles.h5"), p)
+    assert g.vec.shape == (6, 10)
+    assert np.all(g.state == 0)                     # pre_born$ (openPMD status 0) is kept
