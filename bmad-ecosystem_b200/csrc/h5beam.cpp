@@ -733,12 +733,10 @@ const char* species_name(const bmadgpu_param* p) {
   return nullptr;
 }
 
-int write_hdf5(const char* path, const bmadgpu_bunch* b, const bmadgpu_param* param, double s_position,
-               int32_t flags) {
-  if (flags & BMADGPU_BEAM_APPEND) return BMADGPU_EUNSUPPORTED;
-  const char* species = species_name(param);
-  if (!species) return BMADGPU_EUNSUPPORTED;
-  const bool alive_only = (flags & BMADGPU_BEAM_ALIVE_ONLY) != 0;
+// One bunch group "/data/<ib, i5.5>/particles/<species>/" with its records (hdf5_write_beam.f90:95-240).
+int add_bunch(Writer& w, int data, int ib, const bmadgpu_bunch* b, const bmadgpu_param* param, const char* species,
+              double s_position, bool alive_only) {
+  if (!b || b->n < 0 || !b->vec || !b->beta || !b->state) return BMADGPU_EINVAL;
   std::vector<int64_t> idx;
   for (int64_t j = 0; j < b->n; j++)
     if (!alive_only || b->state[j] == 1) idx.push_back(j);
@@ -756,16 +754,9 @@ int write_hdf5(const char* path, const bmadgpu_bunch* b, const bmadgpu_param* pa
   const Unit uev{"eV/c", kECharge / kCLight, {1, 1, -1, 0, 0, 0, 0}};
   const Unit uhbar{"hbar", kECharge * kHbar, {2, 1, -1, 0, 0, 0, 0}};
 
-  Writer w;
-  w.attr_str(0, "dataType", "openPMD");
-  w.attr_str(0, "openPMD", "2.0.0");
-  w.attr_str(0, "openPMDextension", "BeamPhysics;SpeciesType");
-  w.attr_str(0, "basePath", "/data/%T/");
-  w.attr_str(0, "particlesPath", "particles/");
-  w.attr_str(0, "software", "Bmad");
-  w.attr_str(0, "softwareVersion", "1.0");
-  const int data = w.add(0, "data", true);
-  const int bunch = w.add(data, "00001", true);
+  char bunch_name[16];
+  std::snprintf(bunch_name, sizeof bunch_name, "%05d", ib + 1);
+  const int bunch = w.add(data, bunch_name, true);
   const int parts = w.add(bunch, "particles", true);
   const int sp = w.add(parts, species, true);
   w.attr_str(sp, "speciesType", species);
@@ -817,6 +808,29 @@ int write_hdf5(const char* path, const bmadgpu_bunch* b, const bmadgpu_param* pa
   int_record(w, sp, "branchIndex", "ix_branch", u1, br);
   int_record(w, sp, "elementIndex", "ix_ele", u1, el);
   int_record(w, sp, "locationInElement", "location", u1, lc);
+  return BMADGPU_OK;
+}
+
+int write_hdf5(const char* path, const bmadgpu_bunch* bunches, int32_t n_bunch, const bmadgpu_param* param,
+               double s_position, int32_t flags) {
+  if (flags & BMADGPU_BEAM_APPEND) return BMADGPU_EUNSUPPORTED;
+  if (n_bunch < 1 || n_bunch > 2 * Writer::kLeafK * 2 * Writer::kNodeK) return BMADGPU_EINVAL;
+  const char* species = species_name(param);
+  if (!species) return BMADGPU_EUNSUPPORTED;
+  Writer w;
+  w.attr_str(0, "dataType", "openPMD");
+  w.attr_str(0, "openPMD", "2.0.0");
+  w.attr_str(0, "openPMDextension", "BeamPhysics;SpeciesType");
+  w.attr_str(0, "basePath", "/data/%T/");
+  w.attr_str(0, "particlesPath", "particles/");
+  w.attr_str(0, "software", "Bmad");
+  w.attr_str(0, "softwareVersion", "1.0");
+  const int data = w.add(0, "data", true);
+  for (int32_t ib = 0; ib < n_bunch; ib++) {
+    const int r = add_bunch(w, data, ib, &bunches[ib], param, species, s_position,
+                            (flags & BMADGPU_BEAM_ALIVE_ONLY) != 0);
+    if (r) return r;
+  }
 
   const std::vector<uint8_t> bytes = w.finish();
   FILE* f = std::fopen(path, "wb");
@@ -829,10 +843,19 @@ int write_hdf5(const char* path, const bmadgpu_bunch* b, const bmadgpu_param* pa
 
 extern "C" int bmadgpu_beam_write_hdf5(const char* path, const bmadgpu_bunch* host_bunch, const bmadgpu_param* param,
                                        double s_position, int32_t flags) {
-  if (!path || !host_bunch || !param || !host_bunch->vec || !host_bunch->beta || !host_bunch->state)
-    return BMADGPU_EINVAL;
+  if (!path || !host_bunch || !param) return BMADGPU_EINVAL;
   try {
-    return write_hdf5(path, host_bunch, param, s_position, flags);
+    return write_hdf5(path, host_bunch, 1, param, s_position, flags);
+  } catch (const Err& e) {
+    return e.code;
+  }
+}
+
+extern "C" int bmadgpu_beam_write_hdf5_bunches(const char* path, const bmadgpu_bunch* host_bunches, int32_t n_bunch,
+                                               const bmadgpu_param* param, double s_position, int32_t flags) {
+  if (!path || !host_bunches || !param) return BMADGPU_EINVAL;
+  try {
+    return write_hdf5(path, host_bunches, n_bunch, param, s_position, flags);
   } catch (const Err& e) {
     return e.code;
   }

@@ -819,8 +819,16 @@ def beam_read(path, param):
 
 
 def beam_write_hdf5(path, bunch, param, s_position=0.0, flags=0):
-    """Bmad openPMD beam file (HDF5) of a HostBunch, as hdf5_write_beam lays it out."""
+    """Bmad openPMD beam file (HDF5) of a HostBunch, or of a list of them (one bunch group each), as
+    hdf5_write_beam lays it out."""
     lib = load()
+    if isinstance(bunch, (list, tuple)):
+        lib.bmadgpu_beam_write_hdf5_bunches.argtypes = [C.c_char_p, C.POINTER(abi.Bunch), C.c_int32,
+                                                        C.POINTER(abi.Param), C.c_double, C.c_int32]
+        views = (abi.Bunch * len(bunch))(*[b.view() for b in bunch])
+        check_host(lib.bmadgpu_beam_write_hdf5_bunches(path.encode(), views, len(bunch), C.byref(param), s_position,
+                                                       flags))
+        return
     lib.bmadgpu_beam_write_hdf5.argtypes = [C.c_char_p, C.POINTER(abi.Bunch), C.POINTER(abi.Param), C.c_double,
                                             C.c_int32]
     v = bunch.view()

@@ -667,6 +667,10 @@ int bmadgpu_beam_read_ascii(const char* path, const bmadgpu_param* param, bmadgp
  * other species give BMADGPU_EUNSUPPORTED). Spin and macro-charge are written as 0. */
 int bmadgpu_beam_write_hdf5(const char* path, const bmadgpu_bunch* host_bunch, const bmadgpu_param* param,
                             double s_position, int32_t flags);
+/* The same for n_bunch bunches (1 to 256) of one species in one file, /data/00001/ to /data/<n>/,
+ * as hdf5_write_beam writes bunches(:). */
+int bmadgpu_beam_write_hdf5_bunches(const char* path, const bmadgpu_bunch* host_bunches, int32_t n_bunch,
+                                    const bmadgpu_param* param, double s_position, int32_t flags);
 /* hdf5_read_beam (bmad/hdf5/hdf5_read_beam.f90:24-474) without an element: bunch ix_bunch
  * (0-based, in the order of the bunch groups' names) of a file written by Bmad or by the call above,
  * the old layout (records directly in particles/) included. *n_bunch (nullable) is set to the

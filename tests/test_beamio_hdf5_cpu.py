@@ -204,3 +204,31 @@ def test_files_of_other_openpmd_writers():
     g, _ = lib.beam_read_hdf5(os.path.join(GOLDEN, "space_charge_initial_particles.h5"), p)
     assert g.vec.shape == (6, 10)
     assert np.all(g.state == 0)                     # pre_born$ (openPMD status 0) is kept
+
+
+def test_several_bunches_in_one_file(tmp_path):
+    """hdf5_write_beam's bunches(:): one group per bunch, /data/00001/ ... ; each read back by index."""
+    eles, p = rings.ring(10)
+    bunches = []
+    for k, n in enumerate((7, 1, 40)):
+        b = lib.HostBunch.from_vec(rings.matched_gaussian(eles, n, seed=10 + k), p, t=np.full(n, 1e-9 * k))
+        bunches.append(b)
+    bunches[2].state[5] = abi.LOST_NEG_X
+    bunches[2].ix_ele[5] = 12
+    bunches[2].location[:] = abi.DOWNSTREAM_END
+    path = str(tmp_path / "three.h5")
+    lib.beam_write_hdf5(path, bunches, p)
+    for k, b in enumerate(bunches):
+        r, n_bunch = lib.beam_read_hdf5(path, p, k)
+        assert n_bunch == 3 and r.vec.shape == b.vec.shape
+        assert np.allclose(r.vec, b.vec, rtol=4e-16, atol=1e-300)
+        assert np.array_equal(r.state, b.state)
+    r, _ = lib.beam_read_hdf5(path, p, 2)
+    assert r.ix_ele[5] == 12
+    # many bunches: the data group's names span several symbol-table nodes
+    many = [bunches[1]] * 20
+    lib.beam_write_hdf5(path, many, p)
+    r, n_bunch = lib.beam_read_hdf5(path, p, 19)
+    assert n_bunch == 20 and np.allclose(r.vec, bunches[1].vec, rtol=4e-16, atol=1e-300)
+    with pytest.raises(lib.BmadGpuError):
+        lib.beam_write_hdf5(path, [bunches[1]] * 257, p)
