@@ -110,16 +110,20 @@ class Reader {
     return t;
   }
 
-  // Dataspace message (versions 1 and 2): number of elements.
-  static uint64_t parse_space(const uint8_t* p) {
+  // Dataspace message (versions 1 and 2) of len bytes: number of elements.
+  static uint64_t parse_space(const uint8_t* p, uint64_t len) {
+    if (len < 4) throw Err{BMADGPU_EINVAL};
     const int ver = p[0], rank = p[1];
+    if (ver != 1 && ver != 2) throw Err{BMADGPU_EUNSUPPORTED};
     if (ver == 2 && p[3] == 2) return 0;               // null dataspace
-    const uint8_t* dims = p + (ver == 1 ? 8 : 4);
+    const uint64_t head = ver == 1 ? 8 : 4;
+    if (head + 8 * (uint64_t)rank > len) throw Err{BMADGPU_EINVAL};
+    const uint8_t* dims = p + head;
     uint64_t n = 1;
     for (int i = 0; i < rank; i++) {
       uint64_t v = 0;
       for (int b = 7; b >= 0; b--) v = (v << 8) | dims[8 * i + b];
-      n *= v;
+      if (__builtin_mul_overflow(n, v, &n)) throw Err{BMADGPU_EINVAL};
     }
     return n;
   }
@@ -141,9 +145,13 @@ class Reader {
         const uint8_t* b = at(body, size);
         seen++;
         switch (type) {
-          case 0x01: o.count = parse_space(b); break;
-          case 0x03: o.type = parse_type(b); break;
+          case 0x01: o.count = parse_space(b, size); break;
+          case 0x03:
+            if (size < 8) throw Err{BMADGPU_EINVAL};
+            o.type = parse_type(b);
+            break;
           case 0x08: {
+            if (size < 4) throw Err{BMADGPU_EINVAL};
             if (b[0] != 3) throw Err{BMADGPU_EUNSUPPORTED};
             o.is_dataset = true;
             if (b[1] == 0) {
@@ -184,11 +192,14 @@ class Reader {
     Attr a;
     a.type = parse_type(q);
     q += pad(tl);
-    a.count = parse_space(q);
+    a.count = parse_space(q, sl);
     q += pad(sl);
     a.data = q;
-    if (q > b + size || a.count * (uint64_t)a.type.size > (uint64_t)(b + size - q)) throw Err{BMADGPU_EINVAL};
-    o.attrs[name] = a;
+    uint64_t bytes;
+    if (q > b + size || __builtin_mul_overflow(a.count, (uint64_t)a.type.size, &bytes) ||
+        bytes > (uint64_t)(b + size - q))
+      throw Err{BMADGPU_EINVAL};
+    if (a.count > 0) o.attrs[name] = a;                // an attribute without a value reads as absent
   }
 
   std::string heap_name(uint64_t heap, uint64_t off) {
@@ -285,7 +296,9 @@ bool read_record(Reader& r, uint64_t species, const std::string& name, double fa
   out.assign(n, 0.0);
   if (o.is_dataset) {
     if ((int64_t)o.count != n) throw Err{BMADGPU_EINVAL};
-    if (o.data && o.data_bytes < (uint64_t)n * o.type.size) throw Err{BMADGPU_EINVAL};
+    uint64_t need;
+    if (__builtin_mul_overflow((uint64_t)n, (uint64_t)o.type.size, &need) || (o.data && o.data_bytes < need))
+      throw Err{BMADGPU_EINVAL};
     if (o.data)
       for (int64_t j = 0; j < n; j++) out[j] = Reader::real_at(o.type, o.data + (uint64_t)j * o.type.size);
   } else {
@@ -306,7 +319,9 @@ bool read_int_record(Reader& r, uint64_t species, const std::string& name, int64
   out.assign(n, 0);
   if (o.is_dataset) {
     if ((int64_t)o.count != n) throw Err{BMADGPU_EINVAL};
-    if (o.data && o.data_bytes < (uint64_t)n * o.type.size) throw Err{BMADGPU_EINVAL};
+    uint64_t need;
+    if (__builtin_mul_overflow((uint64_t)n, (uint64_t)o.type.size, &need) || (o.data && o.data_bytes < need))
+      throw Err{BMADGPU_EINVAL};
     if (o.data)
       for (int64_t j = 0; j < n; j++) out[j] = Reader::int_at(o.type, o.data + (uint64_t)j * o.type.size);
   } else {

@@ -232,3 +232,27 @@ def test_several_bunches_in_one_file(tmp_path):
     assert n_bunch == 20 and np.allclose(r.vec, bunches[1].vec, rtol=4e-16, atol=1e-300)
     with pytest.raises(lib.BmadGpuError):
         lib.beam_write_hdf5(path, [bunches[1]] * 257, p)
+
+
+def test_corrupted_files_never_read_out_of_bounds(tmp_path):
+    """The reader under AddressSanitizer and UBSan on 1,500 corrupted copies of each reference file."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no g++")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "h5beam_fuzz")
+    build = subprocess.run([gxx, "-std=c++17", "-O1", "-g", "-fsanitize=address,undefined", "-fno-sanitize-recover=all",
+                            "-o", exe, os.path.join(root, "tests", "c", "h5beam_fuzz.cpp"),
+                            os.path.join(root, "bmad-ecosystem_b200", "csrc", "h5beam.cpp"),
+                            os.path.join(root, "bmad-ecosystem_b200", "csrc", "beamio.cpp")],
+                           capture_output=True, text=True)
+    if build.returncode != 0 and "asan" in build.stderr.lower():
+        pytest.skip("no sanitizer runtime")
+    assert build.returncode == 0, build.stderr[-2000:]
+    for i, name in enumerate(("hdf5_test_bunch_old.h5", "sr_wakes_particles3.h5", "space_charge_initial_particles.h5")):
+        run = subprocess.run([exe, os.path.join(GOLDEN, name), str(11 + i), "1500", str(tmp_path / "m.h5")],
+                             capture_output=True, text=True, timeout=600)
+        assert run.returncode == 0, (name, run.stderr[-3000:])
+        assert run.stdout.startswith("read "), run.stdout
