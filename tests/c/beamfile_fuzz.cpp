@@ -1,16 +1,20 @@
-// Mutation check of the HDF5 beam-file reader (bmad-ecosystem_b200/csrc/h5beam.cpp), built with
-// AddressSanitizer and UBSan by tests/test_beamio_hdf5_cpu.py: random bytes of a valid file are
+// Mutation check of the beam-file readers (bmad-ecosystem_b200/csrc/h5beam.cpp, beamio.cpp), built
+// with AddressSanitizer and UBSan by tests/test_beamio_hdf5_cpu.py: random bytes of a valid file are
 // overwritten (and the file sometimes truncated); every read must end with a status code, never
-// with an access outside the file's bytes. Usage: h5beam_fuzz <file.h5> <seed> <iterations> <tmp>
+// with an access outside the file's bytes.
+// Usage: beamfile_fuzz hdf5|ascii <file> <seed> <iterations> <tmp>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <random>
 #include <vector>
 
 #include "../../include/bmadgpu.h"
 
 int main(int argc, char** argv) {
-  if (argc != 5) return 2;
+  if (argc != 6) return 2;
+  const bool hdf5 = std::strcmp(argv[1], "hdf5") == 0;
+  argv++;
   FILE* f = std::fopen(argv[1], "rb");
   if (!f) return 2;
   std::vector<unsigned char> src;
@@ -34,12 +38,13 @@ int main(int argc, char** argv) {
     std::fclose(o);
     int64_t n = 0;
     int32_t nb = 0;
-    int rc = bmadgpu_beam_read_hdf5(argv[4], &p, 0, nullptr, &n, &nb);
+    int rc = hdf5 ? bmadgpu_beam_read_hdf5(argv[4], &p, 0, nullptr, &n, &nb)
+                  : bmadgpu_beam_read_ascii(argv[4], &p, nullptr, &n);
     if (rc == 0 && n > 0 && n < 100000) {
       std::vector<double> vec(6 * n), beta(n), t(n);
       std::vector<int32_t> st(n), ie(n), loc(n);
       bmadgpu_bunch b{n, vec.data(), beta.data(), t.data(), st.data(), ie.data(), nullptr, loc.data()};
-      rc = bmadgpu_beam_read_hdf5(argv[4], &p, 0, &b, &n, &nb);
+      rc = hdf5 ? bmadgpu_beam_read_hdf5(argv[4], &p, 0, &b, &n, &nb) : bmadgpu_beam_read_ascii(argv[4], &p, &b, &n);
     }
     (rc == 0 ? ok : err)++;
   }

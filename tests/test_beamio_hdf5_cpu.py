@@ -235,24 +235,31 @@ def test_several_bunches_in_one_file(tmp_path):
 
 
 def test_corrupted_files_never_read_out_of_bounds(tmp_path):
-    """The reader under AddressSanitizer and UBSan on 1,500 corrupted copies of each reference file."""
+    """The HDF5 and ASCII readers under AddressSanitizer and UBSan on 1,500 corrupted copies of each
+    reference beam file and of an ASCII file written here."""
     import shutil
     import subprocess
     gxx = shutil.which("g++")
     if gxx is None:
         pytest.skip("no g++")
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    exe = str(tmp_path / "h5beam_fuzz")
+    exe = str(tmp_path / "beamfile_fuzz")
     build = subprocess.run([gxx, "-std=c++17", "-O1", "-g", "-fsanitize=address,undefined", "-fno-sanitize-recover=all",
-                            "-o", exe, os.path.join(root, "tests", "c", "h5beam_fuzz.cpp"),
+                            "-o", exe, os.path.join(root, "tests", "c", "beamfile_fuzz.cpp"),
                             os.path.join(root, "bmad-ecosystem_b200", "csrc", "h5beam.cpp"),
                             os.path.join(root, "bmad-ecosystem_b200", "csrc", "beamio.cpp")],
                            capture_output=True, text=True)
     if build.returncode != 0 and "asan" in build.stderr.lower():
         pytest.skip("no sanitizer runtime")
     assert build.returncode == 0, build.stderr[-2000:]
-    for i, name in enumerate(("hdf5_test_bunch_old.h5", "sr_wakes_particles3.h5", "space_charge_initial_particles.h5")):
-        run = subprocess.run([exe, os.path.join(GOLDEN, name), str(11 + i), "1500", str(tmp_path / "m.h5")],
+    b, p = sample(40)
+    v4 = str(tmp_path / "v4.dat")
+    lib.beam_write(v4, b, p)
+    cases = [("hdf5", os.path.join(GOLDEN, n)) for n in
+             ("hdf5_test_bunch_old.h5", "sr_wakes_particles3.h5", "space_charge_initial_particles.h5")]
+    cases += [("ascii", BEAM_1), ("ascii", v4)]
+    for i, (kind, path) in enumerate(cases):
+        run = subprocess.run([exe, kind, path, str(11 + i), "1500", str(tmp_path / "m.bin")],
                              capture_output=True, text=True, timeout=600)
-        assert run.returncode == 0, (name, run.stderr[-3000:])
+        assert run.returncode == 0, (path, run.stderr[-3000:])
         assert run.stdout.startswith("read "), run.stdout
