@@ -14,7 +14,9 @@ from helpers import oracle_libm, oracle_track
 
 abi = load_abi()
 rings = importlib.import_module("bmad-ecosystem_b200.rings")
-HC = os.path.join(ROOT, "bmad-ecosystem_b200", "_build", "libbmadgpu_hostcheck.so")
+# BMADGPU_HOSTCHECK_LIB: another build of the same sources (the sanitizer test passes one)
+HC = os.environ.get("BMADGPU_HOSTCHECK_LIB",
+                    os.path.join(ROOT, "bmad-ecosystem_b200", "_build", "libbmadgpu_hostcheck.so"))
 HC_CR = os.path.join(ROOT, "bmad-ecosystem_b200", "_build", "libbmadgpu_hostcheck_cr.so")
 
 
