@@ -25,6 +25,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
 #include <map>
 #include <string>
 #include <vector>
@@ -840,6 +841,13 @@ int write_hdf5(const char* path, const bmadgpu_bunch* bunches, int32_t n_bunch, 
   w.attr_str(0, "particlesPath", "particles/");
   w.attr_str(0, "software", "Bmad");
   w.attr_str(0, "softwareVersion", "1.0");
+  {  // date_and_time_stamp's "yyyy-mm-dd hh:mm:ss"
+    char stamp[32] = "";
+    const std::time_t now = std::time(nullptr);
+    std::tm tm_now{};
+    if (localtime_r(&now, &tm_now)) std::strftime(stamp, sizeof stamp, "%Y-%m-%d %H:%M:%S", &tm_now);
+    w.attr_str(0, "date", stamp);
+  }
   const int data = w.add(0, "data", true);
   for (int32_t ib = 0; ib < n_bunch; ib++) {
     const int r = add_bunch(w, data, ib, &bunches[ib], param, species, s_position,
