@@ -27,6 +27,7 @@
 #include <cstring>
 #include <ctime>
 #include <map>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -65,6 +66,12 @@ struct Object {
   const uint8_t* data = nullptr;                       // compact or contiguous data (nullptr: unallocated)
   uint64_t data_bytes = 0;
   std::map<std::string, Attr> attrs;
+  struct Raw {
+    int type, flags;
+    const uint8_t* body;
+    uint64_t size;
+  };
+  std::vector<Raw> raw;                                // every message, for copying the object
 };
 
 class Reader {
@@ -145,6 +152,7 @@ class Reader {
         const uint64_t body = p + 8;
         const uint8_t* b = at(body, size);
         seen++;
+        o.raw.push_back({type, (int)u(p + 4, 1), b, size});
         switch (type) {
           case 0x01: o.count = parse_space(b, size); break;
           case 0x03:
@@ -621,7 +629,7 @@ class Writer {
       // symbol-table nodes of at most 2 * kLeafK entries, one B-tree node above them
       const size_t per = 2 * kLeafK;
       const size_t n_snod = kids.empty() ? 0 : (kids.size() + per - 1) / per;
-      if (n_snod > 2 * (size_t)kNodeK) return kUndef;
+      if (n_snod > 2 * (size_t)kNodeK) throw Err{BMADGPU_EUNSUPPORTED};   // one B-tree node only
       const uint64_t tree = alloc(24 + 16 * 2 * kNodeK + 8);
       std::memcpy(out.data() + tree, "TREE", 4);
       poke(tree + 4, 0, 1); poke(tree + 5, 0, 1); poke(tree + 6, n_snod, 2);
@@ -749,7 +757,7 @@ const char* species_name(const bmadgpu_param* p) {
   return nullptr;
 }
 
-// One bunch group "/data/<ib, i5.5>/particles/<species>/" with its records (hdf5_write_beam.f90:95-240).
+// One bunch group "/data/<ib, i5.5>/particles/<species>/" (ib counted from 1) with its records (hdf5_write_beam.f90:95-240).
 int add_bunch(Writer& w, int data, int ib, const bmadgpu_bunch* b, const bmadgpu_param* param, const char* species,
               double s_position, bool alive_only) {
   if (!b || b->n < 0 || !b->vec || !b->beta || !b->state) return BMADGPU_EINVAL;
@@ -771,7 +779,7 @@ int add_bunch(Writer& w, int data, int ib, const bmadgpu_bunch* b, const bmadgpu
   const Unit uhbar{"hbar", kECharge * kHbar, {2, 1, -1, 0, 0, 0, 0}};
 
   char bunch_name[16];
-  std::snprintf(bunch_name, sizeof bunch_name, "%05d", ib + 1);
+  std::snprintf(bunch_name, sizeof bunch_name, "%05d", ib);
   const int bunch = w.add(data, bunch_name, true);
   const int parts = w.add(bunch, "particles", true);
   const int sp = w.add(parts, species, true);
@@ -827,13 +835,100 @@ int add_bunch(Writer& w, int data, int ib, const bmadgpu_bunch* b, const bmadgpu
   return BMADGPU_OK;
 }
 
+int save(const char* path, Writer& w) {
+  const std::vector<uint8_t> bytes = w.finish();
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return BMADGPU_EINVAL;
+  const bool ok = std::fwrite(bytes.data(), 1, bytes.size(), f) == bytes.size();
+  return std::fclose(f) == 0 && ok ? BMADGPU_OK : BMADGPU_EINVAL;
+}
+
+std::string time_stamp() {   // date_and_time_stamp's "yyyy-mm-dd hh:mm:ss"
+  char stamp[32] = "";
+  const std::time_t now = std::time(nullptr);
+  std::tm tm_now{};
+  if (localtime_r(&now, &tm_now)) std::strftime(stamp, sizeof stamp, "%Y-%m-%d %H:%M:%S", &tm_now);
+  return stamp;
+}
+
+bool load_file(const char* path, std::vector<uint8_t>& bytes) {
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return false;
+  uint8_t buf[1 << 16];
+  size_t got;
+  while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) bytes.insert(bytes.end(), buf, buf + got);
+  std::fclose(f);
+  return true;
+}
+
+// Copies the object at addr (a group with its subtree, or a dataset with its data) into writer
+// node ni: attribute, dataspace, datatype and fill messages as they are, storage and symbol
+// tables rebuilt. Objects with shared (committed) messages are not copied, nor objects reached
+// twice (a second hard link, or a cycle in a damaged file).
+void copy_tree(Reader& r, uint64_t addr, Writer& w, int ni, int depth, std::set<uint64_t>& seen) {
+  if (depth > 32) throw Err{BMADGPU_EINVAL};
+  if (!seen.insert(addr).second) throw Err{BMADGPU_EUNSUPPORTED};
+  Object o = r.object(addr);
+  if (o.is_group == o.is_dataset) throw Err{BMADGPU_EUNSUPPORTED};
+  for (const auto& m : o.raw) {
+    if (m.flags & 2) throw Err{BMADGPU_EUNSUPPORTED};                 // shared message
+    if (m.type == 0x01 || m.type == 0x03 || m.type == 0x05 || m.type == 0x0C || m.type == 0x12)
+      w.nodes[ni].msgs.push_back({m.type, m.flags & 1, std::vector<uint8_t>(m.body, m.body + m.size)});
+  }
+  if (o.is_dataset) {
+    if (!o.data) throw Err{BMADGPU_EUNSUPPORTED};                     // storage never written
+    w.nodes[ni].group = false;
+    w.nodes[ni].data.assign(o.data, o.data + o.data_bytes);
+    w.nodes[ni].msgs.push_back({0x08, 0, {}});
+    return;
+  }
+  std::vector<std::pair<std::string, uint64_t>> ch;
+  r.children(o.btree, o.heap, ch);
+  for (auto& c : ch) copy_tree(r, c.second, w, w.add(ni, c.first, true), depth + 1, seen);
+}
+
 int write_hdf5(const char* path, const bmadgpu_bunch* bunches, int32_t n_bunch, const bmadgpu_param* param,
                double s_position, int32_t flags) {
-  if (flags & BMADGPU_BEAM_APPEND) return BMADGPU_EUNSUPPORTED;
   if (n_bunch < 1 || n_bunch > 2 * Writer::kLeafK * 2 * Writer::kNodeK) return BMADGPU_EINVAL;
   const char* species = species_name(param);
   if (!species) return BMADGPU_EUNSUPPORTED;
   Writer w;
+  std::vector<uint8_t> old;
+  if ((flags & BMADGPU_BEAM_APPEND) && load_file(path, old)) {
+    // hdf5_write_beam with append: the file as it is, a lastUpdated stamp, and the new bunches under
+    // the first free numbers of basePath "/data/%T/" (hdf5_write_beam.f90:43-47, 99-106)
+    Reader r(std::move(old));
+    const uint64_t root = r.root();
+    Object ro = r.object(root);
+    if (!ro.attrs.count("basePath") || Reader::str(ro.attrs["basePath"]) != "/data/%T/") return BMADGPU_EUNSUPPORTED;
+    std::set<uint64_t> seen;
+    copy_tree(r, root, w, 0, 0, seen);
+    auto& rm = w.nodes[0].msgs;
+    const std::string stamp = time_stamp();
+    rm.erase(std::remove_if(rm.begin(), rm.end(), [](const Writer::Msg& m) {
+               return m.type == 0x0C && m.body.size() > 8 + 11 && std::memcmp(m.body.data() + 8, "lastUpdated", 12) == 0;
+             }), rm.end());
+    w.attr_str(0, "lastUpdated", stamp);
+    int data = -1;
+    for (auto& k : w.nodes[0].kids)
+      if (k.first == "data") data = k.second;
+    if (data < 0 || !w.nodes[data].group) return BMADGPU_EINVAL;
+    int number = 0;
+    for (int32_t ib = 0; ib < n_bunch; ib++) {
+      bool taken = true;
+      while (taken) {
+        char nm[16];
+        std::snprintf(nm, sizeof nm, "%05d", ++number);
+        taken = false;
+        for (auto& k : w.nodes[data].kids) taken = taken || k.first == nm;
+      }
+      if (w.nodes[data].kids.size() >= (size_t)(2 * Writer::kLeafK * 2 * Writer::kNodeK)) return BMADGPU_EINVAL;
+      const int rr = add_bunch(w, data, number, &bunches[ib], param, species, s_position,
+                               (flags & BMADGPU_BEAM_ALIVE_ONLY) != 0);
+      if (rr) return rr;
+    }
+    return save(path, w);
+  }
   w.attr_str(0, "dataType", "openPMD");
   w.attr_str(0, "openPMD", "2.0.0");
   w.attr_str(0, "openPMDextension", "BeamPhysics;SpeciesType");
@@ -841,25 +936,15 @@ int write_hdf5(const char* path, const bmadgpu_bunch* bunches, int32_t n_bunch, 
   w.attr_str(0, "particlesPath", "particles/");
   w.attr_str(0, "software", "Bmad");
   w.attr_str(0, "softwareVersion", "1.0");
-  {  // date_and_time_stamp's "yyyy-mm-dd hh:mm:ss"
-    char stamp[32] = "";
-    const std::time_t now = std::time(nullptr);
-    std::tm tm_now{};
-    if (localtime_r(&now, &tm_now)) std::strftime(stamp, sizeof stamp, "%Y-%m-%d %H:%M:%S", &tm_now);
-    w.attr_str(0, "date", stamp);
-  }
+  w.attr_str(0, "date", time_stamp());
   const int data = w.add(0, "data", true);
   for (int32_t ib = 0; ib < n_bunch; ib++) {
-    const int r = add_bunch(w, data, ib, &bunches[ib], param, species, s_position,
+    const int r = add_bunch(w, data, ib + 1, &bunches[ib], param, species, s_position,
                             (flags & BMADGPU_BEAM_ALIVE_ONLY) != 0);
     if (r) return r;
   }
 
-  const std::vector<uint8_t> bytes = w.finish();
-  FILE* f = std::fopen(path, "wb");
-  if (!f) return BMADGPU_EINVAL;
-  const bool ok = std::fwrite(bytes.data(), 1, bytes.size(), f) == bytes.size();
-  return std::fclose(f) == 0 && ok ? BMADGPU_OK : BMADGPU_EINVAL;
+  return save(path, w);
 }
 
 }  // namespace

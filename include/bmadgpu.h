@@ -662,7 +662,9 @@ int bmadgpu_beam_read_ascii(const char* path, const bmadgpu_param* param, bmadgp
 /* Bmad's openPMD beam file in HDF5 (hdf5_write_beam, bmad/hdf5/hdf5_write_beam.f90:20-245), written
  * without the HDF5 library in the classic file structures libhdf5 writes by default. One bunch as
  * /data/00001/particles/<species>/; records whose values are all equal become constant record
- * components, as in the reference. flags: ALIVE_ONLY; APPEND gives BMADGPU_EUNSUPPORTED. The
+ * components, as in the reference. flags: ALIVE_ONLY; APPEND (to a file whose basePath is
+ * "/data/%T/": its objects are copied, lastUpdated is stamped and the bunch takes the first free
+ * number; files with shared datatypes give BMADGPU_EUNSUPPORTED). The
  * species name comes from param's mass and charge (electron, positron, proton, anti-proton;
  * other species give BMADGPU_EUNSUPPORTED). Spin and macro-charge are written as 0. */
 int bmadgpu_beam_write_hdf5(const char* path, const bmadgpu_bunch* host_bunch, const bmadgpu_param* param,

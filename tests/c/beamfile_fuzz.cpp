@@ -1,8 +1,8 @@
 // Mutation check of the beam-file readers (bmad-ecosystem_b200/csrc/h5beam.cpp, beamio.cpp), built
 // with AddressSanitizer and UBSan by tests/test_beamio_hdf5_cpu.py: random bytes of a valid file are
-// overwritten (and the file sometimes truncated); every read must end with a status code, never
-// with an access outside the file's bytes.
-// Usage: beamfile_fuzz hdf5|ascii <file> <seed> <iterations> <tmp>
+// overwritten (and the file sometimes truncated); every read, and every append of a bunch to such a
+// file, must end with a status code, never with an access outside the file's bytes.
+// Usage: beamfile_fuzz hdf5|ascii|append <file> <seed> <iterations> <tmp>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -13,7 +13,7 @@
 
 int main(int argc, char** argv) {
   if (argc != 6) return 2;
-  const bool hdf5 = std::strcmp(argv[1], "hdf5") == 0;
+  const bool hdf5 = std::strcmp(argv[1], "hdf5") == 0, append = std::strcmp(argv[1], "append") == 0;
   argv++;
   FILE* f = std::fopen(argv[1], "rb");
   if (!f) return 2;
@@ -38,6 +38,15 @@ int main(int argc, char** argv) {
     std::fclose(o);
     int64_t n = 0;
     int32_t nb = 0;
+    if (append) {
+      std::vector<double> vec(30, 1e-3), beta(5, 0.99), t(5, 0.0);
+      std::vector<int32_t> st(5, 1), ie(5, 0), loc(5, 2);
+      bmadgpu_bunch b{5, vec.data(), beta.data(), t.data(), st.data(), ie.data(), nullptr, loc.data()};
+      int rc = bmadgpu_beam_write_hdf5(argv[4], &b, &p, 0.0, BMADGPU_BEAM_APPEND);
+      if (rc == 0) rc = bmadgpu_beam_read_hdf5(argv[4], &p, 0, nullptr, &n, &nb);
+      (rc == 0 ? ok : err)++;
+      continue;
+    }
     int rc = hdf5 ? bmadgpu_beam_read_hdf5(argv[4], &p, 0, nullptr, &n, &nb)
                   : bmadgpu_beam_read_ascii(argv[4], &p, nullptr, &n);
     if (rc == 0 && n > 0 && n < 100000) {

@@ -112,12 +112,36 @@ def test_alive_only_and_constant_records(tmp_path):
     assert np.allclose(r1.vec, one.vec, rtol=4e-16, atol=1e-300)
 
 
-def test_append_and_unknown_species_are_refused(tmp_path):
+def test_append(tmp_path):
+    """hdf5_write_beam with append: the file's bunches stay, the new one takes the next number."""
+    b, p = sample(20)
+    c, _ = sample(30, seed=4)
+    path = str(tmp_path / "x.h5")
+    lib.beam_write_hdf5(path, b, p, flags=lib.BEAM_APPEND)          # no file yet: a new one
+    lib.beam_write_hdf5(path, c, p, flags=lib.BEAM_APPEND)
+    for k, ref in enumerate((b, c)):
+        r, n_bunch = lib.beam_read_hdf5(path, p, k)
+        assert n_bunch == 2
+        assert np.allclose(r.vec, ref.vec, rtol=4e-16, atol=1e-300) and np.array_equal(r.state, ref.state)
+    # onto a copy of the reference's own file (bunch 1 positrons, bunch 2 photons): both kept
+    old = str(tmp_path / "old.h5")
+    open(old, "wb").write(open(OLD_H5, "rb").read())
+    q = positron_1gev()
+    c = lib.HostBunch.from_vec(c.vec, q, t=c.t)                      # beta of this species and energy
+    lib.beam_write_hdf5(old, c, q, flags=lib.BEAM_APPEND)
+    first, n_bunch = lib.beam_read_hdf5(old, q, 0)
+    assert n_bunch == 3
+    assert np.array_equal(first.vec, lib.beam_read_hdf5(OLD_H5, q, 0)[0].vec)
+    with pytest.raises(lib.BmadGpuError):
+        lib.beam_read_hdf5(old, q, 1)                                  # still the photon bunch
+    third, _ = lib.beam_read_hdf5(old, q, 2)
+    assert np.allclose(third.vec, c.vec, rtol=4e-16, atol=1e-300)
+    assert np.array_equal(third.beta, c.beta)
+
+
+def test_unknown_species_is_refused(tmp_path):
     b, p = sample(20)
     path = str(tmp_path / "x.h5")
-    with pytest.raises(lib.BmadGpuError) as e:
-        lib.beam_write_hdf5(path, b, p, flags=lib.BEAM_APPEND)
-    assert e.value.code == abi.EUNSUPPORTED
     q = abi.Param()
     q.p0c, q.e_tot, q.mass, q.charge = p.p0c, p.e_tot, 105.6583755e6, -1.0     # a muon
     with pytest.raises(lib.BmadGpuError) as e:
@@ -235,8 +259,8 @@ def test_several_bunches_in_one_file(tmp_path):
 
 
 def test_corrupted_files_never_read_out_of_bounds(tmp_path):
-    """The HDF5 and ASCII readers under AddressSanitizer and UBSan on 1,500 corrupted copies of each
-    reference beam file and of an ASCII file written here."""
+    """The HDF5 and ASCII readers, and appending to an HDF5 file, under AddressSanitizer and UBSan on
+    1,500 corrupted copies of each reference beam file and of an ASCII file written here."""
     import shutil
     import subprocess
     gxx = shutil.which("g++")
@@ -257,7 +281,7 @@ def test_corrupted_files_never_read_out_of_bounds(tmp_path):
     lib.beam_write(v4, b, p)
     cases = [("hdf5", os.path.join(GOLDEN, n)) for n in
              ("hdf5_test_bunch_old.h5", "sr_wakes_particles3.h5", "space_charge_initial_particles.h5")]
-    cases += [("ascii", BEAM_1), ("ascii", v4)]
+    cases += [("ascii", BEAM_1), ("ascii", v4), ("append", OLD_H5)]
     for i, (kind, path) in enumerate(cases):
         run = subprocess.run([exe, kind, path, str(11 + i), "1500", str(tmp_path / "m.bin")],
                              capture_output=True, text=True, timeout=600)
