@@ -850,6 +850,28 @@ def beam_read_hdf5(path, param, ix_bunch=0):
     return b, nb.value
 
 
+def write_beam_file(path, bunch, param, s_position=0.0, flags=0):
+    """write_beam_file: HDF5 for names ending in .h5 or .hdf5, else Bmad's ASCII layout."""
+    lib = load()
+    lib.bmadgpu_beam_write_file.argtypes = [C.c_char_p, C.POINTER(abi.Bunch), C.POINTER(abi.Param), C.c_double,
+                                            C.c_int32]
+    v = bunch.view()
+    check_host(lib.bmadgpu_beam_write_file(path.encode(), C.byref(v), C.byref(param), s_position, flags))
+
+
+def read_beam_file(path, param):
+    """read_beam_file: a HostBunch (the first bunch of an HDF5 file) in the format the name gives."""
+    lib = load()
+    lib.bmadgpu_beam_read_file.argtypes = [C.c_char_p, C.POINTER(abi.Param), C.POINTER(abi.Bunch),
+                                           C.POINTER(C.c_int64)]
+    n = C.c_int64()
+    check_host(lib.bmadgpu_beam_read_file(path.encode(), C.byref(param), None, C.byref(n)))
+    b = HostBunch(np.zeros((6, n.value)), np.zeros(n.value), t=np.zeros(n.value))
+    v = b.view()
+    check_host(lib.bmadgpu_beam_read_file(path.encode(), C.byref(param), C.byref(v), C.byref(n)))
+    return b
+
+
 def check_host(code):
     """Status check for the host-only calls (they set no last-error message)."""
     if code != 0:

@@ -160,24 +160,13 @@ def test_truncated_file_is_an_error(tmp_path):
 
 def test_file_name_picks_the_format(tmp_path):
     """write_beam_file / read_beam_file: HDF5 for .h5 and .hdf5 names, ASCII otherwise."""
-    import ctypes as C
-    so = lib.load()
-    so.bmadgpu_beam_write_file.argtypes = [C.c_char_p, C.POINTER(abi.Bunch), C.POINTER(abi.Param), C.c_double,
-                                           C.c_int32]
-    so.bmadgpu_beam_read_file.argtypes = [C.c_char_p, C.POINTER(abi.Param), C.POINTER(abi.Bunch),
-                                          C.POINTER(C.c_int64)]
     b, p = sample(50)
-    v = b.view()
     for name, hdf5 in (("a.h5", True), ("a.hdf5", True), ("a.dat", False), ("a_h5", False)):
         path = str(tmp_path / name)
-        assert so.bmadgpu_beam_write_file(path.encode(), C.byref(v), C.byref(p), 0.0, lib.BEAM_EXACT) == 0
+        lib.write_beam_file(path, b, p, flags=lib.BEAM_EXACT)
         head = open(path, "rb").read(8)
         assert (head == b"\x89HDF\r\n\x1a\n") == hdf5, name
-        n = C.c_int64()
-        assert so.bmadgpu_beam_read_file(path.encode(), C.byref(p), None, C.byref(n)) == 0 and n.value == 50
-        r = lib.HostBunch(np.zeros((6, 50)), np.zeros(50), t=np.zeros(50))
-        rv = r.view()
-        assert so.bmadgpu_beam_read_file(path.encode(), C.byref(p), C.byref(rv), C.byref(n)) == 0
+        r = lib.read_beam_file(path, p)
         assert np.allclose(r.vec, b.vec, rtol=4e-16, atol=1e-300), name
         assert np.array_equal(r.state, b.state), name
 
