@@ -349,8 +349,9 @@ bool is_integer(const std::string& s) {
   return true;
 }
 
-int read_hdf5(const char* path, const bmadgpu_param* param, int32_t ix_bunch, bmadgpu_bunch* b,
+int read_hdf5(const char* path, const bmadgpu_param* param, int32_t ix_bunch, int32_t flags, bmadgpu_bunch* b,
               int64_t* n_particle, int32_t* n_bunch) {
+  const bool at_ele = (flags & BMADGPU_BEAM_AT_ELEMENT) != 0;
   FILE* f = std::fopen(path, "rb");
   if (!f) return BMADGPU_EINVAL;
   std::vector<uint8_t> bytes;
@@ -454,17 +455,19 @@ int read_hdf5(const char* path, const bmadgpu_param* param, int32_t ix_bunch, bm
   const bool have_loc = read_int_record(r, species, "locationInElement", n, loc);
 
   for (int64_t j = 0; j < n; j++) {
-    // a particle without a reference momentum in the file takes the lattice's, as the reference's
-    // reader does when it is given the element (p0c_initial = ele%value(p0c$))
-    const double pc0 = p0c[j] != 0 ? p0c[j] : param->p0c;
-    if (pc0 == 0) return BMADGPU_EINVAL;                       // reference momentum not present
+    // p0c_initial: the file's, or the lattice's where the file has none (the reference's reading
+    // with an element); p0c_final: the lattice's with an element, else p0c_initial
+    // (hdf5_read_beam.f90:283-340, conserve_momentum at its default)
+    const double p_init = p0c[j] != 0 ? p0c[j] : param->p0c;
+    const double pc0 = at_ele ? param->p0c : p_init;
+    if (pc0 == 0 || p_init == 0) return BMADGPU_EINVAL;        // reference momentum not present
     int st = have_state ? (int)state[j] : 1;
     if (st != 1 && st != 0 && software != "Bmad") st = 2;     // alive$, pre_born$ = 0 kept; others lost$ (non-Bmad files)
     double pz;
     if (!have_tot)
       pz = (std::sqrt(v[1][j] * v[1][j] + v[3][j] * v[3][j] + v[5][j] * v[5][j]) - pc0) / pc0;
     else
-      pz = tot_mom[j] / pc0;
+      pz = tot_mom[j] / p_init;
     const double pc = (1 + pz) * pc0;
     const double beta = pc / std::sqrt(pc * pc + param->mass * param->mass);   // convert_pc_to
     b->vec[0 * n + j] = v[0][j];
@@ -476,9 +479,10 @@ int read_hdf5(const char* path, const bmadgpu_param* param, int32_t ix_bunch, bm
     b->beta[j] = beta;
     if (b->t) b->t[j] = t0[j] + dt[j];
     b->state[j] = st;
-    if (b->ix_ele) b->ix_ele[j] = have_ele ? (int32_t)ix_ele[j] - 1 : -1;   // Bmad's 1-based index
+    // with an element, every particle is placed at its exit (the beginning element here)
+    if (b->ix_ele) b->ix_ele[j] = have_ele && !at_ele ? (int32_t)ix_ele[j] - 1 : -1;   // Bmad's 1-based index
     if (b->location) {
-      const int64_t l = have_loc ? loc[j] : 1;
+      const int64_t l = have_loc && !at_ele ? loc[j] : 1;
       b->location[j] = l == -1 ? 1 : l == 0 ? 3 : 2;           // upstream_end$, inside$, downstream_end$
     }
   }
@@ -969,11 +973,11 @@ extern "C" int bmadgpu_beam_write_hdf5_bunches(const char* path, const bmadgpu_b
   }
 }
 
-extern "C" int bmadgpu_beam_read_hdf5(const char* path, const bmadgpu_param* param, int32_t ix_bunch,
+extern "C" int bmadgpu_beam_read_hdf5(const char* path, const bmadgpu_param* param, int32_t ix_bunch, int32_t flags,
                                       bmadgpu_bunch* host_bunch, int64_t* n_particle, int32_t* n_bunch) {
   if (!path || !param || !n_particle) return BMADGPU_EINVAL;
   try {
-    return read_hdf5(path, param, ix_bunch, host_bunch, n_particle, n_bunch);
+    return read_hdf5(path, param, ix_bunch, flags, host_bunch, n_particle, n_bunch);
   } catch (const Err& e) {
     return e.code;
   }
@@ -997,6 +1001,6 @@ extern "C" int bmadgpu_beam_write_file(const char* path, const bmadgpu_bunch* ho
 extern "C" int bmadgpu_beam_read_file(const char* path, const bmadgpu_param* param, bmadgpu_bunch* host_bunch,
                                       int64_t* n_particle) {
   if (!path) return BMADGPU_EINVAL;
-  if (is_hdf5_name(path)) return bmadgpu_beam_read_hdf5(path, param, 0, host_bunch, n_particle, nullptr);
+  if (is_hdf5_name(path)) return bmadgpu_beam_read_hdf5(path, param, 0, 0, host_bunch, n_particle, nullptr);
   return bmadgpu_beam_read_ascii(path, param, host_bunch, n_particle);
 }

@@ -793,7 +793,7 @@ def ltt_run(ctx, lat, bunch, n_turns, averages_file=None, phase_space_file=None,
     return done.value
 
 
-BEAM_ALIVE_ONLY, BEAM_APPEND, BEAM_EXACT = 1, 2, 4
+BEAM_ALIVE_ONLY, BEAM_APPEND, BEAM_EXACT, BEAM_AT_ELEMENT = 1, 2, 4, 8
 
 
 def beam_write(path, bunch, param, s_position=0.0, flags=0):
@@ -835,17 +835,18 @@ def beam_write_hdf5(path, bunch, param, s_position=0.0, flags=0):
     check_host(lib.bmadgpu_beam_write_hdf5(path.encode(), C.byref(v), C.byref(param), s_position, flags))
 
 
-def beam_read_hdf5(path, param, ix_bunch=0):
+def beam_read_hdf5(path, param, ix_bunch=0, flags=0):
     """(HostBunch of bunch ix_bunch, number of bunches) from a Bmad openPMD beam file, as
-    hdf5_read_beam reads it without an element."""
+    hdf5_read_beam reads it without an element (flags BEAM_AT_ELEMENT: with the beginning element)."""
     lib = load()
-    lib.bmadgpu_beam_read_hdf5.argtypes = [C.c_char_p, C.POINTER(abi.Param), C.c_int32, C.POINTER(abi.Bunch),
-                                           C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+    lib.bmadgpu_beam_read_hdf5.argtypes = [C.c_char_p, C.POINTER(abi.Param), C.c_int32, C.c_int32,
+                                           C.POINTER(abi.Bunch), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
     n, nb = C.c_int64(), C.c_int32()
-    check_host(lib.bmadgpu_beam_read_hdf5(path.encode(), C.byref(param), ix_bunch, None, C.byref(n), C.byref(nb)))
+    check_host(lib.bmadgpu_beam_read_hdf5(path.encode(), C.byref(param), ix_bunch, flags, None, C.byref(n),
+                                          C.byref(nb)))
     b = HostBunch(np.zeros((6, n.value)), np.zeros(n.value), t=np.zeros(n.value))
     v = b.view()
-    check_host(lib.bmadgpu_beam_read_hdf5(path.encode(), C.byref(param), ix_bunch, C.byref(v), C.byref(n),
+    check_host(lib.bmadgpu_beam_read_hdf5(path.encode(), C.byref(param), ix_bunch, flags, C.byref(v), C.byref(n),
                                           C.byref(nb)))
     return b, nb.value
 

@@ -647,7 +647,7 @@ int bmadgpu_naff(bmadgpu_ctx* ctx, int32_t n_signals, int32_t n_samples, const d
 /* ---- Beam files (checkpoint / resume) -------------------------------------------------------
  * Bmad's ASCII beam file, version 4 (write_ascii_beam_file / read_beam_ascii,
  * bmad/multiparticle/beam_file_io.f90:112-300, 834-1282). Host-only; no GPU needed. */
-enum { BMADGPU_BEAM_ALIVE_ONLY = 1, BMADGPU_BEAM_APPEND = 2, BMADGPU_BEAM_EXACT = 4 };
+enum { BMADGPU_BEAM_ALIVE_ONLY = 1, BMADGPU_BEAM_APPEND = 2, BMADGPU_BEAM_EXACT = 4, BMADGPU_BEAM_AT_ELEMENT = 8 };
 /* Writes one bunch; flags: ALIVE_ONLY (skip lost particles), APPEND, EXACT (17 significant
  * digits and a beta column, so a resumed run continues bit for bit; otherwise the reference's
  * es23.15). ix_ele is written 1-based as Bmad numbers elements (0 for particles not lost). */
@@ -680,8 +680,11 @@ int bmadgpu_beam_write_hdf5_bunches(const char* path, const bmadgpu_bunch* host_
  * NULL nothing else is read, otherwise host_bunch->n must equal *n_particle. beta comes from the
  * momentum and param's mass. Files using HDF5 structures outside the classic set (superblock
  * version 2 or 3, version-2 object headers, link messages, chunked or filtered storage) and photon
- * bunches give BMADGPU_EUNSUPPORTED. */
-int bmadgpu_beam_read_hdf5(const char* path, const bmadgpu_param* param, int32_t ix_bunch,
+ * bunches give BMADGPU_EUNSUPPORTED. flags: BMADGPU_BEAM_AT_ELEMENT reads as the reference does when
+ * given the lattice's beginning element (as long_term_tracking reads its starting beam): px and py
+ * are divided by param's p0c, beta follows from it, and every particle is placed at the exit of
+ * the beginning element (ix_ele -1, downstream_end); pz stays relative to the file's p0c. */
+int bmadgpu_beam_read_hdf5(const char* path, const bmadgpu_param* param, int32_t ix_bunch, int32_t flags,
                            bmadgpu_bunch* host_bunch, int64_t* n_particle, int32_t* n_bunch);
 /* write_beam_file / read_beam_file (bmad/multiparticle/beam_file_io.f90:29-106, 380-420): HDF5
  * (the two calls above; the first bunch on reading) when the name ends in ".h5" or ".hdf5", else

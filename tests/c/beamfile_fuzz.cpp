@@ -43,17 +43,17 @@ int main(int argc, char** argv) {
       std::vector<int32_t> st(5, 1), ie(5, 0), loc(5, 2);
       bmadgpu_bunch b{5, vec.data(), beta.data(), t.data(), st.data(), ie.data(), nullptr, loc.data()};
       int rc = bmadgpu_beam_write_hdf5(argv[4], &b, &p, 0.0, BMADGPU_BEAM_APPEND);
-      if (rc == 0) rc = bmadgpu_beam_read_hdf5(argv[4], &p, 0, nullptr, &n, &nb);
+      if (rc == 0) rc = bmadgpu_beam_read_hdf5(argv[4], &p, 0, 0, nullptr, &n, &nb);
       (rc == 0 ? ok : err)++;
       continue;
     }
-    int rc = hdf5 ? bmadgpu_beam_read_hdf5(argv[4], &p, 0, nullptr, &n, &nb)
+    int rc = hdf5 ? bmadgpu_beam_read_hdf5(argv[4], &p, 0, 0, nullptr, &n, &nb)
                   : bmadgpu_beam_read_ascii(argv[4], &p, nullptr, &n);
     if (rc == 0 && n > 0 && n < 100000) {
       std::vector<double> vec(6 * n), beta(n), t(n);
       std::vector<int32_t> st(n), ie(n), loc(n);
       bmadgpu_bunch b{n, vec.data(), beta.data(), t.data(), st.data(), ie.data(), nullptr, loc.data()};
-      rc = hdf5 ? bmadgpu_beam_read_hdf5(argv[4], &p, 0, &b, &n, &nb) : bmadgpu_beam_read_ascii(argv[4], &p, &b, &n);
+      rc = hdf5 ? bmadgpu_beam_read_hdf5(argv[4], &p, 0, 0, &b, &n, &nb) : bmadgpu_beam_read_ascii(argv[4], &p, &b, &n);
     }
     (rc == 0 ? ok : err)++;
   }

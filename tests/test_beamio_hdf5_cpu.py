@@ -276,3 +276,26 @@ def test_corrupted_files_never_read_out_of_bounds(tmp_path):
                              capture_output=True, text=True, timeout=600)
         assert run.returncode == 0, (path, run.stderr[-3000:])
         assert run.stdout.startswith("read "), run.stdout
+
+
+def test_reading_at_the_beginning_element(tmp_path):
+    """hdf5_read_beam given the lattice's beginning element (conserve_momentum at its default), for a
+    file whose reference momentum differs from the lattice's: px and py over the lattice's p0c, pz
+    over the file's, beta from (1 + pz) times the lattice's p0c, every particle at the element's exit."""
+    b, p = sample(25)
+    path = str(tmp_path / "p.h5")
+    lib.beam_write_hdf5(path, b, p)                                 # file p0c = p.p0c
+    q = abi.Param()
+    q.mass, q.charge, q.p0c = p.mass, p.charge, p.p0c * 1.01
+    q.e_tot = (q.p0c ** 2 + q.mass ** 2) ** 0.5
+    plain, _ = lib.beam_read_hdf5(path, q)
+    at, _ = lib.beam_read_hdf5(path, q, flags=lib.BEAM_AT_ELEMENT)
+    assert np.allclose(plain.vec, b.vec, rtol=4e-16, atol=1e-300)   # without an element: the file's p0c
+    assert np.allclose(at.vec[[1, 3]], b.vec[[1, 3]] * p.p0c / q.p0c, rtol=1e-15, atol=1e-300)
+    assert np.allclose(at.vec[5], b.vec[5], rtol=4e-16, atol=1e-300)
+    pc = (1 + at.vec[5]) * q.p0c
+    assert np.allclose(at.beta, pc / np.sqrt(pc * pc + q.mass ** 2), rtol=1e-15)
+    # the file stores t - t_ref = -z / (beta c): z follows the new beta
+    assert np.allclose(at.vec[4], b.vec[4] * at.beta / b.beta, rtol=1e-15, atol=1e-300)
+    assert np.all(at.ix_ele == -1) and np.all(at.location == abi.DOWNSTREAM_END)
+    assert np.array_equal(at.state, b.state)
