@@ -14,10 +14,11 @@ from helpers import oracle_libm, oracle_track
 
 abi = load_abi()
 rings = importlib.import_module("bmad-ecosystem_b200.rings")
-# BMADGPU_HOSTCHECK_LIB: another build of the same sources (the sanitizer test passes one)
+# BMADGPU_HOSTCHECK_LIB / _CR_LIB: other builds of the same sources (the sanitizer test passes them)
 HC = os.environ.get("BMADGPU_HOSTCHECK_LIB",
                     os.path.join(ROOT, "bmad-ecosystem_b200", "_build", "libbmadgpu_hostcheck.so"))
-HC_CR = os.path.join(ROOT, "bmad-ecosystem_b200", "_build", "libbmadgpu_hostcheck_cr.so")
+HC_CR = os.environ.get("BMADGPU_HOSTCHECK_CR_LIB",
+                       os.path.join(ROOT, "bmad-ecosystem_b200", "_build", "libbmadgpu_hostcheck_cr.so"))
 
 
 @pytest.fixture(scope="module")
