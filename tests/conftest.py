@@ -28,10 +28,11 @@ _ORACLE = None
 
 
 def load_oracle():
-    """The CPU oracle shared library (built from oracle/ by its Makefile)."""
+    """The CPU oracle shared library (built from oracle/ by its Makefile; BMADGPU_ORACLE_LIB names
+    another build of the same source, as the sanitizer test does)."""
     global _ORACLE
     if _ORACLE is None:
-        path = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+        path = os.environ.get("BMADGPU_ORACLE_LIB") or os.path.join(ROOT, "oracle", "_build", "liboracle.so")
         if not os.path.exists(path):
             subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
         lib = ctypes.CDLL(path)
